@@ -1,0 +1,176 @@
+/*
+ * scmc_gpu.h - C ABI of the B200 (sm_100a) Monte Carlo speckle path.
+ *
+ * This library replaces the Monte Carlo kernels of SCMC (cmu-ci-lab/mcspeckle):
+ * the random walk through a box medium, next-event estimation (NEE) from the
+ * first and last scatterer to every light and view, and the complex phase
+ * accumulation into a speckle field u(v,l) or covariance C(v1,v2,l1,l2).
+ *
+ * Every entry point takes plain pointers and sizes.  Arrays follow MATLAB's
+ * storage: real matrices column-major, complex values interleaved (re, im)
+ * as in MATLAB R2018a+ interleaved complex.  All host-side outputs are
+ * written only on success.  A non-zero return is an scmc_status; the message
+ * is available from scmc_last_error() on the calling thread.
+ */
+#ifndef SCMC_GPU_H
+#define SCMC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCMC_ABI_VERSION 1
+
+typedef enum {
+    SCMC_OK = 0,
+    SCMC_ERR_INVALID = 1,   /* argument validation; message mirrors the reference's error() */
+    SCMC_ERR_CUDA = 2,      /* CUDA runtime / driver error */
+    SCMC_ERR_NOMEM = 3,     /* device or host allocation failed */
+    SCMC_ERR_NODEVICE = 4,  /* no sm_100 device visible */
+    SCMC_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
+    SCMC_ERR_CANCELLED = 6, /* request cancelled through the serving API */
+    SCMC_ERR_LIMIT = 7      /* a path exceeded max_events_per_path */
+} scmc_status;
+
+/* sct_type values, as in scmc.m:249-287 (1 isotropic, 2 tabulated, 3 HG). */
+enum { SCMC_SCT_ISOTROPIC = 1, SCMC_SCT_TABULATED = 2, SCMC_SCT_HG = 3 };
+
+/* Arithmetic of the NEE phase vectors and of the contraction.
+ *  FP64  - reference arithmetic (every step in double); parity mode.
+ *  MIXED - phase argument k*(w.x) reduced mod 2pi in FP64, sincos/exp in FP32,
+ *          contraction on tcgen05 tensor cores with FP16 hi+lo split operands
+ *          and FP32 accumulation, cross-batch sums in FP64.
+ *  FP32  - plain FP32: FP32 phases without FP64 reduction, FP32 CUDA-core
+ *          contraction, FP32 accumulation (the comparison baseline).
+ * The random walk itself is FP64 in every mode, so all three modes see the
+ * same paths for the same seed. */
+enum { SCMC_PREC_FP64 = 0, SCMC_PREC_MIXED = 1, SCMC_PREC_FP32 = 2 };
+
+/* One scattering function: the (sct_type, ampfunc) pair of MCfield.m:1.
+ * For SCMC_SCT_TABULATED the two tables are the fields evalAmp and
+ * sampleIcdf built by tabulatedAmplitudeScatter.m:78-99. */
+typedef struct {
+    int32_t sct_type;
+    double g;                  /* HG anisotropy (ampfunc for sct_type 3) */
+    int32_t table_n;           /* length of the tabulated tables */
+    const double *eval_amp;    /* 2*table_n doubles: interleaved complex evalAmp */
+    const double *sample_icdf; /* table_n doubles: sampleIcdf (angles) */
+} scmc_phase_function;
+
+/* Positional arguments of MCfield / MCcov (MCfield.m:1, MCcov.m:1) plus the
+ * execution controls that MATLAB's list has no slot for. */
+typedef struct {
+    int32_t dim;               /* 2 or 3: size(box_min,1) */
+    double sigt;               /* extinction coefficient 1/MFP */
+    double albedo;
+    double box_min[3];
+    double box_max[3];
+    const double *l;           /* dim x nl, column-major (directions or positions) */
+    int64_t nl;
+    const double *v;           /* dim x nv, column-major */
+    int64_t nv;
+    int32_t is_ff_l;
+    int32_t is_ff_v;
+    int64_t max_itr;           /* number of paths (maxItr) */
+    double lambda;
+    int32_t do_cbs;
+    int32_t smp_flg;           /* 1 uniform, 2 exponential first scatter */
+    scmc_phase_function ampfunc;
+    int32_t has_ampfunc0;      /* 15th argument present */
+    scmc_phase_function ampfunc0;
+    int32_t has_lmean0;        /* 16th argument of MCfield present */
+    double lmean0[3];
+    /* --- execution controls --- */
+    uint64_t seed;             /* Philox-4x32-10 key */
+    uint64_t path_offset;      /* global index of the first path (sharding / replicas) */
+    int64_t norm_itr;          /* path count used in the normalisation; 0 = max_itr */
+    int32_t precision;         /* SCMC_PREC_* */
+    int32_t device;            /* CUDA ordinal */
+    int64_t max_events_per_path; /* 0 = unlimited; exceeding it fails with SCMC_ERR_LIMIT */
+} scmc_mc_args;
+
+/* Positional arguments of MCfieldFourierQuad (MCfieldFourierQuad.m:1). */
+typedef struct {
+    double sigt;
+    double albedo;
+    double box_min[3];
+    double box_max[3];
+    const double *l;           /* 3 x nl light directions */
+    int64_t nl;
+    double v_max;
+    double v_stp;
+    int64_t max_itr;
+    double lambda;
+    int32_t do_cbs;
+    int32_t smp_flg;
+    int32_t has_lmean0;
+    double lmean0[3];
+    double vsign;              /* -1 or +1 */
+    uint64_t seed;
+    uint64_t path_offset;
+    int32_t precision;
+    int32_t device;
+} scmc_fq_args;
+
+/* ---------------------------------------------------------------------------
+ * Field: u = MCfield(sigt, albedo, box_min, box_max, l, v, is_ff_l, is_ff_v,
+ *                     maxItr, lambda, doCBS, smpFlg, sct_type, ampfunc
+ *                     [, ampfunc0 [, lmean0]])                  (MCfield.m:1)
+ * u: nv x nl complex, interleaved, host memory (2*nv*nl doubles).
+ * ------------------------------------------------------------------------- */
+int scmc_field(const scmc_mc_args *args, double *u);
+
+/* Same, with u in device memory (2*nv*nl doubles) and work on `stream`
+ * (a cudaStream_t, NULL = legacy default stream).  Returns after the work is
+ * enqueued and the batch bookkeeping synchronised. */
+int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Covariance: [Ms, Mm] = MCcov(sigt, albedo, box_min, box_max, l, v, is_ff_l,
+ *                  is_ff_v, maxItr, lambda, doCBS, smpFlg, sct_type, ampfunc
+ *                  [, ampfunc0])                                 (MCcov.m:1)
+ * Ms, Mm: nv x nv x nl x nl complex (v1 fastest, then v2, l1, l2),
+ * interleaved, host memory (2*nv*nv*nl*nl doubles each).  Either may be NULL
+ * to skip copying it out.
+ * ------------------------------------------------------------------------- */
+int scmc_cov(const scmc_mc_args *args, double *Ms, double *Mm);
+
+/* Same with Ms, Mm in device memory. */
+int scmc_cov_device(const scmc_mc_args *args, double *d_Ms, double *d_Mm, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Path records for oracle replay.  Walks paths [path_offset, path_offset +
+ * max_itr) exactly as scmc_field (want_phase=1) or scmc_cov (want_phase=0)
+ * do and copies out one record per scattering event, in path order:
+ *   x[3*e..]   event position           ow[3*e..] incoming direction
+ *   x1[3*e..]  first scatterer           w1[3*e..] first outgoing direction
+ *   wpx[e]     weight/px                 xi[e]     random-phase uniform (field)
+ *   plen[e]    1-based event index in its path (pL)
+ *   path[e]    path index relative to path_offset
+ * Each array has room for `capacity` events; *n_events receives the count
+ * (also when it exceeds capacity, in which case nothing is written and
+ * SCMC_ERR_LIMIT is returned).  Arrays for dim=2 still use stride 3.
+ * ------------------------------------------------------------------------- */
+int scmc_export_records(const scmc_mc_args *args, int32_t want_phase, int64_t capacity,
+                        double *x, double *ow, double *x1, double *w1, double *wpx,
+                        double *xi, int32_t *plen, int64_t *path, int64_t *n_events);
+
+/* Philox-4x32-10 uniform / normal streams of one path, as used by the walk:
+ * n values of stream `tag` (0 uniform, 1 normal) of path `path` under `seed`.
+ * Host memory.  Exposed so the random streams can be checked bit for bit. */
+int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, double *out);
+
+/* Library information and error reporting. */
+int scmc_abi_version(void);
+const char *scmc_last_error(void);
+/* Kernel launches issued by this process since load (all entry points). */
+int64_t scmc_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCMC_GPU_H */

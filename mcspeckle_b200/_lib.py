@@ -1,0 +1,76 @@
+"""Loader for the in-tree CUDA library libscmc_gpu.so.
+
+There is no CPU fallback: if the library is missing or no sm_100 device is
+visible, calls fail loudly with ScmcError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from . import _abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libscmc_gpu.so")
+_lock = threading.Lock()
+_lib = None
+
+_STATUS = {
+    _abi.SCMC_ERR_INVALID: "invalid argument",
+    _abi.SCMC_ERR_CUDA: "CUDA error",
+    _abi.SCMC_ERR_NOMEM: "out of memory",
+    _abi.SCMC_ERR_NODEVICE: "no sm_100 device",
+    _abi.SCMC_ERR_TIMEOUT: "device wait timed out",
+    _abi.SCMC_ERR_CANCELLED: "cancelled",
+    _abi.SCMC_ERR_LIMIT: "limit exceeded",
+}
+
+
+class ScmcError(RuntimeError):
+    """A non-zero scmc_status from the C ABI (message from scmc_last_error)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ScmcError(_abi.SCMC_ERR_NODEVICE,
+                            f"libscmc_gpu.so is not built ({LIB_PATH}); run mcspeckle_b200.build.build()")
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int32)
+        lp = C.POINTER(C.c_int64)
+        mp = C.POINTER(_abi.McArgs)
+        L.scmc_abi_version.restype = C.c_int
+        L.scmc_last_error.restype = C.c_char_p
+        L.scmc_launch_count.restype = C.c_int64
+        L.scmc_field.argtypes = [mp, dp]
+        L.scmc_field_device.argtypes = [mp, C.c_void_p, C.c_void_p]
+        L.scmc_cov.argtypes = [mp, dp, dp]
+        L.scmc_cov_device.argtypes = [mp, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.scmc_export_records.argtypes = [mp, C.c_int32, C.c_int64, dp, dp, dp, dp, dp, dp, ip, lp, lp]
+        L.scmc_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
+        for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",
+                     "scmc_export_records", "scmc_philox_stream"):
+            getattr(L, name).restype = C.c_int
+        _lib = L
+        return _lib
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = lib().scmc_last_error().decode(errors="replace")
+        raise ScmcError(status, msg or _STATUS.get(status, f"status {status}"))
+
+
+def launch_count() -> int:
+    return int(lib().scmc_launch_count())

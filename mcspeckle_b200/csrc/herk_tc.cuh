@@ -1,0 +1,487 @@
+// herk_tc.cuh - covariance contraction on tcgen05 tensor cores (sm_100a).
+//
+// Every event contributes one Hermitian rank-1 update C += t t^H
+// (MCcov.m:232-263), t in C^N with N = nv*nl.  A chunk of E events is the
+// complex rank-E update C += T^T conj(T), done as one real GEMM:
+//
+//   K  = 2E (column 2e holds Re, 2e+1 holds Im of event e)
+//   A  = [2N x K]  row 2i   = ( Re t_i,  Im t_i)  per event
+//                  row 2i+1 = ( Im t_i, -Re t_i)
+//   B  = [N  x K]  row j    = ( Re t_j,  Im t_j)  (= the even rows of A)
+//   D  = A B^T     D[2i][j] = Re C[i][j],  D[2i+1][j] = Im C[i][j]
+//
+// Precision: A is split into FP16 hi + lo parts (A = hi + lo to ~2^-22),
+// B is the FP16 hi part; both products accumulate in FP32 in TMEM, so
+// D = (A_hi + A_lo) B_hi^T.  After the chunk the tile is added into an FP64
+// accumulator, which carries the sum across chunks.
+//
+// Kernel shape: one CTA per 128 x 256 output tile of the upper triangle
+// (complex rows 64*tm .. 64*tm+63 against complex columns 256*tn ..).
+// Warp 0 issues TMA loads (128B swizzle, no multicast), warp 1 issues
+// tcgen05.mma (M=128, N=256, K=16, kind::f16) from one lane, all four warps
+// drain TMEM in the epilogue.  3-stage smem ring of 64 KB.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <stdexcept>
+#include <vector>
+
+#include "accum.cuh"
+
+namespace scmc {
+
+constexpr int TC_BM = 128;
+constexpr int TC_BN = 256;
+constexpr int TC_BK = 64;
+constexpr int TC_STAGES = 3;
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;
+constexpr int TC_B_BYTES = TC_BN * TC_BK * 2;
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + TC_B_BYTES;
+constexpr int TC_SMEM_BYTES = TC_STAGES * TC_STAGE_BYTES + 1024 + 256;
+constexpr int TC_TMEM_COLS = 256;
+constexpr unsigned long long TC_WAIT_NS = 2000000000ull;  // 2 s bound on every wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after TC_WAIT_NS without the phase completing.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    unsigned long long t0 = global_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (global_ns() - t0 > TC_WAIT_NS) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, rows of 128 B,
+// 8-row groups 1024 B apart (SBO), LBO unused (1), sm_100 version bits.
+__device__ __forceinline__ uint64_t umma_desc_sw128(const void *smem_tile)
+{
+    uint64_t a = (uint64_t)((smem_u32(smem_tile) & 0x3FFFF) >> 4);
+    return a | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// kind::f16 instruction descriptor: D F32, A/B F16, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int M, int N)
+{
+    return (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// One 128 x 256 tile of D += (A_hi + A_lo) B^T over num_kb K-blocks of 64.
+__global__ void __launch_bounds__(128, 1)
+herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
+               const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int Mr,
+               int N, double *__restrict__ D, int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + TC_STAGES * TC_STAGE_BYTES);
+    uint64_t *empty = full + TC_STAGES;
+    uint64_t *done = empty + TC_STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+    int *issued = abort_flag + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int2 tile = tiles[blockIdx.x];
+    const int row0 = tile.x * TC_BM;
+    const int col0 = tile.y * TC_BN;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        *issued = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % TC_STAGES;
+            if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1)) {
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int *)abort_flag) break;
+            uint8_t *st = base + s * TC_STAGE_BYTES;
+            mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+            tma_load_2d(st, &tm_ahi, kb * TC_BK, row0, &full[s]);
+            tma_load_2d(st + TC_A_BYTES, &tm_alo, kb * TC_BK, row0, &full[s]);
+            tma_load_2d(st + 2 * TC_A_BYTES, &tm_b, kb * TC_BK, col0, &full[s]);
+            *(volatile int *)issued = kb + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        constexpr uint32_t idesc = umma_idesc_f16(TC_BM, TC_BN);
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % TC_STAGES;
+            if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1)) {
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            tc_fence_after();
+            uint8_t *st = base + s * TC_STAGE_BYTES;
+            const uint64_t dh = umma_desc_sw128(st);
+            const uint64_t dl = umma_desc_sw128(st + TC_A_BYTES);
+            const uint64_t db = umma_desc_sw128(st + 2 * TC_A_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < TC_BK / 16; ++kk) {
+                const uint64_t adv = (uint64_t)(kk * 32) >> 4;  // 16 fp16 = 32 B along K
+                umma_f16(tmem, dh + adv, db + adv, idesc, (kb | kk) != 0);
+                umma_f16(tmem, dl + adv, db + adv, idesc, 1u);
+            }
+            umma_commit(&empty[s]);
+        }
+        umma_commit(done);  // fires once every issued MMA has completed
+    }
+    __syncwarp();
+
+    const bool ok = mbar_wait(done, 0);
+    tc_fence_after();
+    __syncthreads();
+    if (!ok || *(volatile int *)abort_flag) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            // wait (bounded) for TMA copies this CTA still has in flight
+            const int n_issued = *(volatile int *)issued;
+            for (int kb = (n_issued > TC_STAGES ? n_issued - TC_STAGES : 0); kb < n_issued; ++kb)
+                (void)mbar_wait(&full[kb % TC_STAGES], (kb / TC_STAGES) & 1);
+        }
+    } else {
+        // Epilogue: TMEM -> registers -> smem transpose -> coalesced FP64 RMW.
+        float *ep = reinterpret_cast<float *>(base) + warp * 32 * 33;
+        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+            uint32_t r[32];
+            tmem_ld32(tbase + c0, r);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) ep[lane * 33 + j] = __uint_as_float(r[j]);
+            __syncwarp();
+            const int n = col0 + c0 + lane;
+#pragma unroll 4
+            for (int rr = 0; rr < 32; ++rr) {
+                const int R = row0 + warp * 32 + rr;
+                if (R < Mr && n < N) {
+                    double *p = D + (int64_t)R * N + n;
+                    *p += (double)ep[rr * 33 + lane];
+                }
+            }
+            __syncwarp();
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Rows of one chunk in the split FP16 K-major layout.  One CTA per group of
+// 32 events; lane = event, so each row write is 32 consecutive half2 (128 B).
+// ---------------------------------------------------------------------------
+template <int DIM, bool SINGLE>
+__global__ void __launch_bounds__(256)
+tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
+               int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo, const float2 *__restrict__ af_tab)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nv = Q.nv, nl = Q.nl;
+    float2 *sa = reinterpret_cast<float2 *>(smem_raw);  // [nv][33]
+    float2 *sa0 = sa + nv * 33;
+    float2 *sb = sa0 + nv * 33;                           // [nl][33]
+    float2 *sb2 = sb + nl * 33;
+    float *ssc = reinterpret_cast<float *>(sb2 + nl * 33);  // [32]
+    EventView *sev = reinterpret_cast<EventView *>(ssc + 32);
+
+    const int64_t g0 = (int64_t)blockIdx.x * 32;
+    const int ne = (int)max((int64_t)0, min((int64_t)32, n_ev - g0));
+    if (threadIdx.x < 32) {
+        EventView ev;
+        if (threadIdx.x < ne) {
+            load_event<DIM, SINGLE>(Q, S, scap, M, mcap, e0 + g0 + threadIdx.x, ev);
+            ssc[threadIdx.x] = (float)sqrt(ev.wpx);
+        } else {
+            ssc[threadIdx.x] = 0.f;
+            ev = EventView{};
+        }
+        sev[threadIdx.x] = ev;
+    }
+    __syncthreads();
+    const int per = nv + nl;
+    for (int idx = threadIdx.x; idx < 32 * per; idx += blockDim.x) {
+        const int k = idx % 32, m = idx / 32;
+        float2 p = make_float2(0.f, 0.f), q = make_float2(0.f, 0.f);
+        if (k < ne) {
+            const EventView &ev = sev[k];
+            if (m < nv) {
+                if (SINGLE) p = phaseatt<DIM, PMIX>(ev.x1, Q.vs + 3 * m, Q.is_ff_v, Q);
+                else nee_view<DIM, PMIX, float2>(Q, m, ev.x, ev.ow, ev.x1, ev.w1, ev.w0p, p, q);
+            } else {
+                const int j = m - nv;
+                if (SINGLE) p = phaseatt<DIM, PMIX>(ev.x1, Q.l + 3 * j, Q.is_ff_l, Q);
+                else nee_light<DIM, PMIX, float2>(Q, j, ev.x, ev.ow, ev.x1, ev.w1, ev.w0p, p, q);
+            }
+        }
+        if (m < nv) {
+            sa[m * 33 + k] = p;
+            sa0[m * 33 + k] = q;
+        } else {
+            sb[(m - nv) * 33 + k] = p;
+            sb2[(m - nv) * 33 + k] = q;
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int N = nv * nl;
+    const float sc = ssc[lane];
+    const int64_t col = 2 * (g0 + lane);
+    for (int i = warp; i < N; i += 8) {
+        const int vi = i % nv, lj = i / nv;
+        float2 t = cmul(sa[vi * 33 + lane], sb[lj * 33 + lane]);
+        if (SINGLE) {
+            float2 af = af_tab ? af_tab[i] : to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[lane].x1));
+            t = cmul(t, af);
+        } else if (Q.cbs) {
+            float2 t2 = cmul(sa0[vi * 33 + lane], sb2[lj * 33 + lane]);
+            t.x += t2.x;
+            t.y += t2.y;
+        }
+        t.x *= sc;
+        t.y *= sc;
+        const __half hr = __float2half_rn(t.x), hi = __float2half_rn(t.y);
+        const __half lr = __float2half_rn(t.x - __half2float(hr));
+        const __half li = __float2half_rn(t.y - __half2float(hi));
+        const int64_t r0 = (int64_t)(2 * i) * K + col, r1 = (int64_t)(2 * i + 1) * K + col;
+        *reinterpret_cast<__half2 *>(Ahi + r0) = __halves2half2(hr, hi);
+        *reinterpret_cast<__half2 *>(Ahi + r1) = __halves2half2(hi, __hneg(hr));
+        *reinterpret_cast<__half2 *>(Alo + r0) = __halves2half2(lr, li);
+        *reinterpret_cast<__half2 *>(Alo + r1) = __halves2half2(li, __hneg(lr));
+    }
+}
+
+// af(l_j . v_i) table for far-field single scattering, flattened i = v + nv*l.
+template <int DIM>
+__global__ void af_table_kernel(NeeParams Q, float2 *__restrict__ tab)
+{
+    const int N = Q.nv * Q.nl;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const int vi = i % Q.nv, lj = i / Q.nv;
+        tab[i] = to_c<float2>(evalampfunc<DIM>(dot3<DIM>(Q.l + 3 * lj, Q.v + 3 * vi), Q.pf));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct TcPlan {
+    int N;
+    int64_t events_per_chunk;
+    int64_t K;
+    std::vector<int2> tiles;
+};
+
+struct TcOperands {
+    __half *ahi, *alo;
+    int2 *tiles;
+    int *err;
+    float2 *af;
+    CUtensorMap m_ahi, m_alo, m_b;
+    int n_tiles;
+};
+
+inline TcPlan tc_plan(int N)
+{
+    TcPlan p;
+    p.N = N;
+    // 16N bytes of operand per event; keep a chunk's operands near 1 GiB
+    int64_t e = ((int64_t)1 << 30) / (16 * (int64_t)N);
+    e = std::max<int64_t>(32, std::min<int64_t>(e, 32768));
+    e = (e / 32) * 32;
+    p.events_per_chunk = e;
+    p.K = 2 * e;
+    const int n_tm = (2 * N + TC_BM - 1) / TC_BM;
+    const int n_tn = (N + TC_BN - 1) / TC_BN;
+    // tn-major order: CTAs resident together share B tiles
+    for (int tn = 0; tn < n_tn; ++tn)
+        for (int tm = 0; tm < n_tm; ++tm)
+            if ((int64_t)(TC_BM / 2) * tm <= (int64_t)TC_BN * tn + TC_BN - 1) p.tiles.push_back(make_int2(tm, tn));
+    return p;
+}
+
+inline size_t tc_align(size_t x) { return (x + 1023) & ~(size_t)1023; }
+
+inline size_t tc_operand_bytes(const TcPlan &p)
+{
+    size_t a = (size_t)2 * p.N * p.K * sizeof(__half);
+    return 2 * tc_align(a) + tc_align(p.tiles.size() * sizeof(int2)) + 1024 + tc_align((size_t)p.N * sizeof(float2));
+}
+
+inline PFN_cuTensorMapEncodeTiled_v12000 tc_encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+            throw std::runtime_error("cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+inline CUtensorMap tc_map(const void *base, uint64_t cols, uint64_t rows, uint64_t row_stride_bytes, uint32_t box_rows)
+{
+    CUtensorMap m;
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {row_stride_bytes};
+    cuuint32_t box[2] = {(cuuint32_t)TC_BK, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = tc_encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+inline TcOperands tc_make_operands(const TcPlan &p, void *mem, cudaStream_t st)
+{
+    TcOperands o{};
+    char *b = reinterpret_cast<char *>(mem);
+    const size_t a = tc_align((size_t)2 * p.N * p.K * sizeof(__half));
+    o.ahi = reinterpret_cast<__half *>(b);
+    o.alo = reinterpret_cast<__half *>(b + a);
+    o.tiles = reinterpret_cast<int2 *>(b + 2 * a);
+    o.err = reinterpret_cast<int *>(b + 2 * a + tc_align(p.tiles.size() * sizeof(int2)));
+    o.af = reinterpret_cast<float2 *>(reinterpret_cast<char *>(o.err) + 1024);
+    o.n_tiles = (int)p.tiles.size();
+    if (cudaMemcpyAsync(o.tiles, p.tiles.data(), p.tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(o.err, 0, sizeof(int), st) != cudaSuccess)
+        throw std::runtime_error("tcgen05 operand set-up failed");
+    const uint64_t K = (uint64_t)p.K;
+    o.m_ahi = tc_map(o.ahi, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
+    o.m_alo = tc_map(o.alo, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
+    o.m_b = tc_map(o.ahi, K, (uint64_t)p.N, 2 * K * 2, TC_BN);
+    return o;
+}
+
+template <int DIM, bool SINGLE>
+inline void tc_rows(const TcPlan &p, const TcOperands &o, const NeeParams &Q, const SingleRec &S, int64_t scap,
+                    const MultiRec &M, int64_t mcap, int64_t e0, int64_t n, bool use_af_table, cudaStream_t st)
+{
+    const size_t smem = sizeof(float2) * 33 * 2 * (size_t)(Q.nv + Q.nl) + 32 * sizeof(float) +
+                        32 * sizeof(EventView) + 64;
+    auto kern = tc_rows_kernel<DIM, SINGLE>;
+    if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        throw std::runtime_error("too many lights/views for the tensor-core row kernel");
+    const int grid = (int)((n + 31) / 32);
+    kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, use_af_table ? o.af : nullptr);
+}
+
+inline void tc_herk(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
+{
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(herk_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES) != cudaSuccess)
+            throw std::runtime_error("cannot reserve shared memory for the tensor-core kernel");
+        attr = true;
+    }
+    const int num_kb = (int)((2 * n + TC_BK - 1) / TC_BK);
+    herk_tc_kernel<<<o.n_tiles, 128, TC_SMEM_BYTES, st>>>(o.m_ahi, o.m_alo, o.m_b, o.tiles, num_kb, 2 * p.N, p.N, D,
+                                                          o.err);
+}
+
+}  // namespace scmc

@@ -1,0 +1,808 @@
+// scmc_capi.cu - host side of libscmc_gpu.so: argument validation, the
+// process-lifetime device context, path batching and the C ABI entry points
+// declared in include/scmc_gpu.h.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/scmc_gpu.h"
+#include "accum.cuh"
+#include "herk_tc.cuh"
+
+using namespace scmc;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+namespace {
+
+struct ScmcError {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw ScmcError{code, msg}; }
+
+void cuda_check(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) {
+        int code = (e == cudaErrorMemoryAllocation) ? SCMC_ERR_NOMEM : SCMC_ERR_CUDA;
+        fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+#define CK(x) cuda_check((x), #x)
+#define LAUNCHED() (g_launches.fetch_add(1, std::memory_order_relaxed))
+
+template <typename F>
+int guarded(F &&f)
+{
+    try {
+        f();
+        return SCMC_OK;
+    } catch (const ScmcError &e) {
+        g_last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        g_last_error = "host allocation failed";
+        return SCMC_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return SCMC_ERR_CUDA;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return SCMC_ERR_CUDA;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// device buffers and the per-device context
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    void *ensure(size_t bytes)
+    {
+        if (bytes <= n) return p;
+        if (p) CK(cudaFree(p));
+        p = nullptr;
+        n = 0;
+        size_t want = bytes + bytes / 8;
+        CK(cudaMalloc(&p, want));
+        n = want;
+        return p;
+    }
+    template <typename T> T *as() { return reinterpret_cast<T *>(p); }
+};
+
+struct Ctx {
+    int device = -1;
+    std::mutex mu;
+    DevBuf counts, mcnt, moff, scan_tmp, ctr, err;
+    DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
+    DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
+    DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
+    DevBuf acc_s, acc_m, rows, tiles, tc_a, tc_scratch;
+    int64_t scap = 0, mcap = 0;
+};
+
+std::mutex g_ctx_mu;
+std::vector<Ctx *> g_ctx;
+
+Ctx &context(int device)
+{
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) fail(SCMC_ERR_NODEVICE, "no CUDA device visible");
+    if (device < 0 || device >= n) fail(SCMC_ERR_INVALID, "invalid device ordinal");
+    if ((int)g_ctx.size() < n) g_ctx.resize(n, nullptr);
+    if (!g_ctx[device]) {
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10) fail(SCMC_ERR_NODEVICE, "an sm_100 (Blackwell) device is required");
+        g_ctx[device] = new Ctx();
+        g_ctx[device]->device = device;
+    }
+    return *g_ctx[device];
+}
+
+// ---------------------------------------------------------------------------
+// validation (messages follow the reference's error() strings)
+// ---------------------------------------------------------------------------
+void validate_pf(const scmc_phase_function &pf, const char *name)
+{
+    if (pf.sct_type < 1 || pf.sct_type > 3) fail(SCMC_ERR_INVALID, std::string("invalid sct_type in ") + name);
+    if (pf.sct_type == SCMC_SCT_TABULATED && (pf.table_n < 2 || !pf.eval_amp || !pf.sample_icdf))
+        fail(SCMC_ERR_INVALID, std::string("tabulated ") + name + " needs evalAmp and sampleIcdf tables");
+    if (pf.sct_type == SCMC_SCT_HG && !(std::fabs(pf.g) <= 1.0)) fail(SCMC_ERR_INVALID, "Invalid g input");
+}
+
+void validate(const scmc_mc_args *a)
+{
+    if (!a) fail(SCMC_ERR_INVALID, "null arguments");
+    if (a->dim != 2 && a->dim != 3) fail(SCMC_ERR_INVALID, "Invalid box size");
+    if (a->nl < 1 || !a->l) fail(SCMC_ERR_INVALID, "Invalid light source input");
+    if (a->nv < 1 || !a->v) fail(SCMC_ERR_INVALID, "Invalid view source input");
+    if (a->max_itr < 0) fail(SCMC_ERR_INVALID, "Invalid photons number");
+    if (!(a->sigt > 0) || !std::isfinite(a->sigt)) fail(SCMC_ERR_INVALID, "sigt must be positive");
+    if (!(a->lambda > 0)) fail(SCMC_ERR_INVALID, "lambda must be positive");
+    if (a->smp_flg != 1 && a->smp_flg != 2) fail(SCMC_ERR_INVALID, "smpFlg must be 1 or 2");
+    if (a->precision < 0 || a->precision > 2) fail(SCMC_ERR_INVALID, "invalid precision mode");
+    for (int k = 0; k < a->dim; ++k)
+        if (!(a->box_max[k] >= a->box_min[k])) fail(SCMC_ERR_INVALID, "Invalid box size");
+    validate_pf(a->ampfunc, "ampfunc");
+    if (a->has_ampfunc0) validate_pf(a->ampfunc0, "ampfunc0");
+}
+
+// ---------------------------------------------------------------------------
+// argument preparation
+// ---------------------------------------------------------------------------
+struct Prepared {
+    WalkParams W;
+    NeeParams Q;
+    double volume;
+};
+
+PhaseFn upload_pf(const scmc_phase_function &pf, DevBuf &amp, DevBuf &icdf, cudaStream_t st)
+{
+    PhaseFn d{};
+    d.sct_type = pf.sct_type;
+    d.g = pf.g;
+    d.table_n = pf.table_n;
+    if (pf.sct_type == SCMC_SCT_TABULATED) {
+        size_t n = (size_t)pf.table_n;
+        amp.ensure(n * sizeof(double2));
+        icdf.ensure(n * sizeof(double));
+        CK(cudaMemcpyAsync(amp.p, pf.eval_amp, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(icdf.p, pf.sample_icdf, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        d.eval_amp = amp.as<double2>();
+        d.sample_icdf = icdf.as<double>();
+    }
+    return d;
+}
+
+Prepared prepare(Ctx &c, const scmc_mc_args *a, int want_phase, cudaStream_t st)
+{
+    Prepared P{};
+    const int dim = a->dim;
+    WalkParams &W = P.W;
+    W.dim = dim;
+    W.smp_flg = a->smp_flg;
+    W.has_pf0 = a->has_ampfunc0;
+    W.want_phase = want_phase;
+    W.sigt = a->sigt;
+    W.albedo = a->albedo;
+    P.volume = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        W.box_min[k] = k < dim ? a->box_min[k] : 0.0;
+        W.box_max[k] = k < dim ? a->box_max[k] : 0.0;
+        W.box_w[k] = W.box_max[k] - W.box_min[k];
+        if (k < dim) P.volume *= W.box_w[k];
+    }
+    // MCfield.m:77-82: unmeanl = mean(l,2) (or lmean0), meanl = unmeanl/norm
+    double nrm = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        double s = 0.0;
+        if (k < dim)
+            for (int64_t j = 0; j < a->nl; ++j) s += a->l[dim * j + k];
+        W.unmeanl[k] = k < dim ? (a->has_lmean0 ? a->lmean0[k] : s / (double)a->nl) : 0.0;
+        nrm += W.unmeanl[k] * W.unmeanl[k];
+    }
+    nrm = std::sqrt(nrm);
+    for (int k = 0; k < 3; ++k) W.meanl[k] = W.unmeanl[k] / nrm;
+    if (a->smp_flg == 2 && W.unmeanl[dim - 1] == 0.0)
+        fail(SCMC_ERR_INVALID, "exponential first-scatter sampling needs a mean light direction with a non-zero last component");
+    W.key0 = (uint32_t)a->seed;
+    W.key1 = (uint32_t)(a->seed >> 32);
+    W.max_events = a->max_events_per_path;
+
+    W.pf = upload_pf(a->ampfunc, c.tab0_amp, c.tab0_icdf, st);
+    if (a->has_ampfunc0) W.pf0 = upload_pf(a->ampfunc0, c.tab1_amp, c.tab1_icdf, st);
+    else W.pf0 = W.pf;
+
+    // directions as [n][3]
+    std::vector<double> hl(3 * a->nl, 0.0), hv(3 * a->nv, 0.0), hvs(3 * a->nv, 0.0);
+    double ff_sign = a->is_ff_v ? -1.0 : 1.0;  // MCfield.m:106
+    for (int64_t j = 0; j < a->nl; ++j)
+        for (int k = 0; k < dim; ++k) hl[3 * j + k] = a->l[dim * j + k];
+    for (int64_t i = 0; i < a->nv; ++i)
+        for (int k = 0; k < dim; ++k) {
+            hv[3 * i + k] = a->v[dim * i + k];
+            hvs[3 * i + k] = ff_sign * a->v[dim * i + k];
+        }
+    c.dirs_l.ensure(hl.size() * 8);
+    c.dirs_v.ensure(hv.size() * 8);
+    c.dirs_vs.ensure(hvs.size() * 8);
+    CK(cudaMemcpyAsync(c.dirs_l.p, hl.data(), hl.size() * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c.dirs_v.p, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c.dirs_vs.p, hvs.data(), hvs.size() * 8, cudaMemcpyHostToDevice, st));
+
+    NeeParams &Q = P.Q;
+    Q.nv = (int)a->nv;
+    Q.nl = (int)a->nl;
+    Q.is_ff_l = a->is_ff_l;
+    Q.is_ff_v = a->is_ff_v;
+    Q.cbs = a->do_cbs;
+    Q.sigt_half = a->sigt / 2.0;
+    Q.kw = SCMC_PI * 2.0 / a->lambda;
+    Q.lambda = a->lambda;
+    for (int k = 0; k < 3; ++k) {
+        Q.box_min[k] = W.box_min[k];
+        Q.box_max[k] = W.box_max[k];
+        Q.meanl[k] = W.meanl[k];
+    }
+    Q.l = c.dirs_l.as<double>();
+    Q.v = c.dirs_v.as<double>();
+    Q.vs = c.dirs_vs.as<double>();
+    Q.has_pf0 = a->has_ampfunc0;
+    Q.pf = W.pf;
+    Q.pf0 = W.pf0;
+    // the host copies above must complete before the vectors go out of scope
+    CK(cudaStreamSynchronize(st));
+    return P;
+}
+
+// ---------------------------------------------------------------------------
+// the walk of one batch of paths -> records
+// ---------------------------------------------------------------------------
+__global__ void count_to_multi_kernel(const int32_t *__restrict__ counts, int64_t n, int64_t *__restrict__ m)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        m[p] = (int64_t)counts[p] - 1;
+}
+
+int sm_count(int device)
+{
+    static int cached[64] = {0};
+    if (device < 64 && cached[device]) return cached[device];
+    int n = 148;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+    if (device < 64) cached[device] = n;
+    return n;
+}
+
+struct Batch {
+    SingleRec S;
+    MultiRec M;
+    int64_t n_paths = 0, n_multi = 0;
+};
+
+template <int DIM>
+void walk_batch_dim(Ctx &c, WalkParams W, int64_t n_paths, cudaStream_t st, Batch &B)
+{
+    const int sms = sm_count(c.device);
+    const int threads = 128;
+    int grid = (int)std::min<int64_t>((n_paths + threads - 1) / threads, (int64_t)sms * 8);
+    if (grid < 1) grid = 1;
+    W.n_paths = n_paths;
+    c.counts.ensure(n_paths * sizeof(int32_t));
+    c.mcnt.ensure(n_paths * sizeof(int64_t));
+    c.moff.ensure((n_paths + 1) * sizeof(int64_t));
+    c.ctr.ensure(2 * sizeof(unsigned long long));
+    c.err.ensure(sizeof(int));
+    unsigned long long *ctr = c.ctr.as<unsigned long long>();
+    CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+    CK(cudaMemsetAsync(c.err.p, 0, sizeof(int), st));
+    walk_count_kernel<DIM><<<grid, threads, 0, st>>>(W, c.counts.as<int32_t>(), ctr, c.err.as<int>());
+    CK(cudaGetLastError());
+    LAUNCHED();
+    count_to_multi_kernel<<<std::max(1, std::min(sms * 4, (int)((n_paths + 255) / 256))), 256, 0, st>>>(
+        c.counts.as<int32_t>(), n_paths, c.mcnt.as<int64_t>());
+    CK(cudaGetLastError());
+    LAUNCHED();
+    size_t tmp = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, c.mcnt.as<int64_t>(), c.moff.as<int64_t>(), n_paths, st));
+    c.scan_tmp.ensure(tmp);
+    CK(cub::DeviceScan::ExclusiveSum(c.scan_tmp.p, tmp, c.mcnt.as<int64_t>(), c.moff.as<int64_t>(), n_paths, st));
+    LAUNCHED();
+    int64_t last[2];
+    int herr = 0;
+    CK(cudaMemcpyAsync(&last[0], c.moff.as<int64_t>() + n_paths - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[1], c.mcnt.as<int64_t>() + n_paths - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&herr, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) fail(SCMC_ERR_LIMIT, "a path exceeded max_events_per_path");
+    const int64_t n_multi = last[0] + last[1];
+
+    // record storage
+    if (c.scap < n_paths) {
+        int64_t cap = n_paths;
+        c.s_x1.ensure(3 * cap * 8);
+        c.s_w1.ensure(3 * cap * 8);
+        c.s_wpx.ensure(cap * 8);
+        c.s_xi.ensure(cap * 8);
+        c.s_nev.ensure(cap * 4);
+        c.scap = cap;
+    }
+    if (c.mcap < std::max<int64_t>(n_multi, 1)) {
+        int64_t cap = std::max<int64_t>(n_multi + n_multi / 4, 1024);
+        c.m_x.ensure(3 * cap * 8);
+        c.m_ow.ensure(3 * cap * 8);
+        c.m_wpx.ensure(cap * 8);
+        c.m_xi.ensure(cap * 8);
+        c.m_path.ensure(cap * 4);
+        c.m_plen.ensure(cap * 4);
+        c.mcap = cap;
+    }
+    B.S = SingleRec{c.s_x1.as<double>(), c.s_w1.as<double>(), c.s_wpx.as<double>(), c.s_xi.as<double>(),
+                    c.s_nev.as<int32_t>()};
+    B.M = MultiRec{c.m_x.as<double>(), c.m_ow.as<double>(), c.m_wpx.as<double>(), c.m_xi.as<double>(),
+                   c.m_path.as<int32_t>(), c.m_plen.as<int32_t>()};
+    B.n_paths = n_paths;
+    B.n_multi = n_multi;
+    CK(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), st));
+    walk_record_kernel<DIM><<<grid, threads, 0, st>>>(W, c.moff.as<int64_t>(), B.S, c.scap, B.M, c.mcap, ctr + 1);
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
+void walk_batch(Ctx &c, const WalkParams &W, int64_t n_paths, cudaStream_t st, Batch &B)
+{
+    if (W.dim == 3) walk_batch_dim<3>(c, W, n_paths, st, B);
+    else walk_batch_dim<2>(c, W, n_paths, st, B);
+}
+
+int64_t path_batch_size(int64_t remaining) { return std::min<int64_t>(remaining, (int64_t)1 << 20); }
+
+// ---------------------------------------------------------------------------
+// field
+// ---------------------------------------------------------------------------
+template <int DIM, int POL, bool SINGLE, typename AccT>
+void launch_field_accum(Ctx &c, const Prepared &P, const Batch &B, AccT *U, int64_t n_ev, cudaStream_t st)
+{
+    if (n_ev <= 0) return;
+    const int nv = P.Q.nv, nl = P.Q.nl;
+    int tv = std::min(nv, 32), tl = std::min(nl, 32);
+    while (tv * tl > kFieldMaxTile) tl /= 2;
+    const int n_vtiles = (nv + tv - 1) / tv, n_ltiles = (nl + tl - 1) / tl;
+    const int tiles = n_vtiles * n_ltiles;
+    const int sms = sm_count(c.device);
+    int64_t target = (int64_t)sms * 6;
+    int64_t ranges = std::max<int64_t>(1, target / tiles);
+    int64_t per = (n_ev + ranges - 1) / ranges;
+    per = std::max<int64_t>(per, kFieldEB * 4);
+    ranges = (n_ev + per - 1) / per;
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using C = typename cplx_t<R>::type;
+    size_t smem = sizeof(C) * (2 * kFieldEB * (tv + tl) + kFieldEB) + sizeof(EventView) * kFieldEB + 16;
+    auto kern = field_accum_kernel<DIM, POL, SINGLE, AccT>;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(tiles, (unsigned)ranges);
+    kern<<<grid, kFieldThreads, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, n_ev, tv, tl, n_vtiles, per, U,
+                                            P.W.want_phase);
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
+template <int DIM, int POL, typename AccT>
+void field_run(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u, cudaStream_t st)
+{
+    const int64_t n = a->nv * a->nl;
+    AccT *Us = reinterpret_cast<AccT *>(c.acc_s.ensure(2 * n * sizeof(AccT)));
+    AccT *Um = reinterpret_cast<AccT *>(c.acc_m.ensure(2 * n * sizeof(AccT)));
+    CK(cudaMemsetAsync(Us, 0, 2 * n * sizeof(AccT), st));
+    CK(cudaMemsetAsync(Um, 0, 2 * n * sizeof(AccT), st));
+    WalkParams W = P.W;
+    for (int64_t done = 0; done < a->max_itr;) {
+        int64_t nb = path_batch_size(a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        launch_field_accum<DIM, POL, true, AccT>(c, P, B, Us, B.n_paths, st);
+        launch_field_accum<DIM, POL, false, AccT>(c, P, B, Um, B.n_multi, st);
+        done += nb;
+    }
+    double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
+    double norm = m > 0 ? std::sqrt(1.0 / m * P.volume * a->sigt) : 0.0;  // MCfield.m:253-254
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 1024);
+    field_finalize_kernel<DIM, AccT><<<std::max(grid, 1), 256, 0, st>>>(P.Q, Us, Um, norm, d_u);
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
+void field_device(const scmc_mc_args *a, double *d_u, cudaStream_t st)
+{
+    validate(a);
+    Ctx &c = context(a->device);
+    std::lock_guard<std::mutex> lk(c.mu);
+    CK(cudaSetDevice(a->device));
+    Prepared P = prepare(c, a, 1, st);
+    double2 *u = reinterpret_cast<double2 *>(d_u);
+    if (a->dim == 3) {
+        if (a->precision == SCMC_PREC_FP64) field_run<3, P64, double>(c, a, P, u, st);
+        else if (a->precision == SCMC_PREC_MIXED) field_run<3, PMIX, double>(c, a, P, u, st);
+        else field_run<3, P32, float>(c, a, P, u, st);
+    } else {
+        if (a->precision == SCMC_PREC_FP64) field_run<2, P64, double>(c, a, P, u, st);
+        else if (a->precision == SCMC_PREC_MIXED) field_run<2, PMIX, double>(c, a, P, u, st);
+        else field_run<2, P32, float>(c, a, P, u, st);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// covariance
+// ---------------------------------------------------------------------------
+std::vector<int2> upper_tiles(int N, int tile)
+{
+    int nt = (N + tile - 1) / tile;
+    std::vector<int2> t;
+    for (int i = 0; i < nt; ++i)
+        for (int j = i; j < nt; ++j) t.push_back(make_int2(i, j));
+    return t;
+}
+
+template <int DIM, int POL, bool SINGLE>
+void cov_rows(Ctx &c, const Prepared &P, const Batch &B, int64_t e0, int64_t n, void *T, cudaStream_t st)
+{
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using C = typename cplx_t<R>::type;
+    const int nv = P.Q.nv, nl = P.Q.nl;
+    int eb = 4;
+    size_t per_ev = sizeof(C) * 2 * (nv + nl) + sizeof(double) + sizeof(EventView);
+    while (eb > 1 && per_ev * eb > 96 * 1024) eb /= 2;
+    size_t smem = per_ev * eb + 64;
+    auto kern = cov_rows_kernel<DIM, POL, SINGLE>;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int grid = (int)((n + eb - 1) / eb);
+    kern<<<grid, 256, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, e0, n, eb, reinterpret_cast<C *>(T));
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
+template <typename R, typename A>
+void herk_cc(Ctx &c, const void *T, int64_t n, int N, void *Cacc, cudaStream_t st)
+{
+    constexpr int RPT = std::is_same<R, double>::value ? 4 : 8;
+    constexpr int BK = std::is_same<R, double>::value ? 8 : 16;
+    std::vector<int2> tl = upper_tiles(N, 16 * RPT);
+    c.tiles.ensure(tl.size() * sizeof(int2));
+    CK(cudaMemcpyAsync(c.tiles.p, tl.data(), tl.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    herk_cc_kernel<R, A, RPT, BK><<<(unsigned)tl.size(), 256, 0, st>>>(
+        reinterpret_cast<const typename cplx_t<R>::type *>(T), n, N, c.tiles.as<int2>(),
+        reinterpret_cast<typename cplx_t<A>::type *>(Cacc));
+    CK(cudaGetLastError());
+    LAUNCHED();
+    CK(cudaStreamSynchronize(st));  // tile list is a stack vector
+}
+
+template <int DIM, int POL>
+void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st)
+{
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using A = R;  // plain FP32 keeps FP32 accumulators; FP64 mode keeps FP64
+    using C = typename cplx_t<R>::type;
+    const int N = (int)(a->nv * a->nl);
+    const size_t acc_bytes = (size_t)N * N * 2 * sizeof(A);
+    void *Cs = c.acc_s.ensure(acc_bytes);
+    void *Cm = c.acc_m.ensure(acc_bytes);
+    CK(cudaMemsetAsync(Cs, 0, acc_bytes, st));
+    CK(cudaMemsetAsync(Cm, 0, acc_bytes, st));
+    int64_t chunk = std::max<int64_t>(64, std::min<int64_t>(8192, ((int64_t)256 << 20) / ((int64_t)N * sizeof(C))));
+    void *T = c.rows.ensure((size_t)chunk * N * sizeof(C));
+    WalkParams W = P.W;
+    for (int64_t done = 0; done < a->max_itr;) {
+        int64_t nb = path_batch_size(a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        for (int64_t e0 = 0; e0 < B.n_paths; e0 += chunk) {
+            int64_t n = std::min(chunk, B.n_paths - e0);
+            cov_rows<DIM, POL, true>(c, P, B, e0, n, T, st);
+            herk_cc<R, A>(c, T, n, N, Cs, st);
+        }
+        for (int64_t e0 = 0; e0 < B.n_multi; e0 += chunk) {
+            int64_t n = std::min(chunk, B.n_multi - e0);
+            cov_rows<DIM, POL, false>(c, P, B, e0, n, T, st);
+            herk_cc<R, A>(c, T, n, N, Cm, st);
+        }
+        done += nb;
+    }
+    double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
+    double sc = m > 0 ? 1.0 / m * P.volume * a->sigt : 0.0;  // MCcov.m:293-299
+    double scm = a->do_cbs ? sc / 2.0 : sc;
+    int64_t total = (int64_t)N * N;
+    int grid = (int)std::min<int64_t>((total + 255) / 256, 4096);
+    if (d_Ms) {
+        cov_finalize_kernel<A><<<grid, 256, 0, st>>>(reinterpret_cast<const A *>(Cs), 0, (int)a->nv, (int)a->nl, sc, d_Ms);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+    if (d_Mm) {
+        cov_finalize_kernel<A><<<grid, 256, 0, st>>>(reinterpret_cast<const A *>(Cm), 0, (int)a->nv, (int)a->nl, scm, d_Mm);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+}
+
+template <int DIM>
+void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st)
+{
+    const int N = (int)(a->nv * a->nl);
+    TcPlan plan = tc_plan(N);
+    const size_t acc_bytes = (size_t)2 * N * N * sizeof(double);
+    double *Ds = reinterpret_cast<double *>(c.acc_s.ensure(acc_bytes));
+    double *Dm = reinterpret_cast<double *>(c.acc_m.ensure(acc_bytes));
+    CK(cudaMemsetAsync(Ds, 0, acc_bytes, st));
+    CK(cudaMemsetAsync(Dm, 0, acc_bytes, st));
+    const int64_t chunk = plan.events_per_chunk;
+    TcOperands ops = tc_make_operands(plan, c.tc_a.ensure(tc_operand_bytes(plan)), st);
+    const bool ffff = a->is_ff_l && a->is_ff_v;
+    if (ffff) {
+        af_table_kernel<DIM><<<std::max(1, std::min(1024, (N + 255) / 256)), 256, 0, st>>>(P.Q, ops.af);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+    WalkParams W = P.W;
+    for (int64_t done = 0; done < a->max_itr;) {
+        int64_t nb = path_batch_size(a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        for (int pass = 0; pass < 2; ++pass) {
+            const bool single = pass == 0;
+            const int64_t n_ev = single ? B.n_paths : B.n_multi;
+            double *D = single ? Ds : Dm;
+            for (int64_t e0 = 0; e0 < n_ev; e0 += chunk) {
+                int64_t n = std::min(chunk, n_ev - e0);
+                if (single) tc_rows<DIM, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
+                else tc_rows<DIM, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
+                CK(cudaGetLastError());
+                LAUNCHED();
+                tc_herk(plan, ops, n, D, st);
+                CK(cudaGetLastError());
+                LAUNCHED();
+            }
+        }
+        done += nb;
+    }
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, ops.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
+    double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
+    double sc = m > 0 ? 1.0 / m * P.volume * a->sigt : 0.0;
+    double scm = a->do_cbs ? sc / 2.0 : sc;
+    int64_t total = (int64_t)N * N;
+    int grid = (int)std::min<int64_t>((total + 255) / 256, 4096);
+    if (d_Ms) {
+        cov_finalize_kernel<double><<<grid, 256, 0, st>>>(Ds, 1, (int)a->nv, (int)a->nl, sc, d_Ms);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+    if (d_Mm) {
+        cov_finalize_kernel<double><<<grid, 256, 0, st>>>(Dm, 1, (int)a->nv, (int)a->nl, scm, d_Mm);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+}
+
+void cov_device(const scmc_mc_args *a, double *d_Ms, double *d_Mm, cudaStream_t st)
+{
+    validate(a);
+    Ctx &c = context(a->device);
+    std::lock_guard<std::mutex> lk(c.mu);
+    CK(cudaSetDevice(a->device));
+    Prepared P = prepare(c, a, 0, st);
+    double2 *Ms = reinterpret_cast<double2 *>(d_Ms), *Mm = reinterpret_cast<double2 *>(d_Mm);
+    if (a->dim == 3) {
+        if (a->precision == SCMC_PREC_FP64) cov_run_cc<3, P64>(c, a, P, Ms, Mm, st);
+        else if (a->precision == SCMC_PREC_FP32) cov_run_cc<3, P32>(c, a, P, Ms, Mm, st);
+        else cov_run_tc<3>(c, a, P, Ms, Mm, st);
+    } else {
+        if (a->precision == SCMC_PREC_FP64) cov_run_cc<2, P64>(c, a, P, Ms, Mm, st);
+        else if (a->precision == SCMC_PREC_FP32) cov_run_cc<2, P32>(c, a, P, Ms, Mm, st);
+        else cov_run_tc<2>(c, a, P, Ms, Mm, st);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// records export
+// ---------------------------------------------------------------------------
+__global__ void expand_records_kernel(SingleRec S, int64_t scap, MultiRec M, int64_t mcap, const int64_t *moff,
+                                      int64_t n_paths, int64_t base_ev, int64_t base_path, double *x, double *ow,
+                                      double *x1, double *w1, double *wpx, double *xi, int32_t *plen, int64_t *path)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n_paths; p += (int64_t)gridDim.x * blockDim.x) {
+        int64_t mo = moff[p];
+        int64_t e = base_ev + mo + p;  // events of earlier paths: singles p + multis mo
+        int nev = S.nev[p];
+        for (int k = 0; k < nev; ++k) {
+            int64_t o = e + k;
+            for (int d = 0; d < 3; ++d) {
+                double xv = k == 0 ? S.x1[d * scap + p] : M.x[d * mcap + mo + k - 1];
+                double ov = k == 0 ? 0.0 : M.ow[d * mcap + mo + k - 1];
+                x[3 * o + d] = xv;
+                ow[3 * o + d] = ov;
+                x1[3 * o + d] = S.x1[d * scap + p];
+                w1[3 * o + d] = S.w1[d * scap + p];
+            }
+            wpx[o] = k == 0 ? S.wpx[p] : M.wpx[mo + k - 1];
+            xi[o] = k == 0 ? S.xi[p] : M.xi[mo + k - 1];
+            plen[o] = k + 1;
+            path[o] = base_path + p;
+        }
+    }
+}
+
+void export_records(const scmc_mc_args *a, int want_phase, int64_t capacity, double *x, double *ow, double *x1,
+                    double *w1, double *wpx, double *xi, int32_t *plen, int64_t *path, int64_t *n_events)
+{
+    validate(a);
+    Ctx &c = context(a->device);
+    std::lock_guard<std::mutex> lk(c.mu);
+    CK(cudaSetDevice(a->device));
+    cudaStream_t st = 0;
+    Prepared P = prepare(c, a, want_phase, st);
+    WalkParams W = P.W;
+    int64_t total = 0;
+    std::vector<Batch> dummy;
+    // first pass: count all events
+    for (int64_t done = 0; done < a->max_itr;) {
+        int64_t nb = path_batch_size(a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        total += B.n_paths + B.n_multi;
+        done += nb;
+    }
+    *n_events = total;
+    if (total > capacity) fail(SCMC_ERR_LIMIT, "record capacity too small");
+    DevBuf out;
+    size_t bytes = (size_t)std::max<int64_t>(total, 1) * (12 * 8 + 8 + 8 + 4 + 8);
+    char *base = reinterpret_cast<char *>(out.ensure(bytes));
+    int64_t T = std::max<int64_t>(total, 1);
+    double *dx = reinterpret_cast<double *>(base);
+    double *dow = dx + 3 * T, *dx1 = dow + 3 * T, *dw1 = dx1 + 3 * T, *dwpx = dw1 + 3 * T, *dxi = dwpx + T;
+    int64_t *dpath = reinterpret_cast<int64_t *>(dxi + T);
+    int32_t *dplen = reinterpret_cast<int32_t *>(dpath + T);
+    int64_t ev = 0;
+    for (int64_t done = 0; done < a->max_itr;) {
+        int64_t nb = path_batch_size(a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        expand_records_kernel<<<256, 128, 0, st>>>(B.S, c.scap, B.M, c.mcap, c.moff.as<int64_t>(), nb, ev, done,
+                                                   dx, dow, dx1, dw1, dwpx, dxi, dplen, dpath);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        ev += B.n_paths + B.n_multi;
+        done += nb;
+    }
+    if (total > 0) {
+        CK(cudaMemcpyAsync(x, dx, 3 * total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ow, dow, 3 * total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(x1, dx1, 3 * total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(w1, dw1, 3 * total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(wpx, dwpx, total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(xi, dxi, total * 8, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(plen, dplen, total * 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(path, dpath, total * 8, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    CK(cudaFree(out.p));
+}
+
+// The per-path streams exactly as the walk draws them (device arithmetic).
+__global__ void philox_stream_kernel(uint64_t seed, uint64_t path, int tag, int64_t n, double *out)
+{
+    PathRng r;
+    r.init((uint32_t)seed, (uint32_t)(seed >> 32), path);
+    for (int64_t i = 0; i < n; ++i) out[i] = tag ? r.randn() : r.rand();
+}
+
+// Host-memory wrappers: device output, then one copy back.
+template <typename F>
+void with_device_outputs(int device, std::vector<std::pair<double *, size_t>> outs, F &&run)
+{
+    CK(cudaSetDevice(device));
+    std::vector<void *> dev(outs.size(), nullptr);
+    try {
+        for (size_t k = 0; k < outs.size(); ++k)
+            if (outs[k].first) CK(cudaMalloc(&dev[k], outs[k].second));
+        run(dev);
+        for (size_t k = 0; k < outs.size(); ++k)
+            if (outs[k].first) CK(cudaMemcpy(outs[k].first, dev[k], outs[k].second, cudaMemcpyDeviceToHost));
+    } catch (...) {
+        for (void *p : dev)
+            if (p) cudaFree(p);
+        throw;
+    }
+    for (void *p : dev)
+        if (p) CK(cudaFree(p));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int scmc_abi_version(void) { return SCMC_ABI_VERSION; }
+
+const char *scmc_last_error(void) { return g_last_error.c_str(); }
+
+int64_t scmc_launch_count(void) { return g_launches.load(); }
+
+int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream)
+{
+    return guarded([&] {
+        if (!d_u) fail(SCMC_ERR_INVALID, "null output");
+        field_device(args, d_u, reinterpret_cast<cudaStream_t>(stream));
+        CK(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+    });
+}
+
+int scmc_field(const scmc_mc_args *args, double *u)
+{
+    return guarded([&] {
+        validate(args);
+        if (!u) fail(SCMC_ERR_INVALID, "null output");
+        size_t bytes = (size_t)args->nv * args->nl * 2 * sizeof(double);
+        with_device_outputs(args->device, {{u, bytes}}, [&](std::vector<void *> &d) {
+            field_device(args, reinterpret_cast<double *>(d[0]), 0);
+            CK(cudaStreamSynchronize(0));
+        });
+    });
+}
+
+int scmc_cov_device(const scmc_mc_args *args, double *d_Ms, double *d_Mm, void *stream)
+{
+    return guarded([&] {
+        cov_device(args, d_Ms, d_Mm, reinterpret_cast<cudaStream_t>(stream));
+        CK(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+    });
+}
+
+int scmc_cov(const scmc_mc_args *args, double *Ms, double *Mm)
+{
+    return guarded([&] {
+        validate(args);
+        size_t n = (size_t)args->nv * args->nv * args->nl * args->nl;
+        size_t bytes = n * 2 * sizeof(double);
+        with_device_outputs(args->device, {{Ms, bytes}, {Mm, bytes}}, [&](std::vector<void *> &d) {
+            cov_device(args, reinterpret_cast<double *>(d[0]), reinterpret_cast<double *>(d[1]), 0);
+            CK(cudaStreamSynchronize(0));
+        });
+    });
+}
+
+int scmc_export_records(const scmc_mc_args *args, int32_t want_phase, int64_t capacity, double *x, double *ow,
+                        double *x1, double *w1, double *wpx, double *xi, int32_t *plen, int64_t *path,
+                        int64_t *n_events)
+{
+    return guarded([&] {
+        if (!n_events) fail(SCMC_ERR_INVALID, "null n_events");
+        export_records(args, want_phase, capacity, x, ow, x1, w1, wpx, xi, plen, path, n_events);
+    });
+}
+
+int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, double *out)
+{
+    return guarded([&] {
+        if (n < 0 || (n > 0 && !out)) fail(SCMC_ERR_INVALID, "invalid output");
+        if (n == 0) return;
+        context(0);
+        CK(cudaSetDevice(0));
+        double *d = nullptr;
+        CK(cudaMalloc(&d, n * sizeof(double)));
+        philox_stream_kernel<<<1, 1>>>(seed, path, tag, n, d);
+        cudaError_t e = cudaGetLastError();
+        LAUNCHED();
+        if (e == cudaSuccess) e = cudaMemcpy(out, d, n * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        CK(e);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,173 @@
+// walk.cuh - the random walk of MCfield.m:112-250 / MCcov.m:112-290.
+//
+// One lane walks one path at a time and takes the next path as soon as its
+// current one leaves the box or is killed, so every lane stays busy until
+// the batch runs out (a flattened event loop: all lanes run the same loop
+// body).  The walk is FP64 in every precision mode, so the three modes see
+// identical paths for the same seed.
+//
+// Two passes share the walk: the count pass stores the number of events of
+// every path; after an exclusive scan the record pass re-walks each path
+// (Philox makes it identical) and writes its events at fixed offsets, in
+// path order.  The first event of a path goes to the single-scattering
+// record (index = path), the others to the multiple-scattering records.
+#pragma once
+
+#include "common.cuh"
+
+namespace scmc {
+
+// Single-scattering records: one per path (SoA, stride = cap).
+struct SingleRec {
+    double *x1;   // 3*cap: first scatterer
+    double *w1;   // 3*cap: first outgoing direction
+    double *wpx;  // weight/px at the first event
+    double *xi;   // random-phase uniform of the first event (field)
+    int32_t *nev; // events of the path
+};
+
+// Multiple-scattering records (SoA, stride = cap).
+struct MultiRec {
+    double *x;     // 3*cap: event position
+    double *ow;    // 3*cap: incoming direction
+    double *wpx;   // weight/px
+    double *xi;    // random-phase uniform (field)
+    int32_t *path; // path index within the batch
+    int32_t *plen; // pL (>= 2)
+};
+
+struct WalkState {
+    double x[3], w[3], ow[3];
+    double px, weight;
+    int pL;
+};
+
+// Initialise a path: first scatterer (MCfield.m:118-125) and first
+// direction (MCfield.m:149-155).
+template <int DIM>
+__device__ __forceinline__ void path_init(const WalkParams &P, PathRng &r, WalkState &s)
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { s.x[k] = 0.0; s.w[k] = 0.0; s.ow[k] = 0.0; }
+    if (P.smp_flg == 1) {
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) s.x[k] = r.rand() * P.box_w[k] + P.box_min[k];
+        s.px = 1.0;
+    } else {
+        exp_smp_x<DIM>(P, s.x, &s.px, r);
+    }
+    if (!P.has_pf0) randn_dir<DIM>(s.w, r);
+    else smpampfunc_general<DIM>(P.meanl, P.pf0, s.w, r);
+    s.pL = 0;
+    s.weight = P.albedo;
+}
+
+// After the event at s.x has been recorded: free flight, box exit, roulette
+// and the next direction (MCfield.m:225-246).  Returns false when the path
+// ends.
+template <int DIM>
+__device__ __forceinline__ bool path_advance(const WalkParams &P, PathRng &r, WalkState &s)
+{
+    double d = -log(-r.rand() + 1.0) / P.sigt;
+    bool out = false;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        s.x[k] = s.x[k] + d * s.w[k];
+        out |= (s.x[k] > P.box_max[k]) || (s.x[k] < P.box_min[k]);
+    }
+    if (out) return false;
+    if (s.weight < kKillThr) {
+        if (r.rand() > P.albedo) return false;
+    } else {
+        s.weight = s.weight * P.albedo;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.ow[k] = s.w[k];
+    smpampfunc_general<DIM>(s.ow, P.pf, s.w, r);
+    return true;
+}
+
+// Pass 1: events per path.
+template <int DIM>
+__global__ void __launch_bounds__(128) walk_count_kernel(WalkParams P, int32_t *__restrict__ counts,
+                                                         unsigned long long *__restrict__ next_path,
+                                                         int *__restrict__ err)
+{
+    PathRng r;
+    WalkState s;
+    int64_t p = -1;
+    int n = 0;
+    for (;;) {
+        if (p < 0) {
+            p = (int64_t)atomicAdd(next_path, 1ull);
+            if (p >= P.n_paths) break;
+            r.init(P.key0, P.key1, P.path_base + (uint64_t)p);
+            path_init<DIM>(P, r, s);
+            n = 0;
+        }
+        ++n;
+        if (P.want_phase) (void)r.rand();  // MCfield.m:220
+        bool alive = path_advance<DIM>(P, r, s);
+        if (alive && P.max_events > 0 && n >= P.max_events) {
+            atomicExch(err, 1);
+            alive = false;
+        }
+        if (!alive) {
+            counts[p] = n;
+            p = -1;
+        }
+    }
+}
+
+// Pass 2: records.  moff[p] = index of the first multiple-scattering record
+// of path p (exclusive scan of counts[p] - 1).
+template <int DIM>
+__global__ void __launch_bounds__(128) walk_record_kernel(WalkParams P, const int64_t *__restrict__ moff,
+                                                          SingleRec S, int64_t scap, MultiRec M,
+                                                          int64_t mcap, unsigned long long *__restrict__ next_path)
+{
+    PathRng r;
+    WalkState s;
+    int64_t p = -1;
+    int64_t mo = 0;
+    for (;;) {
+        if (p < 0) {
+            p = (int64_t)atomicAdd(next_path, 1ull);
+            if (p >= P.n_paths) break;
+            r.init(P.key0, P.key1, P.path_base + (uint64_t)p);
+            path_init<DIM>(P, r, s);
+            mo = moff[p];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                S.x1[k * scap + p] = s.x[k];
+                S.w1[k * scap + p] = s.w[k];
+            }
+        }
+        ++s.pL;
+        double xi = P.want_phase ? r.rand() : 0.0;
+        double wpx = s.weight / s.px;
+        if (s.pL == 1) {
+            S.wpx[p] = wpx;
+            S.xi[p] = xi;
+        } else {
+            int64_t e = mo + (s.pL - 2);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                M.x[k * mcap + e] = s.x[k];
+                M.ow[k * mcap + e] = s.ow[k];
+            }
+            M.wpx[e] = wpx;
+            M.xi[e] = xi;
+            M.path[e] = (int32_t)p;
+            M.plen[e] = s.pL;
+        }
+        bool alive = path_advance<DIM>(P, r, s);
+        if (alive && P.max_events > 0 && s.pL >= P.max_events) alive = false;
+        if (!alive) {
+            S.nev[p] = s.pL;
+            p = -1;
+        }
+    }
+}
+
+}  // namespace scmc

@@ -1,0 +1,192 @@
+"""ctypes front end of oracle/libscmc_oracle.so (test infrastructure only).
+
+The C library restates code/MCfield.m, code/MCcov.m and
+code/MCfieldFourierQuad.m in FP64.  Random numbers come either from tapes
+(the draws a MATLAB run consumed, in order) or from the per-path Philox
+streams the GPU walk uses.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from mcspeckle_b200._abi import ArgsHolder, FqArgs
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libscmc_oracle.so")
+_lib = None
+
+TAPE, PHILOX = 0, 1
+
+
+class RngSpec(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32),
+        ("utape", C.POINTER(C.c_double)),
+        ("un", C.c_int64),
+        ("ntape", C.POINTER(C.c_double)),
+        ("nn", C.c_int64),
+        ("used_u", C.c_int64),
+        ("used_n", C.c_int64),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int32)
+        lp = C.POINTER(C.c_int64)
+        _lib.oracle_field.argtypes = [C.c_void_p, C.POINTER(RngSpec), dp]
+        _lib.oracle_cov.argtypes = [C.c_void_p, C.POINTER(RngSpec), dp, dp, C.c_int]
+        _lib.oracle_records.argtypes = [C.c_void_p, C.POINTER(RngSpec), C.c_int32, C.c_int64,
+                                        dp, dp, dp, dp, dp, dp, ip, lp, lp]
+        _lib.oracle_field_from_records.argtypes = [C.c_void_p, C.c_int64, dp, dp, dp, dp, dp, dp, ip, dp]
+        _lib.oracle_cov_from_records.argtypes = [C.c_void_p, C.c_int64, dp, dp, dp, dp, dp, ip,
+                                                 dp, dp, C.c_int]
+        _lib.oracle_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                              C.POINTER(C.c_uint32)]
+        _lib.oracle_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Rng:
+    """Random source for one oracle call; keeps its tapes alive."""
+
+    def __init__(self, mode=PHILOX, utape=None, ntape=None):
+        self.spec = RngSpec()
+        self.spec.mode = mode
+        self._u = None if utape is None else np.ascontiguousarray(utape, dtype=np.float64)
+        self._n = None if ntape is None else np.ascontiguousarray(ntape, dtype=np.float64)
+        if self._u is not None:
+            self.spec.utape = _dp(self._u)
+            self.spec.un = self._u.size
+        if self._n is not None:
+            self.spec.ntape = _dp(self._n)
+            self.spec.nn = self._n.size
+
+    @classmethod
+    def tape(cls, utape, ntape):
+        return cls(TAPE, utape, ntape)
+
+    @classmethod
+    def philox(cls):
+        return cls(PHILOX)
+
+
+def _check(rc, what):
+    if rc == -1:
+        raise RuntimeError(f"{what}: random tape exhausted")
+    if rc == -3:
+        raise RuntimeError(f"{what}: path exceeded max_events_per_path")
+    if rc != 0:
+        raise RuntimeError(f"{what}: oracle returned {rc}")
+
+
+def field(h: ArgsHolder, rng: Rng) -> np.ndarray:
+    a = h.args
+    u = np.zeros(2 * a.nv * a.nl)
+    _check(lib().oracle_field(C.addressof(a), C.byref(rng.spec), _dp(u)), "oracle_field")
+    return u.view(np.complex128).reshape(a.nv, a.nl, order="F")
+
+
+def cov(h: ArgsHolder, rng: Rng, threads: int = 1):
+    a = h.args
+    n = a.nv * a.nv * a.nl * a.nl
+    Ms = np.zeros(2 * n)
+    Mm = np.zeros(2 * n)
+    _check(lib().oracle_cov(C.addressof(a), C.byref(rng.spec), _dp(Ms), _dp(Mm), threads), "oracle_cov")
+    shp = (a.nv, a.nv, a.nl, a.nl)
+    return (Ms.view(np.complex128).reshape(shp, order="F"),
+            Mm.view(np.complex128).reshape(shp, order="F"))
+
+
+class Records:
+    """Per-event path records (layout of scmc_export_records)."""
+
+    def __init__(self, cap):
+        self.x = np.zeros(3 * cap)
+        self.ow = np.zeros(3 * cap)
+        self.x1 = np.zeros(3 * cap)
+        self.w1 = np.zeros(3 * cap)
+        self.wpx = np.zeros(cap)
+        self.xi = np.zeros(cap)
+        self.plen = np.zeros(cap, dtype=np.int32)
+        self.path = np.zeros(cap, dtype=np.int64)
+        self.n = 0
+
+    def truncate(self, n):
+        self.n = n
+        for k in ("x", "ow", "x1", "w1"):
+            setattr(self, k, getattr(self, k)[: 3 * n].copy())
+        for k in ("wpx", "xi", "plen", "path"):
+            setattr(self, k, getattr(self, k)[:n].copy())
+        return self
+
+    def pointers(self):
+        ip = C.POINTER(C.c_int32)
+        lp = C.POINTER(C.c_int64)
+        return (_dp(self.x), _dp(self.ow), _dp(self.x1), _dp(self.w1), _dp(self.wpx), _dp(self.xi),
+                self.plen.ctypes.data_as(ip), self.path.ctypes.data_as(lp))
+
+
+def records(h: ArgsHolder, rng: Rng, want_phase: bool, capacity: int) -> Records:
+    r = Records(capacity)
+    n = C.c_int64(0)
+    rc = lib().oracle_records(C.addressof(h.args), C.byref(rng.spec), int(want_phase), capacity,
+                              *r.pointers(), C.byref(n))
+    if rc == -2:
+        raise RuntimeError(f"oracle_records: {n.value} events exceed capacity {capacity}")
+    _check(rc, "oracle_records")
+    return r.truncate(n.value)
+
+
+def field_from_records(h: ArgsHolder, r: Records) -> np.ndarray:
+    a = h.args
+    u = np.zeros(2 * a.nv * a.nl)
+    p = r.pointers()
+    lib().oracle_field_from_records(C.addressof(a), r.n, p[0], p[1], p[2], p[3], p[4], p[5], p[6], _dp(u))
+    return u.view(np.complex128).reshape(a.nv, a.nl, order="F")
+
+
+def cov_from_records(h: ArgsHolder, r: Records, threads: int = 1):
+    a = h.args
+    n = a.nv * a.nv * a.nl * a.nl
+    Ms = np.zeros(2 * n)
+    Mm = np.zeros(2 * n)
+    p = r.pointers()
+    lib().oracle_cov_from_records(C.addressof(a), r.n, p[0], p[1], p[2], p[3], p[4], p[6],
+                                  _dp(Ms), _dp(Mm), threads)
+    shp = (a.nv, a.nv, a.nl, a.nl)
+    return (Ms.view(np.complex128).reshape(shp, order="F"),
+            Mm.view(np.complex128).reshape(shp, order="F"))
+
+
+def philox_block(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().oracle_philox4x32_10(c, k, o)
+    return list(o)
+
+
+def philox_stream(seed, path, tag, n):
+    out = np.zeros(n)
+    lib().oracle_philox_stream(seed, path, tag, n, _dp(out))
+    return out

@@ -1,0 +1,68 @@
+/*
+ * scmc_oracle.h - CPU FP64 restatement of SCMC's Monte Carlo path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the oracle the CUDA path is checked
+ * against; nothing in the product links it.  Only tests/, the smoke check
+ * and bench.py's CPU-baseline leg load it.
+ *
+ * Parity pin: tests/golden/ holds outputs of the reference's own .m files
+ * (code/MCfield.m, code/MCcov.m, code/MCfieldFourierQuad.m and the
+ * coreFunctions they call) executed unmodified by a MATLAB-subset
+ * interpreter with rand/randn served from recorded tapes.  In tape mode this
+ * oracle consumes the same tapes in the same order and must reproduce those
+ * outputs; in Philox mode it consumes the per-path counter-based streams the
+ * GPU walk uses.
+ */
+#ifndef SCMC_ORACLE_H
+#define SCMC_ORACLE_H
+
+#include "../include/scmc_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORACLE_RNG_TAPE = 0, ORACLE_RNG_PHILOX = 1 };
+
+typedef struct {
+    int32_t mode;
+    const double *utape; int64_t un;   /* rand() tape (mode TAPE) */
+    const double *ntape; int64_t nn;   /* randn() tape (mode TAPE) */
+    int64_t used_u, used_n;            /* out: draws consumed */
+} oracle_rng_spec;
+
+/* MCfield.m:1-254.  u: 2*nv*nl doubles.  Returns 0, or -1 when a tape ran out. */
+int oracle_field(const scmc_mc_args *a, oracle_rng_spec *rs, double *u);
+
+/* MCcov.m:1-299.  Ms, Mm: 2*nv*nv*nl*nl doubles.  threads<=1: serial. */
+int oracle_cov(const scmc_mc_args *a, oracle_rng_spec *rs, double *Ms, double *Mm, int threads);
+
+/* Walk only, writing records in the layout of scmc_export_records. */
+int oracle_records(const scmc_mc_args *a, oracle_rng_spec *rs, int32_t want_phase,
+                   int64_t capacity, double *x, double *ow, double *x1, double *w1,
+                   double *wpx, double *xi, int32_t *plen, int64_t *path, int64_t *n_events);
+
+/* Accumulate records (from any walk) with MCfield's / MCcov's NEE and update
+ * rules, then normalise by a->norm_itr (or a->max_itr). */
+int oracle_field_from_records(const scmc_mc_args *a, int64_t n, const double *x,
+                              const double *ow, const double *x1, const double *w1,
+                              const double *wpx, const double *xi, const int32_t *plen,
+                              double *u);
+int oracle_cov_from_records(const scmc_mc_args *a, int64_t n, const double *x,
+                            const double *ow, const double *x1, const double *w1,
+                            const double *wpx, const int32_t *plen,
+                            double *Ms, double *Mm, int threads);
+
+/* MCfieldFourierQuad.m:1-304 (isotropic walk, z-plane quadrature, lateral
+ * gridding and a 2-D DFT per plane and light).  u: 2*nv0*nv0*nl doubles. */
+int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double *u);
+
+/* Philox-4x32-10 (Salmon et al., SC'11): one block. */
+void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* The per-path streams (tag 0 uniform, tag 1 normal) of the walk. */
+void oracle_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

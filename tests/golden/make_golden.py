@@ -1,0 +1,271 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference's own .m files (read in place from the reference tree,
+never copied) through the MATLAB-subset interpreter in mlite.py, with
+`rand` / `randn` served from seeded tapes, and stores for every case the
+arguments, the consumed prefix of each tape and the outputs.  The oracle,
+fed the same tapes, must reproduce these outputs (tests/test_oracle_golden.py).
+
+Usage (in a container that has the reference tree):
+    python tests/golden/make_golden.py /path/to/mcspeckle
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import mlite as ml  # noqa: E402
+
+M = ml.M
+TAPE_LEN = 200_000
+
+
+def tapes(seed):
+    g = np.random.default_rng(seed)
+    return g.random(TAPE_LEN), g.standard_normal(TAPE_LEN)
+
+
+def norm_cols(a):
+    a = np.asarray(a, dtype=float)
+    return a / np.linalg.norm(a, axis=0, keepdims=True)
+
+
+def cap_dirs(n, half_deg, zsign, seed):
+    """n directions uniform on the solid-angle cap <= half_deg about zsign*z."""
+    g = np.random.default_rng(seed)
+    c = g.uniform(np.cos(np.deg2rad(half_deg)), 1.0, n)
+    phi = g.uniform(0, 2 * np.pi, n)
+    s = np.sqrt(1 - c * c)
+    return np.stack([s * np.cos(phi), s * np.sin(phi), zsign * c])
+
+
+def to_m(x):
+    if isinstance(x, dict):
+        st = ml.MStruct()
+        for k, v in x.items():
+            st[k] = to_m(v)
+        return st
+    if isinstance(x, str):
+        return ml.MStr(x)
+    if isinstance(x, bool):
+        return M(x)
+    return M(np.asarray(x, dtype=complex if np.iscomplexobj(x) else float))
+
+
+def struct_to_py(st):
+    out = {}
+    for k, v in st.items():
+        if isinstance(v, ml.MStruct):
+            out[k] = struct_to_py(v)
+        elif isinstance(v, ml.MStr):
+            out[k] = str(v)
+        else:
+            out[k] = np.asarray(v)
+    return out
+
+
+class Gen:
+    def __init__(self, ref):
+        self.ref = ref
+        self.path = ml.reference_search_path(ref)
+        self.index = []
+
+    def interp(self, seed):
+        ut, nt = tapes(seed)
+        return ml.Interp(self.path, ut, nt), ut, nt
+
+    def save(self, name, kind, meta, arrays):
+        fn = f"{name}.npz"
+        np.savez_compressed(os.path.join(HERE, fn), meta=json.dumps(meta), **arrays)
+        self.index.append({"name": name, "kind": kind, "file": fn})
+        print(f"  {name}: " + ", ".join(f"{k}{list(np.shape(v))}" for k, v in arrays.items()))
+
+    # -- MCfield / MCcov ------------------------------------------------------
+    def mc_case(self, name, func, seed, *, sigt, albedo, box_min, box_max, l, v, is_ff_l, is_ff_v,
+                max_itr, lam, cbs, smp_flg, sct_type, ampfunc, ampfunc0=None, lmean0=None):
+        it, ut, nt = self.interp(seed)
+        args = [M(float(sigt)), M(float(albedo)), M(np.reshape(box_min, (-1, 1)).astype(float)),
+                M(np.reshape(box_max, (-1, 1)).astype(float)), M(np.asarray(l, float)),
+                M(np.asarray(v, float)), M(bool(is_ff_l)), M(bool(is_ff_v)), M(float(max_itr)),
+                M(float(lam)), M(bool(cbs)), M(float(smp_flg)), M(float(sct_type)), to_m(ampfunc)]
+        if ampfunc0 is not None:
+            args.append(to_m(ampfunc0))
+        if lmean0 is not None:
+            args.append(M(np.reshape(lmean0, (-1, 1)).astype(float)))
+        nout = 1 if func == "MCfield" else 2
+        outs = it.call(func, args, nout)
+        arrays = {"utape": ut[:it.ui], "ntape": nt[:it.ni], "box_min": np.asarray(box_min, float),
+                  "box_max": np.asarray(box_max, float), "l": np.asarray(l, float),
+                  "v": np.asarray(v, float)}
+        meta = {"func": func, "sigt": sigt, "albedo": albedo, "is_ff_l": bool(is_ff_l),
+                "is_ff_v": bool(is_ff_v), "max_itr": max_itr, "lambda": lam, "cbs": bool(cbs),
+                "smp_flg": smp_flg, "sct_type": sct_type, "has_ampfunc0": ampfunc0 is not None,
+                "has_lmean0": lmean0 is not None}
+        self._put_amp(arrays, meta, "ampfunc", ampfunc)
+        if ampfunc0 is not None:
+            self._put_amp(arrays, meta, "ampfunc0", ampfunc0)
+        if lmean0 is not None:
+            arrays["lmean0"] = np.asarray(lmean0, float)
+        if func == "MCfield":
+            arrays["u"] = np.asarray(outs[0], dtype=complex)
+        else:
+            arrays["Ms"] = np.asarray(outs[0], dtype=complex)
+            arrays["Mm"] = np.asarray(outs[1], dtype=complex)
+        self.save(name, func, meta, arrays)
+
+    @staticmethod
+    def _put_amp(arrays, meta, key, amp):
+        if isinstance(amp, dict):
+            meta[key] = "table"
+            arrays[key + "_evalAmp"] = np.asarray(amp["evalAmp"]).reshape(-1).astype(complex)
+            arrays[key + "_sampleIcdf"] = np.asarray(amp["sampleIcdf"], float).reshape(-1)
+        else:
+            meta[key] = float(amp)
+
+    # -- tabulated tables -----------------------------------------------------
+    def table(self, name, theta, f):
+        it, _, _ = self.interp(0)
+        st = it.call("tabulatedAmplitudeScatter", [M(np.asarray(theta, float).reshape(1, -1)),
+                                                   M(np.asarray(f).reshape(1, -1))], 1)[0]
+        py = struct_to_py(st)
+        amp = py["ampfunc"]
+        arrays = {"theta": np.asarray(theta, float).reshape(-1), "f": np.asarray(f).reshape(-1).astype(complex)}
+        for k in ("cs", "samplePdf", "sampleCdf", "sampleIcdf", "evalPdf", "evalAmp"):
+            arrays["out_" + k] = np.asarray(amp[k])
+        meta = {"D": float(np.asarray(py["D"]).reshape(-1)[0]), "albedo": float(np.asarray(py["albedo"]).reshape(-1)[0])}
+        self.save(name, "table", meta, arrays)
+        return {"evalAmp": amp["evalAmp"], "sampleIcdf": amp["sampleIcdf"]}
+
+    # -- scmc.m -----------------------------------------------------------------
+    def scmc_case(self, name, seed, target, views, lights, scatter, iterations, opts):
+        it, ut, nt = self.interp(seed)
+        ta = it.call("boxArea", [M(float(x)) if np.isscalar(x) else M(np.asarray(x, float).reshape(1, -1))
+                                 for x in target], 1)[0]
+        vs = it.call(views[0], [M(np.asarray(a, float)) for a in views[1]], 1)[0]
+        ls = it.call(lights[0], [M(np.asarray(a, float)) for a in lights[1]], 1)[0]
+        sc = it.call(scatter[0], [M(float(a)) for a in scatter[1]], 1)[0]
+        vargs = []
+        for k, val in opts:
+            vargs.append(ml.MStr(k))
+            vargs.append(M(val) if isinstance(val, bool) else M(float(val)))
+        err = None
+        res = {}
+        try:
+            out = it.call("scmc", [ta, vs, ls, sc, M(float(iterations))] + vargs, 1)[0]
+            for k in ("C", "Csingle", "field"):
+                if k in out:
+                    res["out_" + k] = np.asarray(out[k], dtype=complex)
+        except ml.MatlabError as e:
+            err = str(e)
+        arrays = {"utape": ut[:it.ui], "ntape": nt[:it.ni]}
+        arrays.update(res)
+        meta = {"target": [np.asarray(x, float).tolist() for x in target], "views": [views[0], [np.asarray(a, float).tolist() for a in views[1]]],
+                "lights": [lights[0], [np.asarray(a, float).tolist() for a in lights[1]]],
+                "scatter": [scatter[0], list(scatter[1])], "iterations": iterations,
+                "opts": [[k, v] for k, v in opts], "error": err}
+        self.save(name, "scmc", meta, arrays)
+
+    def error_case(self, name, func, args_py, expect_contains=None):
+        it, _, _ = self.interp(0)
+        try:
+            it.call(func, [to_m(a) for a in args_py], 1)
+            msg = None
+        except ml.MatlabError as e:
+            msg = str(e)
+        assert msg is not None, name
+        self.save(name, "error", {"func": func, "error": msg}, {"dummy": np.zeros(1)})
+
+
+def main(ref):
+    g = Gen(ref)
+    print("tables")
+    import scipy.io as sio
+    mat = sio.loadmat(os.path.join(ref, "examples", "buildFarFieldCovMatrix", "scatteringAmplitude.mat"))
+    tab2d = g.table("table_2d_scatteringAmplitude", mat["theta"], mat["farField"])
+    th3 = np.linspace(0, 1, 1001) * np.pi
+    th3[-1] = np.pi
+    it, _, _ = g.interp(0)
+    hg3 = np.sqrt(np.asarray(it.call("evaluateHG", [M(th3.reshape(1, -1)), M(0.7), M(0.0), M(3.0)], 1)[0]))
+    tab3d = g.table("table_3d_hg07", th3, hg3)
+
+    box3 = dict(box_min=[-20, -20, 0], box_max=[20, 20, 15])
+    box2 = dict(box_min=[-20, 0], box_max=[20, 15])
+    L3 = cap_dirs(3, 10, +1, 11)
+    V3r = cap_dirs(4, 10, -1, 12)   # reflection
+    V3t = cap_dirs(4, 10, +1, 13)   # transmission
+    NFv = np.array([[-5.0, 0.0, 6.0, 2.0], [1.0, -3.0, 2.0, 0.5], [-30.0, -30.0, -28.0, 40.0]])
+    NFl = np.array([[0.0, 4.0, -6.0], [2.0, -1.0, 3.0], [-35.0, -40.0, -30.0]])
+
+    print("MCfield / MCcov")
+    common = dict(sigt=0.2, albedo=0.9, lam=1.0, max_itr=40)
+    for func in ("MCfield", "MCcov"):
+        tag = "field" if func == "MCfield" else "cov"
+        g.mc_case(f"{tag}_3d_iso_ff_refl_cbs_exp", func, 101, **common, **box3, l=L3, v=V3r, is_ff_l=1, is_ff_v=1,
+                  cbs=1, smp_flg=2, sct_type=1, ampfunc=0)
+        g.mc_case(f"{tag}_3d_hg_ff_trans_nocbs_unif", func, 102, **common, **box3, l=L3, v=V3t, is_ff_l=1, is_ff_v=1,
+                  cbs=0, smp_flg=1, sct_type=3, ampfunc=0.8)
+        g.mc_case(f"{tag}_3d_hg_nfv_cbs_exp_g0", func, 103, **common, **box3, l=L3, v=NFv, is_ff_l=1, is_ff_v=0,
+                  cbs=1, smp_flg=2, sct_type=3, ampfunc=0.6, ampfunc0=0.3)
+        g.mc_case(f"{tag}_3d_tab_nfl_nfv_cbs_exp", func, 104, **common, **box3, l=NFl, v=NFv, is_ff_l=0, is_ff_v=0,
+                  cbs=1, smp_flg=2, sct_type=2, ampfunc=tab3d)
+        g.mc_case(f"{tag}_3d_tab_ff_refl_cbs_unif_t0", func, 105, **common, **box3, l=L3, v=V3r, is_ff_l=1, is_ff_v=1,
+                  cbs=1, smp_flg=1, sct_type=2, ampfunc=tab3d, ampfunc0=tab3d)
+        g.mc_case(f"{tag}_3d_iso_lowalbedo_roulette", func, 106, sigt=0.3, albedo=0.5, lam=0.7, max_itr=25, **box3,
+                  l=L3, v=V3r, is_ff_l=1, is_ff_v=1, cbs=1, smp_flg=2, sct_type=1, ampfunc=0)
+        g.mc_case(f"{tag}_2d_iso_angles_cbs_exp", func, 107, **common, **box2,
+                  l=np.deg2rad([[0.0, 3.0, -4.0]]), v=np.deg2rad([[180.0, 170.0, 185.0, 200.0]]),
+                  is_ff_l=1, is_ff_v=1, cbs=1, smp_flg=2, sct_type=1, ampfunc=0)
+        g.mc_case(f"{tag}_2d_hg_vectors_nocbs_unif", func, 108, **common, **box2,
+                  l=norm_cols([[0.1, -0.2], [1.0, 1.0]]), v=norm_cols([[0.0, 0.3, -0.1], [1.0, 1.0, 1.0]]),
+                  is_ff_l=1, is_ff_v=1, cbs=0, smp_flg=1, sct_type=3, ampfunc=-0.4)
+        g.mc_case(f"{tag}_2d_tab_measured_cbs_exp", func, 109, **common, **box2,
+                  l=np.deg2rad([[0.0, 20.0]]), v=np.deg2rad([[0.0, 90.0, 180.0, 270.0]]),
+                  is_ff_l=1, is_ff_v=1, cbs=1, smp_flg=2, sct_type=2, ampfunc=tab2d)
+    g.mc_case("field_3d_hg_lmean0", "MCfield", 110, **common, **box3, l=L3, v=V3r, is_ff_l=1, is_ff_v=1,
+              cbs=1, smp_flg=2, sct_type=3, ampfunc=0.5, ampfunc0=0.2, lmean0=[0.1, 0.0, 1.0])
+
+    print("scmc.m")
+    tgt3 = [1.0, 5.0, [0, 15], [-20, 20], [-20, 20]]
+    g.scmc_case("scmc_cov_default_hg", 201, tgt3, ("farFieldSource", [V3r]), ("farFieldSource", [L3]),
+                ("HGScatter", [0.7]), 8, [])
+    g.scmc_case("scmc_cov_single_field_nocbs", 202, tgt3, ("farFieldSource", [V3t]), ("farFieldSource", [L3]),
+                ("isotropicScatter", [0.9]), 8,
+                [("CBS", False), ("singleScattering", True), ("renderField", True), ("uniformFirstScatter", True)])
+    g.scmc_case("scmc_field_only_g0", 203, tgt3, ("farFieldSource", [V3r]), ("farFieldSource", [L3]),
+                ("HGScatter", [0.6, 0.3, 0.95]), 10, [("renderCov", False), ("renderField", True)])
+    g.scmc_case("scmc_parfor_cov_field", 204, tgt3, ("farFieldSource", [V3r]), ("farFieldSource", [L3]),
+                ("HGScatter", [0.5]), 5, [("parforIters", 3), ("renderField", True)])
+    g.scmc_case("scmc_angles_2d", 205, [1.0, 5.0, [0, 15], [-20, 20]],
+                ("farFieldSource", [np.deg2rad([180.0, 175.0]), [0.0]]), ("farFieldSource", [np.deg2rad([0.0, 2.0]), [0.0]]),
+                ("isotropicScatter", []), 6, [])
+    g.scmc_case("scmc_nearfield_views", 206, tgt3, ("nearFieldSource", [NFv]), ("farFieldSource", [L3]),
+                ("HGScatter", [0.4]), 6, [("renderField", True)])
+    g.scmc_case("scmc_err_option", 207, tgt3, ("farFieldSource", [V3r]), ("farFieldSource", [L3]),
+                ("HGScatter", [0.4]), 6, [("mean", False)])
+    g.scmc_case("scmc_err_rng_parfor", 208, tgt3, ("farFieldSource", [V3r]), ("farFieldSource", [L3]),
+                ("HGScatter", [0.4]), 6, [("rng", 5), ("parforIters", 2)])
+    g.scmc_case("scmc_err_cbs_type", 209, tgt3, ("farFieldSource", [V3r]), ("farFieldSource", [L3]),
+                ("HGScatter", [0.4]), 6, [("CBS", 1)])
+
+    print("errors")
+    g.error_case("err_field_box", "MCfield", [0.1, 1.0, np.zeros((3, 2)), np.ones((3, 2)), L3, V3r, True, True,
+                                             2.0, 1.0, True, 2.0, 1.0, 0.0])
+    g.error_case("err_field_light", "MCfield", [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3[:2], V3r, True, True,
+                                               2.0, 1.0, True, 2.0, 1.0, 0.0])
+    g.error_case("err_cov_view", "MCcov", [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3, V3r[:1], True, True,
+                                          2.0, 1.0, True, 2.0, 1.0, 0.0])
+    g.error_case("err_field_nargs", "MCfield", [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3, V3r, True, True,
+                                               2.0, 1.0, True, 2.0, 1.0])
+
+    with open(os.path.join(HERE, "index.json"), "w") as f:
+        json.dump(g.index, f, indent=1)
+    print(f"{len(g.index)} fixtures")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,178 @@
+"""The CPU oracle and the host mirror against the reference itself.
+
+Fixtures in tests/golden/ hold outputs of the reference's own .m files
+(MCfield.m, MCcov.m, scmc.m, tabulatedAmplitudeScatter.m, ...) executed by
+tests/golden/mlite.py with recorded random tapes (tests/golden/make_golden.py).
+Fed the same tapes, the oracle must reproduce them to rounding, and must
+consume exactly as many draws as the reference did.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from mcspeckle_b200 import interface as I
+from mcspeckle_b200 import mc as MC
+from mcspeckle_b200 import scmc_api as S
+
+RTOL = 1e-9
+
+with open(os.path.join(GOLDEN, "index.json")) as f:
+    INDEX = json.load(f)
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False)
+    meta = json.loads(str(z["meta"]))
+    return meta, {k: z[k] for k in z.files if k != "meta"}
+
+
+def relerr(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def amp(meta, arr, key):
+    if meta[key] == "table":
+        return {"evalAmp": arr[key + "_evalAmp"], "sampleIcdf": arr[key + "_sampleIcdf"]}
+    return meta[key]
+
+
+def mc_case_args(meta, arr):
+    args = [meta["sigt"], meta["albedo"], arr["box_min"], arr["box_max"], arr["l"], arr["v"], meta["is_ff_l"],
+            meta["is_ff_v"], meta["max_itr"], meta["lambda"], meta["cbs"], meta["smp_flg"], meta["sct_type"],
+            amp(meta, arr, "ampfunc")]
+    if meta["has_ampfunc0"]:
+        args.append(amp(meta, arr, "ampfunc0"))
+    if meta["has_lmean0"]:
+        if not meta["has_ampfunc0"]:
+            args.append(MC._MISSING)
+        args.append(arr["lmean0"])
+    return args
+
+
+MC_CASES = [e["name"] for e in INDEX if e["kind"] in ("MCfield", "MCcov")]
+TABLE_CASES = [e["name"] for e in INDEX if e["kind"] == "table"]
+SCMC_CASES = [e["name"] for e in INDEX if e["kind"] == "scmc"]
+
+
+def test_fixture_inventory():
+    kinds = {e["kind"] for e in INDEX}
+    assert {"MCfield", "MCcov", "table", "scmc", "error"} <= kinds
+    assert len(MC_CASES) >= 18
+
+
+@pytest.mark.parametrize("name", MC_CASES)
+def test_oracle_matches_reference(oracle_lib, name):
+    O = oracle_lib
+    meta, arr = load(name)
+    h = MC.mc_args(*mc_case_args(meta, arr), seed=0, precision="fp64")
+    rng = O.Rng.tape(arr["utape"], arr["ntape"])
+    if meta["func"] == "MCfield":
+        u = O.field(h, rng)
+        assert u.shape == arr["u"].shape
+        assert relerr(u, arr["u"]) < RTOL
+    else:
+        Ms, Mm = O.cov(h, rng)
+        assert Ms.shape == arr["Ms"].shape
+        assert relerr(Ms, arr["Ms"]) < RTOL
+        assert relerr(Mm, arr["Mm"]) < RTOL
+    # the same number of rand / randn draws as the reference consumed
+    assert rng.spec.used_u == arr["utape"].size
+    assert rng.spec.used_n == arr["ntape"].size
+
+
+@pytest.mark.parametrize("name", TABLE_CASES)
+def test_tabulated_table_matches_reference(name):
+    meta, arr = load(name)
+    s = I.tabulatedAmplitudeScatter(arr["theta"], arr["f"])
+    assert s["D"] == meta["D"]
+    a = s["ampfunc"]
+    for k in ("cs", "samplePdf", "sampleCdf", "sampleIcdf", "evalPdf", "evalAmp"):
+        ref = np.asarray(arr["out_" + k]).reshape(-1)
+        got = np.asarray(a[k]).reshape(-1)
+        assert got.shape == ref.shape, k
+        assert relerr(got, ref) < 1e-12, k
+
+
+class TapeKernels:
+    """MCcov / MCfield on the oracle with a continuing pair of tapes, the way
+    successive calls share MATLAB's global stream."""
+
+    def __init__(self, O, ut, nt):
+        self.O, self.ut, self.nt = O, ut, nt
+        self.pu = self.pn = 0
+
+    def _run(self, fn, args, n_total):
+        h = MC.mc_args(*args, seed=0, norm_itr=n_total, precision="fp64")
+        r = self.O.Rng.tape(self.ut[self.pu:], self.nt[self.pn:])
+        out = fn(h, r)
+        self.pu += r.spec.used_u
+        self.pn += r.spec.used_n
+        return out
+
+    def MCcov(self, *args, seed, n_total):
+        return self._run(self.O.cov, args, n_total)
+
+    def MCfield(self, *args, seed, n_total):
+        return self._run(self.O.field, args, n_total)
+
+
+def make_struct(kind, args):
+    return getattr(I, kind)(*[np.asarray(a) if isinstance(a, list) else a for a in args])
+
+
+@pytest.mark.parametrize("name", SCMC_CASES)
+def test_scmc_dispatch_matches_reference(oracle_lib, name):
+    meta, arr = load(name)
+    t = meta["target"]
+    ta = I.boxArea(*[x[0] if isinstance(x, list) and len(x) == 1 else np.asarray(x) for x in t])
+    views = make_struct(*meta["views"])
+    lights = make_struct(*meta["lights"])
+    sc = make_struct(*meta["scatter"])
+    opts = []
+    for k, v in meta["opts"]:
+        opts += [k, v]
+    if meta["error"] is not None:
+        with pytest.raises(S.ScmcInputError) as ei:
+            S.build_config(ta, views, lights, sc, meta["iterations"], *opts)
+        assert str(ei.value) == meta["error"]
+        return
+    cfg = S.build_config(ta, views, lights, sc, meta["iterations"], *opts)
+    ker = TapeKernels(oracle_lib, arr["utape"], arr["ntape"])
+    res = S.run_config(cfg, ker)
+    for k in ("C", "Csingle", "field"):
+        if "out_" + k in arr:
+            assert k in res, k
+            assert relerr(res[k], arr["out_" + k]) < RTOL, k
+        else:
+            assert k not in res, k
+    assert ker.pu == arr["utape"].size and ker.pn == arr["ntape"].size
+
+
+def test_argument_errors_match_reference():
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_golden as G
+    L3 = G.cap_dirs(3, 10, +1, 11)
+    V3r = G.cap_dirs(4, 10, -1, 12)
+    cases = {
+        "err_field_box": (MC.MCfield, [0.1, 1.0, np.zeros((3, 2)), np.ones((3, 2)), L3, V3r, True, True,
+                                       2.0, 1.0, True, 2.0, 1.0, 0.0]),
+        "err_field_light": (MC.MCfield, [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3[:2], V3r, True, True,
+                                         2.0, 1.0, True, 2.0, 1.0, 0.0]),
+        "err_cov_view": (MC.MCcov, [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3, V3r[:1], True, True,
+                                    2.0, 1.0, True, 2.0, 1.0, 0.0]),
+    }
+    for name, (fn, args) in cases.items():
+        meta, _ = load(name)
+        with pytest.raises(MC.MatlabStyleError) as ei:
+            fn(*args)
+        assert str(ei.value) == meta["error"], name
+    meta, _ = load("err_field_nargs")
+    assert meta["error"] == "Not enough input arguments."
+    with pytest.raises(TypeError):
+        MC.MCfield(0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3, V3r, True, True, 2.0, 1.0, True, 2.0, 1.0)
