@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of SCMC's Monte Carlo covariance path on B200.
+
+Workload: the far-field covariance configuration - MCcov on a homogeneous box
+20 x 20 x 5 MFP (MFP = 10 wavelengths, wavelength 1), Henyey-Greenstein g=0.8,
+sigma_s = 1, sigma_a = 0.01 per MFP, 64 lights and 64 views on regular 8 x 8
+(sin theta_x, sin theta_y) grids spanning +-5 degrees about +z / -z
+(reflection, CBS on, exponential first-scatter sampling), 1e7 paths per GPU
+per step, full 64x64x64x64 complex covariance.  Synthetic: every input is
+generated from fixed seeds; each step walks a fresh Philox path range.
+
+One step = one MCcov solve of --paths paths on every GPU (mixed precision:
+tcgen05 FP16 hi+lo contraction, FP64 cross-chunk sums), plus for N>1 an
+NCCL sum of the partial Ms / Mm.  `value` = paths of all ranks / the max over
+ranks of the CUDA-event time of the K timed steps, outputs in HBM.  `e2e` =
+the same through the host-buffer C ABI call (scmc_cov: inputs from host,
+Ms / Mm copied back to host every step).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC paths/s at 1e-3 rel err vs FP64 (mixed vs FP32 GPU); p50/p99 request latency"
+UNIT = "paths/s"
+WORKLOAD = "MCcov far-field covariance, 64 lights x 64 views (8x8 grids, +-5 deg), HG g=0.8, box 20x20x5 MFP"
+
+
+def grid_dirs(n_side, half_deg, zsign):
+    s = math.sin(math.radians(half_deg))
+    g = np.linspace(-s, s, n_side)
+    sx, sy = np.meshgrid(g, g, indexing="ij")
+    sx, sy = sx.reshape(-1), sy.reshape(-1)
+    return np.stack([sx, sy, zsign * np.sqrt(1 - sx * sx - sy * sy)])
+
+
+def workload_args(n_paths):
+    mfp = 10.0
+    sigt = 1.01 / mfp          # sigma_s + sigma_a = (1 + 0.01) / MFP
+    albedo = 1.0 / 1.01
+    box_min = np.array([-100.0, -100.0, 0.0])
+    box_max = np.array([100.0, 100.0, 50.0])
+    l = grid_dirs(8, 5.0, +1.0)
+    v = grid_dirs(8, 5.0, -1.0)
+    return [sigt, albedo, box_min, box_max, l, v, 1, 1, int(n_paths), 1.0, True, 2, 3, 0.8]
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_oracle_rate(args_fn, target_s=15.0, threads=None):
+    """The FP64 oracle (C restatement of MCcov) on the host cores: paths/s on a
+    bounded sample of the same workload."""
+    from mcspeckle_b200 import mc as MC
+    from oracle import oracle as O
+    O.build()
+    threads = threads or os.cpu_count() or 1
+    n = 2
+    while True:
+        h = MC.mc_args(*args_fn(n), seed=99, precision="fp64")
+        t0 = time.perf_counter()
+        O.cov(h, O.Rng.philox(), threads=threads)
+        dt = time.perf_counter() - t0
+        if dt >= target_s or n >= 4096:
+            return n / dt, n, dt, threads
+        n = max(n + 1, int(n * min(8.0, 1.3 * target_s / max(dt, 1e-3))))
+
+
+def run_reference(a):
+    """--impl reference: the CPU oracle port of the reference's MCcov timed on
+    the host cores (MATLAB / Octave are not available on this box)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    per_step = []
+    sample = None
+    for i in range(a.warmup + a.steps):
+        rate, n, dt, thr = cpu_oracle_rate(workload_args, target_s=a.ref_seconds)
+        if i >= a.warmup:
+            per_step.append((rate, n, dt))
+        sample = (n, thr)
+    value = float(np.median([r for r, _, _ in per_step]))
+    ms = 1000.0 * float(np.mean([n / r for r, n, _ in per_step]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "paths_per_step": sample[0], "full_config_paths": 10_000_000},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": sample[1], "kind": "port",
+                         "sample": f"{sample[0]} paths of the workload per step (oracle/scmc_oracle.c MCcov, FP64, "
+                                   f"{sample[1]} threads; MATLAB/Octave absent on this box)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--paths", type=float, default=1e7, help="paths per GPU per step")
+    ap.add_argument("--accuracy-paths", type=float, default=1e5)
+    ap.add_argument("--fp32-paths", type=float, default=1e5)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.impl == "reference":
+        return run_reference(a)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from mcspeckle_b200 import _lib
+    from mcspeckle_b200 import mc as MC
+
+    P = int(a.paths)
+    N = 64 * 64
+    n_out = N * N
+    stream = torch.cuda.current_stream()
+    Ms = torch.zeros(2 * n_out, dtype=torch.float64, device="cuda")
+    Mm = torch.zeros(2 * n_out, dtype=torch.float64, device="cuda")
+    seed = 0x5C3C0FFEE
+
+    def step_args(step, n=P, precision="mixed"):
+        off = (step * world + rank) * n
+        return MC.mc_args(*workload_args(n), seed=seed, precision=precision, device=local, path_offset=off,
+                          norm_itr=n * world)
+
+    def device_step(step):
+        h = step_args(step)
+        _lib.check(_lib.lib().scmc_cov_device(h.ref, Ms.data_ptr(), Mm.data_ptr(), stream.cuda_stream))
+        if world > 1:
+            dist.all_reduce(Ms)
+            dist.all_reduce(Mm)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for s in range(a.warmup):
+        device_step(s)
+    barrier()
+
+    # timed region (device-resident outputs)
+    clocks = ClockSampler(local)
+    clocks.start()
+    _lib.profile_read(reset=True)
+    _lib.profile_enable(True)
+    l0 = _lib.launch_count()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for s in range(a.steps):
+        device_step(a.warmup + s)
+    e1.record(stream)
+    barrier()
+    ms_total = e0.elapsed_time(e1)
+    launches = _lib.launch_count() - l0
+    _lib.profile_enable(False)
+    prof = _lib.profile_read(reset=True)
+    clk = clocks.stop()
+    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = P * world * a.steps / (ms_max / 1000.0)
+
+    # e2e: the host-buffer C ABI call, outputs copied to pinned host memory
+    host_Ms = torch.empty(2 * n_out, dtype=torch.float64, pin_memory=True)
+    host_Mm = torch.empty(2 * n_out, dtype=torch.float64, pin_memory=True)
+    h_in = step_args(0)
+    h2d = int(h_in.args.nl * 3 * 8 + h_in.args.nv * 3 * 8)
+    barrier()
+    t0 = time.perf_counter()
+    for s in range(a.steps):
+        h = step_args(a.warmup + a.steps + s)
+        if world == 1:
+            dp = ctypes.POINTER(ctypes.c_double)
+            _lib.check(_lib.lib().scmc_cov(h.ref, ctypes.cast(host_Ms.data_ptr(), dp),
+                                           ctypes.cast(host_Mm.data_ptr(), dp)))
+        else:
+            _lib.check(_lib.lib().scmc_cov_device(h.ref, Ms.data_ptr(), Mm.data_ptr(), stream.cuda_stream))
+            dist.all_reduce(Ms)
+            dist.all_reduce(Mm)
+            host_Ms.copy_(Ms, non_blocking=True)
+            host_Mm.copy_(Mm, non_blocking=True)
+            torch.cuda.synchronize()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = P * world * a.steps / float(t.item())
+
+    line = None
+    if rank == 0:
+        peaks, peak_kind = load_peaks()
+        peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+        per_launch_ms = prof["contract_ms"] / max(prof["contract_launches"], 1)
+        flops_per_launch = prof["contract_flops"] / max(prof["contract_launches"], 1)
+        achieved = flops_per_launch / (per_launch_ms / 1000.0) / 1e12
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "herk_tc_traffic.json")
+        if os.path.exists(tf):
+            with open(tf) as f:
+                tj = json.load(f)
+            # bytes per event measured by ncu, scaled to this run's events per launch
+            ev_per_launch = flops_per_launch / (4.0 * N * (N + 1))
+            traffic = tj["dram_bytes_per_event"] * ev_per_launch
+        # accuracy on regenerated paths: mixed and plain FP32 against FP64
+        na = int(a.accuracy_paths)
+        ha = MC.mc_args(*workload_args(na), seed=seed, precision="fp64", device=local)
+        M64 = MC.cov_from_args(ha)
+        Mmx = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision="mixed", device=local))
+        t32 = time.perf_counter()
+        M32 = MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision="fp32",
+                                          device=local))
+        fp32_s = time.perf_counter() - t32
+        if int(a.fp32_paths) != na:
+            M32 = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision="fp32", device=local))
+        C64 = M64[0] + M64[1]
+
+        def rel(x, y):
+            return float(np.linalg.norm((x - y).ravel()) / np.linalg.norm(y.ravel()))
+
+        err_mixed = rel(Mmx[0] + Mmx[1], C64)
+        err_fp32 = rel(M32[0] + M32[1], C64)
+        tmx = time.perf_counter()
+        MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision="mixed", device=local))
+        mixed_small_s = time.perf_counter() - tmx
+        cpu = None
+        if not a.no_cpu_baseline:
+            rate, n, dt, thr = cpu_oracle_rate(workload_args, target_s=a.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
+                   "sample": f"{n} paths of the workload in {dt:.1f} s (oracle MCcov, FP64, {thr} threads)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16x2+f32acc (phases f64-reduced f32, sums f64)", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "paths_per_gpu_per_step": P, "lights": 64, "views": 64,
+                       "output": "Ms, Mm: 64x64x64x64 complex f64", "precision": "mixed",
+                       "parallelism": f"path-range shards x{world}" + (" + NCCL sum" if world > 1 else ""),
+                       "l2": "working set > L2 (1 GiB operand per chunk, 2 x 268 MB accumulators)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": int(2 * n_out * 2 * 8)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "herk_tc_kernel", "peak_source": f"bf16_tflops_sustained ({peak_kind})",
+                         "flops_per_launch": flops_per_launch, "ms_per_launch": per_launch_ms,
+                         "launches": prof["contract_launches"]},
+            "stages_ms": {"walk": prof["walk_ms"], "rows": prof["rows_ms"], "contract": prof["contract_ms"],
+                          "finalize": prof["finalize_ms"]},
+            "accuracy": {"paths": na, "rel_err_mixed_vs_fp64": err_mixed, "rel_err_fp32_vs_fp64": err_fp32,
+                         "tol": 1e-3, "norm": "Frobenius of C = Ms + Mm"},
+            "fp32_gpu": {"paths": int(a.fp32_paths), "value": int(a.fp32_paths) / fp32_s,
+                         "mixed_same_sample": int(a.fp32_paths) / mixed_small_s,
+                         "speedup_mixed_over_fp32": (int(a.fp32_paths) / mixed_small_s) / (int(a.fp32_paths) / fp32_s)},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

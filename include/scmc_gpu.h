@@ -163,6 +163,29 @@ int scmc_export_records(const scmc_mc_args *args, int32_t want_phase, int64_t ca
  * Host memory.  Exposed so the random streams can be checked bit for bit. */
 int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, double *out);
 
+/* ---------------------------------------------------------------------------
+ * Stage timing.  While enabled, every kernel launch of the walk, the row
+ * generation, the contraction and the finalisation is bracketed by CUDA
+ * events on the stream it runs on; scmc_profile_read resolves them.  The
+ * reference has only tic/toc in its scripts; this is the per-stage form.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    int64_t walk_launches;
+    double walk_ms;
+    int64_t rows_launches;      /* NEE vectors + rows / field accumulation */
+    double rows_ms;
+    int64_t contract_launches;  /* Hermitian rank-k updates (tensor / CUDA cores) */
+    double contract_ms;
+    int64_t finalize_launches;
+    double finalize_ms;
+    int64_t paths;              /* paths walked */
+    int64_t events;             /* scattering events (single + multiple) */
+    double contract_flops;      /* algorithmic: 4*N*(N+1) per event, N = nv*nl */
+} scmc_stage_times;
+
+int scmc_profile_enable(int32_t on);
+int scmc_profile_read(scmc_stage_times *out, int32_t reset);
+
 /* Library information and error reporting. */
 int scmc_abi_version(void);
 const char *scmc_last_error(void);

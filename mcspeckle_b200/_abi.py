@@ -92,6 +92,25 @@ class FqArgs(C.Structure):
     ]
 
 
+class StageTimes(C.Structure):
+    _fields_ = [
+        ("walk_launches", C.c_int64),
+        ("walk_ms", C.c_double),
+        ("rows_launches", C.c_int64),
+        ("rows_ms", C.c_double),
+        ("contract_launches", C.c_int64),
+        ("contract_ms", C.c_double),
+        ("finalize_launches", C.c_int64),
+        ("finalize_ms", C.c_double),
+        ("paths", C.c_int64),
+        ("events", C.c_int64),
+        ("contract_flops", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
 

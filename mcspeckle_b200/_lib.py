@@ -59,8 +59,10 @@ def lib():
         L.scmc_cov_device.argtypes = [mp, C.c_void_p, C.c_void_p, C.c_void_p]
         L.scmc_export_records.argtypes = [mp, C.c_int32, C.c_int64, dp, dp, dp, dp, dp, dp, ip, lp, lp]
         L.scmc_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
+        L.scmc_profile_enable.argtypes = [C.c_int32]
+        L.scmc_profile_read.argtypes = [C.POINTER(_abi.StageTimes), C.c_int32]
         for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",
-                     "scmc_export_records", "scmc_philox_stream"):
+                     "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read"):
             getattr(L, name).restype = C.c_int
         _lib = L
         return _lib
@@ -74,3 +76,13 @@ def check(status: int) -> None:
 
 def launch_count() -> int:
     return int(lib().scmc_launch_count())
+
+
+def profile_enable(on: bool = True) -> None:
+    check(lib().scmc_profile_enable(int(on)))
+
+
+def profile_read(reset: bool = True) -> dict:
+    t = _abi.StageTimes()
+    check(lib().scmc_profile_read(C.byref(t), int(reset)))
+    return t.as_dict()

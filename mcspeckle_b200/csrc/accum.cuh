@@ -341,6 +341,7 @@ __global__ void cov_finalize_kernel(const A *__restrict__ Cacc, int layout, int 
             im = (double)Cacc[(2 * a + 1) * N + b];
         }
         if (flip) im = -im;
+        if (i1 == i2) im = 0.0;  // sum of |t_i|^2: real, as the reference's products give
         out[q] = make_double2(scale * re, scale * im);
     }
 }

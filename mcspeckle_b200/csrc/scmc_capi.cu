@@ -44,6 +44,84 @@ void cuda_check(cudaError_t e, const char *what)
 #define CK(x) cuda_check((x), #x)
 #define LAUNCHED() (g_launches.fetch_add(1, std::memory_order_relaxed))
 
+// ---------------------------------------------------------------------------
+// stage timing (scmc_profile_*)
+// ---------------------------------------------------------------------------
+enum Stage { ST_WALK = 0, ST_ROWS = 1, ST_CONTRACT = 2, ST_FINAL = 3 };
+
+struct Profiler {
+    std::mutex mu;
+    std::atomic<bool> on{false};
+    struct Pending {
+        cudaEvent_t a, b;
+        int stage;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    int64_t launches[4] = {0, 0, 0, 0};
+    double ms[4] = {0, 0, 0, 0};
+    int64_t paths = 0, events = 0;
+    double flops = 0;
+
+    cudaEvent_t take()
+    {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        return e;
+    }
+    void resolve_locked()
+    {
+        for (auto &p : pending) {
+            CK(cudaEventSynchronize(p.b));
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, p.a, p.b));
+            ms[p.stage] += t;
+            launches[p.stage] += 1;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+};
+Profiler g_prof;
+
+// Brackets the launches made in its scope with CUDA events when enabled.
+struct StageScope {
+    int stage;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    StageScope(int s, cudaStream_t stream) : stage(s), st(stream)
+    {
+        if (!g_prof.on.load(std::memory_order_relaxed)) return;
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        if (g_prof.pending.size() > 8192) g_prof.resolve_locked();
+        a = g_prof.take();
+        CK(cudaEventRecord(a, st));
+    }
+    ~StageScope() noexcept(false)
+    {
+        if (!a) return;
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        cudaEvent_t b = g_prof.take();
+        CK(cudaEventRecord(b, st));
+        g_prof.pending.push_back({a, b, stage});
+    }
+};
+
+void prof_count(int64_t paths, int64_t events, double flops)
+{
+    if (!g_prof.on.load(std::memory_order_relaxed)) return;
+    std::lock_guard<std::mutex> lk(g_prof.mu);
+    g_prof.paths += paths;
+    g_prof.events += events;
+    g_prof.flops += flops;
+}
+
 template <typename F>
 int guarded(F &&f)
 {
@@ -92,7 +170,7 @@ struct Ctx {
     DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
-    DevBuf acc_s, acc_m, rows, tiles, tc_a, tc_scratch;
+    DevBuf acc_s, acc_m, rows, tiles, tc_a, out0, out1;
     int64_t scap = 0, mcap = 0;
 };
 
@@ -293,9 +371,12 @@ void walk_batch_dim(Ctx &c, WalkParams W, int64_t n_paths, cudaStream_t st, Batc
     unsigned long long *ctr = c.ctr.as<unsigned long long>();
     CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(c.err.p, 0, sizeof(int), st));
-    walk_count_kernel<DIM><<<grid, threads, 0, st>>>(W, c.counts.as<int32_t>(), ctr, c.err.as<int>());
-    CK(cudaGetLastError());
-    LAUNCHED();
+    {
+        StageScope sc(ST_WALK, st);
+        walk_count_kernel<DIM><<<grid, threads, 0, st>>>(W, c.counts.as<int32_t>(), ctr, c.err.as<int>());
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
     count_to_multi_kernel<<<std::max(1, std::min(sms * 4, (int)((n_paths + 255) / 256))), 256, 0, st>>>(
         c.counts.as<int32_t>(), n_paths, c.mcnt.as<int64_t>());
     CK(cudaGetLastError());
@@ -341,9 +422,13 @@ void walk_batch_dim(Ctx &c, WalkParams W, int64_t n_paths, cudaStream_t st, Batc
     B.n_paths = n_paths;
     B.n_multi = n_multi;
     CK(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), st));
-    walk_record_kernel<DIM><<<grid, threads, 0, st>>>(W, c.moff.as<int64_t>(), B.S, c.scap, B.M, c.mcap, ctr + 1);
-    CK(cudaGetLastError());
-    LAUNCHED();
+    {
+        StageScope sc(ST_WALK, st);
+        walk_record_kernel<DIM><<<grid, threads, 0, st>>>(W, c.moff.as<int64_t>(), B.S, c.scap, B.M, c.mcap, ctr + 1);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+    prof_count(n_paths, n_paths + n_multi, 0.0);
 }
 
 void walk_batch(Ctx &c, const WalkParams &W, int64_t n_paths, cudaStream_t st, Batch &B)
@@ -378,6 +463,7 @@ void launch_field_accum(Ctx &c, const Prepared &P, const Batch &B, AccT *U, int6
     auto kern = field_accum_kernel<DIM, POL, SINGLE, AccT>;
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid(tiles, (unsigned)ranges);
+    StageScope sc(ST_ROWS, st);
     kern<<<grid, kFieldThreads, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, n_ev, tv, tl, n_vtiles, per, U,
                                             P.W.want_phase);
     CK(cudaGetLastError());
@@ -405,16 +491,14 @@ void field_run(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u, c
     double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
     double norm = m > 0 ? std::sqrt(1.0 / m * P.volume * a->sigt) : 0.0;  // MCfield.m:253-254
     int grid = (int)std::min<int64_t>((n + 255) / 256, 1024);
+    StageScope sc(ST_FINAL, st);
     field_finalize_kernel<DIM, AccT><<<std::max(grid, 1), 256, 0, st>>>(P.Q, Us, Um, norm, d_u);
     CK(cudaGetLastError());
     LAUNCHED();
 }
 
-void field_device(const scmc_mc_args *a, double *d_u, cudaStream_t st)
+void field_device_locked(Ctx &c, const scmc_mc_args *a, double *d_u, cudaStream_t st)
 {
-    validate(a);
-    Ctx &c = context(a->device);
-    std::lock_guard<std::mutex> lk(c.mu);
     CK(cudaSetDevice(a->device));
     Prepared P = prepare(c, a, 1, st);
     double2 *u = reinterpret_cast<double2 *>(d_u);
@@ -454,6 +538,7 @@ void cov_rows(Ctx &c, const Prepared &P, const Batch &B, int64_t e0, int64_t n, 
     auto kern = cov_rows_kernel<DIM, POL, SINGLE>;
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = (int)((n + eb - 1) / eb);
+    StageScope sc(ST_ROWS, st);
     kern<<<grid, 256, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, e0, n, eb, reinterpret_cast<C *>(T));
     CK(cudaGetLastError());
     LAUNCHED();
@@ -467,11 +552,15 @@ void herk_cc(Ctx &c, const void *T, int64_t n, int N, void *Cacc, cudaStream_t s
     std::vector<int2> tl = upper_tiles(N, 16 * RPT);
     c.tiles.ensure(tl.size() * sizeof(int2));
     CK(cudaMemcpyAsync(c.tiles.p, tl.data(), tl.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-    herk_cc_kernel<R, A, RPT, BK><<<(unsigned)tl.size(), 256, 0, st>>>(
-        reinterpret_cast<const typename cplx_t<R>::type *>(T), n, N, c.tiles.as<int2>(),
-        reinterpret_cast<typename cplx_t<A>::type *>(Cacc));
-    CK(cudaGetLastError());
-    LAUNCHED();
+    {
+        StageScope sc(ST_CONTRACT, st);
+        herk_cc_kernel<R, A, RPT, BK><<<(unsigned)tl.size(), 256, 0, st>>>(
+            reinterpret_cast<const typename cplx_t<R>::type *>(T), n, N, c.tiles.as<int2>(),
+            reinterpret_cast<typename cplx_t<A>::type *>(Cacc));
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+    prof_count(0, 0, 4.0 * (double)N * (double)(N + 1) * (double)n);
     CK(cudaStreamSynchronize(st));  // tile list is a stack vector
 }
 
@@ -512,6 +601,7 @@ void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     double scm = a->do_cbs ? sc / 2.0 : sc;
     int64_t total = (int64_t)N * N;
     int grid = (int)std::min<int64_t>((total + 255) / 256, 4096);
+    StageScope fin(ST_FINAL, st);
     if (d_Ms) {
         cov_finalize_kernel<A><<<grid, 256, 0, st>>>(reinterpret_cast<const A *>(Cs), 0, (int)a->nv, (int)a->nl, sc, d_Ms);
         CK(cudaGetLastError());
@@ -554,13 +644,20 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
             double *D = single ? Ds : Dm;
             for (int64_t e0 = 0; e0 < n_ev; e0 += chunk) {
                 int64_t n = std::min(chunk, n_ev - e0);
-                if (single) tc_rows<DIM, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
-                else tc_rows<DIM, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
-                CK(cudaGetLastError());
-                LAUNCHED();
-                tc_herk(plan, ops, n, D, st);
-                CK(cudaGetLastError());
-                LAUNCHED();
+                {
+                    StageScope sc(ST_ROWS, st);
+                    if (single) tc_rows<DIM, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
+                    else tc_rows<DIM, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
+                    CK(cudaGetLastError());
+                    LAUNCHED();
+                }
+                {
+                    StageScope sc(ST_CONTRACT, st);
+                    tc_herk(plan, ops, n, D, st);
+                    CK(cudaGetLastError());
+                    LAUNCHED();
+                }
+                prof_count(0, 0, 4.0 * (double)N * (double)(N + 1) * (double)n);
             }
         }
         done += nb;
@@ -574,6 +671,7 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     double scm = a->do_cbs ? sc / 2.0 : sc;
     int64_t total = (int64_t)N * N;
     int grid = (int)std::min<int64_t>((total + 255) / 256, 4096);
+    StageScope fin(ST_FINAL, st);
     if (d_Ms) {
         cov_finalize_kernel<double><<<grid, 256, 0, st>>>(Ds, 1, (int)a->nv, (int)a->nl, sc, d_Ms);
         CK(cudaGetLastError());
@@ -586,11 +684,8 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     }
 }
 
-void cov_device(const scmc_mc_args *a, double *d_Ms, double *d_Mm, cudaStream_t st)
+void cov_device_locked(Ctx &c, const scmc_mc_args *a, double *d_Ms, double *d_Mm, cudaStream_t st)
 {
-    validate(a);
-    Ctx &c = context(a->device);
-    std::lock_guard<std::mutex> lk(c.mu);
     CK(cudaSetDevice(a->device));
     Prepared P = prepare(c, a, 0, st);
     double2 *Ms = reinterpret_cast<double2 *>(d_Ms), *Mm = reinterpret_cast<double2 *>(d_Mm);
@@ -700,27 +795,6 @@ __global__ void philox_stream_kernel(uint64_t seed, uint64_t path, int tag, int6
     for (int64_t i = 0; i < n; ++i) out[i] = tag ? r.randn() : r.rand();
 }
 
-// Host-memory wrappers: device output, then one copy back.
-template <typename F>
-void with_device_outputs(int device, std::vector<std::pair<double *, size_t>> outs, F &&run)
-{
-    CK(cudaSetDevice(device));
-    std::vector<void *> dev(outs.size(), nullptr);
-    try {
-        for (size_t k = 0; k < outs.size(); ++k)
-            if (outs[k].first) CK(cudaMalloc(&dev[k], outs[k].second));
-        run(dev);
-        for (size_t k = 0; k < outs.size(); ++k)
-            if (outs[k].first) CK(cudaMemcpy(outs[k].first, dev[k], outs[k].second, cudaMemcpyDeviceToHost));
-    } catch (...) {
-        for (void *p : dev)
-            if (p) cudaFree(p);
-        throw;
-    }
-    for (void *p : dev)
-        if (p) CK(cudaFree(p));
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -738,8 +812,12 @@ int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream)
 {
     return guarded([&] {
         if (!d_u) fail(SCMC_ERR_INVALID, "null output");
-        field_device(args, d_u, reinterpret_cast<cudaStream_t>(stream));
-        CK(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+        validate(args);
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        field_device_locked(c, args, d_u, st);
+        CK(cudaStreamSynchronize(st));
     });
 }
 
@@ -748,19 +826,24 @@ int scmc_field(const scmc_mc_args *args, double *u)
     return guarded([&] {
         validate(args);
         if (!u) fail(SCMC_ERR_INVALID, "null output");
-        size_t bytes = (size_t)args->nv * args->nl * 2 * sizeof(double);
-        with_device_outputs(args->device, {{u, bytes}}, [&](std::vector<void *> &d) {
-            field_device(args, reinterpret_cast<double *>(d[0]), 0);
-            CK(cudaStreamSynchronize(0));
-        });
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const size_t bytes = (size_t)args->nv * args->nl * 2 * sizeof(double);
+        double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
+        field_device_locked(c, args, d, 0);
+        CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
     });
 }
 
 int scmc_cov_device(const scmc_mc_args *args, double *d_Ms, double *d_Mm, void *stream)
 {
     return guarded([&] {
-        cov_device(args, d_Ms, d_Mm, reinterpret_cast<cudaStream_t>(stream));
-        CK(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+        validate(args);
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        cov_device_locked(c, args, d_Ms, d_Mm, st);
+        CK(cudaStreamSynchronize(st));
     });
 }
 
@@ -768,12 +851,50 @@ int scmc_cov(const scmc_mc_args *args, double *Ms, double *Mm)
 {
     return guarded([&] {
         validate(args);
-        size_t n = (size_t)args->nv * args->nv * args->nl * args->nl;
-        size_t bytes = n * 2 * sizeof(double);
-        with_device_outputs(args->device, {{Ms, bytes}, {Mm, bytes}}, [&](std::vector<void *> &d) {
-            cov_device(args, reinterpret_cast<double *>(d[0]), reinterpret_cast<double *>(d[1]), 0);
-            CK(cudaStreamSynchronize(0));
-        });
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const size_t bytes = (size_t)args->nv * args->nv * args->nl * args->nl * 2 * sizeof(double);
+        double *d0 = Ms ? reinterpret_cast<double *>(c.out0.ensure(bytes)) : nullptr;
+        double *d1 = Mm ? reinterpret_cast<double *>(c.out1.ensure(bytes)) : nullptr;
+        cov_device_locked(c, args, d0, d1, 0);
+        if (Ms) CK(cudaMemcpy(Ms, d0, bytes, cudaMemcpyDeviceToHost));
+        if (Mm) CK(cudaMemcpy(Mm, d1, bytes, cudaMemcpyDeviceToHost));
+    });
+}
+
+int scmc_profile_enable(int32_t on)
+{
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        g_prof.on.store(on != 0);
+    });
+}
+
+int scmc_profile_read(scmc_stage_times *out, int32_t reset)
+{
+    return guarded([&] {
+        if (!out) fail(SCMC_ERR_INVALID, "null output");
+        std::lock_guard<std::mutex> lk(g_prof.mu);
+        g_prof.resolve_locked();
+        out->walk_launches = g_prof.launches[ST_WALK];
+        out->walk_ms = g_prof.ms[ST_WALK];
+        out->rows_launches = g_prof.launches[ST_ROWS];
+        out->rows_ms = g_prof.ms[ST_ROWS];
+        out->contract_launches = g_prof.launches[ST_CONTRACT];
+        out->contract_ms = g_prof.ms[ST_CONTRACT];
+        out->finalize_launches = g_prof.launches[ST_FINAL];
+        out->finalize_ms = g_prof.ms[ST_FINAL];
+        out->paths = g_prof.paths;
+        out->events = g_prof.events;
+        out->contract_flops = g_prof.flops;
+        if (reset) {
+            for (int k = 0; k < 4; ++k) {
+                g_prof.launches[k] = 0;
+                g_prof.ms[k] = 0;
+            }
+            g_prof.paths = g_prof.events = 0;
+            g_prof.flops = 0;
+        }
     });
 }
 

@@ -1,0 +1,44 @@
+"""The C-ABI library builds, loads without a GPU and exports every function
+include/scmc_gpu.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "scmc_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(scmc_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_header_declares_the_entry_points():
+    names = declared_functions()
+    for n in ("scmc_field", "scmc_cov", "scmc_field_device", "scmc_cov_device", "scmc_export_records",
+              "scmc_last_error", "scmc_philox_stream"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    from mcspeckle_b200 import build
+    path = build.build()
+    lib = ctypes.CDLL(path)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    lib.scmc_abi_version.restype = ctypes.c_int
+    assert lib.scmc_abi_version() == 1
+
+
+def test_python_struct_matches_header_layout():
+    """The ctypes mirror has the C struct's field order and count."""
+    from mcspeckle_b200 import _abi
+    src = open(HEADER).read()
+    body = src[src.index("typedef struct {\n    int32_t dim;"):]
+    body = body[:body.index("} scmc_mc_args;")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = re.findall(r"(\w+)(?:\[\d+\])?;", body)
+    py = [f[0].rstrip("_") for f in _abi.McArgs._fields_]
+    assert py == [f.rstrip("_") for f in fields]
