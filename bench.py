@@ -178,6 +178,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp16", choices=["mixed", "fp16"],
+                    help="mixed: FP16 hi+lo split (2 tensor products); fp16: one FP16 product")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
@@ -204,7 +206,7 @@ def main():
     Mm = torch.zeros(2 * n_out, dtype=torch.float64, device="cuda")
     seed = 0x5C3C0FFEE
 
-    def step_args(step, n=P, precision="mixed"):
+    def step_args(step, n=P, precision=a.precision):
         off = (step * world + rank) * n
         return MC.mc_args(*workload_args(n), seed=seed, precision=precision, device=local, path_offset=off,
                           norm_itr=n * world)
@@ -297,7 +299,9 @@ def main():
         na = int(a.accuracy_paths)
         ha = MC.mc_args(*workload_args(na), seed=seed, precision="fp64", device=local)
         M64 = MC.cov_from_args(ha)
-        Mmx = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision="mixed", device=local))
+        Mmx = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision=a.precision, device=local))
+        other = "fp16" if a.precision == "mixed" else "mixed"
+        Moth = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision=other, device=local))
         t32 = time.perf_counter()
         M32 = MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision="fp32",
                                           device=local))
@@ -311,9 +315,14 @@ def main():
 
         err_mixed = rel(Mmx[0] + Mmx[1], C64)
         err_fp32 = rel(M32[0] + M32[1], C64)
+        err_other = rel(Moth[0] + Moth[1], C64)
         tmx = time.perf_counter()
-        MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision="mixed", device=local))
+        MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision=a.precision,
+                                    device=local))
         mixed_small_s = time.perf_counter() - tmx
+        tot = time.perf_counter()
+        MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision=other, device=local))
+        other_small_s = time.perf_counter() - tot
         cpu = None
         if not a.no_cpu_baseline:
             rate, n, dt, thr = cpu_oracle_rate(workload_args, target_s=a.cpu_seconds)
@@ -322,9 +331,10 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f16x2+f32acc (phases f64-reduced f32, sums f64)", "data": "synthetic",
+            "dtype": ("f16 hi+lo" if a.precision == "mixed" else "f16") + " x f16 -> f32 (phases f64-reduced f32, sums f64)",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD, "paths_per_gpu_per_step": P, "lights": 64, "views": 64,
-                       "output": "Ms, Mm: 64x64x64x64 complex f64", "precision": "mixed",
+                       "output": "Ms, Mm: 64x64x64x64 complex f64", "precision": a.precision,
                        "parallelism": f"path-range shards x{world}" + (" + NCCL sum" if world > 1 else ""),
                        "l2": "working set > L2 (1 GiB operand per chunk, 2 x 268 MB accumulators)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -337,8 +347,11 @@ def main():
                          "launches": prof["contract_launches"]},
             "stages_ms": {"walk": prof["walk_ms"], "rows": prof["rows_ms"], "contract": prof["contract_ms"],
                           "finalize": prof["finalize_ms"]},
-            "accuracy": {"paths": na, "rel_err_mixed_vs_fp64": err_mixed, "rel_err_fp32_vs_fp64": err_fp32,
+            "accuracy": {"paths": na, f"rel_err_{a.precision}_vs_fp64": err_mixed,
+                         f"rel_err_{other}_vs_fp64": err_other, "rel_err_fp32_vs_fp64": err_fp32,
                          "tol": 1e-3, "norm": "Frobenius of C = Ms + Mm"},
+            "other_precision": {"precision": other, "paths": int(a.fp32_paths),
+                                "value": int(a.fp32_paths) / other_small_s},
             "fp32_gpu": {"paths": int(a.fp32_paths), "value": int(a.fp32_paths) / fp32_s,
                          "mixed_same_sample": int(a.fp32_paths) / mixed_small_s,
                          "speedup_mixed_over_fp32": (int(a.fp32_paths) / mixed_small_s) / (int(a.fp32_paths) / fp32_s)},

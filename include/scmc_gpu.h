@@ -45,9 +45,11 @@ enum { SCMC_SCT_ISOTROPIC = 1, SCMC_SCT_TABULATED = 2, SCMC_SCT_HG = 3 };
  *          and FP32 accumulation, cross-batch sums in FP64.
  *  FP32  - plain FP32: FP32 phases without FP64 reduction, FP32 CUDA-core
  *          contraction, FP32 accumulation (the comparison baseline).
- * The random walk itself is FP64 in every mode, so all three modes see the
- * same paths for the same seed. */
-enum { SCMC_PREC_FP64 = 0, SCMC_PREC_MIXED = 1, SCMC_PREC_FP32 = 2 };
+ *  FP16  - as MIXED but one FP16 product (no lo part): half the tensor work,
+ *          about sqrt(2) times MIXED's error.
+ * The random walk itself is FP64 in every mode, so all modes see the same
+ * paths for the same seed. */
+enum { SCMC_PREC_FP64 = 0, SCMC_PREC_MIXED = 1, SCMC_PREC_FP32 = 2, SCMC_PREC_FP16 = 3 };
 
 /* One scattering function: the (sct_type, ampfunc) pair of MCfield.m:1.
  * For SCMC_SCT_TABULATED the two tables are the fields evalAmp and

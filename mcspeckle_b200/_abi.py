@@ -21,8 +21,8 @@ SCMC_ERR_CANCELLED = 6
 SCMC_ERR_LIMIT = 7
 
 SCT_ISOTROPIC, SCT_TABULATED, SCT_HG = 1, 2, 3
-PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
-PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED, "fp32": PREC_FP32}
+PREC_FP64, PREC_MIXED, PREC_FP32, PREC_FP16 = 0, 1, 2, 3
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED, "fp32": PREC_FP32, "fp16": PREC_FP16}
 
 _dp = C.POINTER(C.c_double)
 

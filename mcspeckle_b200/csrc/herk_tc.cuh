@@ -37,12 +37,16 @@ namespace scmc {
 constexpr int TC_BM = 128;
 constexpr int TC_BN = 256;
 constexpr int TC_BK = 64;
-constexpr int TC_STAGES = 3;
 constexpr int TC_A_BYTES = TC_BM * TC_BK * 2;
 constexpr int TC_B_BYTES = TC_BN * TC_BK * 2;
-constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + TC_B_BYTES;
-constexpr int TC_SMEM_BYTES = TC_STAGES * TC_STAGE_BYTES + 1024 + 256;
 constexpr int TC_TMEM_COLS = 256;
+// SPLIT: A_hi + A_lo + B per stage (64 KB, 3 stages); otherwise A + B (48 KB, 4 stages)
+template <bool SPLIT> struct TcCfg {
+    static constexpr int STAGE_BYTES = (SPLIT ? 2 : 1) * TC_A_BYTES + TC_B_BYTES;
+    static constexpr int STAGES = SPLIT ? 3 : 4;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr int B_OFF = (SPLIT ? 2 : 1) * TC_A_BYTES;
+};
 constexpr unsigned long long TC_WAIT_NS = 2000000000ull;  // 2 s bound on every wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -144,7 +148,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// One 128 x 256 tile of D += (A_hi + A_lo) B^T over num_kb K-blocks of 64.
+// One 128 x 256 tile of D += (A_hi [+ A_lo]) B^T over num_kb K-blocks of 64.
+template <bool SPLIT>
 __global__ void __launch_bounds__(128, 1)
 herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
                const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int Mr,
@@ -152,9 +157,9 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
 {
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
-    uint64_t *full = reinterpret_cast<uint64_t *>(base + TC_STAGES * TC_STAGE_BYTES);
-    uint64_t *empty = full + TC_STAGES;
-    uint64_t *done = empty + TC_STAGES;
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + TcCfg<SPLIT>::STAGES * TcCfg<SPLIT>::STAGE_BYTES);
+    uint64_t *empty = full + TcCfg<SPLIT>::STAGES;
+    uint64_t *done = empty + TcCfg<SPLIT>::STAGES;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
     int *issued = abort_flag + 1;
@@ -165,7 +170,7 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
     const int col0 = tile.y * TC_BN;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_STAGES; ++s) {
+        for (int s = 0; s < TcCfg<SPLIT>::STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -188,38 +193,38 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
     if (warp == 0 && lane == 0) {
         // TMA producer
         for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % TC_STAGES;
-            if (kb >= TC_STAGES && !mbar_wait(&empty[s], ((kb / TC_STAGES) - 1) & 1)) {
+            const int s = kb % TcCfg<SPLIT>::STAGES;
+            if (kb >= TcCfg<SPLIT>::STAGES && !mbar_wait(&empty[s], ((kb / TcCfg<SPLIT>::STAGES) - 1) & 1)) {
                 atomicExch(abort_flag, 1);
                 break;
             }
             if (*(volatile int *)abort_flag) break;
-            uint8_t *st = base + s * TC_STAGE_BYTES;
-            mbar_expect_tx(&full[s], TC_STAGE_BYTES);
+            uint8_t *st = base + s * TcCfg<SPLIT>::STAGE_BYTES;
+            mbar_expect_tx(&full[s], TcCfg<SPLIT>::STAGE_BYTES);
             tma_load_2d(st, &tm_ahi, kb * TC_BK, row0, &full[s]);
-            tma_load_2d(st + TC_A_BYTES, &tm_alo, kb * TC_BK, row0, &full[s]);
-            tma_load_2d(st + 2 * TC_A_BYTES, &tm_b, kb * TC_BK, col0, &full[s]);
+            if (SPLIT) tma_load_2d(st + TC_A_BYTES, &tm_alo, kb * TC_BK, row0, &full[s]);
+            tma_load_2d(st + TcCfg<SPLIT>::B_OFF, &tm_b, kb * TC_BK, col0, &full[s]);
             *(volatile int *)issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
         constexpr uint32_t idesc = umma_idesc_f16(TC_BM, TC_BN);
         for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % TC_STAGES;
-            if (!mbar_wait(&full[s], (kb / TC_STAGES) & 1)) {
+            const int s = kb % TcCfg<SPLIT>::STAGES;
+            if (!mbar_wait(&full[s], (kb / TcCfg<SPLIT>::STAGES) & 1)) {
                 atomicExch(abort_flag, 1);
                 break;
             }
             tc_fence_after();
-            uint8_t *st = base + s * TC_STAGE_BYTES;
+            uint8_t *st = base + s * TcCfg<SPLIT>::STAGE_BYTES;
             const uint64_t dh = umma_desc_sw128(st);
             const uint64_t dl = umma_desc_sw128(st + TC_A_BYTES);
-            const uint64_t db = umma_desc_sw128(st + 2 * TC_A_BYTES);
+            const uint64_t db = umma_desc_sw128(st + TcCfg<SPLIT>::B_OFF);
 #pragma unroll
             for (int kk = 0; kk < TC_BK / 16; ++kk) {
                 const uint64_t adv = (uint64_t)(kk * 32) >> 4;  // 16 fp16 = 32 B along K
                 umma_f16(tmem, dh + adv, db + adv, idesc, (kb | kk) != 0);
-                umma_f16(tmem, dl + adv, db + adv, idesc, 1u);
+                if (SPLIT) umma_f16(tmem, dl + adv, db + adv, idesc, 1u);
             }
             umma_commit(&empty[s]);
         }
@@ -235,8 +240,8 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
             atomicExch(err, 1);
             // wait (bounded) for TMA copies this CTA still has in flight
             const int n_issued = *(volatile int *)issued;
-            for (int kb = (n_issued > TC_STAGES ? n_issued - TC_STAGES : 0); kb < n_issued; ++kb)
-                (void)mbar_wait(&full[kb % TC_STAGES], (kb / TC_STAGES) & 1);
+            for (int kb = (n_issued > TcCfg<SPLIT>::STAGES ? n_issued - TcCfg<SPLIT>::STAGES : 0); kb < n_issued; ++kb)
+                (void)mbar_wait(&full[kb % TcCfg<SPLIT>::STAGES], (kb / TcCfg<SPLIT>::STAGES) & 1);
         }
     } else {
         // Epilogue: TMEM -> registers -> smem transpose -> coalesced FP64 RMW.
@@ -272,7 +277,7 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
 // Rows of one chunk in the split FP16 K-major layout.  One CTA per group of
 // 32 events; lane = event, so each row write is 32 consecutive half2 (128 B).
 // ---------------------------------------------------------------------------
-template <int DIM, bool SINGLE>
+template <int DIM, bool SINGLE, bool SPLIT>
 __global__ void __launch_bounds__(256)
 tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
                int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo, const float2 *__restrict__ af_tab)
@@ -342,13 +347,15 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
         t.x *= sc;
         t.y *= sc;
         const __half hr = __float2half_rn(t.x), hi = __float2half_rn(t.y);
-        const __half lr = __float2half_rn(t.x - __half2float(hr));
-        const __half li = __float2half_rn(t.y - __half2float(hi));
         const int64_t r0 = (int64_t)(2 * i) * K + col, r1 = (int64_t)(2 * i + 1) * K + col;
         *reinterpret_cast<__half2 *>(Ahi + r0) = __halves2half2(hr, hi);
         *reinterpret_cast<__half2 *>(Ahi + r1) = __halves2half2(hi, __hneg(hr));
-        *reinterpret_cast<__half2 *>(Alo + r0) = __halves2half2(lr, li);
-        *reinterpret_cast<__half2 *>(Alo + r1) = __halves2half2(li, __hneg(lr));
+        if (SPLIT) {
+            const __half lr = __float2half_rn(t.x - __half2float(hr));
+            const __half li = __float2half_rn(t.y - __half2float(hi));
+            *reinterpret_cast<__half2 *>(Alo + r0) = __halves2half2(lr, li);
+            *reinterpret_cast<__half2 *>(Alo + r1) = __halves2half2(li, __hneg(lr));
+        }
     }
 }
 
@@ -368,6 +375,7 @@ __global__ void af_table_kernel(NeeParams Q, float2 *__restrict__ tab)
 // ---------------------------------------------------------------------------
 struct TcPlan {
     int N;
+    bool split;
     int64_t events_per_chunk;
     int64_t K;
     std::vector<int2> tiles;
@@ -382,22 +390,27 @@ struct TcOperands {
     int n_tiles;
 };
 
-inline TcPlan tc_plan(int N)
+inline TcPlan tc_plan(int N, bool split)
 {
     TcPlan p;
     p.N = N;
-    // 16N bytes of operand per event; keep a chunk's operands near 1 GiB
-    int64_t e = ((int64_t)1 << 30) / (16 * (int64_t)N);
+    p.split = split;
+    // 8N (16N split) bytes of operand per event; keep a chunk's operands near 1 GiB
+    int64_t e = ((int64_t)1 << 30) / ((split ? 16 : 8) * (int64_t)N);
     e = std::max<int64_t>(32, std::min<int64_t>(e, 32768));
     e = (e / 32) * 32;
     p.events_per_chunk = e;
     p.K = 2 * e;
     const int n_tm = (2 * N + TC_BM - 1) / TC_BM;
     const int n_tn = (N + TC_BN - 1) / TC_BN;
-    // tn-major order: CTAs resident together share B tiles
-    for (int tn = 0; tn < n_tn; ++tn)
-        for (int tm = 0; tm < n_tm; ++tm)
-            if ((int64_t)(TC_BM / 2) * tm <= (int64_t)TC_BN * tn + TC_BN - 1) p.tiles.push_back(make_int2(tm, tn));
+    // Upper-triangle tiles in blocks of GM x GN (tm x tn), so the CTAs of one
+    // wave share A row blocks and B column blocks in L2 while they stream K.
+    const int GM = 16, GN = 8;
+    for (int bn = 0; bn < n_tn; bn += GN)
+        for (int bm = 0; bm < n_tm; bm += GM)
+            for (int tn = bn; tn < std::min(n_tn, bn + GN); ++tn)
+                for (int tm = bm; tm < std::min(n_tm, bm + GM); ++tm)
+                    if ((int64_t)(TC_BM / 2) * tm <= (int64_t)TC_BN * tn + TC_BN - 1) p.tiles.push_back(make_int2(tm, tn));
     return p;
 }
 
@@ -406,7 +419,8 @@ inline size_t tc_align(size_t x) { return (x + 1023) & ~(size_t)1023; }
 inline size_t tc_operand_bytes(const TcPlan &p)
 {
     size_t a = (size_t)2 * p.N * p.K * sizeof(__half);
-    return 2 * tc_align(a) + tc_align(p.tiles.size() * sizeof(int2)) + 1024 + tc_align((size_t)p.N * sizeof(float2));
+    return (p.split ? 2 : 1) * tc_align(a) + tc_align(p.tiles.size() * sizeof(int2)) + 1024 +
+           tc_align((size_t)p.N * sizeof(float2));
 }
 
 inline PFN_cuTensorMapEncodeTiled_v12000 tc_encode_fn()
@@ -442,10 +456,11 @@ inline TcOperands tc_make_operands(const TcPlan &p, void *mem, cudaStream_t st)
     TcOperands o{};
     char *b = reinterpret_cast<char *>(mem);
     const size_t a = tc_align((size_t)2 * p.N * p.K * sizeof(__half));
+    const size_t na = p.split ? 2 : 1;
     o.ahi = reinterpret_cast<__half *>(b);
-    o.alo = reinterpret_cast<__half *>(b + a);
-    o.tiles = reinterpret_cast<int2 *>(b + 2 * a);
-    o.err = reinterpret_cast<int *>(b + 2 * a + tc_align(p.tiles.size() * sizeof(int2)));
+    o.alo = p.split ? reinterpret_cast<__half *>(b + a) : o.ahi;
+    o.tiles = reinterpret_cast<int2 *>(b + na * a);
+    o.err = reinterpret_cast<int *>(b + na * a + tc_align(p.tiles.size() * sizeof(int2)));
     o.af = reinterpret_cast<float2 *>(reinterpret_cast<char *>(o.err) + 1024);
     o.n_tiles = (int)p.tiles.size();
     if (cudaMemcpyAsync(o.tiles, p.tiles.data(), p.tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -458,30 +473,38 @@ inline TcOperands tc_make_operands(const TcPlan &p, void *mem, cudaStream_t st)
     return o;
 }
 
-template <int DIM, bool SINGLE>
+template <int DIM, bool SINGLE, bool SPLIT>
 inline void tc_rows(const TcPlan &p, const TcOperands &o, const NeeParams &Q, const SingleRec &S, int64_t scap,
                     const MultiRec &M, int64_t mcap, int64_t e0, int64_t n, bool use_af_table, cudaStream_t st)
 {
     const size_t smem = sizeof(float2) * 33 * 2 * (size_t)(Q.nv + Q.nl) + 32 * sizeof(float) +
                         32 * sizeof(EventView) + 64;
-    auto kern = tc_rows_kernel<DIM, SINGLE>;
+    auto kern = tc_rows_kernel<DIM, SINGLE, SPLIT>;
     if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         throw std::runtime_error("too many lights/views for the tensor-core row kernel");
     const int grid = (int)((n + 31) / 32);
     kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, use_af_table ? o.af : nullptr);
 }
 
-inline void tc_herk(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
+template <bool SPLIT>
+inline void tc_herk_launch(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
 {
     static bool attr = false;
     if (!attr) {
-        if (cudaFuncSetAttribute(herk_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES) != cudaSuccess)
+        if (cudaFuncSetAttribute(herk_tc_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcCfg<SPLIT>::SMEM_BYTES) != cudaSuccess)
             throw std::runtime_error("cannot reserve shared memory for the tensor-core kernel");
         attr = true;
     }
     const int num_kb = (int)((2 * n + TC_BK - 1) / TC_BK);
-    herk_tc_kernel<<<o.n_tiles, 128, TC_SMEM_BYTES, st>>>(o.m_ahi, o.m_alo, o.m_b, o.tiles, num_kb, 2 * p.N, p.N, D,
-                                                          o.err);
+    herk_tc_kernel<SPLIT><<<o.n_tiles, 128, TcCfg<SPLIT>::SMEM_BYTES, st>>>(o.m_ahi, o.m_alo, o.m_b, o.tiles, num_kb,
+                                                                          2 * p.N, p.N, D, o.err);
+}
+
+inline void tc_herk(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
+{
+    if (p.split) tc_herk_launch<true>(p, o, n, D, st);
+    else tc_herk_launch<false>(p, o, n, D, st);
 }
 
 }  // namespace scmc

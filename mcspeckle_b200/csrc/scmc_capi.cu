@@ -215,7 +215,7 @@ void validate(const scmc_mc_args *a)
     if (!(a->sigt > 0) || !std::isfinite(a->sigt)) fail(SCMC_ERR_INVALID, "sigt must be positive");
     if (!(a->lambda > 0)) fail(SCMC_ERR_INVALID, "lambda must be positive");
     if (a->smp_flg != 1 && a->smp_flg != 2) fail(SCMC_ERR_INVALID, "smpFlg must be 1 or 2");
-    if (a->precision < 0 || a->precision > 2) fail(SCMC_ERR_INVALID, "invalid precision mode");
+    if (a->precision < 0 || a->precision > 3) fail(SCMC_ERR_INVALID, "invalid precision mode");
     for (int k = 0; k < a->dim; ++k)
         if (!(a->box_max[k] >= a->box_min[k])) fail(SCMC_ERR_INVALID, "Invalid box size");
     validate_pf(a->ampfunc, "ampfunc");
@@ -504,11 +504,11 @@ void field_device_locked(Ctx &c, const scmc_mc_args *a, double *d_u, cudaStream_
     double2 *u = reinterpret_cast<double2 *>(d_u);
     if (a->dim == 3) {
         if (a->precision == SCMC_PREC_FP64) field_run<3, P64, double>(c, a, P, u, st);
-        else if (a->precision == SCMC_PREC_MIXED) field_run<3, PMIX, double>(c, a, P, u, st);
+        else if (a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16) field_run<3, PMIX, double>(c, a, P, u, st);
         else field_run<3, P32, float>(c, a, P, u, st);
     } else {
         if (a->precision == SCMC_PREC_FP64) field_run<2, P64, double>(c, a, P, u, st);
-        else if (a->precision == SCMC_PREC_MIXED) field_run<2, PMIX, double>(c, a, P, u, st);
+        else if (a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16) field_run<2, PMIX, double>(c, a, P, u, st);
         else field_run<2, P32, float>(c, a, P, u, st);
     }
 }
@@ -618,7 +618,7 @@ template <int DIM>
 void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st)
 {
     const int N = (int)(a->nv * a->nl);
-    TcPlan plan = tc_plan(N);
+    TcPlan plan = tc_plan(N, a->precision == SCMC_PREC_MIXED);
     const size_t acc_bytes = (size_t)2 * N * N * sizeof(double);
     double *Ds = reinterpret_cast<double *>(c.acc_s.ensure(acc_bytes));
     double *Dm = reinterpret_cast<double *>(c.acc_m.ensure(acc_bytes));
@@ -646,8 +646,13 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
                 int64_t n = std::min(chunk, n_ev - e0);
                 {
                     StageScope sc(ST_ROWS, st);
-                    if (single) tc_rows<DIM, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
-                    else tc_rows<DIM, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
+                    if (plan.split) {
+                        if (single) tc_rows<DIM, true, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
+                        else tc_rows<DIM, false, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
+                    } else {
+                        if (single) tc_rows<DIM, true, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
+                        else tc_rows<DIM, false, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
+                    }
                     CK(cudaGetLastError());
                     LAUNCHED();
                 }

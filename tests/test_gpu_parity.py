@@ -106,12 +106,15 @@ def test_mixed_and_fp32_close_to_fp64(gpu, case):
     Msm, Mmm = MC.cov_from_args(hmx)
     assert rel(Msm, Ms64) < MIXED_TOL
     assert rel(Mmm, Mm64) < MIXED_TOL
+    Ms16, Mm16 = MC.cov_from_args(args_for(case, precision="fp16"))
+    assert rel(Ms16, Ms64) < MIXED_TOL and rel(Mm16, Mm64) < MIXED_TOL
     Ms32, Mm32 = MC.cov_from_args(h32)
     assert rel(Ms32, Ms64) < 1e-2 and rel(Mm32, Mm64) < 1e-2
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp16"])
 @pytest.mark.parametrize("nside_v,nside_l", [(4, 4), (8, 4), (5, 3), (8, 8)])
-def test_tensor_core_cov_tiles(gpu, nside_v, nside_l):
+def test_tensor_core_cov_tiles(gpu, nside_v, nside_l, precision):
     """Mixed (tcgen05) vs FP64 covariance at sizes that exercise several
     tiles, partial tiles and the diagonal tiles of the Hermitian update."""
     l = grid_dirs(nside_l, 5, +1)
@@ -119,7 +122,7 @@ def test_tensor_core_cov_tiles(gpu, nside_v, nside_l):
     base = [1.01 / 10, 1 / 1.01, np.array([-100.0, -100.0, 0.0]), np.array([100.0, 100.0, 50.0]), l, v, 1, 1,
             2000, 1.0, True, 2, 3, 0.8]
     Ms64, Mm64 = MC.cov_from_args(MC.mc_args(*base, seed=SEED, precision="fp64"))
-    Msm, Mmm = MC.cov_from_args(MC.mc_args(*base, seed=SEED, precision="mixed"))
+    Msm, Mmm = MC.cov_from_args(MC.mc_args(*base, seed=SEED, precision=precision))
     assert rel(Msm, Ms64) < MIXED_TOL
     assert rel(Mmm, Mm64) < MIXED_TOL
     # Hermitian structure C(v1,v2,l1,l2) = conj(C(v2,v1,l2,l1))
