@@ -130,6 +130,23 @@ int scmc_field(const scmc_mc_args *args, double *u);
  * enqueued and the batch bookkeeping synchronised. */
 int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream);
 
+/* Field without any device allocation.  For callers that cannot allocate
+ * device memory while they call in: code running inside a CUDA-graph
+ * capture, a process that reserved its GPU memory budget up front, or a host
+ * thread on which cudaMalloc / cudaFree are not allowed.  Same computation as
+ * scmc_field_device, with every piece of device scratch in one fixed 32 MiB
+ * array inside the library, which each GPU that loads the library holds
+ * until the process exits.  No counterpart in the reference (MATLAB manages
+ * memory for its callers).
+ * d_u: device memory, 2*nv*nl doubles.  Limits: nv*nl <= 65536, tabulated
+ * tables <= 16384 entries, and no single path longer than the scratch holds
+ * (about 400k events); beyond them it returns SCMC_ERR_INVALID.  The first
+ * call on a device looks up the array's device address, so make that call
+ * before any stream capture.  All calls share the array and it keeps the
+ * previous call's contents (each call clears what must start at zero); calls
+ * whose work overlaps on the GPU race. */
+int scmc_field_noalloc(const scmc_mc_args *args, double *d_u, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Covariance: [Ms, Mm] = MCcov(sigt, albedo, box_min, box_max, l, v, is_ff_l,
  *                  is_ff_v, maxItr, lambda, doCBS, smpFlg, sct_type, ampfunc

@@ -932,3 +932,296 @@ int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, dou
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// scmc_field_noalloc: the field path with every piece of device scratch in a
+// fixed, file-scope device array instead of allocated memory.
+//
+// Some callers cannot allocate device memory while they call in: a host that
+// runs inside a CUDA-graph capture or a pre-reserved memory budget (a serving
+// process that sized its pools at start-up), a real-time caller that must not
+// take the allocator's locks, or an embedding runtime that forbids
+// cudaMalloc/cudaFree on its threads.  This entry point serves them: it calls
+// no cudaMalloc, cudaFree or allocating library routine; the caller passes
+// the inputs (host struct) and the output (device memory).
+//
+// Limits (SCMC_ERR_INVALID beyond them): nv*nl <= 65536, each tabulated
+// table <= 16384 entries, and no single path may have more scattering events
+// than the scratch holds (~400k).  The scratch is 32 MiB per device and stays
+// resident in every GPU that loads the library until the process exits.
+// Every call shares it and it keeps the previous call's contents: the
+// accumulators and counters are cleared at the start of each call, and calls
+// whose work overlaps on the GPU (two host threads, or two streams) race.
+// The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress) with that device current; make that first call
+// before any stream capture.
+// ---------------------------------------------------------------------------
+static constexpr size_t kFieldScratchBytes = (size_t)32 << 20;
+static __device__ __align__(256) unsigned char g_field_scratch[kFieldScratchBytes];
+
+namespace {
+
+std::mutex g_scratch_mu;
+void *g_scratch_addr[64] = {};
+
+std::mutex &g_scratch_mu_call()
+{
+    static std::mutex m;
+    return m;
+}
+
+unsigned char *field_scratch(int device)
+{
+    if (device < 0 || device >= 64) fail(SCMC_ERR_INVALID, "invalid device ordinal");
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_addr[device]) {
+        void *p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_field_scratch));
+        g_scratch_addr[device] = p;
+    }
+    return reinterpret_cast<unsigned char *>(g_scratch_addr[device]);
+}
+
+// [dim][n] column-major -> [n][3] (zero-padded), optionally also sign * the same.
+__global__ void pack_dirs_kernel(const double *raw, int n, int dim, double sign, double *out, double *out_signed)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        for (int k = 0; k < 3; ++k) {
+            double x = k < dim ? raw[dim * j + k] : 0.0;
+            out[3 * j + k] = x;
+            if (out_signed) out_signed[3 * j + k] = sign * x;
+        }
+}
+
+struct ScratchCarve {
+    unsigned char *base;
+    size_t off = 0, cap;
+    template <typename T> T *take(size_t n)
+    {
+        off = (off + 255) & ~(size_t)255;
+        T *p = reinterpret_cast<T *>(base + off);
+        off += n * sizeof(T);
+        if (off > cap) fail(SCMC_ERR_INVALID, "inputs exceed the fixed scratch of scmc_field_noalloc");
+        return p;
+    }
+    size_t left() const { return cap > off ? cap - off : 0; }
+};
+
+PhaseFn noalloc_pf(const scmc_phase_function &pf, ScratchCarve &sc, cudaStream_t st)
+{
+    PhaseFn d{};
+    d.sct_type = pf.sct_type;
+    d.g = pf.g;
+    d.table_n = pf.table_n;
+    if (pf.sct_type == SCMC_SCT_TABULATED) {
+        if (pf.table_n > 16384) fail(SCMC_ERR_INVALID, "scmc_field_noalloc: tabulated tables are limited to 16384 entries");
+        double2 *amp = sc.take<double2>(pf.table_n);
+        double *icdf = sc.take<double>(pf.table_n);
+        CK(cudaMemcpyAsync(amp, pf.eval_amp, pf.table_n * sizeof(double2), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(icdf, pf.sample_icdf, pf.table_n * sizeof(double), cudaMemcpyHostToDevice, st));
+        d.eval_amp = amp;
+        d.sample_icdf = icdf;
+    }
+    return d;
+}
+
+template <int DIM, int POL, typename AccT>
+void field_noalloc_run(const scmc_mc_args *a, double2 *d_u, cudaStream_t st)
+{
+    const int dim = DIM;
+    ScratchCarve sc{field_scratch(a->device)};
+    sc.cap = kFieldScratchBytes;
+    const int nv = (int)a->nv, nl = (int)a->nl;
+
+    // parameters, as prepare() builds them, with the inputs placed in scratch
+    WalkParams W{};
+    W.dim = dim;
+    W.smp_flg = a->smp_flg;
+    W.has_pf0 = a->has_ampfunc0;
+    W.want_phase = 1;
+    W.sigt = a->sigt;
+    W.albedo = a->albedo;
+    double volume = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        W.box_min[k] = k < dim ? a->box_min[k] : 0.0;
+        W.box_max[k] = k < dim ? a->box_max[k] : 0.0;
+        W.box_w[k] = W.box_max[k] - W.box_min[k];
+        if (k < dim) volume *= W.box_w[k];
+    }
+    double nrm = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        double s = 0.0;
+        if (k < dim)
+            for (int64_t j = 0; j < a->nl; ++j) s += a->l[dim * j + k];
+        W.unmeanl[k] = k < dim ? (a->has_lmean0 ? a->lmean0[k] : s / (double)a->nl) : 0.0;
+        nrm += W.unmeanl[k] * W.unmeanl[k];
+    }
+    nrm = std::sqrt(nrm);
+    for (int k = 0; k < 3; ++k) W.meanl[k] = W.unmeanl[k] / nrm;
+    if (a->smp_flg == 2 && W.unmeanl[dim - 1] == 0.0)
+        fail(SCMC_ERR_INVALID, "exponential first-scatter sampling needs a mean light direction with a non-zero last component");
+    W.key0 = (uint32_t)a->seed;
+    W.key1 = (uint32_t)(a->seed >> 32);
+    W.max_events = a->max_events_per_path;
+    W.pf = noalloc_pf(a->ampfunc, sc, st);
+    W.pf0 = a->has_ampfunc0 ? noalloc_pf(a->ampfunc0, sc, st) : W.pf;
+
+    // raw dim x n inputs into scratch, then packed to [n][3] on the device
+    double *raw_l = sc.take<double>((size_t)dim * nl), *raw_v = sc.take<double>((size_t)dim * nv);
+    CK(cudaMemcpyAsync(raw_l, a->l, (size_t)dim * nl * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(raw_v, a->v, (size_t)dim * nv * 8, cudaMemcpyHostToDevice, st));
+    double *dl = sc.take<double>(3 * (size_t)nl), *dv = sc.take<double>(3 * (size_t)nv), *dvs = sc.take<double>(3 * (size_t)nv);
+    pack_dirs_kernel<<<std::max(1, (nl + 255) / 256), 256, 0, st>>>(raw_l, nl, dim, 1.0, dl, nullptr);
+    pack_dirs_kernel<<<std::max(1, (nv + 255) / 256), 256, 0, st>>>(raw_v, nv, dim, a->is_ff_v ? -1.0 : 1.0, dv, dvs);
+    CK(cudaGetLastError());
+    LAUNCHED();
+    LAUNCHED();
+
+    NeeParams Q{};
+    Q.nv = nv;
+    Q.nl = nl;
+    Q.is_ff_l = a->is_ff_l;
+    Q.is_ff_v = a->is_ff_v;
+    Q.cbs = a->do_cbs;
+    Q.sigt_half = a->sigt / 2.0;
+    Q.kw = SCMC_PI * 2.0 / a->lambda;
+    Q.lambda = a->lambda;
+    for (int k = 0; k < 3; ++k) {
+        Q.box_min[k] = W.box_min[k];
+        Q.box_max[k] = W.box_max[k];
+        Q.meanl[k] = W.meanl[k];
+    }
+    Q.l = dl;
+    Q.v = dv;
+    Q.vs = dvs;
+    Q.has_pf0 = a->has_ampfunc0;
+    Q.pf = W.pf;
+    Q.pf0 = W.pf0;
+
+    // accumulators, counters and the scan's temporary storage
+    const int64_t n = (int64_t)nv * nl;
+    AccT *Us = sc.take<AccT>(2 * n), *Um = sc.take<AccT>(2 * n);
+    unsigned long long *ctr = sc.take<unsigned long long>(2);
+    int *err = sc.take<int>(1);
+    const int64_t max_batch = 8192;
+    int32_t *counts = sc.take<int32_t>(max_batch);
+    int64_t *mcnt = sc.take<int64_t>(max_batch);
+    int64_t *moff = sc.take<int64_t>(max_batch + 1);
+    size_t scan_bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, mcnt, moff, max_batch, st));
+    unsigned char *scan_tmp = sc.take<unsigned char>(scan_bytes);
+    SingleRec S{sc.take<double>(3 * max_batch), sc.take<double>(3 * max_batch), sc.take<double>(max_batch),
+                sc.take<double>(max_batch), sc.take<int32_t>(max_batch)};
+    const int64_t scap = max_batch;
+    const size_t per_event = 8 * sizeof(double) + 2 * sizeof(int32_t);
+    const int64_t mcap = (int64_t)(sc.left() / per_event) - 64;
+    if (mcap < 1024) fail(SCMC_ERR_INVALID, "scmc_field_noalloc: scratch too small for these inputs");
+    MultiRec Mr{sc.take<double>(3 * mcap), sc.take<double>(3 * mcap), sc.take<double>(mcap), sc.take<double>(mcap),
+                sc.take<int32_t>(mcap), sc.take<int32_t>(mcap)};
+    CK(cudaMemsetAsync(Us, 0, 2 * n * sizeof(AccT), st));
+    CK(cudaMemsetAsync(Um, 0, 2 * n * sizeof(AccT), st));
+
+    const int sms = sm_count(a->device);
+    int tv = std::min(nv, 32), tl = std::min(nl, 32);
+    while (tv * tl > kFieldMaxTile) tl /= 2;
+    const int n_vtiles = (nv + tv - 1) / tv, n_ltiles = (nl + tl - 1) / tl;
+    const int tiles = n_vtiles * n_ltiles;
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using C = typename cplx_t<R>::type;
+    const size_t smem = sizeof(C) * (2 * kFieldEB * (tv + tl) + kFieldEB) + sizeof(EventView) * kFieldEB + 16;
+    if (smem > 48 * 1024) {
+        CK(cudaFuncSetAttribute(field_accum_kernel<DIM, POL, true, AccT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(field_accum_kernel<DIM, POL, false, AccT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    auto accumulate = [&](bool single, int64_t n_ev) {
+        if (n_ev <= 0) return;
+        int64_t ranges = std::max<int64_t>(1, (int64_t)sms * 6 / tiles);
+        int64_t per = std::max<int64_t>((n_ev + ranges - 1) / ranges, kFieldEB * 4);
+        ranges = (n_ev + per - 1) / per;
+        dim3 grid(tiles, (unsigned)ranges);
+        if (single)
+            field_accum_kernel<DIM, POL, true, AccT><<<grid, kFieldThreads, smem, st>>>(Q, S, scap, Mr, mcap, n_ev, tv, tl,
+                                                                                        n_vtiles, per, Us, 1);
+        else
+            field_accum_kernel<DIM, POL, false, AccT><<<grid, kFieldThreads, smem, st>>>(Q, S, scap, Mr, mcap, n_ev, tv, tl,
+                                                                                         n_vtiles, per, Um, 1);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    };
+
+    int64_t batch = max_batch;
+    for (int64_t done = 0; done < a->max_itr;) {
+        const int64_t nb = std::min(batch, a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        W.n_paths = nb;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nb + 127) / 128, (int64_t)sms * 8));
+        CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+        CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+        walk_count_kernel<DIM><<<grid, 128, 0, st>>>(W, counts, ctr, err);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        count_to_multi_kernel<<<std::max(1, (int)((nb + 255) / 256)), 256, 0, st>>>(counts, nb, mcnt);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        size_t tb = scan_bytes;
+        CK(cub::DeviceScan::ExclusiveSum(scan_tmp, tb, mcnt, moff, nb, st));
+        LAUNCHED();
+        int64_t last[2];
+        int herr = 0;
+        CK(cudaMemcpyAsync(&last[0], moff + nb - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&last[1], mcnt + nb - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr) fail(SCMC_ERR_LIMIT, "a path exceeded max_events_per_path");
+        const int64_t n_multi = last[0] + last[1];
+        if (n_multi > mcap) {
+            if (nb == 1) fail(SCMC_ERR_INVALID, "scmc_field_noalloc: one path has more events than the fixed scratch holds");
+            batch = std::max<int64_t>(1, nb / 2);
+            continue;  // re-walk a smaller batch (Philox regenerates the same paths)
+        }
+        CK(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), st));
+        walk_record_kernel<DIM><<<grid, 128, 0, st>>>(W, moff, S, scap, Mr, mcap, ctr + 1);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        accumulate(true, nb);
+        accumulate(false, n_multi);
+        done += nb;
+    }
+    const double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
+    const double norm = m > 0 ? std::sqrt(1.0 / m * volume * a->sigt) : 0.0;
+    const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1024));
+    field_finalize_kernel<DIM, AccT><<<fgrid, 256, 0, st>>>(Q, Us, Um, norm, d_u);
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
+}  // namespace
+
+extern "C" int scmc_field_noalloc(const scmc_mc_args *args, double *d_u, void *stream)
+{
+    return guarded([&] {
+        if (!d_u) fail(SCMC_ERR_INVALID, "null output");
+        validate(args);
+        if (args->nv * args->nl > 65536)
+            fail(SCMC_ERR_INVALID, "scmc_field_noalloc: nv*nl is limited to 65536 by its fixed scratch");
+        int ndev = 0, major = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(SCMC_ERR_NODEVICE, "no CUDA device visible");
+        if (args->device < 0 || args->device >= ndev) fail(SCMC_ERR_INVALID, "invalid device ordinal");
+        CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, args->device));
+        if (major < 10) fail(SCMC_ERR_NODEVICE, "an sm_100 (Blackwell) device is required");
+        CK(cudaSetDevice(args->device));
+        std::lock_guard<std::mutex> lk(g_scratch_mu_call());
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        double2 *u = reinterpret_cast<double2 *>(d_u);
+        if (args->dim == 3) {
+            if (args->precision == SCMC_PREC_FP64) field_noalloc_run<3, P64, double>(args, u, st);
+            else if (args->precision == SCMC_PREC_FP32) field_noalloc_run<3, P32, float>(args, u, st);
+            else field_noalloc_run<3, PMIX, double>(args, u, st);
+        } else {
+            if (args->precision == SCMC_PREC_FP64) field_noalloc_run<2, P64, double>(args, u, st);
+            else if (args->precision == SCMC_PREC_FP32) field_noalloc_run<2, P32, float>(args, u, st);
+            else field_noalloc_run<2, PMIX, double>(args, u, st);
+        }
+        CK(cudaStreamSynchronize(st));
+    });
+}
