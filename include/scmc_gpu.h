@@ -183,6 +183,19 @@ int scmc_export_records(const scmc_mc_args *args, int32_t want_phase, int64_t ca
 int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, double *out);
 
 /* ---------------------------------------------------------------------------
+ * u = MCfieldFourierQuad(sigt, albedo, box_min, box_max, l, v_max, v_stp,
+ *                        maxItr, lambda, doCBS, smpFlg, lmean0, vsign)
+ *                                                 (MCfieldFourierQuad.m:1)
+ * u: nv0 x nv0 x nl complex interleaved, nv0 = length(-v_max:v_stp:v_max)
+ * (scmc_fq_grid_size).  Lights are 3 x nl directions.  The reference's FFT
+ * needs integer padding (odd nv0); for even nv0 the same centred-DFT formula
+ * is evaluated with half-integer offsets.
+ * ------------------------------------------------------------------------- */
+int scmc_fq_grid_size(double v_max, double v_stp, int64_t *nv0);
+int scmc_field_fourier_quad(const scmc_fq_args *args, double *u);
+int scmc_field_fourier_quad_device(const scmc_fq_args *args, double *d_u, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Stage timing.  While enabled, every kernel launch of the walk, the row
  * generation, the contraction and the finalisation is bracketed by CUDA
  * events on the stream it runs on; scmc_profile_read resolves them.  The

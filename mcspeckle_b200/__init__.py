@@ -7,11 +7,12 @@ constructors, computed by libscmc_gpu.so (C ABI in include/scmc_gpu.h).
 from ._lib import ScmcError, launch_count
 from .interface import (HGScatter, boxArea, farFieldSource, invCDF, isotropicScatter, nearFieldSource,
                         tabulatedAmplitudeScatter)
+from .fourier_quad import MCfieldFourierQuad, fq_args
 from .mc import MCcov, MCfield, MatlabStyleError, export_records, mc_args, philox_stream, rng
 from .scmc_api import ScmcInputError, scmc
 
 __all__ = [
-    "scmc", "MCfield", "MCcov", "rng", "mc_args", "export_records", "philox_stream",
+    "scmc", "MCfield", "MCcov", "MCfieldFourierQuad", "fq_args", "rng", "mc_args", "export_records", "philox_stream",
     "boxArea", "farFieldSource", "nearFieldSource", "isotropicScatter", "HGScatter",
     "tabulatedAmplitudeScatter", "invCDF", "ScmcError", "ScmcInputError", "MatlabStyleError", "launch_count",
 ]

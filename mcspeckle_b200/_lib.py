@@ -59,10 +59,17 @@ def lib():
         L.scmc_cov_device.argtypes = [mp, C.c_void_p, C.c_void_p, C.c_void_p]
         L.scmc_export_records.argtypes = [mp, C.c_int32, C.c_int64, dp, dp, dp, dp, dp, dp, ip, lp, lp]
         L.scmc_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
+        fq = C.POINTER(_abi.FqArgs)
+        L.scmc_fq_grid_size.argtypes = [C.c_double, C.c_double, C.POINTER(C.c_int64)]
+        L.scmc_field_fourier_quad.argtypes = [fq, dp]
+        L.scmc_field_fourier_quad_device.argtypes = [fq, C.c_void_p, C.c_void_p]
+        L.scmc_field_noalloc.argtypes = [mp, C.c_void_p, C.c_void_p]
         L.scmc_profile_enable.argtypes = [C.c_int32]
         L.scmc_profile_read.argtypes = [C.POINTER(_abi.StageTimes), C.c_int32]
         for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",
-                     "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read"):
+                     "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read",
+                     "scmc_fq_grid_size", "scmc_field_fourier_quad", "scmc_field_fourier_quad_device",
+                     "scmc_field_noalloc"):
             getattr(L, name).restype = C.c_int
         _lib = L
         return _lib

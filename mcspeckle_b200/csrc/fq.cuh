@@ -1,0 +1,256 @@
+// fq.cuh - MCfieldFourierQuad on the GPU (MCfieldFourierQuad.m:77-303).
+//
+// The reference records every vertex of an isotropic walk, sorts vertices
+// by the depth of the view-side vertex, grids them per z plane on the
+// lateral pixel grid and takes fftshift(fft2(ifftshift(.))) per plane and
+// light, then flips, crops, multiplies by exp(zexp0 * tz) and sums planes.
+// That FFT is the centred DFT
+//     X[q] = sum_p x[p] exp(-2 pi i (q-c)(p-c)/M),   c = floor(M/2),
+// evaluated only at the cropped, flipped outputs; here it is evaluated
+// directly for each vertex: output (r1, r2) of plane P receives
+//     c_e * T[r1][p1_e] * T[r2][p2_e],   T[r][p] = exp(-2 pi i m'(r) P(p) / M)
+// with the same pixel indices p1, p2 (rounded positions) and bin indices
+// m'(r) as the reference.  Vertices are bucketed by plane (counting sort),
+// each CTA owns a 32 x 32 output tile of one light and one plane, stages the
+// twiddle columns of a sub-batch of vertices in shared memory, and at the
+// plane's end multiplies by exp(zexp0 * tz) before adding into the FP64 sum.
+#pragma once
+
+#include "accum.cuh"
+
+namespace scmc {
+
+struct FqParams {
+    int nv0, nx, nz, nl, cbs;
+    double box_stp, gx1, gy1;
+    double kw;             // 2 pi / lambda
+    double sigt_half;
+    double bmin_z, bmax_z;
+    double l_diratt, l_idiratt;
+    const double *gz;      // nz plane boundaries
+    const double *l;       // [nl][3]
+};
+
+// One entry per (vertex, pass): pass 0 views from the first scatterer and
+// lights from the vertex (MCfieldFourierQuad.m:224-232 tt = 1), pass 1 the
+// reverse (tt = 2, CBS).
+struct FqEntry {
+    double xl[3];     // light-side position
+    double2 c0;       // pxL * exp(-i k (tz - zv)), light independent
+    int p1, p2;       // 0-based pixel indices of the view-side position
+    int plane;
+};
+
+__device__ __forceinline__ double fq_mround(double x) { return x < 0 ? -floor(-x + 0.5) : floor(x + 0.5); }
+
+// Plane of a view-side depth: plane j holds gz[j] <= z < gz[j+1]; depths at
+// or beyond the last boundary are in no plane (the reference's scan never
+// reaches them).
+__device__ __forceinline__ int fq_plane(const FqParams &F, double z)
+{
+    int lo = 0, hi = F.nz - 1;  // find the first boundary index b in [1, nz-1] with z < gz[b]
+    if (!(z < F.gz[F.nz - 1])) return -1;
+    lo = 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (z < F.gz[mid]) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo - 1;
+}
+
+// Build the entries of a batch: singles are paths 0..n_paths-1, multis
+// follow.  counts[plane] is incremented for the counting sort.
+__global__ void fq_entries_kernel(FqParams F, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_paths,
+                                  int64_t n_multi, FqEntry *__restrict__ out, int *__restrict__ counts)
+{
+    const int64_t nvert = n_paths + n_multi;
+    const int passes = F.cbs ? 2 : 1;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nvert * passes;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int pass = (int)(k / nvert);
+        const int64_t v = k % nvert;
+        double x[3], x1[3], wpx, xi;
+        int pl;
+        if (v < n_paths) {
+            for (int d = 0; d < 3; ++d) x1[d] = x[d] = S.x1[d * scap + v];
+            wpx = S.wpx[v];
+            xi = S.xi[v];
+            pl = 1;
+        } else {
+            const int64_t e = v - n_paths;
+            const int64_t p = M.path[e];
+            for (int d = 0; d < 3; ++d) {
+                x[d] = M.x[d * mcap + e];
+                x1[d] = S.x1[d * scap + p];
+            }
+            wpx = M.wpx[e];
+            xi = M.xi[e];
+            pl = M.plen[e];
+        }
+        const double *xv = pass == 0 ? x1 : x;
+        const double *xl = pass == 0 ? x : x1;
+        FqEntry en;
+        for (int d = 0; d < 3; ++d) en.xl[d] = xl[d];
+        en.plane = fq_plane(F, xv[2]);
+        int p1 = (int)fq_mround((xv[0] - F.gx1) / F.box_stp);
+        int p2 = (int)fq_mround((xv[1] - F.gy1) / F.box_stp);
+        en.p1 = min(max(p1, 0), F.nx - 1);
+        en.p2 = min(max(p2, 0), F.nx - 1);
+        // pxL = sqrt(w/px) e^{2 pi i xi}, /sqrt(2) with CBS after the first event (lines 181-182)
+        double s = sqrt(wpx);
+        if (F.cbs && pl > 1) s = 1.0 / sqrt(2.0) * s;
+        double sp, cp;
+        sincos(2.0 * SCMC_PI * xi, &sp, &cp);
+        double tz = 0.0;
+        if (en.plane >= 0) tz = (F.gz[en.plane] + F.gz[en.plane + 1]) / 2;
+        double sd, cd;
+        sincos(-F.kw * (-xv[2] + tz), &sd, &cd);  // exp(-2 pi i/lambda (-z + tz)) (line 272)
+        en.c0 = make_double2(s * (cp * cd - sp * sd), s * (cp * sd + sp * cd));
+        out[k] = en;
+        if (en.plane >= 0) atomicAdd(&counts[en.plane], 1);
+    }
+}
+
+__global__ void fq_scatter_kernel(const FqEntry *__restrict__ in, int64_t n, const int *__restrict__ offsets,
+                                  int *__restrict__ cursor, FqEntry *__restrict__ out)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const FqEntry e = in[k];
+        if (e.plane < 0) continue;
+        const int pos = offsets[e.plane] + atomicAdd(&cursor[e.plane], 1);
+        out[pos] = e;
+    }
+}
+
+// T[r][p] = exp(-2 pi i m'(r) P(p) / M): the centred DFT's twiddles at the
+// reference's cropped, flipped bins (see the file comment).
+template <typename C>
+__global__ void fq_twiddle_kernel(int nv0, int nx, double M, double nx_pad, double nv_pad, C *__restrict__ T)
+{
+    const double c = floor(M / 2);
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)nv0 * nx;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(k / nx), p = (int)(k % nx);
+        const double m = (M - 1 - ((double)r + nv_pad)) - c;
+        const double P = ((double)p + nx_pad) - c;
+        const double t = fmod(m * P, M);
+        double s, co;
+        sincos(-2.0 * SCMC_PI * t / M, &s, &co);
+        T[k] = to_c<C>(make_double2(co, s));
+    }
+}
+
+constexpr int kFqTile = 32;
+constexpr int kFqEB = 16;
+
+// One CTA: a 32 x 32 tile of (r1, r2) for light j and plane planes[blockIdx.y].
+template <int POL, typename AccT>
+__global__ void __launch_bounds__(256)
+fq_accum_kernel(FqParams F, const FqEntry *__restrict__ E, const int *__restrict__ offsets,
+                const int *__restrict__ planes, const typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type *__restrict__ T,
+                const double2 *__restrict__ zexp0, AccT *__restrict__ U)
+{
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using C = typename cplx_t<R>::type;
+    __shared__ C t1[kFqEB][kFqTile];
+    __shared__ C t2[kFqEB][kFqTile];
+    __shared__ C sc[kFqEB];
+    const int nvt = (F.nv0 + kFqTile - 1) / kFqTile;
+    const int tile = blockIdx.x % (nvt * nvt);
+    const int j = blockIdx.x / (nvt * nvt);
+    const int r10 = (tile % nvt) * kFqTile, r20 = (tile / nvt) * kFqTile;
+    const int plane = planes[blockIdx.y];
+    const int e0 = offsets[plane], e1 = offsets[plane + 1];
+    const double *lj = F.l + 3 * j;
+    C acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = C{};
+    for (int eb = e0; eb < e1; eb += kFqEB) {
+        const int ne = min(kFqEB, e1 - eb);
+        // per entry: the light factor exp(i k l.xl - sigt/2 * slab attenuation) (line 272)
+        if (threadIdx.x < ne) {
+            const FqEntry en = E[eb + threadIdx.x];
+            const double ph = F.kw * (lj[0] * en.xl[0] + lj[1] * en.xl[1] + lj[2] * en.xl[2]);
+            const double at = F.sigt_half * ((en.xl[2] - F.bmin_z) * F.l_diratt + (F.bmax_z - en.xl[2]) * F.l_idiratt);
+            C lf;
+            if constexpr (POL == P64) {
+                double s, co;
+                sincos(ph, &s, &co);
+                const double a = exp(-at);
+                lf = make_double2(a * co, a * s);
+            } else {
+                float s, co;
+                sincosf((float)reduce_2pi(ph), &s, &co);
+                const float a = expf(-(float)at);
+                lf = make_float2(a * co, a * s);
+            }
+            sc[threadIdx.x] = cmul(to_c<C>(en.c0), lf);
+        }
+        for (int idx = threadIdx.x; idx < kFqEB * 2 * kFqTile; idx += blockDim.x) {
+            const int k = idx / (2 * kFqTile), m = idx % (2 * kFqTile);
+            C v = C{};
+            if (k < ne) {
+                const FqEntry &en = E[eb + k];
+                if (m < kFqTile) {
+                    const int r = r10 + m;
+                    if (r < F.nv0) v = T[(int64_t)r * F.nx + en.p1];
+                } else {
+                    const int r = r20 + (m - kFqTile);
+                    if (r < F.nv0) v = T[(int64_t)r * F.nx + en.p2];
+                }
+            }
+            if (m < kFqTile) t1[k][m] = v;
+            else t2[k][m - kFqTile] = v;
+        }
+        __syncthreads();
+        for (int k = 0; k < ne; ++k) {
+            const C s = sc[k];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int o = threadIdx.x + 256 * q;
+                const int a = o % kFqTile, b = o / kFqTile;
+                const C w = cmul(s, t2[k][b]);
+                const C v = cmul(w, t1[k][a]);
+                acc[q].x += v.x;
+                acc[q].y += v.y;
+            }
+        }
+        __syncthreads();
+    }
+    const int nv0 = F.nv0;
+    const double tz = (F.gz[plane] + F.gz[plane + 1]) / 2;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int o = threadIdx.x + 256 * q;
+        const int r1 = r10 + o % kFqTile, r2 = r20 + o / kFqTile;
+        if (r1 < nv0 && r2 < nv0) {
+            const double2 z = zexp0[r1 + (int64_t)nv0 * r2];
+            // exp(zexp0 * tz) (line 281)
+            const double mag = exp(z.x * tz);
+            double s, co;
+            sincos(z.y * tz, &s, &co);
+            const double2 f = make_double2(mag * co, mag * s);
+            const double2 a = make_double2((double)acc[q].x, (double)acc[q].y);
+            const double2 v = cmul(f, a);
+            const int64_t off = 2 * ((int64_t)r1 + (int64_t)nv0 * r2 + (int64_t)nv0 * nv0 * j);
+            atomicAdd(&U[off], (AccT)v.x);
+            atomicAdd(&U[off + 1], (AccT)v.y);
+        }
+    }
+}
+
+template <typename AccT>
+__global__ void fq_finalize_kernel(const AccT *__restrict__ U, const double2 *__restrict__ boxexp0, int nv0, int nl,
+                                   double norm, double2 *__restrict__ u)
+{
+    const int64_t n = (int64_t)nv0 * nv0 * nl;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double2 b = boxexp0[k % ((int64_t)nv0 * nv0)];
+        const double2 a = make_double2((double)U[2 * k], (double)U[2 * k + 1]);
+        const double2 v = cmul(a, b);
+        u[k] = make_double2(norm * v.x, norm * v.y);
+    }
+}
+
+}  // namespace scmc

@@ -15,6 +15,7 @@
 #include "../../include/scmc_gpu.h"
 #include "accum.cuh"
 #include "herk_tc.cuh"
+#include "fq.cuh"
 
 using namespace scmc;
 
@@ -171,6 +172,7 @@ struct Ctx {
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
     DevBuf acc_s, acc_m, rows, tiles, tc_a, out0, out1;
+    DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
 };
 
@@ -800,6 +802,234 @@ __global__ void philox_stream_kernel(uint64_t seed, uint64_t path, int tag, int6
     for (int64_t i = 0; i < n; ++i) out[i] = tag ? r.randn() : r.rand();
 }
 
+// ---------------------------------------------------------------------------
+// MCfieldFourierQuad
+// ---------------------------------------------------------------------------
+int64_t colon_count(double a, double st, double b)
+{
+    if (st == 0 || (st > 0 && a > b) || (st < 0 && a < b)) return 0;
+    double q = (b - a) / st;
+    return (int64_t)std::floor(q + 1e-10 * std::fmax(1.0, std::fabs(q))) + 1;
+}
+
+void validate_fq(const scmc_fq_args *a)
+{
+    if (!a) fail(SCMC_ERR_INVALID, "null arguments");
+    for (int k = 0; k < 3; ++k)
+        if (!(a->box_max[k] >= a->box_min[k])) fail(SCMC_ERR_INVALID, "Invalid box size");
+    if (a->nl < 1 || !a->l) fail(SCMC_ERR_INVALID, "Invalid light source input");
+    if (!(a->sigt > 0) || !(a->lambda > 0)) fail(SCMC_ERR_INVALID, "sigt and lambda must be positive");
+    if (!(a->v_stp > 0) || !(a->v_max >= 0)) fail(SCMC_ERR_INVALID, "v_max must be >= 0 and v_stp > 0");
+    if (a->max_itr < 0) fail(SCMC_ERR_INVALID, "Invalid photons number");
+    if (a->smp_flg != 1 && a->smp_flg != 2) fail(SCMC_ERR_INVALID, "smpFlg must be 1 or 2");
+    if (a->precision < 0 || a->precision > 3) fail(SCMC_ERR_INVALID, "invalid precision mode");
+    if (colon_count(-a->v_max, a->v_stp, a->v_max) > 4096) fail(SCMC_ERR_INVALID, "angular grid longer than 4096");
+}
+
+template <int POL, typename AccT>
+void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
+{
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using Cx = typename cplx_t<R>::type;
+    // geometry, as MCfieldFourierQuad.m:59-138
+    const double lambda = a->lambda, sigt = a->sigt;
+    double bmin[3], bmax[3], bw[3];
+    for (int k = 0; k < 3; ++k) {
+        bmin[k] = a->box_min[k];
+        bmax[k] = a->box_max[k];
+        bw[k] = bmax[k] - bmin[k];
+    }
+    double unmeanl[3] = {0, 0, 1};
+    if (a->has_lmean0)
+        for (int k = 0; k < 3; ++k) unmeanl[k] = a->lmean0[k];
+    const int64_t Nv = colon_count(-a->v_max, a->v_stp, a->v_max);
+    const double box_stp = lambda / (a->v_max * 2 + a->v_stp);
+    const int64_t Nx = (int64_t)std::ceil(bw[0] / box_stp / 2) * 2 + 1;
+    if (Nx > (int64_t)1 << 20) fail(SCMC_ERR_INVALID, "lateral pixel grid too large");
+    const double box_w_n = Nx * box_stp, grow = (box_w_n - bw[0]) / 2;
+    for (int k = 0; k < 2; ++k) {
+        bmin[k] -= grow;
+        bmax[k] += grow;
+        bw[k] = box_w_n;
+    }
+    const double nx_pad = std::fmax((double)(Nv - Nx) / 2, 0.0), nv_pad = std::fmax((double)(Nx - Nv) / 2, 0.0);
+    const double M = (double)Nx + 2 * nx_pad;
+    std::vector<double> theta(Nv);
+    for (int64_t k = 0; k < Nv; ++k) theta[k] = -a->v_max + (double)k * a->v_stp;
+    std::vector<double2> zexp0(Nv * Nv), boxexp0(Nv * Nv);
+    double maxdiff = -INFINITY;
+    std::vector<double> vzr(Nv * Nv), vzi(Nv * Nv);
+    for (int64_t j = 0; j < Nv; ++j)
+        for (int64_t i = 0; i < Nv; ++i) {
+            const double vx = -theta[i], vy = -theta[j], r = 1 - vx * vx - vy * vy;
+            double zr = r >= 0 ? std::sqrt(r) : 0.0, zi = r >= 0 ? 0.0 : std::sqrt(-r);
+            zr *= a->vsign;
+            zi *= a->vsign;
+            vzr[i + Nv * j] = zr;
+            vzi[i + Nv * j] = zi;
+            maxdiff = std::fmax(maxdiff, 1 - std::hypot(zr, zi));
+        }
+    double z_bin = lambda / maxdiff / 5;
+    z_bin = z_bin / 2;
+    const int64_t ng = colon_count(bmin[2], z_bin, bmax[2]);
+    const int64_t Nz = ng + 1;
+    if (Nz > 1000000) fail(SCMC_ERR_INVALID, "too many z planes");
+    std::vector<double> gz(Nz);
+    for (int64_t k = 0; k < ng; ++k) gz[k] = bmin[2] + (double)k * z_bin;
+    gz[ng] = bmax[2];
+    const double twopi = 2 * SCMC_PI;
+    for (int64_t q = 0; q < Nv * Nv; ++q) {
+        const double zr = vzr[q], zi = vzi[q], av = std::hypot(zr, zi);
+        const double dir = zr < 0 ? 1.0 / av : 0.0, idir = zr > 0 ? 1.0 / av : 0.0;
+        // zexp0 = -2 pi i/lambda vz vsign - sigt/2 (diratt - idiratt)
+        zexp0[q] = make_double2(twopi / lambda * zi * a->vsign - sigt / 2 * (dir - idir), -twopi / lambda * zr * a->vsign);
+        const double amp = std::exp(-sigt / 2 * (-bmin[2] * dir + bmax[2] * idir));
+        const double sel = (zr < 0 ? -bmin[2] : 0.0) + (zr > 0 ? bmax[2] : 0.0);
+        // exp(2 pi i/lambda * sel * vz)
+        const double er = -twopi / lambda * sel * zi, ei = twopi / lambda * sel * zr;
+        const double m = amp * std::exp(er);
+        boxexp0[q] = make_double2(m * std::cos(ei), m * std::sin(ei));
+    }
+    const double l_end = a->l[3 * (a->nl - 1) + 2];
+
+    FqParams F{};
+    F.nv0 = (int)Nv;
+    F.nx = (int)Nx;
+    F.nz = (int)Nz;
+    F.nl = (int)a->nl;
+    F.cbs = a->do_cbs;
+    F.box_stp = box_stp;
+    F.gx1 = bmin[0] + box_stp / 2;
+    F.gy1 = bmin[1] + box_stp / 2;
+    F.kw = twopi / lambda;
+    F.sigt_half = sigt / 2;
+    F.bmin_z = bmin[2];
+    F.bmax_z = bmax[2];
+    F.l_diratt = l_end > 0 ? 1.0 / std::fabs(l_end) : 0.0;
+    F.l_idiratt = l_end < 0 ? 1.0 / std::fabs(l_end) : 0.0;
+    double *dgz = reinterpret_cast<double *>(c.fq_gz.ensure(Nz * sizeof(double)));
+    double2 *dz = reinterpret_cast<double2 *>(c.fq_zexp.ensure(Nv * Nv * sizeof(double2)));
+    double2 *db = reinterpret_cast<double2 *>(c.fq_box.ensure(Nv * Nv * sizeof(double2)));
+    double *dl = reinterpret_cast<double *>(c.dirs_l.ensure(3 * a->nl * sizeof(double)));
+    Cx *T = reinterpret_cast<Cx *>(c.fq_tw.ensure(Nv * Nx * sizeof(Cx)));
+    CK(cudaMemcpyAsync(dgz, gz.data(), Nz * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dz, zexp0.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(db, boxexp0.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dl, a->l, 3 * a->nl * sizeof(double), cudaMemcpyHostToDevice, st));
+    F.gz = dgz;
+    F.l = dl;
+    {
+        StageScope sc(ST_ROWS, st);
+        fq_twiddle_kernel<Cx><<<std::max<int64_t>(1, std::min<int64_t>((Nv * Nx + 255) / 256, 4096)), 256, 0, st>>>(
+            (int)Nv, (int)Nx, M, nx_pad, nv_pad, T);
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+    // the walk: isotropic, phase per event, padded box (lines 146-213)
+    WalkParams W{};
+    W.dim = 3;
+    W.smp_flg = a->smp_flg;
+    W.has_pf0 = 0;
+    W.want_phase = 1;
+    W.sigt = sigt;
+    W.albedo = a->albedo;
+    double nrm = 0;
+    for (int k = 0; k < 3; ++k) {
+        W.box_min[k] = bmin[k];
+        W.box_max[k] = bmax[k];
+        W.box_w[k] = bw[k];
+        W.unmeanl[k] = unmeanl[k];
+        nrm += unmeanl[k] * unmeanl[k];
+    }
+    nrm = std::sqrt(nrm);
+    for (int k = 0; k < 3; ++k) W.meanl[k] = unmeanl[k] / nrm;
+    W.pf.sct_type = SCMC_SCT_ISOTROPIC;
+    W.pf0 = W.pf;
+    W.key0 = (uint32_t)a->seed;
+    W.key1 = (uint32_t)(a->seed >> 32);
+    const int64_t nout = Nv * Nv * a->nl;
+    AccT *U = reinterpret_cast<AccT *>(c.acc_s.ensure(2 * nout * sizeof(AccT)));
+    CK(cudaMemsetAsync(U, 0, 2 * nout * sizeof(AccT), st));
+    int *counts = reinterpret_cast<int *>(c.fq_counts.ensure((Nz + 1) * sizeof(int)));
+    int *offsets = reinterpret_cast<int *>(c.fq_offsets.ensure((Nz + 1) * sizeof(int)));
+    int *cursor = reinterpret_cast<int *>(c.fq_cursor.ensure((Nz + 1) * sizeof(int)));
+    int *planes = reinterpret_cast<int *>(c.fq_planes.ensure((Nz + 1) * sizeof(int)));
+    std::vector<int> hcounts(Nz + 1);
+    std::vector<int> hplanes;
+    const int sms = sm_count(c.device);
+    int64_t total_vert = 0;
+    const int passes = a->do_cbs ? 2 : 1;
+    for (int64_t done = 0; done < a->max_itr;) {
+        const int64_t nb = std::min<int64_t>(a->max_itr - done, (int64_t)1 << 18);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        const int64_t nvert = B.n_paths + B.n_multi;
+        total_vert += nvert;
+        const int64_t nent = nvert * passes;
+        if (nent > INT32_MAX) fail(SCMC_ERR_INVALID, "batch too large");
+        FqEntry *Ein = reinterpret_cast<FqEntry *>(c.rows.ensure(2 * nent * sizeof(FqEntry)));
+        FqEntry *Es = Ein + nent;
+        CK(cudaMemsetAsync(counts, 0, (Nz + 1) * sizeof(int), st));
+        {
+            StageScope sc(ST_ROWS, st);
+            fq_entries_kernel<<<(int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16), 256, 0, st>>>(
+                F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein, counts);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        CK(cudaMemcpyAsync(hcounts.data(), counts, Nz * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::vector<int> hoff(Nz + 1, 0);
+        hplanes.clear();
+        for (int64_t k = 0; k < Nz; ++k) {
+            hoff[k + 1] = hoff[k] + hcounts[k];
+            if (hcounts[k] > 0 && k < Nz - 1) hplanes.push_back((int)k);
+        }
+        if (hplanes.empty()) {
+            done += nb;
+            continue;
+        }
+        CK(cudaMemcpyAsync(offsets, hoff.data(), (Nz + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(planes, hplanes.data(), hplanes.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(cursor, 0, (Nz + 1) * sizeof(int), st));
+        {
+            StageScope sc(ST_ROWS, st);
+            fq_scatter_kernel<<<(int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16), 256, 0, st>>>(
+                Ein, nent, offsets, cursor, Es);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
+        for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
+            const unsigned gy = (unsigned)std::min<size_t>(65535, hplanes.size() - p0);
+            dim3 grid((unsigned)(nvt * nvt * a->nl), gy);
+            StageScope sc(ST_CONTRACT, st);
+            fq_accum_kernel<POL, AccT><<<grid, 256, 0, st>>>(F, Es, offsets, planes + p0, T, dz, U);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        CK(cudaStreamSynchronize(st));  // host vectors above are reused next batch
+        done += nb;
+    }
+    const double V = bw[0] * bw[1] * bw[2];
+    const double norm = total_vert > 0 ? std::sqrt(1.0 / (double)total_vert * V * sigt) : 0.0;  // lines 214, 302-303
+    StageScope fin(ST_FINAL, st);
+    fq_finalize_kernel<AccT><<<(int)std::max<int64_t>(1, std::min<int64_t>((nout + 255) / 256, 4096)), 256, 0, st>>>(
+        U, db, (int)Nv, (int)a->nl, norm, d_u);
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
+void fq_device_locked(Ctx &c, const scmc_fq_args *a, double *d_u, cudaStream_t st)
+{
+    CK(cudaSetDevice(a->device));
+    double2 *u = reinterpret_cast<double2 *>(d_u);
+    if (a->precision == SCMC_PREC_FP64) fq_run<P64, double>(c, a, u, st);
+    else if (a->precision == SCMC_PREC_FP32) fq_run<P32, float>(c, a, u, st);
+    else fq_run<PMIX, double>(c, a, u, st);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -864,6 +1094,43 @@ int scmc_cov(const scmc_mc_args *args, double *Ms, double *Mm)
         cov_device_locked(c, args, d0, d1, 0);
         if (Ms) CK(cudaMemcpy(Ms, d0, bytes, cudaMemcpyDeviceToHost));
         if (Mm) CK(cudaMemcpy(Mm, d1, bytes, cudaMemcpyDeviceToHost));
+    });
+}
+
+int scmc_fq_grid_size(double v_max, double v_stp, int64_t *nv0)
+{
+    return guarded([&] {
+        if (!nv0) fail(SCMC_ERR_INVALID, "null output");
+        if (!(v_stp > 0) || !(v_max >= 0)) fail(SCMC_ERR_INVALID, "v_max must be >= 0 and v_stp > 0");
+        *nv0 = colon_count(-v_max, v_stp, v_max);
+    });
+}
+
+int scmc_field_fourier_quad_device(const scmc_fq_args *args, double *d_u, void *stream)
+{
+    return guarded([&] {
+        validate_fq(args);
+        if (!d_u) fail(SCMC_ERR_INVALID, "null output");
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        fq_device_locked(c, args, d_u, st);
+        CK(cudaStreamSynchronize(st));
+    });
+}
+
+int scmc_field_fourier_quad(const scmc_fq_args *args, double *u)
+{
+    return guarded([&] {
+        validate_fq(args);
+        if (!u) fail(SCMC_ERR_INVALID, "null output");
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const int64_t nv0 = colon_count(-args->v_max, args->v_stp, args->v_max);
+        const size_t bytes = (size_t)nv0 * nv0 * args->nl * 2 * sizeof(double);
+        double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
+        fq_device_locked(c, args, d, 0);
+        CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
     });
 }
 

@@ -56,6 +56,7 @@ def lib():
         _lib.oracle_field_from_records.argtypes = [C.c_void_p, C.c_int64, dp, dp, dp, dp, dp, dp, ip, dp]
         _lib.oracle_cov_from_records.argtypes = [C.c_void_p, C.c_int64, dp, dp, dp, dp, dp, ip,
                                                  dp, dp, C.c_int]
+        _lib.oracle_field_fourier_quad.argtypes = [C.POINTER(FqArgs), C.POINTER(RngSpec), dp]
         _lib.oracle_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                               C.POINTER(C.c_uint32)]
         _lib.oracle_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
@@ -190,3 +191,10 @@ def philox_stream(seed, path, tag, n):
     out = np.zeros(n)
     lib().oracle_philox_stream(seed, path, tag, n, _dp(out))
     return out
+
+
+def field_fourier_quad(fa: FqArgs, rng: Rng, nv0: int) -> np.ndarray:
+    """MCfieldFourierQuad on the oracle: nv0 x nv0 x nl complex."""
+    u = np.zeros(2 * nv0 * nv0 * fa.nl)
+    _check(lib().oracle_field_fourier_quad(C.byref(fa), C.byref(rng.spec), _dp(u)), "oracle_field_fourier_quad")
+    return u.view(np.complex128).reshape(nv0, nv0, fa.nl, order="F")

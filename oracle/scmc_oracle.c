@@ -715,3 +715,67 @@ int oracle_cov_from_records(const scmc_mc_args *a, int64_t n, const double *x,
     cov_normalise(a, (cplx *)Ms, (cplx *)Mm);
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* MCfieldFourierQuad.m:154-213: the isotropic walk recording every vertex  */
+/* ------------------------------------------------------------------------ */
+int oracle_internal_fq_walk(const scmc_fq_args *a, const double *bmin, const double *bmax,
+                            const double *unmeanl, oracle_rng_spec *rs, int64_t cap,
+                            double *xL, double *x1L, double *pxr, double *pxi, int64_t *n_vert)
+{
+    rng_t r;
+    rng_init(&r, rs, a->seed);
+    const int dim = 3;
+    double bw[3];
+    for (int k = 0; k < 3; ++k) bw[k] = bmax[k] - bmin[k];
+    int64_t c = 0;
+    int rc = 0;
+    for (int64_t itr = 0; itr < a->max_itr; ++itr) {
+        if (r.mode == ORACLE_RNG_PHILOX) rng_set_path(&r, a->path_offset + (uint64_t)itr);
+        double x[3], x1[3], w[3], px;
+        if (a->smp_flg == 1) {
+            for (int k = 0; k < dim; ++k) x[k] = rand_u(&r) * bw[k] + bmin[k];
+            px = 1.0;
+        } else {
+            exp_smp_x(bmin, bmax, unmeanl, a->sigt, dim, x, &px, &r);
+        }
+        memcpy(x1, x, sizeof x);
+        randn_dir(dim, w, &r);
+        double weight = a->albedo;
+        int p_len = 0;
+        for (;;) {
+            ++p_len;
+            if (c < cap) {
+                for (int k = 0; k < 3; ++k) { xL[3 * c + k] = x[k]; x1L[3 * c + k] = x1[k]; }
+                double s = sqrt(weight / px);
+                double ph = 2 * M_PI * rand_u(&r);
+                double re = s * cos(ph), im = s * sin(ph);
+                if (a->do_cbs && p_len > 1) { re = 1 / sqrt(2.0) * re; im = 1 / sqrt(2.0) * im; }
+                pxr[c] = re;
+                pxi[c] = im;
+            } else {
+                (void)rand_u(&r);
+            }
+            ++c;
+            double d = -log(-rand_u(&r) + 1.0) / a->sigt;
+            int out = 0;
+            for (int k = 0; k < dim; ++k) {
+                x[k] = x[k] + d * w[k];
+                if (x[k] > bmax[k] || x[k] < bmin[k]) out = 1;
+            }
+            if (out) break;
+            if (weight < KILL_THR) {
+                if (rand_u(&r) > a->albedo) break;
+            } else {
+                weight = weight * a->albedo;
+            }
+            randn_dir(dim, w, &r);
+        }
+        if (r.exhausted) { rc = -1; break; }
+    }
+    rs->used_u = r.ui;
+    rs->used_n = r.ni;
+    *n_vert = c;
+    if (!rc && c > cap) rc = -2;
+    return rc;
+}

@@ -170,6 +170,31 @@ class Gen:
                 "opts": [[k, v] for k, v in opts], "error": err}
         self.save(name, "scmc", meta, arrays)
 
+    # -- MCfieldFourierQuad ------------------------------------------------------
+    def fq_case(self, name, seed, *, sigt, albedo, box_min, box_max, l, v_max, v_stp, max_itr, lam, cbs,
+                smp_flg, lmean0, vsign):
+        it, ut, nt = self.interp(seed)
+        args = [M(float(sigt)), M(float(albedo)), M(np.reshape(box_min, (-1, 1)).astype(float)),
+                M(np.reshape(box_max, (-1, 1)).astype(float)), M(np.asarray(l, float)), M(float(v_max)),
+                M(float(v_stp)), M(float(max_itr)), M(float(lam)), M(bool(cbs)), M(float(smp_flg)),
+                M(np.zeros((0, 0))) if lmean0 is None else M(np.reshape(lmean0, (-1, 1)).astype(float)),
+                M(float(vsign))]
+        err = None
+        arrays = {}
+        try:
+            u = it.call("MCfieldFourierQuad", args, 1)[0]
+            arrays["u"] = np.asarray(u, dtype=complex)
+        except ml.MatlabError as e:
+            err = str(e)
+        arrays.update({"utape": ut[:it.ui], "ntape": nt[:it.ni], "box_min": np.asarray(box_min, float),
+                       "box_max": np.asarray(box_max, float), "l": np.asarray(l, float)})
+        if lmean0 is not None:
+            arrays["lmean0"] = np.asarray(lmean0, float)
+        meta = {"sigt": sigt, "albedo": albedo, "v_max": v_max, "v_stp": v_stp, "max_itr": max_itr, "lambda": lam,
+                "cbs": bool(cbs), "smp_flg": smp_flg, "vsign": vsign, "has_lmean0": lmean0 is not None,
+                "error": err}
+        self.save(name, "fourier_quad", meta, arrays)
+
     def error_case(self, name, func, args_py, expect_contains=None):
         it, _, _ = self.interp(0)
         try:
@@ -228,6 +253,18 @@ def main(ref):
                   is_ff_l=1, is_ff_v=1, cbs=1, smp_flg=2, sct_type=2, ampfunc=tab2d)
     g.mc_case("field_3d_hg_lmean0", "MCfield", 110, **common, **box3, l=L3, v=V3r, is_ff_l=1, is_ff_v=1,
               cbs=1, smp_flg=2, sct_type=3, ampfunc=0.5, ampfunc0=0.2, lmean0=[0.1, 0.0, 1.0])
+
+    print("MCfieldFourierQuad")
+    Lq = cap_dirs(2, 8, +1, 21)
+    g.fq_case("fq_wide_box_cbs_exp", 301, sigt=0.1, albedo=0.9, box_min=[-60, -60, 0], box_max=[60, 60, 20], l=Lq,
+              v_max=0.2, v_stp=0.01, max_itr=25, lam=1.0, cbs=1, smp_flg=2, lmean0=None, vsign=-1)
+    g.fq_case("fq_narrow_box_nocbs_unif", 302, sigt=0.15, albedo=0.8, box_min=[-10, -10, 0], box_max=[10, 10, 8],
+              l=Lq, v_max=0.2, v_stp=0.01, max_itr=25, lam=1.0, cbs=0, smp_flg=1, lmean0=[0.0, 0.1, 1.0], vsign=1)
+    g.fq_case("fq_narrow_box_cbs_refl", 303, sigt=0.12, albedo=1.0, box_min=[-8, -8, 0], box_max=[8, 8, 10],
+              l=cap_dirs(3, 5, +1, 22), v_max=0.3, v_stp=0.02, max_itr=20, lam=0.8, cbs=1, smp_flg=2, lmean0=None,
+              vsign=-1)
+    g.fq_case("fq_even_grid_errors", 304, sigt=0.1, albedo=0.9, box_min=[-10, -10, 0], box_max=[10, 10, 8], l=Lq,
+              v_max=0.195, v_stp=0.01, max_itr=5, lam=1.0, cbs=1, smp_flg=2, lmean0=None, vsign=-1)
 
     print("scmc.m")
     tgt3 = [1.0, 5.0, [0, 15], [-20, 20], [-20, 20]]

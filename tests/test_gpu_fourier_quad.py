@@ -1,0 +1,64 @@
+"""MCfieldFourierQuad on the GPU against the FP64 oracle (same Philox paths).
+
+The oracle restates MCfieldFourierQuad.m and is pinned to the reference by
+the golden fixtures (tests/test_oracle_golden.py); the GPU evaluates the
+same centred DFT per vertex instead of gridding + FFT.
+"""
+import numpy as np
+import pytest
+
+from cases import cap_dirs
+from mcspeckle_b200 import fourier_quad as FQ
+
+pytestmark = pytest.mark.gpu
+SEED = 4242
+
+
+def rel(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+FQ_CASES = {
+    # wide box: pixel grid longer than the angular grid (crop of the FFT)
+    "wide_cbs_exp": dict(sigt=0.1, albedo=0.9, box_min=[-60, -60, 0], box_max=[60, 60, 20], v_max=0.2, v_stp=0.01,
+                         lam=1.0, cbs=1, smp=2, lmean0=None, vsign=-1, n=400),
+    # narrow box: angular grid longer than the pixel grid (zero padding)
+    "narrow_nocbs_unif": dict(sigt=0.15, albedo=0.8, box_min=[-10, -10, 0], box_max=[10, 10, 8], v_max=0.2,
+                              v_stp=0.01, lam=1.0, cbs=0, smp=1, lmean0=[0.0, 0.1, 1.0], vsign=1, n=400),
+    # an even grid length (half-integer padding: the extension)
+    "even_grid": dict(sigt=0.1, albedo=0.9, box_min=[-10, -10, 0], box_max=[10, 10, 8], v_max=0.195, v_stp=0.01,
+                      lam=1.0, cbs=1, smp=2, lmean0=None, vsign=-1, n=300),
+    # evanescent corners of the grid (|v| > 1) and reflection
+    "wide_angles": dict(sigt=0.12, albedo=1.0, box_min=[-8, -8, 0], box_max=[8, 8, 10], v_max=0.9, v_stp=0.05,
+                        lam=0.8, cbs=1, smp=2, lmean0=None, vsign=-1, n=300),
+}
+
+
+def args_for(c, precision, seed=SEED):
+    L = cap_dirs(2, 8, +1, 21)
+    return FQ.fq_args(c["sigt"], c["albedo"], c["box_min"], c["box_max"], L, c["v_max"], c["v_stp"], c["n"],
+                      c["lam"], c["cbs"], c["smp"], c["lmean0"], c["vsign"], seed=seed, precision=precision)
+
+
+@pytest.mark.parametrize("name", list(FQ_CASES))
+def test_fourier_quad_fp64_matches_oracle(gpu, oracle_lib, name):
+    h = args_for(FQ_CASES[name], "fp64")
+    u = FQ.field_fourier_quad_from_args(h)
+    uo = oracle_lib.field_fourier_quad(h.args, oracle_lib.Rng.philox(), h.nv0)
+    assert u.shape == uo.shape
+    assert rel(u, uo) < 1e-10
+
+
+@pytest.mark.parametrize("name", list(FQ_CASES))
+def test_fourier_quad_mixed_close_to_fp64(gpu, name):
+    u64 = FQ.field_fourier_quad_from_args(args_for(FQ_CASES[name], "fp64"))
+    umx = FQ.field_fourier_quad_from_args(args_for(FQ_CASES[name], "mixed"))
+    assert rel(umx, u64) < 1e-3
+
+
+def test_fourier_quad_grid_size(gpu):
+    import ctypes
+    from mcspeckle_b200 import _lib
+    n = ctypes.c_int64()
+    _lib.check(_lib.lib().scmc_fq_grid_size(255 / 256, 1 / 128, ctypes.byref(n)))
+    assert n.value == 256 == FQ.grid_length(255 / 256, 1 / 128)
