@@ -161,6 +161,37 @@ int scmc_cov(const scmc_mc_args *args, double *Ms, double *Mm);
 int scmc_cov_device(const scmc_mc_args *args, double *d_Ms, double *d_Mm, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Heterogeneous (voxel) medium:
+ *   [Ms, Mm, mean1] = MCCovHetro(sigt, albedo, box_min, box_max, box_bin, l, v,
+ *        is_ff_l, is_ff_v, maxItr, lambda, doCBS, smpFlg, sct_type, ampfunc
+ *        [, ampfunc0 [, lrad]])                              (MCCovHetro.m:1)
+ *   u = MCsampleHetro(sigt, albedo, box_min, box_max, box_bin, l, v, is_ff_l,
+ *        is_ff_v, maxItr, lambda, doCBS, smpFlg, sct_type, ampfunc
+ *        [, ampfunc0 [, lmean0]])                          (MCsampleHetro.m:1)
+ * `mc` carries the shared positional arguments (mc.sigt is unused: sigt is
+ * the voxel grid).  Voxels follow findBin.m: nb = round((box_max-box_min)./
+ * box_bin) per axis, x fastest.  Free flights are delta (Woodcock) tracking
+ * against max(sigt) (smpWoodcock.m), NEE attenuation marches voxel to voxel
+ * (evalphaseattHetro.m).  smpFlg 1 picks the first voxel with probability
+ * proportional to sigt (invCDFvec.m / smpicdf.m); smpFlg 2 launches from a
+ * plane (expSmpXHetro.m), whose lateral axes are null(meanl') - passed in
+ * null_basis as MATLAB's SVD-based null() gives them (dim x (dim-1),
+ * column-major).  Outputs as MCcov / MCfield; mean1: nv x nl complex.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    scmc_mc_args mc;
+    const double *sigt_grid;    /* prod(nb) extinction values */
+    const double *albedo_grid;  /* prod(nb) albedos, or NULL for the scalar mc.albedo */
+    double box_bin[3];
+    int32_t has_lrad;           /* 17th argument of MCCovHetro (plane launch radius) */
+    double lrad;
+    double null_basis[6];
+} scmc_hetero_args;
+
+int scmc_cov_hetero(const scmc_hetero_args *args, double *Ms, double *Mm, double *mean1);
+int scmc_field_hetero(const scmc_hetero_args *args, double *u);
+
+/* ---------------------------------------------------------------------------
  * Path records for oracle replay.  Walks paths [path_offset, path_offset +
  * max_itr) exactly as scmc_field (want_phase=1) or scmc_cov (want_phase=0)
  * do and copies out one record per scattering event, in path order:

@@ -92,6 +92,18 @@ class FqArgs(C.Structure):
     ]
 
 
+class HeteroArgs(C.Structure):
+    _fields_ = [
+        ("mc", McArgs),
+        ("sigt_grid", _dp),
+        ("albedo_grid", _dp),
+        ("box_bin", C.c_double * 3),
+        ("has_lrad", C.c_int32),
+        ("lrad", C.c_double),
+        ("null_basis", C.c_double * 6),
+    ]
+
+
 class StageTimes(C.Structure):
     _fields_ = [
         ("walk_launches", C.c_int64),

@@ -13,7 +13,7 @@ import subprocess
 
 import numpy as np
 
-from mcspeckle_b200._abi import ArgsHolder, FqArgs
+from mcspeckle_b200._abi import ArgsHolder, FqArgs, HeteroArgs
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libscmc_oracle.so")
@@ -56,6 +56,8 @@ def lib():
         _lib.oracle_field_from_records.argtypes = [C.c_void_p, C.c_int64, dp, dp, dp, dp, dp, dp, ip, dp]
         _lib.oracle_cov_from_records.argtypes = [C.c_void_p, C.c_int64, dp, dp, dp, dp, dp, ip,
                                                  dp, dp, C.c_int]
+        _lib.oracle_cov_hetero.argtypes = [C.POINTER(HeteroArgs), C.POINTER(RngSpec), dp, dp, dp, C.c_int]
+        _lib.oracle_field_hetero.argtypes = [C.POINTER(HeteroArgs), C.POINTER(RngSpec), dp]
         _lib.oracle_field_fourier_quad.argtypes = [C.POINTER(FqArgs), C.POINTER(RngSpec), dp]
         _lib.oracle_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                               C.POINTER(C.c_uint32)]
@@ -198,3 +200,21 @@ def field_fourier_quad(fa: FqArgs, rng: Rng, nv0: int) -> np.ndarray:
     u = np.zeros(2 * nv0 * nv0 * fa.nl)
     _check(lib().oracle_field_fourier_quad(C.byref(fa), C.byref(rng.spec), _dp(u)), "oracle_field_fourier_quad")
     return u.view(np.complex128).reshape(nv0, nv0, fa.nl, order="F")
+
+
+def cov_hetero(h, rng: Rng, threads: int = 1):
+    """MCCovHetro on the oracle -> Ms, Mm, mean1."""
+    n = h.nv * h.nv * h.nl * h.nl
+    Ms, Mm, m1 = np.zeros(2 * n), np.zeros(2 * n), np.zeros(2 * h.nv * h.nl)
+    _check(lib().oracle_cov_hetero(C.byref(h.args), C.byref(rng.spec), _dp(Ms), _dp(Mm), _dp(m1), threads),
+           "oracle_cov_hetero")
+    shp = (h.nv, h.nv, h.nl, h.nl)
+    return (Ms.view(np.complex128).reshape(shp, order="F"), Mm.view(np.complex128).reshape(shp, order="F"),
+            m1.view(np.complex128).reshape(h.nv, h.nl, order="F"))
+
+
+def field_hetero(h, rng: Rng) -> np.ndarray:
+    """MCsampleHetro on the oracle -> u."""
+    u = np.zeros(2 * h.nv * h.nl)
+    _check(lib().oracle_field_hetero(C.byref(h.args), C.byref(rng.spec), _dp(u)), "oracle_field_hetero")
+    return u.view(np.complex128).reshape(h.nv, h.nl, order="F")

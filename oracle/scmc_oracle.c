@@ -779,3 +779,393 @@ int oracle_internal_fq_walk(const scmc_fq_args *a, const double *bmin, const dou
     if (!rc && c > cap) rc = -2;
     return rc;
 }
+
+/* ======================================================================== */
+/* Heterogeneous (voxel) medium: MCCovHetro.m, MCsampleHetro.m              */
+/* ======================================================================== */
+
+typedef struct {
+    int dim;
+    const double *sigt, *alb;
+    double alb_scalar;
+    double bmin[3], bmax[3], bbin[3];
+    int64_t nb[3];
+    double sigt_max;
+    int bad;  /* a voxel march ran away (guard) */
+} grid_t;
+
+static void grid_init(grid_t *g, const scmc_hetero_args *a)
+{
+    memset(g, 0, sizeof *g);
+    g->dim = a->mc.dim;
+    g->sigt = a->sigt_grid;
+    g->alb = a->albedo_grid;
+    g->alb_scalar = a->mc.albedo;
+    int64_t n = 1;
+    for (int k = 0; k < g->dim; ++k) {
+        g->bmin[k] = a->mc.box_min[k];
+        g->bmax[k] = a->mc.box_max[k];
+        g->bbin[k] = a->box_bin[k];
+        g->nb[k] = (int64_t)mround((g->bmax[k] - g->bmin[k]) / g->bbin[k]); /* findBin.m:4 */
+        n *= g->nb[k];
+    }
+    g->sigt_max = -INFINITY;
+    for (int64_t i = 0; i < n; ++i) g->sigt_max = fmax(g->sigt_max, g->sigt[i]);
+}
+
+static int64_t grid_count(const grid_t *g)
+{
+    int64_t n = 1;
+    for (int k = 0; k < g->dim; ++k) n *= g->nb[k];
+    return n;
+}
+
+/* findBin.m:1-17: 0-based linear voxel index (x fastest) and the voxel's
+ * bounds.  Subscripts outside 1..nb (a point on the lower face, or rounding)
+ * are clamped; the reference would index out of range there. */
+static int64_t find_bin(const grid_t *g, const double *x, double *bmn, double *bmx)
+{
+    int64_t ind = 0, stride = 1;
+    for (int j = 0; j < g->dim; ++j) {
+        double ii = ceil((x[j] - g->bmin[j]) / g->bbin[j]);
+        if (ii < 1) ii = 1;
+        if (ii > (double)g->nb[j]) ii = (double)g->nb[j];
+        ind += (int64_t)(ii - 1) * stride;
+        stride *= g->nb[j];
+        if (bmn) {
+            bmn[j] = g->bmin[j] + g->bbin[j] * (ii - 1);
+            bmx[j] = bmn[j] + g->bbin[j];
+        }
+    }
+    return ind;
+}
+
+static double grid_albedo(const grid_t *g, const double *x)
+{
+    return g->alb ? g->alb[find_bin(g, x, NULL, NULL)] : g->alb_scalar;
+}
+
+static int outside(const grid_t *g, const double *x)
+{
+    for (int k = 0; k < g->dim; ++k)
+        if (x[k] > g->bmax[k] || x[k] < g->bmin[k]) return 1;
+    return 0;
+}
+
+/* cubeDist.m:1-17 with the nudged exit point xd = x + (d + ep) v,
+ * ep = 1e-4 max|vmax - vmin|. */
+static double cube_dist_exit(const double *x, const double *vmin, const double *vmax, const double *v, int dim,
+                             double *xd)
+{
+    double d = cube_dist(x, vmin, vmax, v, dim);
+    double ep = 0.0;
+    for (int k = 0; k < dim; ++k) ep = fmax(ep, fabs(vmax[k] - vmin[k]));
+    ep = pow(0.1, 4) * ep;
+    for (int k = 0; k < dim; ++k) xd[k] = x[k] + (d + ep) * v[k];
+    return d;
+}
+
+/* evalphaseattHetro.m:1-52 for one direction / position. */
+static cplx phaseatt_hetero(grid_t *g, const double *x, const double *v, int is_ff, double lambda)
+{
+    const int dim = g->dim;
+    double pv, rv, nd, dir[3];
+    if (is_ff) {
+        pv = dotn(x, v, dim);
+        rv = 1.0;
+        nd = pow(10.0, 12);
+        for (int k = 0; k < dim; ++k) dir[k] = v[k];
+    } else {
+        double d[3], s = 0.0;
+        for (int k = 0; k < dim; ++k) { d[k] = x[k] - v[k]; s += d[k] * d[k]; }
+        nd = sqrt(s);
+        for (int k = 0; k < dim; ++k) dir[k] = d[k] / nd;
+        pv = nd;
+        rv = 1.0 / pow(nd + 0.01 * lambda, (dim - 1) / 2.0);
+    }
+    double m[3], nx[3], bmn[3], bmx[3];
+    for (int k = 0; k < dim; ++k) { m[k] = -dir[k]; nx[k] = x[k]; }
+    double bdv = 0.0, wbdv = 0.0;
+    for (int guard = 0; guard < 1000000; ++guard) {
+        int64_t bi = find_bin(g, nx, bmn, bmx);
+        double dd = cube_dist_exit(nx, bmn, bmx, m, dim, nx);
+        bdv = bdv + dd;
+        wbdv = wbdv + dd * g->sigt[bi];
+        if (bdv >= nd) {
+            double md = bdv - nd;
+            bdv = nd;
+            wbdv = wbdv - md * g->sigt[bi];
+            break;
+        }
+        if (outside(g, nx)) break;
+        if (guard == 999999) g->bad = 1;
+    }
+    double ph = (M_PI * 2.0 / lambda) * pv;
+    return exp(-(1.0 / 2.0 * wbdv)) * (cos(ph) + I * sin(ph)) * rv;
+}
+
+/* smpWoodcock.m:1-15: delta tracking against max(sigt). */
+static double smp_woodcock(grid_t *g, const double *x, const double *v, rng_t *r)
+{
+    double d = 0.0, nx[3];
+    for (int guard = 0; guard < 100000000; ++guard) {
+        d = d - log(1 - rand_u(r)) / g->sigt_max;
+        for (int k = 0; k < g->dim; ++k) nx[k] = x[k] + d * v[k];
+        if (outside(g, nx)) break;
+        int64_t bi = find_bin(g, nx, NULL, NULL);
+        if (rand_u(r) <= (g->sigt[bi] / g->sigt_max)) break;
+        if (r->exhausted) break;
+    }
+    return d;
+}
+
+/* cubeProj.m:1-18.  Returns 0 and the entry point when d >= 0. */
+static int cube_proj(const double *x, const double *vmin, const double *vmax, const double *v, int dim, double *xd)
+{
+    const double thr = pow(0.1, 7);
+    double d = -INFINITY;
+    for (int j = 0; j < dim; ++j) {
+        double den = fmax(fabs(v[j]), thr);
+        double bd = (v[j] <= 0) ? (x[j] - vmax[j]) / den : (-x[j] + vmin[j]) / den;
+        d = fmax(d, bd);
+    }
+    if (d < 0) return -1;
+    double ep = 0.0;
+    for (int k = 0; k < dim; ++k) ep = fmax(ep, fabs(vmax[k] - vmin[k]));
+    ep = pow(0.1, 4) * ep;
+    for (int k = 0; k < dim; ++k) xd[k] = x[k] + (d + ep) * v[k];
+    return 0;
+}
+
+/* expSmpXHetro.m:1-31.  `basis` is null(lmean') (dim x (dim-1), column-major). */
+static int exp_smp_x_hetero(grid_t *g, const double *lmean, double lrad, const double *basis, double *x, double *px,
+                            rng_t *r)
+{
+    const int dim = g->dim;
+    double mx = 0.0;
+    for (int k = 0; k < dim; ++k) mx = fmax(mx, fmax(fabs(g->bmax[k]), fabs(g->bmin[k])));
+    double q[2];
+    for (int k = 0; k < dim - 1; ++k) q[k] = (rand_u(r) - 0.5) * lrad;
+    double x0[3];
+    for (int k = 0; k < dim; ++k) {
+        double s = 0.0;
+        for (int c = 0; c < dim - 1; ++c) s += basis[k + dim * c] * q[c];
+        x0[k] = s - lmean[k] * mx * dim;
+    }
+    if (cube_proj(x0, g->bmin, g->bmax, lmean, dim, x) != 0 || outside(g, x)) { *px = 0; return -1; }
+    double d = smp_woodcock(g, x, lmean, r);
+    for (int k = 0; k < dim; ++k) x[k] = x[k] + d * lmean[k];
+    if (outside(g, x)) { *px = 0; return -1; }
+    cplx e = phaseatt_hetero(g, x, lmean, 1, 1.0);
+    double p = cabs(e) * cabs(e);
+    *px = p / pow(lrad, dim - 1);
+    return 0;
+}
+
+/* invCDFvec.m:1-7 = cumsum(hist(cdf, N)): N equal bins between min and max
+ * of cdf, [e_k, e_k+1) with the last bin closed; smpicdf.m: icdf(ceil(rand*N)). */
+static int64_t *inv_cdf_vec(const double *cdf, int64_t n, int64_t N)
+{
+    int64_t *h = calloc(N, sizeof(int64_t));
+    double lo = cdf[0], hi = cdf[0];
+    for (int64_t i = 0; i < n; ++i) { lo = fmin(lo, cdf[i]); hi = fmax(hi, cdf[i]); }
+    double norm = (double)N / (hi - lo);
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t b = (hi > lo) ? (int64_t)((cdf[i] - lo) * norm) : 0;
+        if (b >= N) b = N - 1;
+        /* keep the bin consistent with its edges lo + k (hi-lo)/N */
+        double step = (hi - lo) / (double)N;
+        if (b > 0 && cdf[i] < lo + b * step) b -= 1;
+        if (b < N - 1 && cdf[i] >= lo + (b + 1) * step) b += 1;
+        h[b]++;
+    }
+    for (int64_t i = 1; i < N; ++i) h[i] += h[i - 1];
+    return h;
+}
+
+typedef struct {
+    int cov;              /* 1: MCCovHetro, 0: MCsampleHetro */
+    cplx *Ms, *Mm, *mean1, *u;
+    int threads;
+} hsink_t;
+
+static int hetero_walk(const scmc_hetero_args *a, oracle_rng_spec *rs, hsink_t *sk)
+{
+    const scmc_mc_args *mc = &a->mc;
+    const int dim = mc->dim;
+    const int nv = (int)mc->nv, nl = (int)mc->nl;
+    grid_t g;
+    grid_init(&g, a);
+    rng_t r;
+    rng_init(&r, rs, mc->seed);
+    nee_t c;
+    nee_alloc(&c, mc); /* directions, far-field amplitude table, unmeanl (lmean0 honoured) */
+    if (sk->cov) {     /* MCCovHetro.m:38: always mean(l,2) */
+        for (int k = 0; k < dim; ++k) {
+            double s = 0.0;
+            for (int j = 0; j < nl; ++j) s += mc->l[dim * j + k];
+            c.unmeanl[k] = s / nl;
+        }
+        double n = sqrt(dotn(c.unmeanl, c.unmeanl, dim));
+        for (int k = 0; k < dim; ++k) c.meanl[k] = c.unmeanl[k] / n;
+    }
+    const int64_t ng = grid_count(&g);
+    double ssum = 0.0;
+    for (int64_t i = 0; i < ng; ++i) ssum += g.sigt[i];
+    double *cdf = malloc(sizeof(double) * ng);
+    double acc = 0.0;
+    for (int64_t i = 0; i < ng; ++i) { acc += g.sigt[i] / ssum; cdf[i] = acc; }
+    const int64_t Nicdf = ng * 100;
+    int64_t *icdf = inv_cdf_vec(cdf, ng, Nicdf);
+    free(cdf);
+    double vb = 1.0;
+    for (int k = 0; k < dim; ++k) vb *= g.bbin[k];
+    const double V = ssum * vb; /* MCCovHetro.m:64 */
+    double lrad = 0.0;
+    for (int k = 0; k < dim; ++k) lrad += (g.bmax[k] - g.bmin[k]) * (g.bmax[k] - g.bmin[k]);
+    lrad = a->has_lrad ? a->lrad : sqrt(lrad);
+    cplx *ul0 = malloc(sizeof(cplx) * nl);
+    int rc = 0;
+    for (int64_t itr = 0; itr < mc->max_itr; ++itr) {
+        if (r.mode == ORACLE_RNG_PHILOX) rng_set_path(&r, mc->path_offset + (uint64_t)itr);
+        double x[3] = {0, 0, 0}, w[3] = {0, 0, 0}, ow[3] = {0, 0, 0}, px;
+        if (mc->smp_flg == 1) {
+            /* smpicdf.m + MCCovHetro.m:93-95 */
+            int64_t i = (int64_t)ceil(rand_u(&r) * (double)Nicdf);
+            if (i < 1) i = 1;
+            int64_t bin = icdf[i - 1] - 1; /* 1-based voxel index -> 0-based */
+            int64_t rem = bin;
+            for (int k = 0; k < dim; ++k) {
+                int64_t ii = rem % g.nb[k];
+                rem /= g.nb[k];
+                double bmn = g.bmin[k] + g.bbin[k] * (double)ii;
+                x[k] = rand_u(&r) * g.bbin[k] + bmn;
+            }
+            px = 1.0 / V;
+        } else {
+            if (exp_smp_x_hetero(&g, c.meanl, lrad, a->null_basis, x, &px, &r) != 0) {
+                if (r.exhausted) { rc = -1; break; }
+                continue; /* MCCovHetro.m:113-115 */
+            }
+        }
+        if (outside(&g, x)) continue;
+        double x1[3], w1[3];
+        memcpy(x1, x, sizeof x);
+        if (!mc->has_ampfunc0) randn_dir(dim, w, &r);
+        else smpampfunc_general(c.meanl, &mc->ampfunc0, dim, w, &r);
+        memcpy(w1, w, sizeof w);
+        /* per-path vectors with the voxel-marched attenuation */
+        if (!c.is_ff_v)
+            for (int i = 0; i < nv; ++i) {
+                double d[3], s = 0.0;
+                for (int k = 0; k < dim; ++k) { d[k] = c.v[dim * i + k] - x[k]; s += d[k] * d[k]; }
+                s = sqrt(s);
+                for (int k = 0; k < dim; ++k) c.rv[dim * i + k] = d[k] / s;
+            }
+        if (!c.is_ff_l)
+            for (int j = 0; j < nl; ++j) {
+                double d[3], s = 0.0;
+                for (int k = 0; k < dim; ++k) { d[k] = x[k] - c.l[dim * j + k]; s += d[k] * d[k]; }
+                s = sqrt(s);
+                for (int k = 0; k < dim; ++k) c.rl[dim * j + k] = d[k] / s;
+            }
+        if (!(c.is_ff_v && c.is_ff_l))
+            for (int j = 0; j < nl; ++j)
+                for (int i = 0; i < nv; ++i)
+                    c.af_vl[i + nv * j] = evalampfunc(dotn(c.rl + dim * j, c.rv + dim * i, dim), c.pf, dim);
+        c.w0p = !c.has_pf0 ? 1.0 / sqrt(pow(2.0, dim - 1) * M_PI) : creal(evalampfunc(dotn(c.meanl, w, dim), c.pf0, dim));
+        for (int j = 0; j < nl; ++j) {
+            cplx af_l = evalampfunc(dotn(w, c.rl + dim * j, dim), c.pf, dim) / c.w0p;
+            c.e_l0[j] = phaseatt_hetero(&g, x, c.l + dim * j, c.is_ff_l, mc->lambda);
+            c.e_l0_ms[j] = c.e_l0[j] * af_l;
+            if (sk->cov) ul0[j] = evalphaseatt1(x, c.l + dim * j, c.is_ff_l, 0.0, mc->lambda, c.bmin, c.bmax, dim);
+        }
+        for (int i = 0; i < nv; ++i) {
+            c.e_v0[i] = phaseatt_hetero(&g, x, c.vs + dim * i, c.is_ff_v, mc->lambda);
+            if (c.cbs) {
+                cplx af_v = evalampfunc(-dotn(w, c.rv + dim * i, dim), c.pf, dim) / c.w0p;
+                c.e_v0_ms[i] = c.e_v0[i] * af_v;
+            }
+        }
+        int pL = 0;
+        double weight = grid_albedo(&g, x);
+        for (;;) {
+            ++pL;
+            if (pL > 1) {
+                for (int i = 0; i < nv; ++i) {
+                    cplx e_v = phaseatt_hetero(&g, x, c.vs + dim * i, c.is_ff_v, mc->lambda);
+                    c.e_v_ms[i] = e_v * evalampfunc(dotn(ow, c.rv + dim * i, dim), c.pf, dim);
+                }
+                if (c.cbs)
+                    for (int j = 0; j < nl; ++j) {
+                        cplx e_l = phaseatt_hetero(&g, x, c.l + dim * j, c.is_ff_l, mc->lambda);
+                        c.e_l_ms[j] = e_l * evalampfunc(-dotn(ow, c.rl + dim * j, dim), c.pf, dim);
+                    }
+            }
+            const double wpx = weight / px;
+            if (sk->cov) {
+                if (pL == 1)
+                    for (int j = 0; j < nl; ++j)
+                        for (int i = 0; i < nv; ++i)
+                            sk->mean1[i + nv * j] += wpx * c.af_vl[i + nv * j] * (c.e_v0[i] * ul0[j]);
+                cov_update(&c, pL, wpx, sk->Ms, sk->Mm, sk->threads);
+            } else {
+                double xi = rand_u(&r); /* MCsampleHetro.m:187, after the NEE */
+                field_update(&c, pL, wpx, xi, sk->u);
+            }
+            double d = smp_woodcock(&g, x, w, &r);
+            for (int k = 0; k < dim; ++k) x[k] = x[k] + d * w[k];
+            if (outside(&g, x)) break;
+            if (weight < KILL_THR) {
+                if (rand_u(&r) > grid_albedo(&g, x)) break;
+            } else {
+                weight = weight * grid_albedo(&g, x);
+            }
+            memcpy(ow, w, sizeof w);
+            smpampfunc_general(ow, &mc->ampfunc, dim, w, &r);
+            if (r.exhausted) break;
+        }
+        if (r.exhausted) { rc = -1; break; }
+    }
+    if (g.bad) rc = -5;
+    rs->used_u = r.ui;
+    rs->used_n = r.ni;
+    free(icdf);
+    free(ul0);
+    nee_free(&c);
+    return rc;
+}
+
+int oracle_cov_hetero(const scmc_hetero_args *a, oracle_rng_spec *rs, double *Ms, double *Mm, double *mean1,
+                      int threads)
+{
+    const scmc_mc_args *mc = &a->mc;
+    int64_t n = mc->nv * mc->nv * mc->nl * mc->nl;
+    memset(Ms, 0, sizeof(double) * 2 * n);
+    memset(Mm, 0, sizeof(double) * 2 * n);
+    memset(mean1, 0, sizeof(double) * 2 * mc->nv * mc->nl);
+    hsink_t sk = {1, (cplx *)Ms, (cplx *)Mm, (cplx *)mean1, NULL, threads};
+    int rc = hetero_walk(a, rs, &sk);
+    /* MCCovHetro.m:262-276: CBS /2, then /maxItr only (px carries the volume) */
+    double m = (double)(mc->norm_itr > 0 ? mc->norm_itr : mc->max_itr);
+    for (int64_t i = 0; i < n; ++i) {
+        if (mc->do_cbs) sk.Mm[i] = sk.Mm[i] / 2.0;
+        sk.Mm[i] = sk.Mm[i] / m;
+        sk.Ms[i] = sk.Ms[i] / m;
+    }
+    /* cs = 1 (for tabulated tables the reference reads a missing field) */
+    for (int64_t i = 0; i < mc->nv * mc->nl; ++i) sk.mean1[i] = sk.mean1[i] / m / sqrt(1.0);
+    return rc;
+}
+
+int oracle_field_hetero(const scmc_hetero_args *a, oracle_rng_spec *rs, double *u)
+{
+    const scmc_mc_args *mc = &a->mc;
+    memset(u, 0, sizeof(double) * 2 * mc->nv * mc->nl);
+    hsink_t sk = {0, NULL, NULL, NULL, (cplx *)u, 1};
+    int rc = hetero_walk(a, rs, &sk);
+    double m = (double)(mc->norm_itr > 0 ? mc->norm_itr : mc->max_itr);
+    double f = sqrt(1.0 / m); /* MCsampleHetro.m:222 */
+    for (int64_t i = 0; i < mc->nv * mc->nl; ++i) sk.u[i] *= f;
+    return rc;
+}

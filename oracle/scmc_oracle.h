@@ -57,6 +57,11 @@ int oracle_cov_from_records(const scmc_mc_args *a, int64_t n, const double *x,
  * gridding and a 2-D DFT per plane and light).  u: 2*nv0*nv0*nl doubles. */
 int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double *u);
 
+/* MCCovHetro.m:1-276 (Ms, Mm, mean1) and MCsampleHetro.m:1-227 (u). */
+int oracle_cov_hetero(const scmc_hetero_args *a, oracle_rng_spec *rs, double *Ms, double *Mm, double *mean1,
+                      int threads);
+int oracle_field_hetero(const scmc_hetero_args *a, oracle_rng_spec *rs, double *u);
+
 /* Philox-4x32-10 (Salmon et al., SC'11): one block. */
 void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* The per-path streams (tag 0 uniform, tag 1 normal) of the walk. */

@@ -195,6 +195,50 @@ class Gen:
                 "error": err}
         self.save(name, "fourier_quad", meta, arrays)
 
+    # -- MCCovHetro / MCsampleHetro ----------------------------------------------
+    def hetero_case(self, name, func, seed, *, sigt, albedo, box_min, box_max, box_bin, l, v, is_ff_l, is_ff_v,
+                    max_itr, lam, cbs, smp_flg, sct_type, ampfunc, ampfunc0=None, extra=None):
+        it, ut, nt = self.interp(seed)
+        sg = np.asarray(sigt, float)
+        args = [M(sg), M(np.asarray(albedo, float)), M(np.reshape(box_min, (-1, 1)).astype(float)),
+                M(np.reshape(box_max, (-1, 1)).astype(float)), M(np.reshape(box_bin, (-1, 1)).astype(float)),
+                M(np.asarray(l, float)), M(np.asarray(v, float)), M(bool(is_ff_l)), M(bool(is_ff_v)),
+                M(float(max_itr)), M(float(lam)), M(bool(cbs)), M(float(smp_flg)), M(float(sct_type)), to_m(ampfunc)]
+        if ampfunc0 is not None or extra is not None:
+            args.append(to_m(ampfunc0) if ampfunc0 is not None else M(np.zeros((0, 0))))
+        if extra is not None:
+            args.append(M(np.reshape(extra, (-1, 1)).astype(float)) if np.size(extra) > 1 else M(float(extra)))
+        nout = 3 if func == "MCCovHetro" else 1
+        outs = it.call(func, args, nout)
+        dim = np.size(box_min)
+        lm = np.asarray(l, float)
+        if lm.shape[0] == 1:
+            lm = np.vstack([np.sin(lm), np.cos(lm)])
+        if func == "MCCovHetro":
+            unmeanl = lm.mean(axis=1)
+        else:
+            unmeanl = np.asarray(extra, float).reshape(-1) if (extra is not None and np.size(extra) == dim) \
+                else lm.mean(axis=1)
+        meanl = unmeanl / np.linalg.norm(unmeanl)
+        nb = it.call("null", [M(meanl.reshape(1, -1))], 1)[0]
+        arrays = {"utape": ut[:it.ui], "ntape": nt[:it.ni], "sigt": sg, "albedo": np.asarray(albedo, float),
+                  "box_min": np.asarray(box_min, float), "box_max": np.asarray(box_max, float),
+                  "box_bin": np.asarray(box_bin, float), "l": np.asarray(l, float), "v": np.asarray(v, float),
+                  "null_basis": np.asarray(nb, float)}
+        meta = {"func": func, "is_ff_l": bool(is_ff_l), "is_ff_v": bool(is_ff_v), "max_itr": max_itr,
+                "lambda": lam, "cbs": bool(cbs), "smp_flg": smp_flg, "sct_type": sct_type,
+                "has_ampfunc0": ampfunc0 is not None, "extra": None if extra is None else np.asarray(extra, float).tolist()}
+        self._put_amp(arrays, meta, "ampfunc", ampfunc)
+        if ampfunc0 is not None:
+            self._put_amp(arrays, meta, "ampfunc0", ampfunc0)
+        if func == "MCCovHetro":
+            arrays["Ms"] = np.asarray(outs[0], dtype=complex)
+            arrays["Mm"] = np.asarray(outs[1], dtype=complex)
+            arrays["mean1"] = np.asarray(outs[2], dtype=complex)
+        else:
+            arrays["u"] = np.asarray(outs[0], dtype=complex)
+        self.save(name, "hetero", meta, arrays)
+
     def error_case(self, name, func, args_py, expect_contains=None):
         it, _, _ = self.interp(0)
         try:
@@ -265,6 +309,35 @@ def main(ref):
               vsign=-1)
     g.fq_case("fq_even_grid_errors", 304, sigt=0.1, albedo=0.9, box_min=[-10, -10, 0], box_max=[10, 10, 8], l=Lq,
               v_max=0.195, v_stp=0.01, max_itr=5, lam=1.0, cbs=1, smp_flg=2, lmean0=None, vsign=-1)
+
+    print("hetero")
+    g2 = np.random.default_rng(7)
+    sig2 = np.array([[1 / 30, 0, 1 / 60], [0, 1 / 120, 1 / 30]]).T  # testHetroCov.m's grid, 3 x 2
+    L2 = np.pi - np.deg2rad([[0.0, 4.0, 12.0]])
+    V2 = np.deg2rad([[-30.0, 10.0, 170.0, 200.0]])
+    hb2 = dict(box_min=[-60, -60], box_max=[60, 60], box_bin=[40, 60])
+    sig3 = g2.lognormal(np.log(0.15), 0.5, size=(2, 2, 3))
+    hb3 = dict(box_min=[-20, -20, 0], box_max=[20, 20, 15], box_bin=[20, 20, 5])
+    for func in ("MCCovHetro", "MCsampleHetro"):
+        tag = "hcov" if func == "MCCovHetro" else "hfield"
+        g.hetero_case(f"{tag}_2d_iso_voxelpick_cbs", func, 401, sigt=sig2, albedo=1.0, **hb2, l=L2, v=V2,
+                      is_ff_l=1, is_ff_v=1, max_itr=30, lam=1.0, cbs=1, smp_flg=1, sct_type=1, ampfunc=0)
+        g.hetero_case(f"{tag}_2d_hg_plane_nocbs", func, 402, sigt=sig2, albedo=0.9, **hb2, l=L2, v=V2,
+                      is_ff_l=1, is_ff_v=1, max_itr=30, lam=1.0, cbs=0, smp_flg=2, sct_type=3, ampfunc=0.5)
+        g.hetero_case(f"{tag}_3d_hg_plane_cbs_albgrid", func, 403, sigt=sig3,
+                      albedo=g2.uniform(0.7, 1.0, size=(2, 2, 3)), **hb3, l=L3, v=V3r, is_ff_l=1, is_ff_v=1,
+                      max_itr=25, lam=1.0, cbs=1, smp_flg=2, sct_type=3, ampfunc=0.7)
+        # tabulated scatter only for MCsampleHetro: MCCovHetro.m:271-272 reads
+        # ampfunc.pdf, a field tabulatedAmplitudeScatter does not build
+        st, amp = (2, tab3d) if func == "MCsampleHetro" else (3, 0.3)
+        g.hetero_case(f"{tag}_3d_voxelpick_nfv", func, 404, sigt=sig3, albedo=0.95, **hb3, l=L3, v=NFv,
+                      is_ff_l=1, is_ff_v=0, max_itr=20, lam=1.0, cbs=1, smp_flg=1, sct_type=st, ampfunc=amp)
+    g.hetero_case("hcov_3d_iso_plane_lrad_g0", "MCCovHetro", 405, sigt=sig3, albedo=1.0, **hb3, l=L3, v=V3t,
+                  is_ff_l=1, is_ff_v=1, max_itr=25, lam=0.9, cbs=0, smp_flg=2, sct_type=3, ampfunc=0.4,
+                  ampfunc0=0.2, extra=30.0)
+    g.hetero_case("hfield_3d_hg_plane_lmean0", "MCsampleHetro", 406, sigt=sig3, albedo=1.0, **hb3, l=L3, v=V3r,
+                  is_ff_l=1, is_ff_v=1, max_itr=25, lam=1.0, cbs=1, smp_flg=2, sct_type=3, ampfunc=0.6,
+                  ampfunc0=0.3, extra=[0.1, 0.0, 1.0])
 
     print("scmc.m")
     tgt3 = [1.0, 5.0, [0, 15], [-20, 20], [-20, 20]]

@@ -778,8 +778,13 @@ def do_assign(A, subs, B):
         if isinstance(s, str) and s == ":":
             ext = shape[k]
             if ext == 0:
-                # A(:, j) = B on an empty array takes its extent from B
-                ext = Bv.shape[k] if k < Bv.ndim else 1
+                # A(:, j) = B on an empty array: the colon takes the elements of B
+                # that the other subscripts do not account for
+                others = 1
+                for kk, ss in enumerate(subs):
+                    if kk != k and not (isinstance(ss, str) and ss == ":"):
+                        others *= _index_list(ss, shape[kk]).size
+                ext = max(Bv.size // max(others, 1), 1)
                 new_shape[k] = ext
             idx.append(np.arange(ext))
         else:
@@ -1579,6 +1584,20 @@ def b_isnumeric(it, args, nargout):
     return M(isinstance(a, np.ndarray) and a.dtype != bool)
 
 
+def b_hist(it, args, nargout):
+    """hist(y, N): counts in N equal-width bins between min(y) and max(y)
+    ([e_k, e_k+1), last bin closed) - MATLAB's documented binning."""
+    y = _as_float(args[0]).reshape(-1, order="F")
+    n = int(scalar(args[1])) if len(args) > 1 else 10
+    lo, hi = float(np.min(y)), float(np.max(y))
+    if hi == lo:
+        counts = np.zeros(n)
+        counts[0] = y.size
+    else:
+        counts, _ = np.histogram(y, bins=n, range=(lo, hi))
+    return M(counts.astype(float).reshape(1, -1))
+
+
 def b_sinc(it, args, nargout):
     return np.sinc(_as_float(args[0]))
 
@@ -1734,7 +1753,7 @@ BUILTINS = {
     "rand": b_rand("u"), "randn": b_rand("n"), "bsxfun": b_bsxfun,
     "isscalar": b_isscalar, "isvector": b_isvector, "isreal": b_isreal, "isnumeric": b_isnumeric,
     "islogical": b_islogical, "isinf": b_isinf, "isnan": b_isnan, "isfield": b_isfield,
-    "strcmp": b_strcmp, "strncmpi": b_strncmpi, "char": b_char, "sinc": b_sinc, "null": b_null,
+    "hist": b_hist, "strcmp": b_strcmp, "strncmpi": b_strncmpi, "char": b_char, "sinc": b_sinc, "null": b_null,
     "logical": b_logical, "double": b_double,
     "deg2rad": lambda it, a, n: _as_float(a[0]) * (math.pi / 180.0),
     "rad2deg": lambda it, a, n: _as_float(a[0]) * (180.0 / math.pi),

@@ -200,3 +200,39 @@ def test_fourier_quad_oracle_matches_reference(oracle_lib, name):
         assert relerr(u, arr["u"]) < RTOL
     assert rng.spec.used_u == arr["utape"].size
     assert rng.spec.used_n == arr["ntape"].size
+
+
+HETERO_CASES = [e["name"] for e in INDEX if e["kind"] == "hetero"]
+
+
+def hetero_case_args(meta, arr):
+    args = [arr["sigt"], arr["albedo"], arr["box_min"], arr["box_max"], arr["box_bin"], arr["l"], arr["v"],
+            meta["is_ff_l"], meta["is_ff_v"], meta["max_itr"], meta["lambda"], meta["cbs"], meta["smp_flg"],
+            meta["sct_type"], amp(meta, arr, "ampfunc")]
+    args.append(amp(meta, arr, "ampfunc0") if meta["has_ampfunc0"] else MC._MISSING)
+    args.append(np.asarray(meta["extra"]) if meta["extra"] is not None else MC._MISSING)
+    return args
+
+
+@pytest.mark.parametrize("name", HETERO_CASES)
+def test_hetero_oracle_matches_reference(oracle_lib, name):
+    from mcspeckle_b200 import hetero as H
+    meta, arr = load(name)
+    cov = meta["func"] == "MCCovHetro"
+    h = H.hetero_args(cov, *hetero_case_args(meta, arr), seed=0, precision="fp64", basis=arr["null_basis"])
+    # the null-space axes the reference used (MATLAB's null() run by the
+    # interpreter) are the ones this host mirror computes itself
+    L = arr["l"] if arr["l"].shape[0] > 1 else np.vstack([np.sin(arr["l"]), np.cos(arr["l"])])
+    um = np.asarray(meta["extra"], float).reshape(-1) if (not cov and meta["extra"] is not None) else L.mean(axis=1)
+    assert np.allclose(H.null_basis(um / np.linalg.norm(um)), arr["null_basis"])
+    rng = oracle_lib.Rng.tape(arr["utape"], arr["ntape"])
+    if cov:
+        Ms, Mm, m1 = oracle_lib.cov_hetero(h, rng)
+        assert relerr(Ms, arr["Ms"]) < RTOL
+        assert relerr(Mm, arr["Mm"]) < RTOL
+        assert relerr(m1, np.asarray(arr["mean1"]).reshape(m1.shape, order="F")) < RTOL
+    else:
+        u = oracle_lib.field_hetero(h, rng)
+        assert relerr(u, np.asarray(arr["u"]).reshape(u.shape, order="F")) < RTOL
+    assert rng.spec.used_u == arr["utape"].size
+    assert rng.spec.used_n == arr["ntape"].size
