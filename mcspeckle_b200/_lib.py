@@ -64,12 +64,15 @@ def lib():
         L.scmc_field_fourier_quad.argtypes = [fq, dp]
         L.scmc_field_fourier_quad_device.argtypes = [fq, C.c_void_p, C.c_void_p]
         L.scmc_field_noalloc.argtypes = [mp, C.c_void_p, C.c_void_p]
+        hp = C.POINTER(_abi.HeteroArgs)
+        L.scmc_cov_hetero.argtypes = [hp, dp, dp, dp]
+        L.scmc_field_hetero.argtypes = [hp, dp]
         L.scmc_profile_enable.argtypes = [C.c_int32]
         L.scmc_profile_read.argtypes = [C.POINTER(_abi.StageTimes), C.c_int32]
         for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",
                      "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read",
                      "scmc_fq_grid_size", "scmc_field_fourier_quad", "scmc_field_fourier_quad_device",
-                     "scmc_field_noalloc"):
+                     "scmc_field_noalloc", "scmc_cov_hetero", "scmc_field_hetero"):
             getattr(L, name).restype = C.c_int
         _lib = L
         return _lib

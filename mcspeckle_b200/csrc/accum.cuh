@@ -65,7 +65,8 @@ template <typename A> struct acc_ptr;
 template <int DIM, int POL, bool SINGLE, typename AccT>
 __global__ void __launch_bounds__(kFieldThreads)
 field_accum_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_events,
-                   int tv, int tl, int n_vtiles, int64_t ev_per_cta, AccT *__restrict__ U, int field_phase)
+                   int tv, int tl, int n_vtiles, int64_t ev_per_cta, AccT *__restrict__ U, int field_phase,
+                   int mean_mode = 0)
 {
     using R = typename std::conditional<POL == P64, double, float>::type;
     using C = typename cplx_t<R>::type;
@@ -97,7 +98,7 @@ field_accum_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t m
             EventView ev;
             load_event<DIM, SINGLE>(Q, S, scap, M, mcap, eb + threadIdx.x, ev);
             sev[threadIdx.x] = ev;
-            double s = sqrt(ev.wpx);
+            double s = mean_mode ? ev.wpx : sqrt(ev.wpx);
             if (!SINGLE && Q.cbs) s *= 1.0 / sqrt(2.0);
             double2 rot = make_double2(1.0, 0.0);
             if (field_phase) {
@@ -126,7 +127,8 @@ field_accum_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t m
                 int j = l0 + (m - tv);
                 C b = C{}, b2 = C{};
                 if (j < Q.nl) {
-                    if (SINGLE) b = phaseatt<DIM, POL>(ev.x1, Q.l + 3 * j, Q.is_ff_l, Q);
+                    if (SINGLE && mean_mode) b = phase_plain<DIM, POL>(ev.x1, Q.l + 3 * j, Q.is_ff_l, Q);
+                    else if (SINGLE) b = phaseatt<DIM, POL>(ev.x1, Q.l + 3 * j, Q.is_ff_l, Q);
                     else nee_light<DIM, POL, C>(Q, j, ev.x, ev.ow, ev.x1, ev.w1, ev.w0p, b, b2);
                 }
                 sb[k * tl + (m - tv)] = b;

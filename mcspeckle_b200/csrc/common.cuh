@@ -28,6 +28,25 @@ struct PhaseFn {
     const double *sample_icdf; // table_n angles (sampleIcdf)
 };
 
+// Voxel medium of MCCovHetro.m / MCsampleHetro.m (device functions in hgrid.cuh).
+struct HGrid {
+    int dim;
+    const double *sigt;      // prod(nb) values, x fastest (findBin.m order)
+    const double *alb;       // prod(nb) albedos or nullptr
+    double alb_scalar;
+    double bmin[3], bmax[3], bbin[3];
+    int nb[3];
+    double sigt_max;
+    // first-scatter sampling
+    const double *cdf;       // cumsum(sigt / sum(sigt)), prod(nb) values (MCCovHetro.m:62)
+    int64_t n_vox;
+    int64_t n_icdf;          // prod(nb) * 100 (MCCovHetro.m:63)
+    double cdf_lo, cdf_step; // hist bins of invCDFvec.m
+    double inv_V;            // px = 1/V, V = sum(sigt) prod(box_bin)
+    double lrad;
+    double basis[6];         // null(meanl'), dim x (dim-1) column-major
+};
+
 // Everything the walk needs, passed by value.
 struct WalkParams {
     int dim;
@@ -42,6 +61,8 @@ struct WalkParams {
     uint64_t path_base;        // global index of path 0 of this batch
     int64_t n_paths;
     int64_t max_events;        // 0 = unlimited
+    int hetero;                // voxel medium (Woodcock flights, voxel albedo)
+    HGrid hg;
 };
 
 // ---------------------------------------------------------------------------

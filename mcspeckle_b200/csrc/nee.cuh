@@ -19,6 +19,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "hgrid.cuh"
 
 namespace scmc {
 
@@ -34,6 +35,8 @@ struct NeeParams {
     int has_pf0;
     double meanl[3];
     PhaseFn pf, pf0;
+    int hetero;              // voxel medium: attenuation marched through hg
+    HGrid hg;
 };
 
 template <typename T> struct cplx_t;
@@ -63,10 +66,51 @@ __device__ __forceinline__ double reduce_2pi(double ph)
 }
 
 // phaseatt for one direction / position, FP64 inputs.  evalphaseatt.m:1-21.
+// evalphaseattHetro.m:1-52: as evalphaseatt, with the optical depth marched
+// voxel by voxel (far field: to the box; near field: to the source).
+template <int DIM, int POL>
+__device__ __noinline__ typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type
+phaseatt_hetero(const double *x, const double *d, int is_ff, const NeeParams &Q)
+{
+    double pv, rv, nd, dir[3] = {0, 0, 0};
+    if (is_ff) {
+        pv = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) { pv += x[k] * d[k]; dir[k] = d[k]; }
+        rv = 1.0;
+        nd = 1.0e12;
+    } else {
+        double dd[3];
+        nd = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) { dd[k] = x[k] - d[k]; nd += dd[k] * dd[k]; }
+        nd = sqrt(nd);
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) dir[k] = dd[k] / nd;
+        pv = nd;
+        rv = (DIM == 3) ? 1.0 / (nd + 0.01 * Q.lambda) : 1.0 / sqrt(nd + 0.01 * Q.lambda);
+    }
+    const double wbdv = hg_optical_depth<DIM>(Q.hg, x, dir, nd);
+    const double ph = Q.kw * pv;
+    if constexpr (POL == P64) {
+        double s, c;
+        sincos(ph, &s, &c);
+        const double a = exp(-(1.0 / 2.0 * wbdv)) * rv;
+        return make_double2(a * c, a * s);
+    } else {
+        float s, c;
+        if (POL == PMIX) sincosf((float)reduce_2pi(ph), &s, &c);
+        else sincosf((float)ph, &s, &c);
+        const float a = expf(-(float)(0.5 * wbdv)) * (float)rv;
+        return make_float2(a * c, a * s);
+    }
+}
+
 template <int DIM, int POL>
 __device__ __forceinline__ typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type
 phaseatt(const double *x, const double *d, int is_ff, const NeeParams &Q)
 {
+    if (Q.hetero) return phaseatt_hetero<DIM, POL>(x, d, is_ff, Q);
     if constexpr (POL == P32) {
         float xf[3], df[3];
 #pragma unroll
@@ -133,6 +177,36 @@ phaseatt(const double *x, const double *d, int is_ff, const NeeParams &Q)
             float a = expf(-(float)at) * (float)rv;
             return make_float2(a * c, a * s);
         }
+    }
+}
+
+// evalphaseatt with sigt = 0 (MCCovHetro.m:152: u_l0 for the mean field):
+// exp(i k pv) rv, no attenuation.
+template <int DIM, int POL>
+__device__ __forceinline__ typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type
+phase_plain(const double *x, const double *d, int is_ff, const NeeParams &Q)
+{
+    double pv = 0.0, rv = 1.0;
+    if (is_ff) {
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) pv += x[k] * d[k];
+    } else {
+        double nd = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) nd += (x[k] - d[k]) * (x[k] - d[k]);
+        nd = sqrt(nd);
+        pv = nd;
+        rv = (DIM == 3) ? 1.0 / (nd + 0.01 * Q.lambda) : 1.0 / sqrt(nd + 0.01 * Q.lambda);
+    }
+    const double ph = Q.kw * pv;
+    if constexpr (POL == P64) {
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        return make_double2(rv * cs, rv * sn);
+    } else {
+        float sn, cs;
+        sincosf((float)reduce_2pi(ph), &sn, &cs);
+        return make_float2((float)rv * cs, (float)rv * sn);
     }
 }
 

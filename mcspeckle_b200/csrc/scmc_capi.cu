@@ -171,7 +171,7 @@ struct Ctx {
     DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
-    DevBuf acc_s, acc_m, rows, tiles, tc_a, out0, out1;
+    DevBuf acc_s, acc_m, rows, tiles, tc_a, out0, out1, out2;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
 };
@@ -445,7 +445,8 @@ int64_t path_batch_size(int64_t remaining) { return std::min<int64_t>(remaining,
 // field
 // ---------------------------------------------------------------------------
 template <int DIM, int POL, bool SINGLE, typename AccT>
-void launch_field_accum(Ctx &c, const Prepared &P, const Batch &B, AccT *U, int64_t n_ev, cudaStream_t st)
+void launch_field_accum(Ctx &c, const Prepared &P, const Batch &B, AccT *U, int64_t n_ev, cudaStream_t st,
+                        int mean_mode = 0)
 {
     if (n_ev <= 0) return;
     const int nv = P.Q.nv, nl = P.Q.nl;
@@ -467,7 +468,7 @@ void launch_field_accum(Ctx &c, const Prepared &P, const Batch &B, AccT *U, int6
     dim3 grid(tiles, (unsigned)ranges);
     StageScope sc(ST_ROWS, st);
     kern<<<grid, kFieldThreads, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, n_ev, tv, tl, n_vtiles, per, U,
-                                            P.W.want_phase);
+                                            mean_mode ? 0 : P.W.want_phase, mean_mode);
     CK(cudaGetLastError());
     LAUNCHED();
 }
@@ -567,7 +568,8 @@ void herk_cc(Ctx &c, const void *T, int64_t n, int N, void *Cacc, cudaStream_t s
 }
 
 template <int DIM, int POL>
-void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st)
+void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st,
+                double *mean1_acc = nullptr)
 {
     using R = typename std::conditional<POL == P64, double, float>::type;
     using A = R;  // plain FP32 keeps FP32 accumulators; FP64 mode keeps FP64
@@ -586,6 +588,7 @@ void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
+        if (mean1_acc) launch_field_accum<DIM, POL, true, double>(c, P, B, mean1_acc, B.n_paths, st, 1);
         for (int64_t e0 = 0; e0 < B.n_paths; e0 += chunk) {
             int64_t n = std::min(chunk, B.n_paths - e0);
             cov_rows<DIM, POL, true>(c, P, B, e0, n, T, st);
@@ -617,7 +620,8 @@ void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
 }
 
 template <int DIM>
-void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st)
+void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st,
+                double *mean1_acc = nullptr)
 {
     const int N = (int)(a->nv * a->nl);
     TcPlan plan = tc_plan(N, a->precision == SCMC_PREC_MIXED);
@@ -640,6 +644,7 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
+        if (mean1_acc) launch_field_accum<DIM, PMIX, true, double>(c, P, B, mean1_acc, B.n_paths, st, 1);
         for (int pass = 0; pass < 2; ++pass) {
             const bool single = pass == 0;
             const int64_t n_ev = single ? B.n_paths : B.n_multi;
@@ -800,6 +805,144 @@ __global__ void philox_stream_kernel(uint64_t seed, uint64_t path, int tag, int6
     PathRng r;
     r.init((uint32_t)seed, (uint32_t)(seed >> 32), path);
     for (int64_t i = 0; i < n; ++i) out[i] = tag ? r.randn() : r.rand();
+}
+
+// ---------------------------------------------------------------------------
+// heterogeneous medium (MCCovHetro / MCsampleHetro)
+// ---------------------------------------------------------------------------
+struct HeteroBufs {
+    DevBuf sigt, alb, cdf, mean1, zeros;
+};
+HeteroBufs g_hbufs[64];
+
+// The positional arguments as the homogeneous kernels see them (sigt = 1 and
+// unit volume, so their normalisations reduce to 1/maxItr, MCCovHetro.m:268-269)
+// plus the voxel grid.
+Prepared prepare_hetero(Ctx &c, const scmc_hetero_args *h, int want_phase, bool cov, cudaStream_t st,
+                        scmc_mc_args &mc)
+{
+    mc = h->mc;
+    mc.sigt = 1.0;
+    if (cov) mc.has_lmean0 = 0;  // MCCovHetro.m:38 uses mean(l,2)
+    validate(&mc);
+    if (!h->sigt_grid) fail(SCMC_ERR_INVALID, "null sigt grid");
+    if (mc.smp_flg == 1 && h->has_lrad)
+        fail(SCMC_ERR_INVALID, "lrad with uniform voxel sampling (smpFlg 1) is not supported");
+    const int dim = mc.dim;
+    HGrid g{};
+    g.dim = dim;
+    int64_t nv = 1;
+    double vb = 1.0, diag = 0.0;
+    for (int k = 0; k < dim; ++k) {
+        if (!(h->box_bin[k] > 0)) fail(SCMC_ERR_INVALID, "box_bin must be positive");
+        g.bmin[k] = mc.box_min[k];
+        g.bmax[k] = mc.box_max[k];
+        g.bbin[k] = h->box_bin[k];
+        g.nb[k] = (int)std::llround((g.bmax[k] - g.bmin[k]) / g.bbin[k]);  // findBin.m:4
+        if (g.nb[k] < 1) fail(SCMC_ERR_INVALID, "the box holds no voxel");
+        nv *= g.nb[k];
+        vb *= g.bbin[k];
+        diag += (g.bmax[k] - g.bmin[k]) * (g.bmax[k] - g.bmin[k]);
+    }
+    g.n_vox = nv;
+    g.n_icdf = nv * 100;  // MCCovHetro.m:63
+    double ssum = 0.0, smax = 0.0;
+    std::vector<double> cdf(nv);
+    for (int64_t i = 0; i < nv; ++i) {
+        if (!(h->sigt_grid[i] >= 0)) fail(SCMC_ERR_INVALID, "sigt must be non-negative");
+        ssum += h->sigt_grid[i];
+        smax = std::fmax(smax, h->sigt_grid[i]);
+    }
+    if (!(smax > 0)) fail(SCMC_ERR_INVALID, "sigt grid is all zero");
+    double acc = 0.0, lo = INFINITY, hi = -INFINITY;
+    for (int64_t i = 0; i < nv; ++i) {
+        acc += h->sigt_grid[i] / ssum;
+        cdf[i] = acc;
+        lo = std::fmin(lo, acc);
+        hi = std::fmax(hi, acc);
+    }
+    g.sigt_max = smax;
+    g.cdf_lo = lo;
+    g.cdf_step = (hi - lo) / (double)g.n_icdf;
+    g.inv_V = 1.0 / (ssum * vb);  // px = 1/V, V = sum(sigt) prod(box_bin)
+    g.lrad = h->has_lrad ? h->lrad : std::sqrt(diag);
+    for (int k = 0; k < 6; ++k) g.basis[k] = h->null_basis[k];
+    HeteroBufs &hb = g_hbufs[c.device];
+    double *dsig = reinterpret_cast<double *>(hb.sigt.ensure(nv * sizeof(double)));
+    double *dcdf = reinterpret_cast<double *>(hb.cdf.ensure(nv * sizeof(double)));
+    CK(cudaMemcpyAsync(dsig, h->sigt_grid, nv * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(dcdf, cdf.data(), nv * sizeof(double), cudaMemcpyHostToDevice, st));
+    g.sigt = dsig;
+    g.cdf = dcdf;
+    g.alb_scalar = mc.albedo;
+    g.alb = nullptr;
+    if (h->albedo_grid) {
+        double *dalb = reinterpret_cast<double *>(hb.alb.ensure(nv * sizeof(double)));
+        CK(cudaMemcpyAsync(dalb, h->albedo_grid, nv * sizeof(double), cudaMemcpyHostToDevice, st));
+        g.alb = dalb;
+    }
+    Prepared P = prepare(c, &mc, want_phase, st);  // synchronises the stream (host vectors above)
+    P.volume = 1.0;
+    P.W.hetero = 1;
+    P.W.hg = g;
+    P.Q.hetero = 1;
+    P.Q.hg = g;
+    return P;
+}
+
+void cov_hetero_locked(Ctx &c, const scmc_hetero_args *h, double *d_Ms, double *d_Mm, double *d_mean1,
+                       cudaStream_t st)
+{
+    CK(cudaSetDevice(h->mc.device));
+    scmc_mc_args mc;
+    Prepared P = prepare_hetero(c, h, 0, true, st, mc);
+    HeteroBufs &hb = g_hbufs[c.device];
+    const int64_t n1 = mc.nv * mc.nl;
+    double *m1 = reinterpret_cast<double *>(hb.mean1.ensure(2 * n1 * sizeof(double)));
+    double *z = reinterpret_cast<double *>(hb.zeros.ensure(2 * n1 * sizeof(double)));
+    CK(cudaMemsetAsync(m1, 0, 2 * n1 * sizeof(double), st));
+    CK(cudaMemsetAsync(z, 0, 2 * n1 * sizeof(double), st));
+    double2 *Ms = reinterpret_cast<double2 *>(d_Ms), *Mm = reinterpret_cast<double2 *>(d_Mm);
+    const scmc_mc_args *a = &mc;
+    if (mc.dim == 3) {
+        if (mc.precision == SCMC_PREC_FP64) cov_run_cc<3, P64>(c, a, P, Ms, Mm, st, m1);
+        else if (mc.precision == SCMC_PREC_FP32) cov_run_cc<3, P32>(c, a, P, Ms, Mm, st, m1);
+        else cov_run_tc<3>(c, a, P, Ms, Mm, st, m1);
+    } else {
+        if (mc.precision == SCMC_PREC_FP64) cov_run_cc<2, P64>(c, a, P, Ms, Mm, st, m1);
+        else if (mc.precision == SCMC_PREC_FP32) cov_run_cc<2, P32>(c, a, P, Ms, Mm, st, m1);
+        else cov_run_tc<2>(c, a, P, Ms, Mm, st, m1);
+    }
+    if (d_mean1) {
+        // MCCovHetro.m:276: mean1 / maxItr / sqrt(cs), cs = 1 (see the header)
+        const double m = (double)(mc.norm_itr > 0 ? mc.norm_itr : mc.max_itr);
+        const double norm = m > 0 ? 1.0 / m : 0.0;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n1 + 255) / 256, 1024));
+        if (mc.dim == 3)
+            field_finalize_kernel<3, double><<<grid, 256, 0, st>>>(P.Q, m1, z, norm, reinterpret_cast<double2 *>(d_mean1));
+        else
+            field_finalize_kernel<2, double><<<grid, 256, 0, st>>>(P.Q, m1, z, norm, reinterpret_cast<double2 *>(d_mean1));
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+}
+
+void field_hetero_locked(Ctx &c, const scmc_hetero_args *h, double *d_u, cudaStream_t st)
+{
+    CK(cudaSetDevice(h->mc.device));
+    scmc_mc_args mc;
+    Prepared P = prepare_hetero(c, h, 1, false, st, mc);
+    double2 *u = reinterpret_cast<double2 *>(d_u);
+    const scmc_mc_args *a = &mc;
+    if (mc.dim == 3) {
+        if (mc.precision == SCMC_PREC_FP64) field_run<3, P64, double>(c, a, P, u, st);
+        else if (mc.precision == SCMC_PREC_FP32) field_run<3, P32, float>(c, a, P, u, st);
+        else field_run<3, PMIX, double>(c, a, P, u, st);
+    } else {
+        if (mc.precision == SCMC_PREC_FP64) field_run<2, P64, double>(c, a, P, u, st);
+        else if (mc.precision == SCMC_PREC_FP32) field_run<2, P32, float>(c, a, P, u, st);
+        else field_run<2, PMIX, double>(c, a, P, u, st);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1130,6 +1273,39 @@ int scmc_field_fourier_quad(const scmc_fq_args *args, double *u)
         const size_t bytes = (size_t)nv0 * nv0 * args->nl * 2 * sizeof(double);
         double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
         fq_device_locked(c, args, d, 0);
+        CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
+    });
+}
+
+int scmc_cov_hetero(const scmc_hetero_args *args, double *Ms, double *Mm, double *mean1)
+{
+    return guarded([&] {
+        if (!args) fail(SCMC_ERR_INVALID, "null arguments");
+        validate(&args->mc);
+        Ctx &c = context(args->mc.device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const size_t bytes = (size_t)args->mc.nv * args->mc.nv * args->mc.nl * args->mc.nl * 2 * sizeof(double);
+        const size_t b1 = (size_t)args->mc.nv * args->mc.nl * 2 * sizeof(double);
+        double *d0 = Ms ? reinterpret_cast<double *>(c.out0.ensure(bytes)) : nullptr;
+        double *d1 = Mm ? reinterpret_cast<double *>(c.out1.ensure(bytes)) : nullptr;
+        double *d2 = mean1 ? reinterpret_cast<double *>(c.out2.ensure(b1)) : nullptr;
+        cov_hetero_locked(c, args, d0, d1, d2, 0);
+        if (Ms) CK(cudaMemcpy(Ms, d0, bytes, cudaMemcpyDeviceToHost));
+        if (Mm) CK(cudaMemcpy(Mm, d1, bytes, cudaMemcpyDeviceToHost));
+        if (mean1) CK(cudaMemcpy(mean1, d2, b1, cudaMemcpyDeviceToHost));
+    });
+}
+
+int scmc_field_hetero(const scmc_hetero_args *args, double *u)
+{
+    return guarded([&] {
+        if (!args || !u) fail(SCMC_ERR_INVALID, "null arguments");
+        validate(&args->mc);
+        Ctx &c = context(args->mc.device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const size_t bytes = (size_t)args->mc.nv * args->mc.nl * 2 * sizeof(double);
+        double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
+        field_hetero_locked(c, args, d, 0);
         CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
     });
 }

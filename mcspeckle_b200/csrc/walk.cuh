@@ -14,6 +14,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "hgrid.cuh"
 
 namespace scmc {
 
@@ -40,15 +41,129 @@ struct WalkState {
     double x[3], w[3], ow[3];
     double px, weight;
     int pL;
+    bool dead;   // dropped before its first event (voxel-medium plane launch missed)
 };
 
-// Initialise a path: first scatterer (MCfield.m:118-125) and first
-// direction (MCfield.m:149-155).
+// smpWoodcock.m:1-15: delta tracking against max(sigt) along v from x.
 template <int DIM>
-__device__ __forceinline__ void path_init(const WalkParams &P, PathRng &r, WalkState &s)
+__device__ __forceinline__ double hg_woodcock(const HGrid &g, const double *x, const double *v, PathRng &r)
+{
+    double d = 0.0, nx[3] = {0, 0, 0};
+    for (int guard = 0; guard < (1 << 24); ++guard) {
+        d = d - log(1 - r.rand()) / g.sigt_max;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) nx[k] = x[k] + d * v[k];
+        if (hg_outside(g, nx)) break;
+        const int64_t bi = hg_find_bin(g, nx, nullptr, nullptr);
+        if (r.rand() <= (g.sigt[bi] / g.sigt_max)) break;
+    }
+    return d;
+}
+
+// First scatterer in the voxel medium (MCCovHetro.m:90-115).  Returns false
+// when the path is dropped (plane launch missing the box).
+template <int DIM>
+__device__ __forceinline__ bool hg_first_scatter(const WalkParams &P, PathRng &r, WalkState &s)
+{
+    const HGrid &g = P.hg;
+    if (P.smp_flg == 1) {
+        // smpicdf.m over invCDFvec.m: voxel = count of cdf values below the
+        // upper edge of hist bin i, i = ceil(rand * N)
+        int64_t i = (int64_t)ceil(r.rand() * (double)g.n_icdf);
+        i = i < 1 ? 1 : i;
+        int64_t cnt;
+        if (g.n_vox == 1 || i >= g.n_icdf) {
+            cnt = g.n_vox;
+        } else {
+            const double edge = g.cdf_lo + (double)i * g.cdf_step;
+            int64_t lo = 0, hi = g.n_vox;  // first k with cdf[k] >= edge
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (g.cdf[mid] < edge) lo = mid + 1;
+                else hi = mid;
+            }
+            cnt = lo;
+        }
+        int64_t rem = (cnt < 1 ? 1 : cnt) - 1;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            const int64_t ii = rem % g.nb[k];
+            rem /= g.nb[k];
+            const double bmn = g.bmin[k] + g.bbin[k] * (double)ii;
+            s.x[k] = r.rand() * g.bbin[k] + bmn;
+        }
+        s.px = g.inv_V;
+        return !hg_outside(g, s.x);
+    }
+    // expSmpXHetro.m:1-31: launch from a plane across meanl, enter the box,
+    // one Woodcock flight; px = |transmittance|^2 / lrad^(dim-1)
+    double mx = 0.0;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) mx = fmax(mx, fmax(fabs(g.bmax[k]), fabs(g.bmin[k])));
+    double q[2] = {0, 0};
+#pragma unroll
+    for (int k = 0; k < DIM - 1; ++k) q[k] = (r.rand() - 0.5) * g.lrad;
+    double x0[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        double a = 0.0;
+#pragma unroll
+        for (int c = 0; c < DIM - 1; ++c) a += g.basis[k + DIM * c] * q[c];
+        x0[k] = a - P.meanl[k] * mx * DIM;
+    }
+    // cubeProj.m:1-18
+    const double thr = 1.0000000000000004e-07;
+    double d = -INFINITY;
+#pragma unroll
+    for (int j = 0; j < DIM; ++j) {
+        const double den = fmax(fabs(P.meanl[j]), thr);
+        const double bd = (P.meanl[j] <= 0) ? (x0[j] - g.bmax[j]) / den : (-x0[j] + g.bmin[j]) / den;
+        d = fmax(d, bd);
+    }
+    if (!(d >= 0)) return false;
+    double ep = 0.0;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) ep = fmax(ep, fabs(g.bmax[k] - g.bmin[k]));
+    ep = 1.0000000000000002e-04 * ep;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) s.x[k] = x0[k] + (d + ep) * P.meanl[k];
+    if (hg_outside(g, s.x)) return false;
+    const double dw = hg_woodcock<DIM>(g, s.x, P.meanl, r);
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) s.x[k] = s.x[k] + dw * P.meanl[k];
+    if (hg_outside(g, s.x)) return false;
+    const double wbdv = hg_optical_depth<DIM>(g, s.x, P.meanl, 1.0e12);
+    const double e = exp(-(1.0 / 2.0 * wbdv));
+    s.px = e * e / pow(g.lrad, (double)(DIM - 1));
+    return true;
+}
+
+// Initialise a path: first scatterer (MCfield.m:118-125) and first
+// direction (MCfield.m:149-155).  Returns false for a dropped path (voxel
+// medium only), which the walk records as one event of zero weight.
+template <int DIM>
+__device__ __forceinline__ bool path_init(const WalkParams &P, PathRng &r, WalkState &s)
 {
 #pragma unroll
     for (int k = 0; k < 3; ++k) { s.x[k] = 0.0; s.w[k] = 0.0; s.ow[k] = 0.0; }
+    s.dead = false;
+    if (P.hetero) {
+        const bool ok = hg_first_scatter<DIM>(P, r, s);
+        s.dead = !ok;
+        if (!ok) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) { s.x[k] = k < DIM ? 0.5 * (P.box_min[k] + P.box_max[k]) : 0.0; s.w[k] = P.meanl[k]; }
+            s.px = 1.0;
+            s.pL = 0;
+            s.weight = 0.0;
+            return false;
+        }
+        if (!P.has_pf0) randn_dir<DIM>(s.w, r);
+        else smpampfunc_general<DIM>(P.meanl, P.pf0, s.w, r);
+        s.pL = 0;
+        s.weight = hg_albedo(P.hg, s.x);
+        return true;
+    }
     if (P.smp_flg == 1) {
 #pragma unroll
         for (int k = 0; k < DIM; ++k) s.x[k] = r.rand() * P.box_w[k] + P.box_min[k];
@@ -60,6 +175,7 @@ __device__ __forceinline__ void path_init(const WalkParams &P, PathRng &r, WalkS
     else smpampfunc_general<DIM>(P.meanl, P.pf0, s.w, r);
     s.pL = 0;
     s.weight = P.albedo;
+    return true;
 }
 
 // After the event at s.x has been recorded: free flight, box exit, roulette
@@ -68,6 +184,23 @@ __device__ __forceinline__ void path_init(const WalkParams &P, PathRng &r, WalkS
 template <int DIM>
 __device__ __forceinline__ bool path_advance(const WalkParams &P, PathRng &r, WalkState &s)
 {
+    if (s.dead) return false;  // a dropped path is one zero-weight event
+    if (P.hetero) {
+        // MCCovHetro.m:238-254: Woodcock flight, voxel albedo
+        const double d = hg_woodcock<DIM>(P.hg, s.x, s.w, r);
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) s.x[k] = s.x[k] + d * s.w[k];
+        if (hg_outside(P.hg, s.x)) return false;
+        if (s.weight < kKillThr) {
+            if (r.rand() > hg_albedo(P.hg, s.x)) return false;
+        } else {
+            s.weight = s.weight * hg_albedo(P.hg, s.x);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s.ow[k] = s.w[k];
+        smpampfunc_general<DIM>(s.ow, P.pf, s.w, r);
+        return true;
+    }
     double d = -log(-r.rand() + 1.0) / P.sigt;
     bool out = false;
 #pragma unroll
