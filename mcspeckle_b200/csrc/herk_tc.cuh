@@ -152,9 +152,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
 template <bool SPLIT>
 __global__ void __launch_bounds__(128, 1)
 herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
-               const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int Mr,
-               int N, double *__restrict__ D, int *__restrict__ err)
+               const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int kb_per_split,
+               int Mr, int N, double *__restrict__ D, int *__restrict__ err)
 {
+    // split-K: blockIdx.y takes K-blocks [kb0, kb0 + nkb) and owns the slice
+    // D + blockIdx.y * Mr * N; the host makes every slice non-empty.
+    const int kb0 = (int)blockIdx.y * kb_per_split;
+    const int nkb = min(num_kb, kb0 + kb_per_split) - kb0;
+    if (nkb <= 0) return;
+    D += (int64_t)blockIdx.y * Mr * N;
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
     uint64_t *full = reinterpret_cast<uint64_t *>(base + TcCfg<SPLIT>::STAGES * TcCfg<SPLIT>::STAGE_BYTES);
@@ -192,7 +198,7 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
 
     if (warp == 0 && lane == 0) {
         // TMA producer
-        for (int kb = 0; kb < num_kb; ++kb) {
+        for (int kb = 0; kb < nkb; ++kb) {
             const int s = kb % TcCfg<SPLIT>::STAGES;
             if (kb >= TcCfg<SPLIT>::STAGES && !mbar_wait(&empty[s], ((kb / TcCfg<SPLIT>::STAGES) - 1) & 1)) {
                 atomicExch(abort_flag, 1);
@@ -201,15 +207,16 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
             if (*(volatile int *)abort_flag) break;
             uint8_t *st = base + s * TcCfg<SPLIT>::STAGE_BYTES;
             mbar_expect_tx(&full[s], TcCfg<SPLIT>::STAGE_BYTES);
-            tma_load_2d(st, &tm_ahi, kb * TC_BK, row0, &full[s]);
-            if (SPLIT) tma_load_2d(st + TC_A_BYTES, &tm_alo, kb * TC_BK, row0, &full[s]);
-            tma_load_2d(st + TcCfg<SPLIT>::B_OFF, &tm_b, kb * TC_BK, col0, &full[s]);
+            const int kx = (kb0 + kb) * TC_BK;
+            tma_load_2d(st, &tm_ahi, kx, row0, &full[s]);
+            if (SPLIT) tma_load_2d(st + TC_A_BYTES, &tm_alo, kx, row0, &full[s]);
+            tma_load_2d(st + TcCfg<SPLIT>::B_OFF, &tm_b, kx, col0, &full[s]);
             *(volatile int *)issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
         constexpr uint32_t idesc = umma_idesc_f16(TC_BM, TC_BN);
-        for (int kb = 0; kb < num_kb; ++kb) {
+        for (int kb = 0; kb < nkb; ++kb) {
             const int s = kb % TcCfg<SPLIT>::STAGES;
             if (!mbar_wait(&full[s], (kb / TcCfg<SPLIT>::STAGES) & 1)) {
                 atomicExch(abort_flag, 1);
@@ -486,19 +493,32 @@ inline void tc_rows(const TcPlan &p, const TcOperands &o, const NeeParams &Q, co
     kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, use_af_table ? o.af : nullptr);
 }
 
+// D[ks][Mr][N] += A B^T over num_kb K-blocks, split ksplit ways along K.
 template <bool SPLIT>
-inline void tc_herk_launch(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
+inline void tc_gemm_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, const CUtensorMap &m_b,
+                           const int2 *tiles, int n_tiles, int num_kb, int ksplit, int Mr, int N, double *D, int *err,
+                           cudaStream_t st)
 {
-    static bool attr = false;
-    if (!attr) {
+    static uint64_t attr_set = 0;  // one bit per device ordinal
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
+    if (dev < 64 && !((attr_set >> dev) & 1)) {
         if (cudaFuncSetAttribute(herk_tc_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TcCfg<SPLIT>::SMEM_BYTES) != cudaSuccess)
             throw std::runtime_error("cannot reserve shared memory for the tensor-core kernel");
-        attr = true;
+        attr_set |= (uint64_t)1 << dev;
     }
+    const int kb_per = (num_kb + ksplit - 1) / ksplit;
+    const int ks = (num_kb + kb_per - 1) / kb_per;  // every slice non-empty
+    herk_tc_kernel<SPLIT><<<dim3((unsigned)n_tiles, (unsigned)ks), 128, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
+        m_ahi, m_alo, m_b, tiles, num_kb, kb_per, Mr, N, D, err);
+}
+
+template <bool SPLIT>
+inline void tc_herk_launch(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
+{
     const int num_kb = (int)((2 * n + TC_BK - 1) / TC_BK);
-    herk_tc_kernel<SPLIT><<<o.n_tiles, 128, TcCfg<SPLIT>::SMEM_BYTES, st>>>(o.m_ahi, o.m_alo, o.m_b, o.tiles, num_kb,
-                                                                          2 * p.N, p.N, D, o.err);
+    tc_gemm_launch<SPLIT>(o.m_ahi, o.m_alo, o.m_b, o.tiles, o.n_tiles, num_kb, 1, 2 * p.N, p.N, D, o.err, st);
 }
 
 inline void tc_herk(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)

@@ -15,6 +15,7 @@
 #include "../../include/scmc_gpu.h"
 #include "accum.cuh"
 #include "herk_tc.cuh"
+#include "field_tc.cuh"
 #include "fq.cuh"
 
 using namespace scmc;
@@ -171,7 +172,7 @@ struct Ctx {
     DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
-    DevBuf acc_s, acc_m, rows, tiles, tc_a, out0, out1, out2;
+    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
 };
@@ -473,9 +474,101 @@ void launch_field_accum(Ctx &c, const Prepared &P, const Batch &B, AccT *U, int6
     LAUNCHED();
 }
 
+// The tensor-core field path pays off once the output fills a good part of a
+// 128 x 256 tile; smaller fields stay on the CUDA-core accumulation.
+bool use_field_tc(const scmc_mc_args *a)
+{
+    return (a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16) && a->nv >= 64 && a->nl >= 32;
+}
+
+template <int DIM>
+void field_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u, cudaStream_t st)
+{
+    const int nv = (int)a->nv, nl = (int)a->nl;
+    const bool split = a->precision == SCMC_PREC_MIXED;
+    const int terms_m = a->do_cbs ? 2 : 1;
+    const FieldTcPlan plan = field_tc_plan(nv, nl, terms_m, split, sm_count(c.device));
+    const bool ffff = a->is_ff_l && a->is_ff_v;
+    const size_t slice = (size_t)2 * nv * nl;
+    const size_t d_bytes = (size_t)plan.ksplit * slice * sizeof(double);
+    double *Ds = reinterpret_cast<double *>(c.acc_s.ensure(ffff ? d_bytes : slice * sizeof(double)));
+    double *Dm = reinterpret_cast<double *>(c.acc_m.ensure(d_bytes));
+    CK(cudaMemsetAsync(Ds, 0, ffff ? d_bytes : slice * sizeof(double), st));
+    CK(cudaMemsetAsync(Dm, 0, d_bytes, st));
+    FieldTcOps ops = field_tc_ops(plan, c.tc_a.ensure(field_tc_bytes(plan)), st);
+    const size_t smem = field_tc_rows_smem();
+    const int64_t chunk = plan.events_per_chunk;
+    const int phase = P.W.want_phase;
+    WalkParams W = P.W;
+    for (int64_t done = 0; done < a->max_itr;) {
+        int64_t nb = path_batch_size(a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        if (!ffff) launch_field_accum<DIM, PMIX, true, double>(c, P, B, Ds, B.n_paths, st);
+        for (int pass = ffff ? 0 : 1; pass < 2; ++pass) {
+            const bool single = pass == 0;
+            const int terms = single ? 1 : terms_m;
+            const int64_t n_ev = single ? B.n_paths : B.n_multi;
+            double *D = single ? Ds : Dm;
+            for (int64_t e0 = 0; e0 < n_ev; e0 += chunk) {
+                const int64_t n = std::min(chunk, n_ev - e0);
+                const unsigned grid = (unsigned)((n + 31) / 32);
+                {
+                    StageScope sc(ST_ROWS, st);
+#define SCMC_FT_ROWS(S_, P_)                                                                                      \
+    do {                                                                                                          \
+        auto k_ = field_tc_rows_kernel<DIM, S_, P_>;                                                              \
+        if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+        k_<<<grid, 256, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, e0, n, terms, plan.K, ops.ahi, ops.alo, ops.b,  \
+                                    phase);                                                                       \
+    } while (0)
+                    if (single && split) SCMC_FT_ROWS(true, true);
+                    else if (single) SCMC_FT_ROWS(true, false);
+                    else if (split) SCMC_FT_ROWS(false, true);
+                    else SCMC_FT_ROWS(false, false);
+#undef SCMC_FT_ROWS
+                    CK(cudaGetLastError());
+                    LAUNCHED();
+                }
+                {
+                    StageScope sc(ST_CONTRACT, st);
+                    const int num_kb = (int)((2 * terms * n + TC_BK - 1) / TC_BK);
+                    if (split)
+                        tc_gemm_launch<true>(ops.m_ahi, ops.m_alo, ops.m_b, ops.tiles, ops.n_tiles, num_kb,
+                                             plan.ksplit, 2 * nv, nl, D, ops.err, st);
+                    else
+                        tc_gemm_launch<false>(ops.m_ahi, ops.m_alo, ops.m_b, ops.tiles, ops.n_tiles, num_kb,
+                                              plan.ksplit, 2 * nv, nl, D, ops.err, st);
+                    CK(cudaGetLastError());
+                    LAUNCHED();
+                }
+                prof_count(0, 0, 8.0 * nv * nl * terms * (double)n);
+            }
+        }
+        done += nb;
+    }
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, ops.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
+    const double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
+    const double norm = m > 0 ? std::sqrt(1.0 / m * P.volume * a->sigt) : 0.0;  // MCfield.m:253-254
+    const int64_t n = (int64_t)nv * nl;
+    StageScope sc(ST_FINAL, st);
+    field_tc_finalize_kernel<DIM><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 2048)), 256, 0,
+                                    st>>>(P.Q, Ds, ffff ? plan.ksplit : 0, Dm, plan.ksplit, norm, d_u);
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
 template <int DIM, int POL, typename AccT>
 void field_run(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u, cudaStream_t st)
 {
+    if (POL == PMIX && use_field_tc(a)) {
+        field_run_tc<DIM>(c, a, P, d_u, st);
+        return;
+    }
     const int64_t n = a->nv * a->nl;
     AccT *Us = reinterpret_cast<AccT *>(c.acc_s.ensure(2 * n * sizeof(AccT)));
     AccT *Um = reinterpret_cast<AccT *>(c.acc_m.ensure(2 * n * sizeof(AccT)));
