@@ -57,6 +57,147 @@ def workload_args(n_paths):
     return [sigt, albedo, box_min, box_max, l, v, 1, 1, int(n_paths), 1.0, True, 2, 3, 0.8]
 
 
+# ---------------------------------------------------------------------------
+# served stream: uneven MCfield requests with Poisson arrivals
+# ---------------------------------------------------------------------------
+SERVED_WORKLOAD = ("served MCfield stream: lights 1-256, views 1-1024, paths log-uniform; box 5-50 MFP "
+                   "(MFP 10 wavelengths, thickness 1/4 of the side), HG g~U(0,0.95), sigma_a~U(0,0.05), "
+                   "isotropic/HG/tabulated 1:2:1, far field, CBS, Poisson arrivals")
+
+
+def cap_dirs(n, half_deg, zsign, rng):
+    """n directions uniform on the solid-angle cap <= half_deg about zsign*z."""
+    c = rng.uniform(math.cos(math.radians(half_deg)), 1.0, n)
+    phi = rng.uniform(0, 2 * math.pi, n)
+    s = np.sqrt(1 - c * c)
+    return np.stack([s * np.cos(phi), s * np.sin(phi), zsign * c])
+
+
+def hg_table(g, n=1001):
+    """A tabulated phase function (tabulatedAmplitudeScatter of an HG lobe)."""
+    from mcspeckle_b200 import interface as I
+    th = np.linspace(0, 1, n) * np.pi
+    f = np.sqrt((1 - g * g) / (4 * np.pi * (1 + g * g - 2 * g * np.cos(th)) ** 1.5))
+    t = I.tabulatedAmplitudeScatter(th, f)["ampfunc"]
+    return {"evalAmp": t["evalAmp"], "sampleIcdf": t["sampleIcdf"]}
+
+
+def served_requests(n, seed=5, paths=(1e5, 1e8), nv_max=1024, nl_max=256, side_mfp=(5.0, 50.0)):
+    """The served stream: n MCfield requests with log-uniform sizes and budgets
+    and media drawn per request.  Returns dicts with the positional MCfield
+    arguments, the Philox key and the sizes."""
+    rng = np.random.default_rng(seed)
+
+    def logu(lo, hi):
+        return math.exp(rng.uniform(math.log(lo), math.log(hi)))
+
+    out = []
+    mfp = 10.0
+    for i in range(n):
+        nl = max(1, min(nl_max, int(round(logu(1, nl_max)))))
+        nv = max(1, min(nv_max, int(round(logu(1, nv_max)))))
+        n_paths = int(round(logu(*paths)))
+        side = logu(*side_mfp) * mfp
+        g = float(rng.uniform(0.0, 0.95))
+        sa = float(rng.uniform(0.0, 0.05))
+        kind = ["iso", "hg", "hg", "tab"][int(rng.integers(0, 4))]
+        sct, amp = {"iso": (1, 0), "hg": (3, g), "tab": (2, None)}[kind]
+        if kind == "tab":
+            amp = hg_table(g)
+        l = cap_dirs(nl, 10.0, +1.0, rng)
+        v = cap_dirs(nv, 10.0, -1.0, rng)
+        args = [(1.0 + sa) / mfp, 1.0 / (1.0 + sa), np.array([-side / 2, -side / 2, 0.0]),
+                np.array([side / 2, side / 2, side / 4]), l, v, 1, 1, n_paths, 1.0, True, 2, sct, amp]
+        out.append({"args": args, "seed": 0x5E4E0000 + i, "paths": n_paths, "nv": nv, "nl": nl, "scatter": kind})
+    return out
+
+
+def serve(reqs, slots=8, rate=None, precision="mixed", device=0, budget=80e9):
+    """Runs the requests through the request server.  rate None: all submitted
+    at once (closed batch); else Poisson arrivals at `rate` requests/s.
+    Returns per-request infos (server clock) and the results."""
+    from mcspeckle_b200 import mc as MC
+    from mcspeckle_b200.serving import Server
+    holders = [MC.mc_args(*r["args"], seed=r["seed"], precision=precision, device=device) for r in reqs]
+    gaps = np.random.default_rng(11).exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
+    arrive = np.cumsum(gaps) - gaps[0]
+    tickets = [None] * len(reqs)
+    with Server(device=device, slots=slots, hbm_budget=budget) as srv:
+        ready = threading.Event()
+
+        def submitter():
+            t0 = time.perf_counter()
+            for i, h in enumerate(holders):
+                dt = arrive[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets[i] = srv.submit_field(h)
+                if i == 0:
+                    ready.set()
+            ready.set()
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        infos, results = [], []
+        for i in range(len(reqs)):
+            while tickets[i] is None:
+                time.sleep(0.0005)
+            u, info = srv.wait(tickets[i])
+            infos.append(info)
+            results.append(u)
+        th.join()
+        stats = srv.stats()
+    return infos, results, stats
+
+
+def served_summary(reqs, infos):
+    lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
+    t0 = min(i["submit_ms"] for i in infos)
+    t1 = max(i["done_ms"] for i in infos)
+    paths = sum(r["paths"] for r in reqs)
+    busy = sum(i["device_ms"] for i in infos)
+    return {"requests": len(reqs), "paths": int(paths), "makespan_s": (t1 - t0) / 1000.0,
+            "paths_per_s": paths / ((t1 - t0) / 1000.0), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "sum_device_ms": busy}
+
+
+def run_served_leg(a, device):
+    """Served stream at reduced path budgets: closed batch (capacity), then
+    Poisson arrivals at 85% of that capacity (latency), then a plain FP32
+    one-request-at-a-time pass and the same requests served, on a prefix."""
+    from mcspeckle_b200 import mc as MC
+    lo, hi = a.served_paths_min, a.served_paths_max
+    reqs = served_requests(a.served_requests, paths=(lo, hi))
+    infos, _, st_closed = serve(reqs, slots=a.slots, device=device)
+    closed = served_summary(reqs, infos)
+    rate = 0.85 * len(reqs) / closed["makespan_s"]
+    infos, _, st_open = serve(reqs, slots=a.slots, rate=rate, device=device)
+    opened = served_summary(reqs, infos)
+    # plain FP32, one request at a time, on a prefix of the stream (bounded time)
+    t0 = time.perf_counter()
+    k = 0
+    while k < len(reqs) and time.perf_counter() - t0 < a.served_fp32_seconds:
+        r = reqs[k]
+        MC.field_from_args(MC.mc_args(*r["args"], seed=r["seed"], precision="fp32", device=device))
+        k += 1
+    fp32_s = time.perf_counter() - t0
+    prefix = reqs[:k]
+    infos_p, _, _ = serve(prefix, slots=a.slots, device=device)
+    served_prefix = served_summary(prefix, infos_p)
+    fp32_rate = sum(r["paths"] for r in prefix) / fp32_s
+    return {
+        "workload": SERVED_WORKLOAD, "requests": len(reqs), "paths_range": [lo, hi],
+        "path_budget_note": "config budgets 1e5-1e8 scaled to the stated range so the leg runs in about a minute",
+        "slots": a.slots, "hbm_budget_gb": 80, "precision": "mixed",
+        "closed_batch": closed, "poisson": dict(opened, offered_load=0.85, rate_per_s=rate),
+        "peak_reserved_gb": max(st_closed["peak_reserved_bytes"], st_open["peak_reserved_bytes"]) / 1e9,
+        "fp32_one_at_a_time": {"requests": k, "paths_per_s": fp32_rate, "seconds": fp32_s},
+        "served_same_prefix": {"requests": k, "paths_per_s": served_prefix["paths_per_s"]},
+        "speedup_vs_fp32_one_at_a_time": served_prefix["paths_per_s"] / fp32_rate,
+    }
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -180,6 +321,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp16", choices=["mixed", "fp16"],
                     help="mixed: FP16 hi+lo split (2 tensor products); fp16: one FP16 product")
+    ap.add_argument("--served-requests", type=int, default=200)
+    ap.add_argument("--served-paths-min", type=float, default=1e4)
+    ap.add_argument("--served-paths-max", type=float, default=1e7)
+    ap.add_argument("--served-fp32-seconds", type=float, default=20.0)
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--no-served", action="store_true")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
@@ -323,6 +470,7 @@ def main():
         tot = time.perf_counter()
         MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision=other, device=local))
         other_small_s = time.perf_counter() - tot
+        served = None if a.no_served else run_served_leg(a, local)
         cpu = None
         if not a.no_cpu_baseline:
             rate, n, dt, thr = cpu_oracle_rate(workload_args, target_s=a.cpu_seconds)
@@ -355,6 +503,7 @@ def main():
             "fp32_gpu": {"paths": int(a.fp32_paths), "value": int(a.fp32_paths) / fp32_s,
                          "mixed_same_sample": int(a.fp32_paths) / mixed_small_s,
                          "speedup_mixed_over_fp32": (int(a.fp32_paths) / mixed_small_s) / (int(a.fp32_paths) / fp32_s)},
+            "serving": served,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -249,6 +249,72 @@ typedef struct {
 int scmc_profile_enable(int32_t on);
 int scmc_profile_read(scmc_stage_times *out, int32_t reset);
 
+/* ---------------------------------------------------------------------------
+ * Serving: a request server for streams of MCfield / MCcov solves of uneven
+ * sizes.  No reference counterpart (the reference solves one call at a time
+ * in the MATLAB interpreter, parfor workers aside: scmc.m:421-445); the
+ * requests are exactly scmc_field / scmc_cov calls, with the same arguments
+ * and results.
+ *
+ * The server owns n_slots worker slots, each with its own CUDA stream and
+ * scratch memory (stream-ordered allocations).  A submitted request waits in
+ * a FIFO queue until a slot is free and its estimated device memory fits the
+ * HBM budget next to the requests already running; then it runs on that
+ * slot's stream, so requests on different slots overlap on the device.  The
+ * output arrays stay owned by the caller and must stay valid until
+ * scmc_server_wait has reported the request finished.  A request's result does
+ * not depend on what else runs: each path draws from its own Philox stream
+ * and every accumulator is private to the slot.
+ * ------------------------------------------------------------------------- */
+typedef struct scmc_server scmc_server;
+
+enum { SCMC_REQ_FIELD = 0, SCMC_REQ_COV = 1 };
+
+typedef struct {
+    int64_t ticket;
+    int32_t kind;           /* SCMC_REQ_* */
+    int32_t slot;           /* worker slot that ran it (-1 while queued) */
+    int32_t status;         /* scmc_status of the solve once finished */
+    int32_t finished;       /* 0 queued or running, 1 finished */
+    double submit_ms;       /* host steady clock, ms since the server was created */
+    double start_ms;        /* admitted to a slot */
+    double done_ms;         /* result copied to the caller's arrays */
+    double device_ms;       /* CUDA-event time on the slot stream, first to last launch */
+    int64_t reserved_bytes; /* device memory reserved against the budget */
+    int64_t peak_bytes;     /* device memory the slot actually held for it */
+    int64_t paths;          /* max_itr of the request */
+} scmc_request_info;
+
+typedef struct {
+    int32_t n_slots;
+    int32_t busy_slots;
+    int64_t queued;
+    int64_t completed;
+    int64_t failed;
+    int64_t budget_bytes;
+    int64_t reserved_bytes;      /* now */
+    int64_t peak_reserved_bytes; /* high-water mark */
+    int64_t paths_completed;
+} scmc_server_stats;
+
+/* hbm_budget_bytes <= 0: 80% of the device's free memory at creation. */
+int scmc_server_create(int32_t device, int32_t n_slots, int64_t hbm_budget_bytes, scmc_server **out);
+/* kind SCMC_REQ_FIELD: out0 = u (2*nv*nl doubles), out1 unused.
+ * kind SCMC_REQ_COV: out0 = Ms, out1 = Mm (each 2*(nv*nl)^2 doubles; either may
+ * be NULL).  Arguments are validated and copied at submission; a request
+ * whose estimate alone exceeds the budget is refused with SCMC_ERR_NOMEM. */
+int scmc_server_submit(scmc_server *s, int32_t kind, const scmc_mc_args *args, double *out0, double *out1,
+                       int64_t *ticket);
+/* Waits up to timeout_ms (< 0: no limit) for the request.  Returns the
+ * request's status when it has finished (its message via scmc_last_error),
+ * SCMC_ERR_TIMEOUT while it has not; info (may be NULL) is filled either way.
+ * A finished request's record is dropped after the first successful wait. */
+int scmc_server_wait(scmc_server *s, int64_t ticket, int64_t timeout_ms, scmc_request_info *info);
+int scmc_server_stats_read(scmc_server *s, scmc_server_stats *out);
+/* Runs the requests already admitted to completion, cancels the queued ones
+ * (SCMC_ERR_CANCELLED) and frees the server. */
+int scmc_server_destroy(scmc_server *s);
+
 /* Library information and error reporting. */
 int scmc_abi_version(void);
 const char *scmc_last_error(void);

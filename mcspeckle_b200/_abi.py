@@ -123,6 +123,49 @@ class StageTimes(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+SCMC_REQ_FIELD = 0
+SCMC_REQ_COV = 1
+
+
+class RequestInfo(C.Structure):
+    """scmc_request_info: one served request's timeline and memory."""
+    _fields_ = [
+        ("ticket", C.c_int64),
+        ("kind", C.c_int32),
+        ("slot", C.c_int32),
+        ("status", C.c_int32),
+        ("finished", C.c_int32),
+        ("submit_ms", C.c_double),
+        ("start_ms", C.c_double),
+        ("done_ms", C.c_double),
+        ("device_ms", C.c_double),
+        ("reserved_bytes", C.c_int64),
+        ("peak_bytes", C.c_int64),
+        ("paths", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    """scmc_server_stats."""
+    _fields_ = [
+        ("n_slots", C.c_int32),
+        ("busy_slots", C.c_int32),
+        ("queued", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("budget_bytes", C.c_int64),
+        ("reserved_bytes", C.c_int64),
+        ("peak_reserved_bytes", C.c_int64),
+        ("paths_completed", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
 

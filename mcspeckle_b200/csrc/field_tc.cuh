@@ -32,7 +32,8 @@ struct FieldTcOps {
 };
 
 // sms: multiprocessors; the K split fills them when the output has few tiles.
-inline FieldTcPlan field_tc_plan(int nv, int nl, int terms, bool split, int sms)
+// chunk_bytes bounds the operand memory of one chunk of events.
+inline FieldTcPlan field_tc_plan(int nv, int nl, int terms, bool split, int sms, size_t chunk_bytes = (size_t)1 << 30)
 {
     FieldTcPlan p;
     p.nv = nv;
@@ -41,7 +42,7 @@ inline FieldTcPlan field_tc_plan(int nv, int nl, int terms, bool split, int sms)
     p.split = split;
     // bytes per event: A (hi [+ lo]) 2nv rows and B nl rows, 2 fp16 per term
     const int64_t per = (int64_t)terms * 4 * ((split ? 2 : 1) * 2 * (int64_t)nv + nl);
-    int64_t e = ((int64_t)1 << 30) / std::max<int64_t>(per, 1);
+    int64_t e = (int64_t)chunk_bytes / std::max<int64_t>(per, 1);
     e = std::max<int64_t>(32, std::min<int64_t>(e, (int64_t)1 << 18));
     e = (e / 32) * 32;
     p.events_per_chunk = e;

@@ -27,6 +27,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <stdexcept>
 #include <vector>
 
@@ -397,13 +398,13 @@ struct TcOperands {
     int n_tiles;
 };
 
-inline TcPlan tc_plan(int N, bool split)
+inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30)
 {
     TcPlan p;
     p.N = N;
     p.split = split;
-    // 8N (16N split) bytes of operand per event; keep a chunk's operands near 1 GiB
-    int64_t e = ((int64_t)1 << 30) / ((split ? 16 : 8) * (int64_t)N);
+    // 8N (16N split) bytes of operand per event; keep a chunk's operands near chunk_bytes
+    int64_t e = (int64_t)chunk_bytes / ((split ? 16 : 8) * (int64_t)N);
     e = std::max<int64_t>(32, std::min<int64_t>(e, 32768));
     e = (e / 32) * 32;
     p.events_per_chunk = e;
@@ -499,14 +500,14 @@ inline void tc_gemm_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, c
                            const int2 *tiles, int n_tiles, int num_kb, int ksplit, int Mr, int N, double *D, int *err,
                            cudaStream_t st)
 {
-    static uint64_t attr_set = 0;  // one bit per device ordinal
+    static std::atomic<uint64_t> attr_set{0};  // one bit per device ordinal
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
-    if (dev < 64 && !((attr_set >> dev) & 1)) {
+    if (dev >= 64 || !((attr_set.load() >> dev) & 1)) {
         if (cudaFuncSetAttribute(herk_tc_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  TcCfg<SPLIT>::SMEM_BYTES) != cudaSuccess)
             throw std::runtime_error("cannot reserve shared memory for the tensor-core kernel");
-        attr_set |= (uint64_t)1 << dev;
+        if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
     }
     const int kb_per = (num_kb + ksplit - 1) / ksplit;
     const int ks = (num_kb + kb_per - 1) / kb_per;  // every slice non-empty

@@ -37,7 +37,17 @@ struct NeeParams {
     PhaseFn pf, pf0;
     int hetero;              // voxel medium: attenuation marched through hg
     HGrid hg;
+    float fbox_min[3], fbox_max[3];  // FP32 copies for the attenuation of PMIX / P32
 };
+
+// Fill the FP32 copies of the box (call after box_min / box_max are set).
+inline void nee_set_fbox(NeeParams &Q)
+{
+    for (int k = 0; k < 3; ++k) {
+        Q.fbox_min[k] = (float)Q.box_min[k];
+        Q.fbox_max[k] = (float)Q.box_max[k];
+    }
+}
 
 template <typename T> struct cplx_t;
 template <> struct cplx_t<double> { using type = double2; };
@@ -145,6 +155,42 @@ phaseatt(const double *x, const double *d, int is_ff, const NeeParams &Q)
         sincosf((float)Q.kw * pv, &s, &c);
         float a = expf(-(float)Q.sigt_half * bdv) * rv;
         return make_float2(a * c, a * s);
+    } else if constexpr (POL == PMIX) {
+        // Only the phase argument k*pv needs FP64: it is formed and reduced
+        // mod 2pi in FP64.  The attenuation exp(-sigt/2*bdv)*rv, whose
+        // relative error is that of bdv, is evaluated in FP32.
+        float xf[3], u[3], rv = 1.f;
+        double pv = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) xf[k] = (float)x[k];
+        float nearest = INFINITY;
+        if (is_ff) {
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) { pv += x[k] * d[k]; u[k] = -(float)d[k]; }
+        } else {
+            double dd[3], nd = 0.0;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) { dd[k] = x[k] - d[k]; nd += dd[k] * dd[k]; }
+            nd = sqrt(nd);
+            const float ndf = (float)nd, inv = 1.f / ndf;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) u[k] = -(float)dd[k] * inv;
+            pv = nd;
+            const float t = ndf + 0.01f * (float)Q.lambda;
+            rv = (DIM == 3) ? __frcp_rn(t) : rsqrtf(t);
+            nearest = ndf;
+        }
+        float bdv = nearest;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) {
+            const float den = fmaxf(fabsf(u[j]), 1.0000000000000004e-07f);
+            const float num = (u[j] <= 0.f) ? (xf[j] - Q.fbox_min[j]) : (Q.fbox_max[j] - xf[j]);
+            bdv = fminf(bdv, __fdividef(num, den));
+        }
+        float s, c;
+        __sincosf((float)reduce_2pi(Q.kw * pv), &s, &c);
+        const float a = __expf(-(float)Q.sigt_half * bdv) * rv;
+        return make_float2(a * c, a * s);
     } else {
         double pv, rv, bdv, u[3];
         if (is_ff) {
@@ -166,17 +212,46 @@ phaseatt(const double *x, const double *d, int is_ff, const NeeParams &Q)
         }
         double ph = Q.kw * pv;
         double at = Q.sigt_half * bdv;
-        if constexpr (POL == P64) {
-            double s, c;
-            sincos(ph, &s, &c);
-            double a = exp(-at) * rv;
-            return make_double2(a * c, a * s);
-        } else {
-            float s, c;
-            sincosf((float)reduce_2pi(ph), &s, &c);
-            float a = expf(-(float)at) * (float)rv;
-            return make_float2(a * c, a * s);
+        double s, c;
+        sincos(ph, &s, &c);
+        double a = exp(-at) * rv;
+        return make_double2(a * c, a * s);
+    }
+}
+
+// Scattering amplitude af(c) in the arithmetic of the policy.  P64 is
+// evalampfunc (FP64, evalampfunc_general.m:1-19).  PMIX / P32 evaluate it in
+// FP32: HG as sqrt((1-g^2)/(4pi)) * den^(-3/4) (3-D) or sqrt((1-g^2)/(2pi)) *
+// den^(-1/2) (2-D) with den = 1 + g^2 - 2gc (formed in FP64 for PMIX, where
+// it cancels for forward lobes); tabulated as the nearest entry of the
+// angle acos(c), taken as 2 asin(sqrt((1-c)/2)) (or pi minus its mirror for
+// c < 0) so that FP32 keeps the angle accurate near 0 and pi.
+template <int DIM, int POL>
+__device__ __forceinline__ typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type
+amp_eval(double c, const PhaseFn &pf)
+{
+    if constexpr (POL == P64) {
+        return evalampfunc<DIM>(c, pf);
+    } else {
+        if (pf.sct_type == 1) return make_float2((float)(1.0 / sqrt((DIM == 3 ? 4.0 : 2.0) * SCMC_PI)), 0.f);
+        if (pf.sct_type == 2) {
+            const double cc = fmin(fmax(c, -1.0), 1.0);
+            float ang;
+            if (cc >= 0.0) ang = 2.f * asinf(sqrtf((float)(0.5 * (1.0 - cc))));
+            else ang = (float)SCMC_PI - 2.f * asinf(sqrtf((float)(0.5 * (1.0 + cc))));
+            const float span = (DIM == 2) ? (float)(2.0 * SCMC_PI) : (float)SCMC_PI;
+            int idx = (int)roundf(ang * (float)(pf.table_n - 1) / span);
+            idx = idx < 0 ? 0 : (idx > pf.table_n - 1 ? pf.table_n - 1 : idx);
+            const double2 t = pf.eval_amp[idx];
+            return make_float2((float)t.x, (float)t.y);
         }
+        const double g = pf.g;
+        float den;
+        if (POL == PMIX) den = (float)fma(-2.0 * g, c, 1.0 + g * g);
+        else den = 1.f + (float)g * (float)g - 2.f * (float)g * (float)c;
+        const float r = rsqrtf(den);
+        if (DIM == 3) return make_float2((float)sqrt((1.0 - g * g) / (4.0 * SCMC_PI)) * r * sqrtf(r), 0.f);
+        return make_float2((float)sqrt((1.0 - g * g) / (2.0 * SCMC_PI)) * r, 0.f);
     }
 }
 
@@ -279,13 +354,13 @@ __device__ __forceinline__ void nee_view(const NeeParams &Q, int i, const double
     view_dir<DIM>(Q, i, x1, rv);
     const double *vsi = Q.vs + 3 * i;
     C e = phaseatt<DIM, POL>(x, vsi, Q.is_ff_v, Q);
-    double2 af = evalampfunc<DIM>(dot3<DIM>(ow, rv), Q.pf);
-    a = cmul(e, to_c<C>(af));
+    C af = amp_eval<DIM, POL>(dot3<DIM>(ow, rv), Q.pf);
+    a = cmul(e, af);
     if (Q.cbs) {
         C e0 = phaseatt<DIM, POL>(x1, vsi, Q.is_ff_v, Q);
-        double2 af0 = evalampfunc<DIM>(-dot3<DIM>(w1, rv), Q.pf);
-        af0.x /= w0p; af0.y /= w0p;
-        a0 = cmul(e0, to_c<C>(af0));
+        C af0 = amp_eval<DIM, POL>(-dot3<DIM>(w1, rv), Q.pf);
+        af0 = cscale<C>(af0, 1.0 / w0p);
+        a0 = cmul(e0, af0);
     } else {
         a0 = C{};
     }
@@ -300,13 +375,13 @@ __device__ __forceinline__ void nee_light(const NeeParams &Q, int j, const doubl
     light_dir<DIM>(Q, j, x1, rl);
     const double *lj = Q.l + 3 * j;
     C e0 = phaseatt<DIM, POL>(x1, lj, Q.is_ff_l, Q);
-    double2 af = evalampfunc<DIM>(dot3<DIM>(w1, rl), Q.pf);
-    af.x /= w0p; af.y /= w0p;
-    b = cmul(e0, to_c<C>(af));
+    C af = amp_eval<DIM, POL>(dot3<DIM>(w1, rl), Q.pf);
+    af = cscale<C>(af, 1.0 / w0p);
+    b = cmul(e0, af);
     if (Q.cbs) {
         C e = phaseatt<DIM, POL>(x, lj, Q.is_ff_l, Q);
-        double2 af2 = evalampfunc<DIM>(-dot3<DIM>(ow, rl), Q.pf);
-        b2 = cmul(e, to_c<C>(af2));
+        C af2 = amp_eval<DIM, POL>(-dot3<DIM>(ow, rl), Q.pf);
+        b2 = cmul(e, af2);
     } else {
         b2 = C{};
     }

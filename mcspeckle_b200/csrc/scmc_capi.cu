@@ -5,7 +5,12 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -148,19 +153,32 @@ int guarded(F &&f)
 // ---------------------------------------------------------------------------
 // device buffers and the per-device context
 // ---------------------------------------------------------------------------
+// Scratch that grows on demand.  With a stream set (server slots) the memory
+// comes from the stream-ordered pool, so growing or releasing it never
+// synchronises the device with other slots' work.
 struct DevBuf {
     void *p = nullptr;
     size_t n = 0;
+    cudaStream_t ast = nullptr;
+    bool ordered = false;
     void *ensure(size_t bytes)
     {
         if (bytes <= n) return p;
-        if (p) CK(cudaFree(p));
-        p = nullptr;
-        n = 0;
+        release();
         size_t want = bytes + bytes / 8;
-        CK(cudaMalloc(&p, want));
+        if (ordered) CK(cudaMallocAsync(&p, want, ast));
+        else CK(cudaMalloc(&p, want));
         n = want;
         return p;
+    }
+    void release()
+    {
+        if (p) {
+            if (ordered) CK(cudaFreeAsync(p, ast));
+            else CK(cudaFree(p));
+        }
+        p = nullptr;
+        n = 0;
     }
     template <typename T> T *as() { return reinterpret_cast<T *>(p); }
 };
@@ -175,6 +193,35 @@ struct Ctx {
     DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
+    size_t tc_chunk_bytes = (size_t)1 << 30;  // operand memory per tensor-core chunk
+
+    template <typename F> void each(F &&f)
+    {
+        DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
+                         &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
+                         &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0,
+                         &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_counts, &fq_offsets, &fq_cursor,
+                         &fq_planes};
+        for (DevBuf *b : all) f(*b);
+    }
+    void set_stream_ordered(cudaStream_t st)
+    {
+        each([&](DevBuf &b) {
+            b.ast = st;
+            b.ordered = true;
+        });
+    }
+    size_t held()
+    {
+        size_t t = 0;
+        each([&](DevBuf &b) { t += b.n; });
+        return t;
+    }
+    void release_all()
+    {
+        each([](DevBuf &b) { b.release(); });
+        scap = mcap = 0;
+    }
 };
 
 std::mutex g_ctx_mu;
@@ -322,6 +369,7 @@ Prepared prepare(Ctx &c, const scmc_mc_args *a, int want_phase, cudaStream_t st)
         Q.box_max[k] = W.box_max[k];
         Q.meanl[k] = W.meanl[k];
     }
+    nee_set_fbox(Q);
     Q.l = c.dirs_l.as<double>();
     Q.v = c.dirs_v.as<double>();
     Q.vs = c.dirs_vs.as<double>();
@@ -487,7 +535,7 @@ void field_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u
     const int nv = (int)a->nv, nl = (int)a->nl;
     const bool split = a->precision == SCMC_PREC_MIXED;
     const int terms_m = a->do_cbs ? 2 : 1;
-    const FieldTcPlan plan = field_tc_plan(nv, nl, terms_m, split, sm_count(c.device));
+    const FieldTcPlan plan = field_tc_plan(nv, nl, terms_m, split, sm_count(c.device), c.tc_chunk_bytes);
     const bool ffff = a->is_ff_l && a->is_ff_v;
     const size_t slice = (size_t)2 * nv * nl;
     const size_t d_bytes = (size_t)plan.ksplit * slice * sizeof(double);
@@ -717,7 +765,7 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
                 double *mean1_acc = nullptr)
 {
     const int N = (int)(a->nv * a->nl);
-    TcPlan plan = tc_plan(N, a->precision == SCMC_PREC_MIXED);
+    TcPlan plan = tc_plan(N, a->precision == SCMC_PREC_MIXED, c.tc_chunk_bytes);
     const size_t acc_bytes = (size_t)2 * N * N * sizeof(double);
     double *Ds = reinterpret_cast<double *>(c.acc_s.ensure(acc_bytes));
     double *Dm = reinterpret_cast<double *>(c.acc_m.ensure(acc_bytes));
@@ -1266,7 +1314,13 @@ void fq_device_locked(Ctx &c, const scmc_fq_args *a, double *d_u, cudaStream_t s
     else fq_run<PMIX, double>(c, a, u, st);
 }
 
+#include "server.cuh"
+
 }  // namespace
+
+struct scmc_server {
+    Server impl;
+};
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -1627,6 +1681,7 @@ void field_noalloc_run(const scmc_mc_args *a, double2 *d_u, cudaStream_t st)
         Q.box_max[k] = W.box_max[k];
         Q.meanl[k] = W.meanl[k];
     }
+    nee_set_fbox(Q);
     Q.l = dl;
     Q.v = dv;
     Q.vs = dvs;
@@ -1759,5 +1814,121 @@ extern "C" int scmc_field_noalloc(const scmc_mc_args *args, double *d_u, void *s
             else field_noalloc_run<2, PMIX, double>(args, u, st);
         }
         CK(cudaStreamSynchronize(st));
+    });
+}
+
+// ---------------------------------------------------------------------------
+// serving (scmc_server_*)
+// ---------------------------------------------------------------------------
+extern "C" int scmc_server_create(int32_t device, int32_t n_slots, int64_t hbm_budget_bytes, scmc_server **out)
+{
+    return guarded([&] {
+        if (!out) fail(SCMC_ERR_INVALID, "null output");
+        if (n_slots < 1 || n_slots > 64) fail(SCMC_ERR_INVALID, "n_slots must be between 1 and 64");
+        context(device);  // checks the ordinal and the architecture
+        CK(cudaSetDevice(device));
+        if (hbm_budget_bytes <= 0) {
+            size_t fr = 0, tot = 0;
+            CK(cudaMemGetInfo(&fr, &tot));
+            hbm_budget_bytes = (int64_t)(0.8 * (double)fr);
+        }
+        // keep freed slot memory cached in this process's pool up to the budget
+        cudaMemPool_t pool;
+        CK(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t thr = (uint64_t)hbm_budget_bytes;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+        scmc_server *s = new scmc_server();
+        s->impl.device = device;
+        s->impl.n_slots = n_slots;
+        s->impl.budget = hbm_budget_bytes;
+        s->impl.start();
+        *out = s;
+    });
+}
+
+extern "C" int scmc_server_submit(scmc_server *s, int32_t kind, const scmc_mc_args *args, double *out0, double *out1,
+                                  int64_t *ticket)
+{
+    return guarded([&] {
+        if (!s || !ticket) fail(SCMC_ERR_INVALID, "null server or ticket");
+        if (kind != SCMC_REQ_FIELD && kind != SCMC_REQ_COV) fail(SCMC_ERR_INVALID, "unknown request kind");
+        validate(args);
+        if (args->device != s->impl.device) fail(SCMC_ERR_INVALID, "request device differs from the server's device");
+        if (kind == SCMC_REQ_FIELD && !out0) fail(SCMC_ERR_INVALID, "null output");
+        Request *r = new Request();
+        r->kind = kind;
+        r->args.take(*args);
+        r->out0 = out0;
+        r->out1 = kind == SCMC_REQ_COV ? out1 : nullptr;
+        r->estimate = request_estimate(kind, r->args.a, sm_count(s->impl.device), s->impl.chunk_bytes);
+        if (r->estimate > s->impl.budget) {
+            delete r;
+            fail(SCMC_ERR_NOMEM, "request needs more device memory than the server's HBM budget");
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->impl.mu);
+            if (s->impl.stopping) {
+                delete r;
+                fail(SCMC_ERR_CANCELLED, "server is shutting down");
+            }
+            r->ticket = s->impl.next_ticket++;
+            r->submit_ms = s->impl.now_ms();
+            s->impl.table[r->ticket] = r;
+            s->impl.queue.push_back(r);
+            *ticket = r->ticket;
+        }
+        s->impl.cv_work.notify_all();
+    });
+}
+
+extern "C" int scmc_server_wait(scmc_server *s, int64_t ticket, int64_t timeout_ms, scmc_request_info *info)
+{
+    int result = SCMC_OK;
+    const int g = guarded([&] {
+        if (!s) fail(SCMC_ERR_INVALID, "null server");
+        std::unique_lock<std::mutex> lk(s->impl.mu);
+        auto it = s->impl.table.find(ticket);
+        if (it == s->impl.table.end()) fail(SCMC_ERR_INVALID, "unknown ticket");
+        Request *r = it->second;
+        auto pred = [&] { return r->finished != 0; };
+        if (timeout_ms < 0) s->impl.cv_done.wait(lk, pred);
+        else s->impl.cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred);
+        s->impl.info(*r, info);
+        if (!r->finished) {
+            result = SCMC_ERR_TIMEOUT;
+            g_last_error = "request has not finished";
+            return;
+        }
+        result = r->status;
+        g_last_error = r->message;
+        s->impl.table.erase(it);
+        delete r;
+    });
+    return g != SCMC_OK ? g : result;
+}
+
+extern "C" int scmc_server_stats_read(scmc_server *s, scmc_server_stats *out)
+{
+    return guarded([&] {
+        if (!s || !out) fail(SCMC_ERR_INVALID, "null server or output");
+        std::lock_guard<std::mutex> lk(s->impl.mu);
+        out->n_slots = s->impl.n_slots;
+        out->busy_slots = s->impl.busy;
+        out->queued = (int64_t)s->impl.queue.size();
+        out->completed = s->impl.completed;
+        out->failed = s->impl.failed;
+        out->budget_bytes = s->impl.budget;
+        out->reserved_bytes = s->impl.reserved;
+        out->peak_reserved_bytes = s->impl.peak_reserved;
+        out->paths_completed = s->impl.paths_completed;
+    });
+}
+
+extern "C" int scmc_server_destroy(scmc_server *s)
+{
+    return guarded([&] {
+        if (!s) return;
+        s->impl.shutdown();
+        delete s;
     });
 }

@@ -42,3 +42,31 @@ def test_python_struct_matches_header_layout():
     fields = re.findall(r"(\w+)(?:\[\d+\])?;", body)
     py = [f[0].rstrip("_") for f in _abi.McArgs._fields_]
     assert py == [f.rstrip("_") for f in fields]
+
+
+def _header_fields(name):
+    src = open(HEADER).read()
+    body = src[:src.index("} %s;" % name)]
+    body = body[body.rindex("typedef struct {"):]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    return re.findall(r"(\w+)(?:\[\d+\])?;", body)
+
+
+def test_serving_structs_match_header_layout():
+    from mcspeckle_b200 import _abi
+    assert [f[0] for f in _abi.RequestInfo._fields_] == _header_fields("scmc_request_info")
+    assert [f[0] for f in _abi.ServerStats._fields_] == _header_fields("scmc_server_stats")
+    assert [f[0] for f in _abi.StageTimes._fields_] == _header_fields("scmc_stage_times")
+
+
+def test_server_create_without_gpu_fails_loudly():
+    """No CPU fallback: without a visible sm_100 device the server refuses."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    import ctypes as C
+    from mcspeckle_b200 import _abi, _lib
+    h = C.c_void_p()
+    st = _lib.lib().scmc_server_create(0, 2, 0, C.byref(h))
+    assert st in (_abi.SCMC_ERR_NODEVICE, _abi.SCMC_ERR_CUDA)
+    assert not h.value
