@@ -131,9 +131,10 @@ int scmc_field(const scmc_mc_args *args, double *u);
 int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream);
 
 /* Field without any device allocation.  For callers that cannot allocate
- * device memory while they call in: code running inside a CUDA-graph
- * capture, a process that reserved its GPU memory budget up front, or a host
- * thread on which cudaMalloc / cudaFree are not allowed.  Same computation as
+ * device memory while they call in: a process that reserved its GPU memory
+ * budget up front, a real-time loop that must not take the allocator's locks
+ * or let cudaFree synchronise the device, or a host thread on which
+ * cudaMalloc / cudaFree are not allowed.  Same computation as
  * scmc_field_device, with every piece of device scratch in one fixed 32 MiB
  * array inside the library, which each GPU that loads the library holds
  * until the process exits.  No counterpart in the reference (MATLAB manages
@@ -244,6 +245,9 @@ typedef struct {
     int64_t paths;              /* paths walked */
     int64_t events;             /* scattering events (single + multiple) */
     double contract_flops;      /* algorithmic: 4*N*(N+1) per event, N = nv*nl */
+    double contract_busy_ms;    /* time with at least one contraction in flight (launches on
+                                   several streams overlap; each instant counts once) */
+    double rows_busy_ms;        /* the same for the row generation */
 } scmc_stage_times;
 
 int scmc_profile_enable(int32_t on);

@@ -117,6 +117,8 @@ class StageTimes(C.Structure):
         ("paths", C.c_int64),
         ("events", C.c_int64),
         ("contract_flops", C.c_double),
+        ("contract_busy_ms", C.c_double),
+        ("rows_busy_ms", C.c_double),
     ]
 
     def as_dict(self):

@@ -322,9 +322,10 @@ herk_cc_kernel(const typename cplx_t<R>::type *__restrict__ T, int64_t n_ev, int
 // Full nv x nv x nl x nl output from the Hermitian accumulator.
 // layout 0: C[i][j] complex row-major; layout 1: real-expanded D[2i+p][j].
 template <typename A>
-__global__ void cov_finalize_kernel(const A *__restrict__ Cacc, int layout, int nv, int nl, double scale,
-                                    double2 *__restrict__ out)
+__global__ void cov_finalize_kernel(const A *__restrict__ Cacc, const A *__restrict__ Cacc2, int layout, int nv, int nl,
+                                    double scale, double2 *__restrict__ out)
 {
+    // Cacc2 (may be null): a second partial accumulator of the same layout, added in.
     const int64_t N = (int64_t)nv * nl;
     const int64_t total = N * N;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
@@ -335,12 +336,13 @@ __global__ void cov_finalize_kernel(const A *__restrict__ Cacc, int layout, int 
         bool flip = i1 > i2;
         int64_t a = flip ? i2 : i1, b = flip ? i1 : i2;
         double re, im;
-        if (layout == 0) {
-            re = (double)Cacc[2 * (a * N + b)];
-            im = (double)Cacc[2 * (a * N + b) + 1];
-        } else {
-            re = (double)Cacc[(2 * a) * N + b];
-            im = (double)Cacc[(2 * a + 1) * N + b];
+        const int64_t ore = layout == 0 ? 2 * (a * N + b) : (2 * a) * N + b;
+        const int64_t oim = layout == 0 ? ore + 1 : ore + N;
+        re = (double)Cacc[ore];
+        im = (double)Cacc[oim];
+        if (Cacc2) {
+            re += (double)Cacc2[ore];
+            im += (double)Cacc2[oim];
         }
         if (flip) im = -im;
         if (i1 == i2) im = 0.0;  // sum of |t_i|^2: real, as the reference's products give

@@ -282,6 +282,240 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
 }
 
 // ---------------------------------------------------------------------------
+// The same product on a CTA pair (cluster of 2, tcgen05 cta_group::2).
+//
+// A pair owns a 256 x 256 tile of D: CTA r loads its 128 rows of A and half
+// of the 256 B rows (B rows col0 + 128 r ..) into its own shared memory, and
+// the leader (rank 0) issues one M=256 N=256 K=16 MMA that reads both CTAs'
+// tiles; CTA r's TMEM holds D rows 128 r .. 128 r + 127.  Per SM and K block
+// that is 32 KB of TMA traffic (48 KB hi+lo) instead of 48 KB (64 KB) for the
+// single-CTA kernel at the same MMA work.  The loads are plain (no multicast);
+// their completion is counted on the leader's barrier.  The leader's MMA
+// commits arrive on both CTAs' barriers (commit multicast).  Every wait is
+// bounded as in herk_tc_kernel.
+// ---------------------------------------------------------------------------
+#ifndef SCMC_PAIR_STAGES_FP16
+#define SCMC_PAIR_STAGES_FP16 4
+#endif
+template <bool SPLIT> struct Tc2Cfg {
+    static constexpr int A_BYTES = 128 * TC_BK * 2;   // this CTA's 128 rows of A
+    static constexpr int B_BYTES = 128 * TC_BK * 2;   // this CTA's half of B
+    static constexpr int STAGE_BYTES = (SPLIT ? 2 : 1) * A_BYTES + B_BYTES;
+    // 129 KB (FP16) / 145 KB (hi+lo) of ring, so a row-generation CTA of the
+    // next chunk (about 72 KB at 64 x 64) fits on the same SM beside it.
+    static constexpr int STAGES = SPLIT ? 3 : SCMC_PAIR_STAGES_FP16;
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+    static constexpr int B_OFF = (SPLIT ? 2 : 1) * A_BYTES;
+};
+
+__device__ __forceinline__ uint32_t cluster_ctarank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// Address of the same shared-memory offset in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t addr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t ld_shared_cluster_u32(uint32_t addr)
+{
+    uint32_t v;
+    asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// TMA load into this CTA's shared memory whose completion is counted on a
+// barrier of either CTA of the pair (cluster address).  No multicast.
+__device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *map, int x, int y, uint32_t bar_cluster)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_f16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                              uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+// Arrive on the barrier at this offset in both CTAs once the leader's issued
+// MMAs have completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t *bar)
+{
+    const uint16_t mask = 0x3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(mask)
+        : "memory");
+}
+
+template <bool SPLIT>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
+herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
+                const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int kb_per_split,
+                int Mr, int N, double *__restrict__ D, int *__restrict__ err)
+{
+    using Cfg = Tc2Cfg<SPLIT>;
+    extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + Cfg::STAGES * Cfg::STAGE_BYTES);
+    uint64_t *empty = full + Cfg::STAGES;
+    uint64_t *done = empty + Cfg::STAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+    int *issued = abort_flag + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    // The split-K range is the same for both CTAs of a pair (same blockIdx.y),
+    // so either both return here or neither does.
+    const int kb0 = (int)blockIdx.y * kb_per_split;
+    const int nkb = min(num_kb, kb0 + kb_per_split) - kb0;
+    if (nkb <= 0) return;
+    D += (int64_t)blockIdx.y * Mr * N;
+    const int2 tile = tiles[blockIdx.x >> 1];
+    const int arow0 = tile.x * 256 + (int)rank * 128;  // this CTA's A rows = its D rows
+    const int col0 = tile.y * 256;                     // the pair's D columns
+    const int brow0 = col0 + (int)rank * 128;          // this CTA's B rows
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < Cfg::STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        *issued = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    cluster_sync_all();  // both CTAs' barriers exist before any load or commit reaches them
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer (both CTAs); completion counted on the leader's full[s]
+        const uint32_t full0 = mapa_shared(smem_u32(&full[0]), 0);
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % Cfg::STAGES;
+            if (kb >= Cfg::STAGES && !mbar_wait(&empty[s], ((kb / Cfg::STAGES) - 1) & 1)) {
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int *)abort_flag) break;
+            uint8_t *st = base + s * Cfg::STAGE_BYTES;
+            if (rank == 0) mbar_expect_tx(&full[s], 2 * Cfg::STAGE_BYTES);
+            const uint32_t fb = full0 + (uint32_t)(s * sizeof(uint64_t));
+            const int kx = (kb0 + kb) * TC_BK;
+            tma_load_2d_pair(st, &tm_ahi, kx, arow0, fb);
+            if (SPLIT) tma_load_2d_pair(st + Cfg::A_BYTES, &tm_alo, kx, arow0, fb);
+            tma_load_2d_pair(st + Cfg::B_OFF, &tm_b, kx, brow0, fb);
+            *(volatile int *)issued = kb + 1;
+        }
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // MMA issuer (leader only)
+        constexpr uint32_t idesc = umma_idesc_f16(256, 256);
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % Cfg::STAGES;
+            if (!mbar_wait(&full[s], (kb / Cfg::STAGES) & 1)) {
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            tc_fence_after();
+            uint8_t *st = base + s * Cfg::STAGE_BYTES;
+            const uint64_t dh = umma_desc_sw128(st);
+            const uint64_t dl = umma_desc_sw128(st + Cfg::A_BYTES);
+            const uint64_t db = umma_desc_sw128(st + Cfg::B_OFF);
+#pragma unroll
+            for (int kk = 0; kk < TC_BK / 16; ++kk) {
+                const uint64_t adv = (uint64_t)(kk * 32) >> 4;
+                umma_f16_pair(tmem, dh + adv, db + adv, idesc, (kb | kk) != 0);
+                if (SPLIT) umma_f16_pair(tmem, dl + adv, db + adv, idesc, 1u);
+            }
+            umma_commit_pair(&empty[s]);
+        }
+        umma_commit_pair(done);  // both CTAs' done[] once every issued MMA has completed
+    }
+    __syncwarp();
+
+    const bool ok = mbar_wait(done, 0);
+    tc_fence_after();
+    __syncthreads();
+    const bool failed = !ok || *(volatile int *)abort_flag;
+    if (!failed) {
+        // Epilogue: this CTA's 128 rows x 256 columns, TMEM -> smem transpose -> FP64 RMW.
+        float *ep = reinterpret_cast<float *>(base) + warp * 32 * 33;
+        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < 256; c0 += 32) {
+            uint32_t r[32];
+            tmem_ld32(tbase + c0, r);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) ep[lane * 33 + j] = __uint_as_float(r[j]);
+            __syncwarp();
+            const int n = col0 + c0 + lane;
+#pragma unroll 4
+            for (int rr = 0; rr < 32; ++rr) {
+                const int R = arow0 + warp * 32 + rr;
+                if (R < Mr && n < N) {
+                    double *p = D + (int64_t)R * N + n;
+                    *p += (double)ep[rr * 33 + lane];
+                }
+            }
+            __syncwarp();
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync_all();
+    if (threadIdx.x == 0) {
+        // After a failure anywhere in the pair, the leader waits (bounded) for
+        // every copy still in flight from either CTA before the pair exits.
+        const int peer_abort = (int)ld_shared_cluster_u32(mapa_shared(smem_u32(abort_flag), rank ^ 1u));
+        if (failed || peer_abort) {
+            atomicExch(err, 1);
+            if (rank == 0) {
+                const int mine = *(volatile int *)issued;
+                const int peer = (int)ld_shared_cluster_u32(mapa_shared(smem_u32(issued), 1));
+                const int n_issued = max(mine, peer);
+                for (int kb = (n_issued > Cfg::STAGES ? n_issued - Cfg::STAGES : 0); kb < n_issued; ++kb)
+                    (void)mbar_wait(&full[kb % Cfg::STAGES], (kb / Cfg::STAGES) & 1);
+            }
+        }
+    }
+    cluster_sync_all();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Rows of one chunk in the split FP16 K-major layout.  One CTA per group of
 // 32 events; lane = event, so each row write is 32 consecutive half2 (128 B).
 // ---------------------------------------------------------------------------
@@ -337,32 +571,43 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
         }
     }
     __syncthreads();
+    // t_i, i = v + nv*l: light-outer, view-inner, so the light factor (times
+    // the event scale) is loaded once per light and rows advance by pointer
+    // increments (no integer division per entry).
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int N = nv * nl;
     const float sc = ssc[lane];
     const int64_t col = 2 * (g0 + lane);
-    for (int i = warp; i < N; i += 8) {
-        const int vi = i % nv, lj = i / nv;
-        float2 t = cmul(sa[vi * 33 + lane], sb[lj * 33 + lane]);
-        if (SINGLE) {
-            float2 af = af_tab ? af_tab[i] : to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[lane].x1));
-            t = cmul(t, af);
-        } else if (Q.cbs) {
-            float2 t2 = cmul(sa0[vi * 33 + lane], sb2[lj * 33 + lane]);
-            t.x += t2.x;
-            t.y += t2.y;
-        }
-        t.x *= sc;
-        t.y *= sc;
-        const __half hr = __float2half_rn(t.x), hi = __float2half_rn(t.y);
-        const int64_t r0 = (int64_t)(2 * i) * K + col, r1 = (int64_t)(2 * i + 1) * K + col;
-        *reinterpret_cast<__half2 *>(Ahi + r0) = __halves2half2(hr, hi);
-        *reinterpret_cast<__half2 *>(Ahi + r1) = __halves2half2(hi, __hneg(hr));
-        if (SPLIT) {
-            const __half lr = __float2half_rn(t.x - __half2float(hr));
-            const __half li = __float2half_rn(t.y - __half2float(hi));
-            *reinterpret_cast<__half2 *>(Alo + r0) = __halves2half2(lr, li);
-            *reinterpret_cast<__half2 *>(Alo + r1) = __halves2half2(li, __hneg(lr));
+    const int64_t step = 16 * K;  // 8 views = 16 real rows
+    const bool cbs = !SINGLE && Q.cbs;
+    for (int lj = 0; lj < nl; ++lj) {
+        float2 bl = sb[lj * 33 + lane], bl2 = sb2[lj * 33 + lane];
+        bl.x *= sc;
+        bl.y *= sc;
+        bl2.x *= sc;
+        bl2.y *= sc;
+        const int64_t i0 = (int64_t)nv * lj + warp;
+        __half *ph = Ahi + 2 * i0 * K + col;
+        __half *pl = Alo + 2 * i0 * K + col;
+        for (int vi = warp; vi < nv; vi += 8, ph += step, pl += step) {
+            float2 t = cmul(sa[vi * 33 + lane], bl);
+            if (SINGLE) {
+                const float2 af =
+                    af_tab ? af_tab[vi + nv * lj] : to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[lane].x1));
+                t = cmul(t, af);
+            } else if (cbs) {
+                const float2 t2 = cmul(sa0[vi * 33 + lane], bl2);
+                t.x += t2.x;
+                t.y += t2.y;
+            }
+            const __half hr = __float2half_rn(t.x), hi = __float2half_rn(t.y);
+            *reinterpret_cast<__half2 *>(ph) = __halves2half2(hr, hi);
+            *reinterpret_cast<__half2 *>(ph + K) = __halves2half2(hi, __hneg(hr));
+            if (SPLIT) {
+                const __half lr = __float2half_rn(t.x - __half2float(hr));
+                const __half li = __float2half_rn(t.y - __half2float(hi));
+                *reinterpret_cast<__half2 *>(pl) = __halves2half2(lr, li);
+                *reinterpret_cast<__half2 *>(pl + K) = __halves2half2(li, __hneg(lr));
+            }
         }
     }
 }
@@ -384,6 +629,7 @@ __global__ void af_table_kernel(NeeParams Q, float2 *__restrict__ tab)
 struct TcPlan {
     int N;
     bool split;
+    bool pair;  // CTA-pair kernel (256 x 256 tiles) instead of single-CTA 128 x 256
     int64_t events_per_chunk;
     int64_t K;
     std::vector<int2> tiles;
@@ -394,7 +640,7 @@ struct TcOperands {
     int2 *tiles;
     int *err;
     float2 *af;
-    CUtensorMap m_ahi, m_alo, m_b;
+    CUtensorMap m_ahi, m_alo, m_b, m_b_half;  // m_b_half: 128-row boxes of B for the CTA pair
     int n_tiles;
 };
 
@@ -405,20 +651,24 @@ inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30)
     p.split = split;
     // 8N (16N split) bytes of operand per event; keep a chunk's operands near chunk_bytes
     int64_t e = (int64_t)chunk_bytes / ((split ? 16 : 8) * (int64_t)N);
-    e = std::max<int64_t>(32, std::min<int64_t>(e, 32768));
+    e = std::max<int64_t>(32, std::min<int64_t>(e, 65536));
     e = (e / 32) * 32;
     p.events_per_chunk = e;
     p.K = 2 * e;
-    const int n_tm = (2 * N + TC_BM - 1) / TC_BM;
+    // The pair kernel pays off once a 256-row tile is mostly real rows.
+    p.pair = 2 * N >= 256;
+    const int bm_rows = p.pair ? 256 : TC_BM;  // real-expanded rows per tile
+    const int n_tm = (2 * N + bm_rows - 1) / bm_rows;
     const int n_tn = (N + TC_BN - 1) / TC_BN;
-    // Upper-triangle tiles in blocks of GM x GN (tm x tn), so the CTAs of one
-    // wave share A row blocks and B column blocks in L2 while they stream K.
-    const int GM = 16, GN = 8;
+    // Upper-triangle tiles (complex rows bm_rows/2 * tm .. against columns
+    // TC_BN * tn ..) in blocks of GM x GN, so the CTAs of one wave share A row
+    // blocks and B column blocks in L2 while they stream K.
+    const int GM = p.pair ? 8 : 16, GN = 8;
     for (int bn = 0; bn < n_tn; bn += GN)
         for (int bm = 0; bm < n_tm; bm += GM)
             for (int tn = bn; tn < std::min(n_tn, bn + GN); ++tn)
                 for (int tm = bm; tm < std::min(n_tm, bm + GM); ++tm)
-                    if ((int64_t)(TC_BM / 2) * tm <= (int64_t)TC_BN * tn + TC_BN - 1) p.tiles.push_back(make_int2(tm, tn));
+                    if ((int64_t)(bm_rows / 2) * tm <= (int64_t)TC_BN * tn + TC_BN - 1) p.tiles.push_back(make_int2(tm, tn));
     return p;
 }
 
@@ -478,6 +728,7 @@ inline TcOperands tc_make_operands(const TcPlan &p, void *mem, cudaStream_t st)
     o.m_ahi = tc_map(o.ahi, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
     o.m_alo = tc_map(o.alo, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
     o.m_b = tc_map(o.ahi, K, (uint64_t)p.N, 2 * K * 2, TC_BN);
+    o.m_b_half = tc_map(o.ahi, K, (uint64_t)p.N, 2 * K * 2, TC_BN / 2);
     return o;
 }
 
@@ -515,11 +766,36 @@ inline void tc_gemm_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, c
         m_ahi, m_alo, m_b, tiles, num_kb, kb_per, Mr, N, D, err);
 }
 
+// D[ks][Mr][N] += A B^T on CTA pairs: tiles are 256 x 256 (pair rows x columns),
+// m_b_half has 128-row boxes.
+template <bool SPLIT>
+inline void tc_gemm2_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, const CUtensorMap &m_b_half,
+                            const int2 *tiles, int n_tiles, int num_kb, int ksplit, int Mr, int N, double *D, int *err,
+                            cudaStream_t st)
+{
+    static std::atomic<uint64_t> attr_set{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
+    if (dev >= 64 || !((attr_set.load() >> dev) & 1)) {
+        if (cudaFuncSetAttribute(herk_tc2_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Tc2Cfg<SPLIT>::SMEM_BYTES) != cudaSuccess)
+            throw std::runtime_error("cannot reserve shared memory for the CTA-pair tensor-core kernel");
+        if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
+    }
+    const int kb_per = (num_kb + ksplit - 1) / ksplit;
+    const int ks = (num_kb + kb_per - 1) / kb_per;
+    herk_tc2_kernel<SPLIT><<<dim3(2u * (unsigned)n_tiles, (unsigned)ks), 128, Tc2Cfg<SPLIT>::SMEM_BYTES, st>>>(
+        m_ahi, m_alo, m_b_half, tiles, num_kb, kb_per, Mr, N, D, err);
+}
+
 template <bool SPLIT>
 inline void tc_herk_launch(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
 {
     const int num_kb = (int)((2 * n + TC_BK - 1) / TC_BK);
-    tc_gemm_launch<SPLIT>(o.m_ahi, o.m_alo, o.m_b, o.tiles, o.n_tiles, num_kb, 1, 2 * p.N, p.N, D, o.err, st);
+    if (p.pair)
+        tc_gemm2_launch<SPLIT>(o.m_ahi, o.m_alo, o.m_b_half, o.tiles, o.n_tiles, num_kb, 1, 2 * p.N, p.N, D, o.err, st);
+    else
+        tc_gemm_launch<SPLIT>(o.m_ahi, o.m_alo, o.m_b, o.tiles, o.n_tiles, num_kb, 1, 2 * p.N, p.N, D, o.err, st);
 }
 
 inline void tc_herk(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)

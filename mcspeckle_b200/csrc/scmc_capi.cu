@@ -4,6 +4,7 @@
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -67,6 +68,31 @@ struct Profiler {
     std::vector<cudaEvent_t> pool;
     int64_t launches[4] = {0, 0, 0, 0};
     double ms[4] = {0, 0, 0, 0};
+    // Launch intervals relative to `ref` (recorded when profiling is switched
+    // on), so that launches overlapping on several streams are counted once
+    // in the busy time of their stage.
+    cudaEvent_t ref = nullptr;
+    std::vector<std::pair<float, float>> iv[4];
+
+    double busy_ms(int stage)
+    {
+        auto &v = iv[stage];
+        std::sort(v.begin(), v.end());
+        double t = 0.0, s = 0.0, e = -1.0;
+        bool open = false;
+        for (auto &x : v) {
+            if (!open || x.first > e) {
+                if (open) t += e - s;
+                s = x.first;
+                e = x.second;
+                open = true;
+            } else if (x.second > e) {
+                e = x.second;
+            }
+        }
+        if (open) t += e - s;
+        return t;
+    }
     int64_t paths = 0, events = 0;
     double flops = 0;
 
@@ -89,6 +115,12 @@ struct Profiler {
             CK(cudaEventElapsedTime(&t, p.a, p.b));
             ms[p.stage] += t;
             launches[p.stage] += 1;
+            if (ref) {
+                float t0 = 0.f, t1 = 0.f;
+                CK(cudaEventElapsedTime(&t0, ref, p.a));
+                CK(cudaEventElapsedTime(&t1, ref, p.b));
+                iv[p.stage].emplace_back(t0, t1);
+            }
             pool.push_back(p.a);
             pool.push_back(p.b);
         }
@@ -193,7 +225,31 @@ struct Ctx {
     DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
-    size_t tc_chunk_bytes = (size_t)1 << 30;  // operand memory per tensor-core chunk
+    size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
+    // Extra streams and events of the covariance pipeline: the walk and row
+    // generation run on `aux`, contractions alternate between the caller's
+    // stream and `aux2`.
+    cudaStream_t aux = nullptr, aux2 = nullptr;
+    cudaEvent_t ev[9] = {};
+
+    void destroy_aux()
+    {
+        if (!aux) return;
+        for (auto &e : ev) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
+        cudaStreamDestroy(aux);
+        cudaStreamDestroy(aux2);
+        aux = aux2 = nullptr;
+    }
+    void make_aux()
+    {
+        if (aux) return;
+        CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&aux2, cudaStreamNonBlocking));
+        for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
 
     template <typename F> void each(F &&f)
     {
@@ -749,12 +805,12 @@ void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     int grid = (int)std::min<int64_t>((total + 255) / 256, 4096);
     StageScope fin(ST_FINAL, st);
     if (d_Ms) {
-        cov_finalize_kernel<A><<<grid, 256, 0, st>>>(reinterpret_cast<const A *>(Cs), 0, (int)a->nv, (int)a->nl, sc, d_Ms);
+        cov_finalize_kernel<A><<<grid, 256, 0, st>>>(reinterpret_cast<const A *>(Cs), nullptr, 0, (int)a->nv, (int)a->nl, sc, d_Ms);
         CK(cudaGetLastError());
         LAUNCHED();
     }
     if (d_Mm) {
-        cov_finalize_kernel<A><<<grid, 256, 0, st>>>(reinterpret_cast<const A *>(Cm), 0, (int)a->nv, (int)a->nl, scm, d_Mm);
+        cov_finalize_kernel<A><<<grid, 256, 0, st>>>(reinterpret_cast<const A *>(Cm), nullptr, 0, (int)a->nv, (int)a->nl, scm, d_Mm);
         CK(cudaGetLastError());
         LAUNCHED();
     }
@@ -764,61 +820,90 @@ template <int DIM>
 void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms, double2 *d_Mm, cudaStream_t st,
                 double *mean1_acc = nullptr)
 {
+    // Three streams: the walk and the row generation on `rs`, contractions of
+    // even chunks on `st` and of odd chunks on `cs1`, each into its own FP64
+    // accumulator.  Rows of later chunks overlap the contraction in flight,
+    // and the tail wave of one contraction overlaps the head of the next.
+    // Three operand buffers: rows of chunk i reuse the buffer of chunk i-3.
     const int N = (int)(a->nv * a->nl);
     TcPlan plan = tc_plan(N, a->precision == SCMC_PREC_MIXED, c.tc_chunk_bytes);
     const size_t acc_bytes = (size_t)2 * N * N * sizeof(double);
-    double *Ds = reinterpret_cast<double *>(c.acc_s.ensure(acc_bytes));
-    double *Dm = reinterpret_cast<double *>(c.acc_m.ensure(acc_bytes));
-    CK(cudaMemsetAsync(Ds, 0, acc_bytes, st));
-    CK(cudaMemsetAsync(Dm, 0, acc_bytes, st));
+    double *Ds0 = reinterpret_cast<double *>(c.acc_s.ensure(2 * acc_bytes));
+    double *Dm0 = reinterpret_cast<double *>(c.acc_m.ensure(2 * acc_bytes));
+    double *Ds[2] = {Ds0, Ds0 + acc_bytes / sizeof(double)};
+    double *Dm[2] = {Dm0, Dm0 + acc_bytes / sizeof(double)};
+    CK(cudaMemsetAsync(Ds0, 0, 2 * acc_bytes, st));
+    CK(cudaMemsetAsync(Dm0, 0, 2 * acc_bytes, st));
     const int64_t chunk = plan.events_per_chunk;
-    TcOperands ops = tc_make_operands(plan, c.tc_a.ensure(tc_operand_bytes(plan)), st);
+    constexpr int NB = 3;
+    const size_t ob = tc_operand_bytes(plan);
+    char *omem = reinterpret_cast<char *>(c.tc_a.ensure(NB * ob));
+    TcOperands ops[NB];
+    for (int k = 0; k < NB; ++k) ops[k] = tc_make_operands(plan, omem + k * ob, st);
+    for (int k = 1; k < NB; ++k) ops[k].af = ops[0].af;
     const bool ffff = a->is_ff_l && a->is_ff_v;
     if (ffff) {
-        af_table_kernel<DIM><<<std::max(1, std::min(1024, (N + 255) / 256)), 256, 0, st>>>(P.Q, ops.af);
+        af_table_kernel<DIM><<<std::max(1, std::min(1024, (N + 255) / 256)), 256, 0, st>>>(P.Q, ops[0].af);
         CK(cudaGetLastError());
         LAUNCHED();
     }
+    c.make_aux();
+    cudaStream_t rs = c.aux, cs1 = c.aux2;
+    cudaEvent_t *ev_rows = &c.ev[0], *ev_free = &c.ev[3];
+    cudaEvent_t ev_setup = c.ev[6], ev_end_rs = c.ev[7], ev_end_c1 = c.ev[8];
+    CK(cudaEventRecord(ev_setup, st));
+    CK(cudaStreamWaitEvent(rs, ev_setup, 0));   // accumulators, operands, af table, mean1
+    CK(cudaStreamWaitEvent(cs1, ev_setup, 0));
+    int64_t chunk_id = 0;
     WalkParams W = P.W;
     for (int64_t done = 0; done < a->max_itr;) {
         int64_t nb = path_batch_size(a->max_itr - done);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
-        walk_batch(c, W, nb, st, B);
-        if (mean1_acc) launch_field_accum<DIM, PMIX, true, double>(c, P, B, mean1_acc, B.n_paths, st, 1);
+        walk_batch(c, W, nb, rs, B);  // after the previous batch's rows (same stream)
+        if (mean1_acc) launch_field_accum<DIM, PMIX, true, double>(c, P, B, mean1_acc, B.n_paths, rs, 1);
         for (int pass = 0; pass < 2; ++pass) {
             const bool single = pass == 0;
             const int64_t n_ev = single ? B.n_paths : B.n_multi;
-            double *D = single ? Ds : Dm;
-            for (int64_t e0 = 0; e0 < n_ev; e0 += chunk) {
-                int64_t n = std::min(chunk, n_ev - e0);
+            for (int64_t e0 = 0; e0 < n_ev; e0 += chunk, ++chunk_id) {
+                const int64_t n = std::min(chunk, n_ev - e0);
+                const int b = (int)(chunk_id % NB), d = (int)(chunk_id & 1);
+                cudaStream_t cs = d ? cs1 : st;
+                if (chunk_id >= NB) CK(cudaStreamWaitEvent(rs, ev_free[b], 0));  // chunk_id - NB has read buffer b
                 {
-                    StageScope sc(ST_ROWS, st);
+                    StageScope sc(ST_ROWS, rs);
                     if (plan.split) {
-                        if (single) tc_rows<DIM, true, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
-                        else tc_rows<DIM, false, true>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
+                        if (single) tc_rows<DIM, true, true>(plan, ops[b], P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, rs);
+                        else tc_rows<DIM, false, true>(plan, ops[b], P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, rs);
                     } else {
-                        if (single) tc_rows<DIM, true, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, st);
-                        else tc_rows<DIM, false, false>(plan, ops, P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, st);
+                        if (single) tc_rows<DIM, true, false>(plan, ops[b], P.Q, B.S, c.scap, B.M, c.mcap, e0, n, ffff, rs);
+                        else tc_rows<DIM, false, false>(plan, ops[b], P.Q, B.S, c.scap, B.M, c.mcap, e0, n, false, rs);
                     }
                     CK(cudaGetLastError());
                     LAUNCHED();
                 }
+                CK(cudaEventRecord(ev_rows[b], rs));
+                CK(cudaStreamWaitEvent(cs, ev_rows[b], 0));
                 {
-                    StageScope sc(ST_CONTRACT, st);
-                    tc_herk(plan, ops, n, D, st);
+                    StageScope sc(ST_CONTRACT, cs);
+                    tc_herk(plan, ops[b], n, single ? Ds[d] : Dm[d], cs);
                     CK(cudaGetLastError());
                     LAUNCHED();
                 }
+                CK(cudaEventRecord(ev_free[b], cs));
                 prof_count(0, 0, 4.0 * (double)N * (double)(N + 1) * (double)n);
             }
         }
         done += nb;
     }
-    int herr = 0;
-    CK(cudaMemcpyAsync(&herr, ops.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaEventRecord(ev_end_rs, rs));
+    CK(cudaEventRecord(ev_end_c1, cs1));
+    CK(cudaStreamWaitEvent(st, ev_end_rs, 0));
+    CK(cudaStreamWaitEvent(st, ev_end_c1, 0));
+    int herr[NB] = {0, 0, 0};
+    for (int k = 0; k < NB; ++k) CK(cudaMemcpyAsync(&herr[k], ops[k].err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
+    if (herr[0] || herr[1] || herr[2]) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
     double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
     double sc = m > 0 ? 1.0 / m * P.volume * a->sigt : 0.0;
     double scm = a->do_cbs ? sc / 2.0 : sc;
@@ -826,12 +911,12 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     int grid = (int)std::min<int64_t>((total + 255) / 256, 4096);
     StageScope fin(ST_FINAL, st);
     if (d_Ms) {
-        cov_finalize_kernel<double><<<grid, 256, 0, st>>>(Ds, 1, (int)a->nv, (int)a->nl, sc, d_Ms);
+        cov_finalize_kernel<double><<<grid, 256, 0, st>>>(Ds[0], Ds[1], 1, (int)a->nv, (int)a->nl, sc, d_Ms);
         CK(cudaGetLastError());
         LAUNCHED();
     }
     if (d_Mm) {
-        cov_finalize_kernel<double><<<grid, 256, 0, st>>>(Dm, 1, (int)a->nv, (int)a->nl, scm, d_Mm);
+        cov_finalize_kernel<double><<<grid, 256, 0, st>>>(Dm[0], Dm[1], 1, (int)a->nv, (int)a->nl, scm, d_Mm);
         CK(cudaGetLastError());
         LAUNCHED();
     }
@@ -1461,6 +1546,14 @@ int scmc_profile_enable(int32_t on)
 {
     return guarded([&] {
         std::lock_guard<std::mutex> lk(g_prof.mu);
+        if (on && !g_prof.on.load()) {
+            // time origin of the launch intervals: recorded now on the legacy stream
+            if (g_prof.ref) CK(cudaEventDestroy(g_prof.ref));
+            g_prof.ref = nullptr;
+            g_prof.resolve_locked();
+            CK(cudaEventCreate(&g_prof.ref));
+            CK(cudaEventRecord(g_prof.ref, 0));
+        }
         g_prof.on.store(on != 0);
     });
 }
@@ -1482,10 +1575,13 @@ int scmc_profile_read(scmc_stage_times *out, int32_t reset)
         out->paths = g_prof.paths;
         out->events = g_prof.events;
         out->contract_flops = g_prof.flops;
+        out->contract_busy_ms = g_prof.busy_ms(ST_CONTRACT);
+        out->rows_busy_ms = g_prof.busy_ms(ST_ROWS);
         if (reset) {
             for (int k = 0; k < 4; ++k) {
                 g_prof.launches[k] = 0;
                 g_prof.ms[k] = 0;
+                g_prof.iv[k].clear();
             }
             g_prof.paths = g_prof.events = 0;
             g_prof.flops = 0;
@@ -1528,8 +1624,8 @@ int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, dou
 // fixed, file-scope device array instead of allocated memory.
 //
 // Some callers cannot allocate device memory while they call in: a host that
-// runs inside a CUDA-graph capture or a pre-reserved memory budget (a serving
-// process that sized its pools at start-up), a real-time caller that must not
+// runs under a pre-reserved memory budget (a serving process that sized its
+// pools at start-up), a real-time caller that must not
 // take the allocator's locks, or an embedding runtime that forbids
 // cudaMalloc/cudaFree on its threads.  This entry point serves them: it calls
 // no cudaMalloc, cudaFree or allocating library routine; the caller passes

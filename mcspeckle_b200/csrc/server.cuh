@@ -76,8 +76,11 @@ int64_t request_estimate(int kind, const scmc_mc_args &a, int sms, size_t chunk_
     } else {
         const double N = nv * nl;
         const bool tc = a.precision == SCMC_PREC_MIXED || a.precision == SCMC_PREC_FP16;
-        acc = 2.0 * 2 * N * N * 8 + 2.0 * 2 * N * N * 8;  // accumulators + device copies of Ms, Mm
-        if (tc) acc += (double)tc_operand_bytes(tc_plan((int)N, a.precision == SCMC_PREC_MIXED, chunk_bytes));
+        // tensor-core path: two accumulators each for Ms and Mm and three
+        // operand buffers; CUDA-core path: one accumulator each and a row buffer;
+        // both: device copies of Ms, Mm
+        acc = (tc ? 4.0 : 2.0) * 2 * N * N * 8 + 2.0 * 2 * N * N * 8;
+        if (tc) acc += 3.0 * (double)tc_operand_bytes(tc_plan((int)N, a.precision == SCMC_PREC_MIXED, chunk_bytes));
         else acc += 256.0 * (1 << 20);
     }
     // every scratch buffer is allocated 1/8 above its request (DevBuf::ensure)
@@ -205,6 +208,7 @@ struct Server {
             cv_done.notify_all();
             cv_work.notify_all();
         }
+        c.destroy_aux();
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaStreamDestroy(st);

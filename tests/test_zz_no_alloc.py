@@ -1,6 +1,7 @@
 """scmc_field_noalloc - the field entry point for callers that cannot
-allocate device memory (inside a CUDA-graph capture, under a pre-sized memory
-budget, or on threads where cudaMalloc is not allowed).
+allocate device memory (under a pre-sized memory budget, in a real-time loop
+that must not take the allocator's locks, or on threads where cudaMalloc is
+not allowed).
 
 It is called through the C ABI and compared with scmc_field, the existing
 entry point, on two calls in a row: different path counts and seeds, so a
