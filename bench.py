@@ -307,14 +307,224 @@ def run_reference(a):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the other configurations, one JSON line each (`--workload`); the default line
+# above is the far-field covariance
+# ---------------------------------------------------------------------------
+def grid_rect(nx, ny, half_deg, zsign):
+    """nx x ny directions on a regular (sin theta_x, sin theta_y) grid."""
+    s = math.sin(math.radians(half_deg))
+    sx, sy = np.meshgrid(np.linspace(-s, s, nx), np.linspace(-s, s, ny), indexing="ij")
+    sx, sy = sx.reshape(-1), sy.reshape(-1)
+    return np.stack([sx, sy, zsign * np.sqrt(1 - sx * sx - sy * sy)])
+
+
+def hg_mixture_table(n_bins, seed):
+    """Tabulated amplitude of a seeded mixture of 3 HG lobes (g in [-0.3, 0.95],
+    weights from Dirichlet(1,1,1)) on n_bins angles in [0, pi]."""
+    from mcspeckle_b200 import interface as I
+    g_rng = np.random.default_rng(seed)
+    gs = g_rng.uniform(-0.3, 0.95, 3)
+    w = g_rng.dirichlet([1.0, 1.0, 1.0])
+    th = np.linspace(0, 1, n_bins) * np.pi
+    c = np.cos(th)
+    pdf = sum(wk * (1 - gk * gk) / (4 * np.pi * (1 + gk * gk - 2 * gk * c) ** 1.5) for wk, gk in zip(w, gs))
+    t = I.tabulatedAmplitudeScatter(th, np.sqrt(pdf))["ampfunc"]
+    return {"evalAmp": t["evalAmp"], "sampleIcdf": t["sampleIcdf"]}, gs.tolist(), w.tolist()
+
+
+ACC_MASK = None  # entries excluded from the accuracy comparison of a workload
+
+
+def workload_spec(name):
+    """(description, make(n, precision, seed, offset, norm) -> holder, device solve,
+    host solve, output doubles, oracle solve, dominant-kernel roofline kind)."""
+    from mcspeckle_b200 import _lib
+    from mcspeckle_b200 import mc as MC
+    from mcspeckle_b200 import fourier_quad as FQ
+    from mcspeckle_b200 import hetero as H
+    L = _lib.lib()
+    if name == "field16":
+        rng = np.random.default_rng(0)
+        l16 = cap_dirs(16, 10.0, +1.0, rng)
+        v16 = cap_dirs(16, 10.0, -1.0, rng)
+        base = [0.1, 1.0, np.array([-100.0, -100.0, 0.0]), np.array([100.0, 100.0, 50.0]), l16, v16, 1, 1, 0,
+                1.0, True, 2, 1, 0]
+
+        def make(n, prec, seed, off=0, norm=0):
+            b = list(base)
+            b[8] = int(n)
+            return MC.mc_args(*b, seed=seed, precision=prec, path_offset=off, norm_itr=norm)
+
+        def dev(h, outs, stream):
+            _lib.check(L.scmc_field_device(h.ref, outs[0].data_ptr(), stream))
+
+        def oracle(h, O):
+            return O.field(h, O.Rng.philox())
+        return ("MCfield far field, 16 lights x 16 views within 10 deg of +z / -z, isotropic, box 20x20x5 MFP "
+                "(MFP 10 wavelengths), CBS, 1e5 paths per step", make, dev, MC.field_from_args, [2 * 16 * 16],
+                oracle, None)
+    if name == "fq256":
+        mfp = 100.0
+        base = dict(sigt=1.005 / mfp, albedo=1 / 1.005, box_min=[-25 * mfp, -25 * mfp, 0.0],
+                    box_max=[25 * mfp, 25 * mfp, 10 * mfp], l=np.array([[0.0], [0.0], [1.0]]),
+                    v_max=255.0 / 256.0, v_stp=1.0 / 128.0)
+
+        def make(n, prec, seed, off=0, norm=0):
+            return FQ.fq_args(base["sigt"], base["albedo"], base["box_min"], base["box_max"], base["l"],
+                              base["v_max"], base["v_stp"], int(n), 1.0, True, 2, None, -1, seed=seed,
+                              precision=prec, path_offset=off)
+
+        def dev(h, outs, stream):
+            _lib.check(L.scmc_field_fourier_quad_device(h.ref, outs[0].data_ptr(), stream))
+
+        def oracle(h, O):
+            return O.field_fourier_quad(h.args, O.Rng.philox(), h.nv0)
+        th = -base["v_max"] + np.arange(256) * base["v_stp"]
+        # accuracy over the propagating directions only: where vx^2 + vy^2 > 1 the
+        # reference's plane factor grows exponentially with depth (evanescent)
+        global ACC_MASK
+        ACC_MASK = (th[:, None] ** 2 + th[None, :] ** 2 < 1.0)[:, :, None]
+        return ("MCfieldFourierQuad, box 50x50x10 MFP (MFP 100 wavelengths), sigma_a 0.005 per MFP, plane wave "
+                "along +z, 256x256 angular grid (v_max 255/256, v_stp 1/128: 0.5-wavelength lateral pitch), CBS; "
+                "isotropic as the reference (HG g=0.9 and the point source are not built)",
+                make, dev, FQ.field_fourier_quad_from_args, [2 * 256 * 256], oracle, None)
+    if name == "hetero128":
+        mfp = 10.0
+        g = np.random.default_rng(4)
+        sig = np.exp(g.normal(0.0, 0.5, (128, 128, 128))) / mfp
+        table, gs, ws = hg_mixture_table(1024, 5)
+        bmin, bmax = np.array([-100.0, -100.0, 0.0]), np.array([100.0, 100.0, 50.0])
+        bbin = (bmax - bmin) / 128.0
+        l = grid_rect(16, 8, 5.0, +1.0)
+        v = grid_rect(16, 8, 5.0, -1.0)
+
+        def make(n, prec, seed, off=0, norm=0):
+            return H.hetero_args(True, sig, 1.0, bmin, bmax, bbin, l, v, 1, 1, int(n), 1.0, True, 2, 2, table,
+                                 seed=seed, precision=prec, path_offset=off, norm_itr=norm)
+
+        def dev(h, outs, stream):
+            _lib.check(L.scmc_cov_hetero_device(h.ref, outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(),
+                                                stream))
+
+        def oracle(h, O):
+            return O.cov_hetero(h, O.Rng.philox(), threads=os.cpu_count() or 1)[:2]
+        n2 = 128 * 128
+        return (f"MCCovHetro, sigma_s on a 128^3 grid log-normal(0, 0.5) per MFP (MFP 10 wavelengths, nearest "
+                f"voxel as the reference), box 20x20x5 MFP, Woodcock tracking, tabulated phase function on 1024 "
+                f"theta bins from 3 HG lobes g={[round(x, 3) for x in gs]} w={[round(x, 3) for x in ws]}, "
+                f"128 lights x 128 views (16x8 grids of +-5 deg), CBS",
+                make, dev, lambda h: H.cov_hetero_from_args(h)[:2], [2 * n2 * n2, 2 * n2 * n2, 2 * n2], oracle,
+                "tensor")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def run_workload(a):
+    """One JSON line for a non-default configuration, 1 GPU: device-timed
+    steps of fresh path ranges (outputs in HBM), the host-buffer call, stage
+    times, accuracy against FP64 on a smaller sample, the CPU oracle on a
+    bounded sample."""
+    import torch
+    from mcspeckle_b200 import _lib
+    desc, make, dev, host, sizes, oracle_fn, bound = workload_spec(a.workload)
+    prec = a.precision
+    P = int(a.paths if a.paths is not None else {"field16": 1e5, "fq256": 1e5, "hetero128": 2e4}[a.workload])
+    stream = torch.cuda.current_stream()
+    outs = [torch.zeros(n, dtype=torch.float64, device="cuda") for n in sizes]
+    seed = 0
+
+    def step(i):
+        dev(make(P, prec, seed, off=i * P, norm=P), outs, stream.cuda_stream)
+
+    for i in range(a.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    _lib.profile_read(reset=True)
+    _lib.profile_enable(True)
+    l0 = _lib.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(a.steps):
+        step(a.warmup + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = _lib.launch_count() - l0
+    _lib.profile_enable(False)
+    prof = _lib.profile_read(reset=True)
+    clk = clocks.stop()
+    value = P * a.steps / (ms / 1000.0)
+    # e2e: the host-buffer call (results copied to host every step)
+    t0 = time.perf_counter()
+    for i in range(a.steps):
+        host(make(P, prec, seed, off=(a.warmup + a.steps + i) * P, norm=P))
+    e2e = P * a.steps / (time.perf_counter() - t0)
+    # accuracy on a smaller sample, same paths in every precision
+    na = int(a.accuracy_paths if a.accuracy_paths is not None else
+             {"field16": 1e5, "fq256": 2e4, "hetero128": 1e3}[a.workload])
+    ref = host(make(na, "fp64", 7))
+    ref = ref if isinstance(ref, tuple) else (ref,)
+
+    def rel(x):
+        x = x if isinstance(x, tuple) else (x,)
+        num = den = 0.0
+        for xa, ra in zip(x, ref):
+            m = np.isfinite(ra) if ACC_MASK is None else np.broadcast_to(ACC_MASK, ra.shape)
+            num += float(np.linalg.norm((xa - ra)[m])) ** 2
+            den += float(np.linalg.norm(ra[m])) ** 2
+        return math.sqrt(num / den)
+    acc = {"paths": na, "tol": 1e-3}
+    for pz in ("mixed", "fp16", "fp32"):
+        acc[f"rel_err_{pz}_vs_fp64"] = rel(host(make(na, pz, 7)))
+    # plain FP32 GPU, one solve, same paths as one timed step
+    t32 = time.perf_counter()
+    host(make(P, "fp32", seed))
+    fp32_value = P / (time.perf_counter() - t32)
+    roof = None
+    if bound == "tensor" and prof["contract_launches"]:
+        peaks, peak_kind = load_peaks()
+        peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+        achieved = prof["contract_flops"] / (prof["contract_busy_ms"] / 1000.0) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "herk_tc2_kernel", "peak_source": f"bf16_tflops_sustained ({peak_kind})",
+                "flops": prof["contract_flops"], "contract_busy_ms": prof["contract_busy_ms"]}
+    cpu = None
+    if not a.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        n = {"field16": 2000, "fq256": 20, "hetero128": 16}[a.workload]
+        h = make(n, "fp64", 99)
+        tc = time.perf_counter()
+        oracle_fn(h, O)
+        dt = time.perf_counter() - tc
+        thr = (os.cpu_count() or 1) if a.workload == "hetero128" else 1
+        cpu = {"value": n / dt, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"{n} paths of the workload in {dt:.1f} s (FP64 oracle, {thr} thread(s))"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": prec, "data": "synthetic",
+            "config": {"workload": a.workload, "description": desc, "paths_per_step": P, "precision": prec},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": int(sum(sizes) * 8)},
+            "gpu_launches": int(launches), "roofline": roof,
+            "stages_ms": {k: prof[k] for k in ("walk_ms", "rows_ms", "contract_ms", "finalize_ms",
+                                               "contract_busy_ms", "rows_busy_ms")},
+            "accuracy": acc, "fp32_gpu": {"paths": P, "value": fp32_value}, "cpu_baseline": cpu, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--paths", type=float, default=1e7, help="paths per GPU per step")
-    ap.add_argument("--accuracy-paths", type=float, default=1e5)
+    ap.add_argument("--paths", type=float, default=None, help="paths per GPU per step (cov64: 1e7)")
+    ap.add_argument("--accuracy-paths", type=float, default=None, help="(cov64: 1e5)")
     ap.add_argument("--fp32-paths", type=float, default=1e5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=15.0)
@@ -327,9 +537,18 @@ def main():
     ap.add_argument("--served-fp32-seconds", type=float, default=20.0)
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--workload", default="cov64", choices=["cov64", "field16", "fq256", "hetero128"],
+                    help="cov64: the far-field covariance (the default line); the others print one line of "
+                         "their own (1 GPU): field16, fq256, hetero128")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload != "cov64":
+        import torch
+        torch.cuda.set_device(0)
+        return run_workload(a)
+    a.paths = 1e7 if a.paths is None else a.paths
+    a.accuracy_paths = 1e5 if a.accuracy_paths is None else a.accuracy_paths
 
     import torch
     import torch.distributed as dist

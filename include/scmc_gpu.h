@@ -191,6 +191,9 @@ typedef struct {
 
 int scmc_cov_hetero(const scmc_hetero_args *args, double *Ms, double *Mm, double *mean1);
 int scmc_field_hetero(const scmc_hetero_args *args, double *u);
+/* Same with the outputs in device memory and the work on `stream`. */
+int scmc_cov_hetero_device(const scmc_hetero_args *args, double *d_Ms, double *d_Mm, double *d_mean1, void *stream);
+int scmc_field_hetero_device(const scmc_hetero_args *args, double *d_u, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Path records for oracle replay.  Walks paths [path_offset, path_offset +

@@ -67,6 +67,8 @@ def lib():
         hp = C.POINTER(_abi.HeteroArgs)
         L.scmc_cov_hetero.argtypes = [hp, dp, dp, dp]
         L.scmc_field_hetero.argtypes = [hp, dp]
+        L.scmc_cov_hetero_device.argtypes = [hp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.scmc_field_hetero_device.argtypes = [hp, C.c_void_p, C.c_void_p]
         vp = C.c_void_p
         L.scmc_server_create.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.POINTER(vp)]
         L.scmc_server_submit.argtypes = [vp, C.c_int32, mp, dp, dp, C.POINTER(C.c_int64)]
@@ -78,7 +80,8 @@ def lib():
         for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",
                      "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read",
                      "scmc_fq_grid_size", "scmc_field_fourier_quad", "scmc_field_fourier_quad_device",
-                     "scmc_field_noalloc", "scmc_cov_hetero", "scmc_field_hetero", "scmc_server_create",
+                     "scmc_field_noalloc", "scmc_cov_hetero", "scmc_field_hetero", "scmc_cov_hetero_device",
+                     "scmc_field_hetero_device", "scmc_server_create",
                      "scmc_server_submit", "scmc_server_wait", "scmc_server_stats_read", "scmc_server_destroy"):
             getattr(L, name).restype = C.c_int
         _lib = L

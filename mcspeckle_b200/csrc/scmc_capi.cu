@@ -1542,6 +1542,32 @@ int scmc_field_hetero(const scmc_hetero_args *args, double *u)
     });
 }
 
+int scmc_cov_hetero_device(const scmc_hetero_args *args, double *d_Ms, double *d_Mm, double *d_mean1, void *stream)
+{
+    return guarded([&] {
+        if (!args) fail(SCMC_ERR_INVALID, "null arguments");
+        validate(&args->mc);
+        Ctx &c = context(args->mc.device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        cov_hetero_locked(c, args, d_Ms, d_Mm, d_mean1, st);
+        CK(cudaStreamSynchronize(st));
+    });
+}
+
+int scmc_field_hetero_device(const scmc_hetero_args *args, double *d_u, void *stream)
+{
+    return guarded([&] {
+        if (!args || !d_u) fail(SCMC_ERR_INVALID, "null arguments");
+        validate(&args->mc);
+        Ctx &c = context(args->mc.device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        field_hetero_locked(c, args, d_u, st);
+        CK(cudaStreamSynchronize(st));
+    });
+}
+
 int scmc_profile_enable(int32_t on)
 {
     return guarded([&] {
