@@ -16,6 +16,8 @@
 // plane's end multiplies by exp(zexp0 * tz) before adding into the FP64 sum.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "accum.cuh"
 
 namespace scmc {
@@ -240,14 +242,91 @@ fq_accum_kernel(FqParams F, const FqEntry *__restrict__ E, const int *__restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core form (MIXED / FP16).  Per plane P and light j the DFT sum is the
+// complex product F_P = A_P B_P^T over the plane's entries e:
+//     A_P[r1][e] = s_e(j) T[r1][p1_e],   B_P[r2][e] = T[r2][p2_e],
+// with s_e(j) = c0_e * exp(i k l_j.xl_e - sigt/2 * slab attenuation).  The
+// entries, sorted by plane, are laid out in blocks of 32 (a plane's last block
+// zero-padded), in the real expansion of the tensor-core field path
+//     A[2r1] = (Re a, -Im a), A[2r1+1] = (Im a, Re a), B[r2] = (Re b, Im b),
+// two K columns per entry, so one 64-column K block never spans two planes.
+// herk_tc_kernel computes F_P per plane (one grid row per plane) and its
+// epilogue multiplies by exp(zexp0 * tz_P) and adds into the output, which
+// for this form is stored [light][r1][r2] (r2 fastest).
+// ---------------------------------------------------------------------------
+template <bool SPLIT>
+__global__ void __launch_bounds__(256)
+fq_tc_rows_kernel(FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk, int light,
+                  const float2 *__restrict__ T, int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo,
+                  __half *__restrict__ Bm)
+{
+    __shared__ float2 ss[32];
+    __shared__ int sp1[32], sp2[32];
+    const int2 bk = blk[blockIdx.x];  // (first entry, entries in this block)
+    if (threadIdx.x < 32) {
+        float2 sv = make_float2(0.f, 0.f);
+        int p1 = 0, p2 = 0;
+        if ((int)threadIdx.x < bk.y) {
+            const FqEntry en = E[bk.x + threadIdx.x];
+            const double *lj = F.l + 3 * light;
+            const double ph = F.kw * (lj[0] * en.xl[0] + lj[1] * en.xl[1] + lj[2] * en.xl[2]);
+            const double at =
+                F.sigt_half * ((en.xl[2] - F.bmin_z) * F.l_diratt + (F.bmax_z - en.xl[2]) * F.l_idiratt);
+            float sn, cs;
+            sincosf((float)reduce_2pi(ph), &sn, &cs);
+            const float amp = expf(-(float)at);
+            sv = cmul(to_c<float2>(en.c0), make_float2(amp * cs, amp * sn));
+            p1 = en.p1;
+            p2 = en.p2;
+        }
+        ss[threadIdx.x] = sv;
+        sp1[threadIdx.x] = p1;
+        sp2[threadIdx.x] = p2;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t col = 2 * ((int64_t)blockIdx.x * 32 + lane);
+    const float2 sv = ss[lane];
+    const int p1 = sp1[lane], p2 = sp2[lane];
+    const bool live = lane < bk.y;
+    for (int r = warp; r < F.nv0; r += 8) {
+        float2 av = make_float2(0.f, 0.f), bv = make_float2(0.f, 0.f);
+        if (live) {
+            av = cmul(sv, T[(int64_t)r * F.nx + p1]);
+            bv = T[(int64_t)r * F.nx + p2];
+        }
+        const __half hr = __float2half_rn(av.x), hi = __float2half_rn(av.y);
+        __half *e = Ahi + (int64_t)(2 * r) * K + col;
+        *reinterpret_cast<__half2 *>(e) = __halves2half2(hr, __hneg(hi));
+        *reinterpret_cast<__half2 *>(e + K) = __halves2half2(hi, hr);
+        if (SPLIT) {
+            const __half lr = __float2half_rn(av.x - __half2float(hr));
+            const __half li = __float2half_rn(av.y - __half2float(hi));
+            __half *o = Alo + (int64_t)(2 * r) * K + col;
+            *reinterpret_cast<__half2 *>(o) = __halves2half2(lr, __hneg(li));
+            *reinterpret_cast<__half2 *>(o + K) = __halves2half2(li, lr);
+        }
+        *reinterpret_cast<__half2 *>(Bm + (int64_t)r * K + col) =
+            __halves2half2(__float2half_rn(bv.x), __float2half_rn(bv.y));
+    }
+}
+
+// u = norm * boxexp0 o U.  r2_fast: U is stored [light][r1][r2] (the
+// tensor-core form) instead of u's [light][r2][r1].
 template <typename AccT>
 __global__ void fq_finalize_kernel(const AccT *__restrict__ U, const double2 *__restrict__ boxexp0, int nv0, int nl,
-                                   double norm, double2 *__restrict__ u)
+                                   double norm, double2 *__restrict__ u, int r2_fast = 0)
 {
     const int64_t n = (int64_t)nv0 * nv0 * nl;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         const double2 b = boxexp0[k % ((int64_t)nv0 * nv0)];
-        const double2 a = make_double2((double)U[2 * k], (double)U[2 * k + 1]);
+        int64_t src = k;
+        if (r2_fast) {
+            const int64_t r1 = k % nv0, r2 = (k / nv0) % nv0, j = k / ((int64_t)nv0 * nv0);
+            src = r2 + nv0 * (r1 + nv0 * j);
+        }
+        const double2 a = make_double2((double)U[2 * src], (double)U[2 * src + 1]);
         const double2 v = cmul(a, b);
         u[k] = make_double2(norm * v.x, norm * v.y);
     }

@@ -223,7 +223,7 @@ struct Ctx {
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
     DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2;
-    DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
+    DevBuf fq_gz, fq_zexp, fq_zt, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
     // Extra streams and events of the covariance pipeline: the walk and row
@@ -256,7 +256,7 @@ struct Ctx {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
                          &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0,
-                         &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_counts, &fq_offsets, &fq_cursor,
+                         &out1, &out2, &fq_gz, &fq_zexp, &fq_zt, &fq_box, &fq_tw, &fq_counts, &fq_offsets, &fq_cursor,
                          &fq_planes};
         for (DevBuf *b : all) f(*b);
     }
@@ -1195,6 +1195,98 @@ void validate_fq(const scmc_fq_args *a)
     if (colon_count(-a->v_max, a->v_stp, a->v_max) > 4096) fail(SCMC_ERR_INVALID, "angular grid longer than 4096");
 }
 
+// The per-plane DFT sums of one batch on tcgen05 (fq.cuh, tensor-core form),
+// added into U stored [light][r1][r2].  dzt: zexp0 stored [r1][r2].
+// Nonempty planes are taken in groups of at most kFqTcEntries padded entries
+// (operand memory) and kFqTcPlanes planes.
+constexpr int64_t kFqTcEntries = (int64_t)1 << 18;
+constexpr int kFqTcPlanes = 2048;
+
+void fq_tc_batch(Ctx &c, const FqParams &F, const FqEntry *Es, const std::vector<int> &hcounts,
+                 const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *T, const double2 *dzt,
+                 double *U, bool split, cudaStream_t st)
+{
+    const int nv0 = F.nv0;
+    const int Mr = 2 * nv0;
+    std::vector<int2> tiles;
+    for (int tn = 0; tn < (nv0 + TC_BN - 1) / TC_BN; ++tn)
+        for (int tm = 0; tm < (Mr + TC_BM - 1) / TC_BM; ++tm) tiles.push_back(make_int2(tm, tn));
+    size_t g0 = 0;
+    while (g0 < hplanes.size()) {
+        // group [g0, g1): blocks of 32 entries per plane
+        std::vector<int2> blk, kr;
+        std::vector<int> gpl;
+        size_t g1 = g0;
+        int64_t nblk = 0;
+        while (g1 < hplanes.size() && (int)gpl.size() < kFqTcPlanes) {
+            const int p = hplanes[g1];
+            const int cnt = hcounts[p];
+            const int nb = (cnt + 31) / 32;
+            if (!gpl.empty() && (nblk + nb) * 32 > kFqTcEntries) break;
+            kr.push_back(make_int2((int)nblk, nb));
+            for (int b = 0; b < nb; ++b) blk.push_back(make_int2(hoff[p] + 32 * b, std::min(32, cnt - 32 * b)));
+            gpl.push_back(p);
+            nblk += nb;
+            ++g1;
+        }
+        const int64_t K = 64 * nblk;
+        const size_t ab = tc_align((size_t)Mr * K * sizeof(__half)), bb = tc_align((size_t)nv0 * K * sizeof(__half));
+        const size_t meta = tc_align(tiles.size() * sizeof(int2)) + tc_align(kr.size() * sizeof(int2)) +
+                            tc_align(blk.size() * sizeof(int2)) + tc_align(gpl.size() * sizeof(int)) + 1024;
+        char *mem = reinterpret_cast<char *>(c.tc_a.ensure((split ? 2 : 1) * ab + bb + meta));
+        __half *ahi = reinterpret_cast<__half *>(mem);
+        __half *alo = split ? reinterpret_cast<__half *>(mem + ab) : ahi;
+        __half *bm = reinterpret_cast<__half *>(mem + (split ? 2 : 1) * ab);
+        char *q = mem + (split ? 2 : 1) * ab + bb;
+        int2 *d_tiles = reinterpret_cast<int2 *>(q);
+        q += tc_align(tiles.size() * sizeof(int2));
+        int2 *d_kr = reinterpret_cast<int2 *>(q);
+        q += tc_align(kr.size() * sizeof(int2));
+        int2 *d_blk = reinterpret_cast<int2 *>(q);
+        q += tc_align(blk.size() * sizeof(int2));
+        int *d_pl = reinterpret_cast<int *>(q);
+        q += tc_align(gpl.size() * sizeof(int));
+        int *d_err = reinterpret_cast<int *>(q);
+        CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_kr, kr.data(), kr.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_blk, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_pl, gpl.data(), gpl.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+        const CUtensorMap m_ahi = tc_map(ahi, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
+        const CUtensorMap m_alo = tc_map(alo, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
+        const CUtensorMap m_b = tc_map(bm, (uint64_t)K, (uint64_t)nv0, (uint64_t)K * 2, TC_BN);
+        for (int j = 0; j < F.nl; ++j) {
+            {
+                StageScope sc(ST_ROWS, st);
+                if (split)
+                    fq_tc_rows_kernel<true><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, T, K, ahi, alo, bm);
+                else
+                    fq_tc_rows_kernel<false><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, T, K, ahi, alo, bm);
+                CK(cudaGetLastError());
+                LAUNCHED();
+            }
+            {
+                StageScope sc(ST_CONTRACT, st);
+                const PlaneEpi pe{dzt, F.gz, d_pl, U + 2 * (int64_t)nv0 * nv0 * j, nv0};
+                if (split)
+                    tc_gemm_planes_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, (int)gpl.size(),
+                                                Mr, nv0, pe, d_err, st);
+                else
+                    tc_gemm_planes_launch<false>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, (int)gpl.size(),
+                                                 Mr, nv0, pe, d_err, st);
+                CK(cudaGetLastError());
+                LAUNCHED();
+            }
+            prof_count(0, 0, 8.0 * (double)nv0 * nv0 * (double)(hoff[gpl.back() + 1] - hoff[gpl.front()]));
+        }
+        int herr = 0;
+        CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));  // the group's host vectors and operand memory are reused
+        if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
+        g0 = g1;
+    }
+}
+
 template <int POL, typename AccT>
 void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
 {
@@ -1283,6 +1375,12 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
     Cx *T = reinterpret_cast<Cx *>(c.fq_tw.ensure(Nv * Nx * sizeof(Cx)));
     CK(cudaMemcpyAsync(dgz, gz.data(), Nz * sizeof(double), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dz, zexp0.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
+    // [r1][r2] copy of zexp0 for the tensor-core form
+    std::vector<double2> zexp0t(Nv * Nv);
+    for (int64_t r1 = 0; r1 < Nv; ++r1)
+        for (int64_t r2 = 0; r2 < Nv; ++r2) zexp0t[r2 + Nv * r1] = zexp0[r1 + Nv * r2];
+    double2 *dzt = reinterpret_cast<double2 *>(c.fq_zt.ensure(Nv * Nv * sizeof(double2)));
+    CK(cudaMemcpyAsync(dzt, zexp0t.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(db, boxexp0.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dl, a->l, 3 * a->nl * sizeof(double), cudaMemcpyHostToDevice, st));
     F.gz = dgz;
@@ -1328,6 +1426,9 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
     const int sms = sm_count(c.device);
     int64_t total_vert = 0;
     const int passes = a->do_cbs ? 2 : 1;
+    // MIXED / FP16 with at least 64 angles per axis: the per-plane sums on tcgen05
+    const bool use_tc = POL == PMIX && (a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16) &&
+                        Nv >= 64;
     for (int64_t done = 0; done < a->max_itr;) {
         const int64_t nb = std::min<int64_t>(a->max_itr - done, (int64_t)1 << 18);
         W.path_base = a->path_offset + (uint64_t)done;
@@ -1369,14 +1470,19 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
             CK(cudaGetLastError());
             LAUNCHED();
         }
-        const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
-        for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
-            const unsigned gy = (unsigned)std::min<size_t>(65535, hplanes.size() - p0);
-            dim3 grid((unsigned)(nvt * nvt * a->nl), gy);
-            StageScope sc(ST_CONTRACT, st);
-            fq_accum_kernel<POL, AccT><<<grid, 256, 0, st>>>(F, Es, offsets, planes + p0, T, dz, U);
-            CK(cudaGetLastError());
-            LAUNCHED();
+        if (use_tc) {
+            fq_tc_batch(c, F, Es, hcounts, hoff, hplanes, reinterpret_cast<const float2 *>(T), dzt,
+                        reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, st);
+        } else {
+            const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
+            for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
+                const unsigned gy = (unsigned)std::min<size_t>(65535, hplanes.size() - p0);
+                dim3 grid((unsigned)(nvt * nvt * a->nl), gy);
+                StageScope sc(ST_CONTRACT, st);
+                fq_accum_kernel<POL, AccT><<<grid, 256, 0, st>>>(F, Es, offsets, planes + p0, T, dz, U);
+                CK(cudaGetLastError());
+                LAUNCHED();
+            }
         }
         CK(cudaStreamSynchronize(st));  // host vectors above are reused next batch
         done += nb;
@@ -1385,7 +1491,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
     const double norm = total_vert > 0 ? std::sqrt(1.0 / (double)total_vert * V * sigt) : 0.0;  // lines 214, 302-303
     StageScope fin(ST_FINAL, st);
     fq_finalize_kernel<AccT><<<(int)std::max<int64_t>(1, std::min<int64_t>((nout + 255) / 256, 4096)), 256, 0, st>>>(
-        U, db, (int)Nv, (int)a->nl, norm, d_u);
+        U, db, (int)Nv, (int)a->nl, norm, d_u, use_tc ? 1 : 0);
     CK(cudaGetLastError());
     LAUNCHED();
 }

@@ -62,3 +62,45 @@ def test_fourier_quad_grid_size(gpu):
     n = ctypes.c_int64()
     _lib.check(_lib.lib().scmc_fq_grid_size(255 / 256, 1 / 128, ctypes.byref(n)))
     assert n.value == 256 == FQ.grid_length(255 / 256, 1 / 128)
+
+
+# Grids of at least 64 angles per axis: MIXED / FP16 run the per-plane sums on
+# tcgen05 (one GEMM slice per z plane, plane factor applied on reduction).
+TC_CASES = {
+    "tc_wide_cbs": dict(sigt=0.1, albedo=0.9, box_min=[-60, -60, 0], box_max=[60, 60, 20], v_max=0.32, v_stp=0.01,
+                        lam=1.0, cbs=1, smp=2, lmean0=None, vsign=-1, n=300),
+    "tc_narrow_nocbs": dict(sigt=0.15, albedo=0.8, box_min=[-10, -10, 0], box_max=[10, 10, 8], v_max=0.32,
+                            v_stp=0.01, lam=1.0, cbs=0, smp=1, lmean0=[0.0, 0.1, 1.0], vsign=1, n=300),
+    "tc_even_grid": dict(sigt=0.1, albedo=0.9, box_min=[-30, -30, 0], box_max=[30, 30, 12], v_max=0.635,
+                         v_stp=0.01, lam=1.0, cbs=1, smp=2, lmean0=None, vsign=-1, n=200),
+    "tc_wide_angles": dict(sigt=0.12, albedo=1.0, box_min=[-8, -8, 0], box_max=[8, 8, 10], v_max=0.9, v_stp=0.025,
+                           lam=0.8, cbs=1, smp=2, lmean0=None, vsign=-1, n=200),
+}
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp16"])
+@pytest.mark.parametrize("name", list(TC_CASES))
+def test_fourier_quad_tensor_cores_close_to_fp64(gpu, name, precision):
+    from mcspeckle_b200 import _lib
+    c = TC_CASES[name]
+    h64 = args_for(c, "fp64")
+    assert h64.nv0 >= 64
+    u64 = FQ.field_fourier_quad_from_args(h64)
+    _lib.profile_read(reset=True)
+    _lib.profile_enable(True)
+    try:
+        u = FQ.field_fourier_quad_from_args(args_for(c, precision))
+    finally:
+        _lib.profile_enable(False)
+    prof = _lib.profile_read(reset=True)
+    assert prof["contract_flops"] > 0  # the tensor-core form ran
+    assert u.shape == u64.shape and np.isfinite(u).all()
+    assert rel(u, u64) < 1e-3
+
+
+def test_fourier_quad_tensor_cores_fp64_anchor(gpu, oracle_lib):
+    """The FP64 reference of the tensor-core tests is the oracle's estimator."""
+    h = args_for(TC_CASES["tc_wide_cbs"], "fp64")
+    u = FQ.field_fourier_quad_from_args(h)
+    uo = oracle_lib.field_fourier_quad(h.args, oracle_lib.Rng.philox(), h.nv0)
+    assert rel(u, uo) < 1e-10
