@@ -149,6 +149,24 @@ int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream);
 int scmc_field_noalloc(const scmc_mc_args *args, double *d_u, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Field on a wave: u = MCfieldOnWave(sigt, albedo, box_min, box_max, l, v,
+ *     is_ff_l, is_ff_v, maxItr, lambda, doCBS, smpFlg, sct_type, ampfunc,
+ *     ampfunc0, lmean0, Wl)                               (MCfieldOnWave.m:1)
+ * The field of all lights at once, each weighted by the complex Wl_j: equal
+ * to the MCfield result times Wl on the same paths, at O(nv + nl) instead of
+ * O(nv nl) work per event.  Wl: nl complex (2*nl doubles, interleaved; the
+ * reference needs it as a 1 x Nl row).  u: nv complex (2*nv doubles).  The
+ * reference requires ampfunc0 and lmean0 (positional); here they may be
+ * omitted (has_ampfunc0 / has_lmean0 = 0) with MCfield's defaults.  For
+ * isotropic scattering the reference's single-scattering line
+ * (MCfieldOnWave.m:221) is consistent only for one light; this computes
+ * sum_j af e_l0_j Wl_j, which agrees with it there.
+ * ------------------------------------------------------------------------- */
+int scmc_field_onwave(const scmc_mc_args *args, const double *Wl, double *u);
+/* Same with u in device memory (Wl stays in host memory) and work on `stream`. */
+int scmc_field_onwave_device(const scmc_mc_args *args, const double *Wl, double *d_u, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Covariance: [Ms, Mm] = MCcov(sigt, albedo, box_min, box_max, l, v, is_ff_l,
  *                  is_ff_v, maxItr, lambda, doCBS, smpFlg, sct_type, ampfunc
  *                  [, ampfunc0])                                 (MCcov.m:1)

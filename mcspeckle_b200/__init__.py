@@ -9,11 +9,11 @@ from .interface import (HGScatter, boxArea, farFieldSource, invCDF, isotropicSca
                         tabulatedAmplitudeScatter)
 from .fourier_quad import MCfieldFourierQuad, fq_args
 from .hetero import MCCovHetro, MCsampleHetro, hetero_args
-from .mc import MCcov, MCfield, MatlabStyleError, export_records, mc_args, philox_stream, rng
+from .mc import MCcov, MCfield, MCfieldOnWave, MatlabStyleError, export_records, mc_args, philox_stream, rng
 from .scmc_api import ScmcInputError, scmc
 
 __all__ = [
-    "scmc", "MCfield", "MCcov", "MCfieldFourierQuad", "fq_args", "MCCovHetro", "MCsampleHetro", "hetero_args", "rng", "mc_args", "export_records", "philox_stream",
+    "scmc", "MCfield", "MCcov", "MCfieldOnWave", "MCfieldFourierQuad", "fq_args", "MCCovHetro", "MCsampleHetro", "hetero_args", "rng", "mc_args", "export_records", "philox_stream",
     "boxArea", "farFieldSource", "nearFieldSource", "isotropicScatter", "HGScatter",
     "tabulatedAmplitudeScatter", "invCDF", "ScmcError", "ScmcInputError", "MatlabStyleError", "launch_count",
 ]

@@ -56,6 +56,8 @@ def lib():
         L.scmc_field.argtypes = [mp, dp]
         L.scmc_field_device.argtypes = [mp, C.c_void_p, C.c_void_p]
         L.scmc_cov.argtypes = [mp, dp, dp]
+        L.scmc_field_onwave.argtypes = [mp, dp, dp]
+        L.scmc_field_onwave_device.argtypes = [mp, dp, C.c_void_p, C.c_void_p]
         L.scmc_cov_device.argtypes = [mp, C.c_void_p, C.c_void_p, C.c_void_p]
         L.scmc_export_records.argtypes = [mp, C.c_int32, C.c_int64, dp, dp, dp, dp, dp, dp, ip, lp, lp]
         L.scmc_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
@@ -81,7 +83,7 @@ def lib():
                      "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read",
                      "scmc_fq_grid_size", "scmc_field_fourier_quad", "scmc_field_fourier_quad_device",
                      "scmc_field_noalloc", "scmc_cov_hetero", "scmc_field_hetero", "scmc_cov_hetero_device",
-                     "scmc_field_hetero_device", "scmc_server_create",
+                     "scmc_field_hetero_device", "scmc_field_onwave", "scmc_field_onwave_device", "scmc_server_create",
                      "scmc_server_submit", "scmc_server_wait", "scmc_server_stats_read", "scmc_server_destroy"):
             getattr(L, name).restype = C.c_int
         _lib = L

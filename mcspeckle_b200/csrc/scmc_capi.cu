@@ -23,6 +23,7 @@
 #include "herk_tc.cuh"
 #include "field_tc.cuh"
 #include "fq.cuh"
+#include "onwave.cuh"
 
 using namespace scmc;
 
@@ -222,7 +223,7 @@ struct Ctx {
     DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
-    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2;
+    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl;
     DevBuf fq_gz, fq_zexp, fq_zt, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
@@ -255,7 +256,7 @@ struct Ctx {
     {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
-                         &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0,
+                         &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl,
                          &out1, &out2, &fq_gz, &fq_zexp, &fq_zt, &fq_box, &fq_tw, &fq_counts, &fq_offsets, &fq_cursor,
                          &fq_planes};
         for (DevBuf *b : all) f(*b);
@@ -710,6 +711,76 @@ void field_device_locked(Ctx &c, const scmc_mc_args *a, double *d_u, cudaStream_
         if (a->precision == SCMC_PREC_FP64) field_run<2, P64, double>(c, a, P, u, st);
         else if (a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16) field_run<2, PMIX, double>(c, a, P, u, st);
         else field_run<2, P32, float>(c, a, P, u, st);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// field on a wave (MCfieldOnWave.m): lights combined with weights Wl
+// ---------------------------------------------------------------------------
+template <int DIM, int POL>
+void onwave_run(Ctx &c, const scmc_mc_args *a, const Prepared &P, const double2 *d_wl, double2 *d_u,
+                cudaStream_t st)
+{
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using C = typename cplx_t<R>::type;
+    const int nv = (int)a->nv, nl = (int)a->nl;
+    double2 *U = reinterpret_cast<double2 *>(c.acc_f.ensure(nv * sizeof(double2)));
+    CK(cudaMemsetAsync(U, 0, nv * sizeof(double2), st));
+    const int nvc = std::min(nv, kOwMaxViews);
+    const int nchunks = (nv + nvc - 1) / nvc;
+    const size_t smem = onwave_smem(nvc, nl, sizeof(C));
+    if (smem > 227 * 1024) fail(SCMC_ERR_INVALID, "too many lights for the field on a wave");
+    auto ks = onwave_accum_kernel<DIM, POL, true>;
+    auto km = onwave_accum_kernel<DIM, POL, false>;
+    if (smem > 48 * 1024) {
+        CK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(km, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    const int sms = sm_count(c.device);
+    WalkParams W = P.W;
+    for (int64_t done = 0; done < a->max_itr;) {
+        int64_t nb = path_batch_size(a->max_itr - done);
+        W.path_base = a->path_offset + (uint64_t)done;
+        Batch B;
+        walk_batch(c, W, nb, st, B);
+        for (int pass = 0; pass < 2; ++pass) {
+            const int64_t n_ev = pass == 0 ? B.n_paths : B.n_multi;
+            if (n_ev <= 0) continue;
+            const int64_t target = std::max<int64_t>(1, (int64_t)sms * 4 / nchunks);
+            const int64_t per = std::max<int64_t>(kOwWarps * 4, (n_ev + target - 1) / target);
+            dim3 grid((unsigned)((n_ev + per - 1) / per), (unsigned)nchunks);
+            StageScope sc(ST_ROWS, st);
+            if (pass == 0) ks<<<grid, kOwWarps * 32, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, n_ev, per, nvc, d_wl, U);
+            else km<<<grid, kOwWarps * 32, smem, st>>>(P.Q, B.S, c.scap, B.M, c.mcap, n_ev, per, nvc, d_wl, U);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        done += nb;
+    }
+    const double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
+    const double norm = m > 0 ? std::sqrt(1.0 / m * P.volume * a->sigt) : 0.0;  // MCfieldOnWave.m:265-266
+    StageScope fin(ST_FINAL, st);
+    onwave_finalize_kernel<<<std::max(1, std::min(1024, (nv + 255) / 256)), 256, 0, st>>>(U, nv, norm, d_u);
+    CK(cudaGetLastError());
+    LAUNCHED();
+}
+
+void onwave_device_locked(Ctx &c, const scmc_mc_args *a, const double *Wl, double *d_u, cudaStream_t st)
+{
+    CK(cudaSetDevice(a->device));
+    if (!Wl) fail(SCMC_ERR_INVALID, "null light weights");
+    Prepared P = prepare(c, a, 1, st);
+    double2 *dw = reinterpret_cast<double2 *>(c.wl.ensure(a->nl * sizeof(double2)));
+    CK(cudaMemcpyAsync(dw, Wl, a->nl * sizeof(double2), cudaMemcpyHostToDevice, st));
+    double2 *u = reinterpret_cast<double2 *>(d_u);
+    if (a->dim == 3) {
+        if (a->precision == SCMC_PREC_FP64) onwave_run<3, P64>(c, a, P, dw, u, st);
+        else if (a->precision == SCMC_PREC_FP32) onwave_run<3, P32>(c, a, P, dw, u, st);
+        else onwave_run<3, PMIX>(c, a, P, dw, u, st);
+    } else {
+        if (a->precision == SCMC_PREC_FP64) onwave_run<2, P64>(c, a, P, dw, u, st);
+        else if (a->precision == SCMC_PREC_FP32) onwave_run<2, P32>(c, a, P, dw, u, st);
+        else onwave_run<2, PMIX>(c, a, P, dw, u, st);
     }
 }
 
@@ -1547,6 +1618,33 @@ int scmc_field(const scmc_mc_args *args, double *u)
         const size_t bytes = (size_t)args->nv * args->nl * 2 * sizeof(double);
         double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
         field_device_locked(c, args, d, 0);
+        CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
+    });
+}
+
+int scmc_field_onwave_device(const scmc_mc_args *args, const double *Wl, double *d_u, void *stream)
+{
+    return guarded([&] {
+        if (!d_u) fail(SCMC_ERR_INVALID, "null output");
+        validate(args);
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        onwave_device_locked(c, args, Wl, d_u, st);
+        CK(cudaStreamSynchronize(st));
+    });
+}
+
+int scmc_field_onwave(const scmc_mc_args *args, const double *Wl, double *u)
+{
+    return guarded([&] {
+        validate(args);
+        if (!u) fail(SCMC_ERR_INVALID, "null output");
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const size_t bytes = (size_t)args->nv * 2 * sizeof(double);
+        double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
+        onwave_device_locked(c, args, Wl, d, 0);
         CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
     });
 }

@@ -116,6 +116,17 @@ def field_from_args(h: ArgsHolder) -> np.ndarray:
     return u.view(np.complex128).reshape(a.nv, a.nl, order="F")
 
 
+def field_onwave_from_args(h: ArgsHolder, Wl) -> np.ndarray:
+    a = h.args
+    w = np.ascontiguousarray(np.asarray(Wl, dtype=np.complex128).reshape(-1))
+    if w.size != a.nl:
+        raise MatlabStyleError("Wl needs one weight per light")
+    u = np.zeros(2 * a.nv)
+    dp = C.POINTER(C.c_double)
+    _lib.check(_lib.lib().scmc_field_onwave(h.ref, w.view(np.float64).ctypes.data_as(dp), u.ctypes.data_as(dp)))
+    return u.view(np.complex128).reshape(a.nv, 1)
+
+
 def cov_from_args(h: ArgsHolder):
     a = h.args
     n = a.nv * a.nv * a.nl * a.nl
@@ -139,6 +150,13 @@ def MCcov(sigt, albedo, box_min, box_max, l, v, is_ff_l, is_ff_v, maxItr, lambda
     """Single- and multiple-scattering covariances Ms, Mm (Nv x Nv x Nl x Nl), as code/MCcov.m:1-299."""
     return cov_from_args(mc_args(sigt, albedo, box_min, box_max, l, v, is_ff_l, is_ff_v, maxItr, lambda_,
                                  doCBS, smpFlg, sct_type, ampfunc, ampfunc0, **gpu))
+
+
+def MCfieldOnWave(sigt, albedo, box_min, box_max, l, v, is_ff_l, is_ff_v, maxItr, lambda_, doCBS, smpFlg,
+                  sct_type, ampfunc, ampfunc0, lmean0, Wl, **gpu) -> np.ndarray:
+    """Field of the lights combined with complex weights Wl (MCfieldOnWave.m:1-267): Nv x 1."""
+    return field_onwave_from_args(mc_args(sigt, albedo, box_min, box_max, l, v, is_ff_l, is_ff_v, maxItr, lambda_,
+                                          doCBS, smpFlg, sct_type, ampfunc, ampfunc0, lmean0, **gpu), Wl)
 
 
 class Records:

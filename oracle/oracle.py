@@ -51,6 +51,7 @@ def lib():
         lp = C.POINTER(C.c_int64)
         _lib.oracle_field.argtypes = [C.c_void_p, C.POINTER(RngSpec), dp]
         _lib.oracle_cov.argtypes = [C.c_void_p, C.POINTER(RngSpec), dp, dp, C.c_int]
+        _lib.oracle_field_onwave.argtypes = [C.c_void_p, dp, C.POINTER(RngSpec), dp]
         _lib.oracle_records.argtypes = [C.c_void_p, C.POINTER(RngSpec), C.c_int32, C.c_int64,
                                         dp, dp, dp, dp, dp, dp, ip, lp, lp]
         _lib.oracle_field_from_records.argtypes = [C.c_void_p, C.c_int64, dp, dp, dp, dp, dp, dp, ip, dp]
@@ -107,6 +108,18 @@ def field(h: ArgsHolder, rng: Rng) -> np.ndarray:
     u = np.zeros(2 * a.nv * a.nl)
     _check(lib().oracle_field(C.addressof(a), C.byref(rng.spec), _dp(u)), "oracle_field")
     return u.view(np.complex128).reshape(a.nv, a.nl, order="F")
+
+
+def field_onwave(h: ArgsHolder, Wl, rng: Rng) -> np.ndarray:
+    """MCfieldOnWave.m: the field of the lights combined with weights Wl (nl complex)."""
+    a = h.args
+    w = np.ascontiguousarray(np.asarray(Wl, dtype=np.complex128).reshape(-1))
+    if w.size != a.nl:
+        raise ValueError("Wl needs one weight per light")
+    wd = w.view(np.float64)
+    u = np.zeros(2 * a.nv)
+    _check(lib().oracle_field_onwave(C.addressof(a), _dp(wd), C.byref(rng.spec), _dp(u)), "oracle_field_onwave")
+    return u.view(np.complex128).reshape(a.nv, 1)
 
 
 def cov(h: ArgsHolder, rng: Rng, threads: int = 1):

@@ -500,9 +500,39 @@ static void cov_update(nee_t *c, int pL, double wpx, cplx *Ms, cplx *Mm, int thr
 /* The walk (MCfield.m:112-250, MCcov.m:112-290)                             */
 /* ------------------------------------------------------------------------ */
 
+/* MCfieldOnWave.m:177-222: the lights combined with weights Wl before the
+ * update.  Single scattering: u_i += e_v0_i * sum_j af_ij e_l0_j Wl_j
+ * (line 221); multiple: u_i += e_v_ms_i * sum_j e_l0_ms_j Wl_j, with CBS
+ * (u + e_v0_ms_i * sum_j e_l_ms_j Wl_j) / sqrt2 (lines 177, 212, 223-226). */
+static void field_update_onwave(nee_t *c, int pL, double wpx, double xi, const cplx *Wl, cplx *u)
+{
+    int nv = c->nv, nl = c->nl;
+    double s = sqrt(wpx);
+    double ph = 2.0 * M_PI * xi;
+    cplx rot = cos(ph) + I * sin(ph);
+    if (pL == 1) {
+        for (int i = 0; i < nv; ++i) {
+            cplx acc = 0.0;
+            for (int j = 0; j < nl; ++j) acc += c->af_vl[i + nv * j] * (c->e_l0[j] * Wl[j]);
+            u[i] += (s * (c->e_v0[i] * acc)) * rot;
+        }
+        return;
+    }
+    cplx b = 0.0, b2 = 0.0;
+    for (int j = 0; j < nl; ++j) b += c->e_l0_ms[j] * Wl[j];
+    if (c->cbs)
+        for (int j = 0; j < nl; ++j) b2 += c->e_l_ms[j] * Wl[j];
+    for (int i = 0; i < nv; ++i) {
+        cplx t = c->e_v_ms[i] * b;
+        if (c->cbs) t = 1.0 / sqrt(2.0) * (t + c->e_v0_ms[i] * b2);
+        u[i] += (s * t) * rot;
+    }
+}
+
 typedef struct {
-    int kind;          /* 0 field, 1 cov, 2 records */
+    int kind;          /* 0 field, 1 cov, 2 records, 3 field on a wave (weighted lights) */
     cplx *u, *Ms, *Mm;
+    const cplx *Wl;    /* kind 3: light weights */
     int threads;
     /* records */
     int64_t cap, n;
@@ -564,6 +594,7 @@ static int walk(const scmc_mc_args *a, oracle_rng_spec *rs, int with_phase, sink
             } else {
                 if (pL > 1) nee_event(&c, x, ow);
                 if (sk->kind == 0) field_update(&c, pL, wpx, xi, sk->u);
+                else if (sk->kind == 3) field_update_onwave(&c, pL, wpx, xi, sk->Wl, sk->u);
                 else cov_update(&c, pL, wpx, sk->Ms, sk->Mm, sk->threads);
             }
             /* free flight (MCfield.m:225-232) */
@@ -634,6 +665,23 @@ int oracle_field(const scmc_mc_args *a, oracle_rng_spec *rs, double *u)
     sk.u = uc;
     int rc = walk(a, rs, 1, &sk);
     field_normalise(a, uc);
+    return rc;
+}
+
+int oracle_field_onwave(const scmc_mc_args *a, const double *Wl, oracle_rng_spec *rs, double *u)
+{
+    cplx *uc = (cplx *)u;
+    memset(u, 0, sizeof(double) * 2 * a->nv);
+    sink_t sk;
+    memset(&sk, 0, sizeof sk);
+    sk.kind = 3;
+    sk.u = uc;
+    sk.Wl = (const cplx *)Wl;
+    int rc = walk(a, rs, 1, &sk);
+    /* MCfield.m:253-254 normalisation over the nv entries */
+    scmc_mc_args one = *a;
+    one.nl = 1;
+    field_normalise(&one, uc);
     return rc;
 }
 

@@ -34,6 +34,10 @@ typedef struct {
 /* MCfield.m:1-254.  u: 2*nv*nl doubles.  Returns 0, or -1 when a tape ran out. */
 int oracle_field(const scmc_mc_args *a, oracle_rng_spec *rs, double *u);
 
+/* MCfieldOnWave.m:1-267: the field of the lights combined with complex
+ * weights Wl (2*nl doubles, interleaved).  u: 2*nv doubles. */
+int oracle_field_onwave(const scmc_mc_args *a, const double *Wl, oracle_rng_spec *rs, double *u);
+
 /* MCcov.m:1-299.  Ms, Mm: 2*nv*nv*nl*nl doubles.  threads<=1: serial. */
 int oracle_cov(const scmc_mc_args *a, oracle_rng_spec *rs, double *Ms, double *Mm, int threads);
 

@@ -118,6 +118,29 @@ class Gen:
             arrays["Mm"] = np.asarray(outs[1], dtype=complex)
         self.save(name, func, meta, arrays)
 
+    # -- MCfieldOnWave ---------------------------------------------------------
+    def onwave_case(self, name, seed, *, sigt, albedo, box_min, box_max, l, v, is_ff_l, is_ff_v, max_itr, lam, cbs,
+                    smp_flg, sct_type, ampfunc, ampfunc0, lmean0, Wl):
+        """MCfieldOnWave takes ampfunc0, lmean0 and Wl positionally (17 arguments);
+        Wl is passed as a 1 x Nl row, the shape its element-wise products need."""
+        it, ut, nt = self.interp(seed)
+        args = [M(float(sigt)), M(float(albedo)), M(np.reshape(box_min, (-1, 1)).astype(float)),
+                M(np.reshape(box_max, (-1, 1)).astype(float)), M(np.asarray(l, float)),
+                M(np.asarray(v, float)), M(bool(is_ff_l)), M(bool(is_ff_v)), M(float(max_itr)),
+                M(float(lam)), M(bool(cbs)), M(float(smp_flg)), M(float(sct_type)), to_m(ampfunc), to_m(ampfunc0),
+                M(np.reshape(lmean0, (-1, 1)).astype(float)), M(np.asarray(Wl, complex).reshape(1, -1))]
+        u = it.call("MCfieldOnWave", args, 1)[0]
+        arrays = {"utape": ut[:it.ui], "ntape": nt[:it.ni], "box_min": np.asarray(box_min, float),
+                  "box_max": np.asarray(box_max, float), "l": np.asarray(l, float), "v": np.asarray(v, float),
+                  "lmean0": np.asarray(lmean0, float), "Wl": np.asarray(Wl, complex).reshape(-1),
+                  "u": np.asarray(u, dtype=complex)}
+        meta = {"func": "MCfieldOnWave", "sigt": sigt, "albedo": albedo, "is_ff_l": bool(is_ff_l),
+                "is_ff_v": bool(is_ff_v), "max_itr": max_itr, "lambda": lam, "cbs": bool(cbs), "smp_flg": smp_flg,
+                "sct_type": sct_type, "has_ampfunc0": True, "has_lmean0": True}
+        self._put_amp(arrays, meta, "ampfunc", ampfunc)
+        self._put_amp(arrays, meta, "ampfunc0", ampfunc0)
+        self.save(name, "onwave", meta, arrays)
+
     @staticmethod
     def _put_amp(arrays, meta, key, amp):
         if isinstance(amp, dict):
@@ -250,6 +273,22 @@ class Gen:
         self.save(name, "error", {"func": func, "error": msg}, {"dummy": np.zeros(1)})
 
 
+def onwave_cases(g, common, box3, box2, L3, V3r, NFv, tab3d):
+    print("MCfieldOnWave")
+    wr = np.random.default_rng(17)
+    W3 = wr.random(3) * np.exp(2j * np.pi * wr.random(3))
+    g.onwave_case("onwave_3d_hg_ff_refl_cbs_exp", 120, **common, **box3, l=L3, v=V3r, is_ff_l=1, is_ff_v=1, cbs=1,
+                  smp_flg=2, sct_type=3, ampfunc=0.7, ampfunc0=0.4, lmean0=[0.0, 0.1, 1.0], Wl=W3)
+    g.onwave_case("onwave_3d_tab_nfv_nocbs_unif", 121, **common, **box3, l=L3, v=NFv, is_ff_l=1, is_ff_v=0, cbs=0,
+                  smp_flg=1, sct_type=2, ampfunc=tab3d, ampfunc0=tab3d, lmean0=[0.0, 0.0, 1.0], Wl=W3)
+    # isotropic: the reference's single-scattering line is consistent only for one light
+    g.onwave_case("onwave_3d_iso_one_light_cbs", 122, **common, **box3, l=L3[:, :1], v=V3r, is_ff_l=1, is_ff_v=1,
+                  cbs=1, smp_flg=2, sct_type=1, ampfunc=0, ampfunc0=0, lmean0=[0.0, 0.0, 1.0], Wl=W3[:1])
+    g.onwave_case("onwave_2d_hg_cbs", 123, **common, **box2, l=np.vstack([np.sin([0.0, 0.05]), np.cos([0.0, 0.05])]),
+                  v=np.vstack([np.sin([3.1, 3.2, 3.0]), np.cos([3.1, 3.2, 3.0])]), is_ff_l=1, is_ff_v=1, cbs=1,
+                  smp_flg=2, sct_type=3, ampfunc=0.5, ampfunc0=0.5, lmean0=[0.0, 1.0], Wl=W3[:2])
+
+
 def main(ref):
     g = Gen(ref)
     print("tables")
@@ -367,6 +406,8 @@ def main(ref):
                                              2.0, 1.0, True, 2.0, 1.0, 0.0])
     g.error_case("err_field_light", "MCfield", [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3[:2], V3r, True, True,
                                                2.0, 1.0, True, 2.0, 1.0, 0.0])
+    onwave_cases(g, common, box3, box2, L3, V3r, NFv, tab3d)
+
     g.error_case("err_cov_view", "MCcov", [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3, V3r[:1], True, True,
                                           2.0, 1.0, True, 2.0, 1.0, 0.0])
     g.error_case("err_field_nargs", "MCfield", [0.1, 1.0, np.zeros((3, 1)), np.ones((3, 1)), L3, V3r, True, True,
@@ -377,5 +418,26 @@ def main(ref):
     print(f"{len(g.index)} fixtures")
 
 
+def only_onwave(ref):
+    """Add the MCfieldOnWave fixtures to an existing index (the other fixtures
+    are left as they are)."""
+    g = Gen(ref)
+    with open(os.path.join(HERE, "index.json")) as f:
+        g.index = [e for e in json.load(f) if e["kind"] != "onwave"]
+    z = np.load(os.path.join(HERE, "table_3d_hg07.npz"))
+    tab3d = {"evalAmp": z["out_evalAmp"], "sampleIcdf": z["out_sampleIcdf"]}
+    onwave_cases(g, dict(sigt=0.2, albedo=0.9, lam=1.0, max_itr=40), dict(box_min=[-20, -20, 0], box_max=[20, 20, 15]),
+                 dict(box_min=[-20, 0], box_max=[20, 15]), cap_dirs(3, 10, +1, 11), cap_dirs(4, 10, -1, 12),
+                 np.array([[-5.0, 0.0, 6.0, 2.0], [1.0, -3.0, 2.0, 0.5], [-30.0, -30.0, -28.0, 40.0]]), tab3d)
+    with open(os.path.join(HERE, "index.json"), "w") as f:
+        json.dump(g.index, f, indent=1)
+    print(f"{len(g.index)} fixtures")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref = args[0] if args else "/root/reference"
+    if "--only-onwave" in sys.argv:
+        only_onwave(ref)
+    else:
+        main(ref)

@@ -236,3 +236,38 @@ def test_hetero_oracle_matches_reference(oracle_lib, name):
         assert relerr(u, np.asarray(arr["u"]).reshape(u.shape, order="F")) < RTOL
     assert rng.spec.used_u == arr["utape"].size
     assert rng.spec.used_n == arr["ntape"].size
+
+
+ONWAVE_CASES = [e["name"] for e in INDEX if e["kind"] == "onwave"]
+
+
+def test_onwave_fixture_inventory():
+    assert len(ONWAVE_CASES) >= 4
+
+
+@pytest.mark.parametrize("name", ONWAVE_CASES)
+def test_onwave_oracle_matches_reference(oracle_lib, name):
+    """MCfieldOnWave.m (lights combined with complex weights Wl) run by the
+    reference interpreter vs the oracle on the same tapes."""
+    O = oracle_lib
+    meta, arr = load(name)
+    h = MC.mc_args(*mc_case_args(meta, arr), seed=0, precision="fp64")
+    rng = O.Rng.tape(arr["utape"], arr["ntape"])
+    u = O.field_onwave(h, arr["Wl"], rng)
+    assert u.shape == arr["u"].shape
+    assert relerr(u, arr["u"]) < RTOL
+    assert rng.spec.used_u == arr["utape"].size
+    assert rng.spec.used_n == arr["ntape"].size
+
+
+def test_onwave_oracle_equals_field_times_weights(oracle_lib):
+    """On the same (Philox) paths the weighted-light field is the full field
+    times Wl (HG: the single-scattering amplitude is a full matrix)."""
+    O = oracle_lib
+    meta, arr = load("onwave_3d_hg_ff_refl_cbs_exp")
+    args = mc_case_args(meta, arr)
+    args[8] = 60
+    h = MC.mc_args(*args, seed=5, precision="fp64")
+    u = O.field_onwave(h, arr["Wl"], O.Rng.philox())
+    U = O.field(h, O.Rng.philox())
+    assert relerr(u, U @ arr["Wl"].reshape(-1, 1)) < 1e-12
