@@ -248,6 +248,20 @@ int scmc_fq_grid_size(double v_max, double v_stp, int64_t *nv0);
 int scmc_field_fourier_quad(const scmc_fq_args *args, double *u);
 int scmc_field_fourier_quad_device(const scmc_fq_args *args, double *d_u, void *stream);
 
+/* u = MCfieldFourierQuadOnWave(sigt, albedo, box_min, box_max, l, v_max,
+ *       v_stp, maxItr, lambda, doCBS, smpFlg, lmean0, Wl, vsign)
+ *                                             (MCfieldFourierQuadOnWave.m:1)
+ * The lights combined with complex weights Wl (2*nl doubles, interleaved,
+ * host memory) into one nv0 x nv0 field (2*nv0*nv0 doubles), with that
+ * file's conventions: the lateral pixel count takes the parity of the angular
+ * grid (so even grids need no half-integer padding), vsign enters the light
+ * and vertex phases and zexp0 has the opposite phase sign.  The light weight
+ * of each vertex is evaluated at that vertex (the formula of line 279); the
+ * reference's lines 282-292 evaluate the plane's j-th weight at the j-th
+ * vertex of the whole depth-sorted list instead. */
+int scmc_field_fourier_quad_onwave(const scmc_fq_args *args, const double *Wl, double *u);
+int scmc_field_fourier_quad_onwave_device(const scmc_fq_args *args, const double *Wl, double *d_u, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Stage timing.  While enabled, every kernel launch of the walk, the row
  * generation, the contraction and the finalisation is bracketed by CUDA

@@ -7,13 +7,13 @@ constructors, computed by libscmc_gpu.so (C ABI in include/scmc_gpu.h).
 from ._lib import ScmcError, launch_count
 from .interface import (HGScatter, boxArea, farFieldSource, invCDF, isotropicScatter, nearFieldSource,
                         tabulatedAmplitudeScatter)
-from .fourier_quad import MCfieldFourierQuad, fq_args
+from .fourier_quad import MCfieldFourierQuad, MCfieldFourierQuadOnWave, fq_args
 from .hetero import MCCovHetro, MCsampleHetro, hetero_args
 from .mc import MCcov, MCfield, MCfieldOnWave, MatlabStyleError, export_records, mc_args, philox_stream, rng
 from .scmc_api import ScmcInputError, scmc
 
 __all__ = [
-    "scmc", "MCfield", "MCcov", "MCfieldOnWave", "MCfieldFourierQuad", "fq_args", "MCCovHetro", "MCsampleHetro", "hetero_args", "rng", "mc_args", "export_records", "philox_stream",
+    "scmc", "MCfield", "MCcov", "MCfieldOnWave", "MCfieldFourierQuad", "MCfieldFourierQuadOnWave", "fq_args", "MCCovHetro", "MCsampleHetro", "hetero_args", "rng", "mc_args", "export_records", "philox_stream",
     "boxArea", "farFieldSource", "nearFieldSource", "isotropicScatter", "HGScatter",
     "tabulatedAmplitudeScatter", "invCDF", "ScmcError", "ScmcInputError", "MatlabStyleError", "launch_count",
 ]

@@ -65,6 +65,8 @@ def lib():
         L.scmc_fq_grid_size.argtypes = [C.c_double, C.c_double, C.POINTER(C.c_int64)]
         L.scmc_field_fourier_quad.argtypes = [fq, dp]
         L.scmc_field_fourier_quad_device.argtypes = [fq, C.c_void_p, C.c_void_p]
+        L.scmc_field_fourier_quad_onwave.argtypes = [fq, dp, dp]
+        L.scmc_field_fourier_quad_onwave_device.argtypes = [fq, dp, C.c_void_p, C.c_void_p]
         L.scmc_field_noalloc.argtypes = [mp, C.c_void_p, C.c_void_p]
         hp = C.POINTER(_abi.HeteroArgs)
         L.scmc_cov_hetero.argtypes = [hp, dp, dp, dp]
@@ -83,7 +85,8 @@ def lib():
                      "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read",
                      "scmc_fq_grid_size", "scmc_field_fourier_quad", "scmc_field_fourier_quad_device",
                      "scmc_field_noalloc", "scmc_cov_hetero", "scmc_field_hetero", "scmc_cov_hetero_device",
-                     "scmc_field_hetero_device", "scmc_field_onwave", "scmc_field_onwave_device", "scmc_server_create",
+                     "scmc_field_hetero_device", "scmc_field_onwave", "scmc_field_onwave_device", "scmc_field_fourier_quad_onwave",
+                     "scmc_field_fourier_quad_onwave_device", "scmc_server_create",
                      "scmc_server_submit", "scmc_server_wait", "scmc_server_stats_read", "scmc_server_destroy"):
             getattr(L, name).restype = C.c_int
         _lib = L

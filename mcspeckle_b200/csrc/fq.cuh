@@ -31,7 +31,52 @@ struct FqParams {
     double l_diratt, l_idiratt;
     const double *gz;      // nz plane boundaries
     const double *l;       // [nl][3]
+    // phase conventions: MCfieldFourierQuad uses light phase +k l.x and
+    // vertex phase -k (-z1 + tz); MCfieldFourierQuadOnWave uses vsign for both
+    double lsign = 1.0, vsign_vertex = -1.0;
+    // MCfieldFourierQuadOnWave: lights combined with weights wl (nl of them)
+    // into one output light; null for MCfieldFourierQuad
+    const double2 *wl = nullptr;
 };
+
+// The light factor of an entry for output light j (MCfieldFourierQuad.m:272):
+// exp(i k l_j.xl - sigt/2 * slab attenuation); with weights
+// (MCfieldFourierQuadOnWave.m:278-302) sum_j wl_j exp(i vsign k l_j.xl) times
+// the same attenuation.  Phases are reduced mod 2 pi in FP64 outside P64.
+template <int POL>
+__device__ __forceinline__ typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type
+fq_light_factor(const FqParams &F, int j, const double *xl)
+{
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using C = typename cplx_t<R>::type;
+    const double at = F.sigt_half * ((xl[2] - F.bmin_z) * F.l_diratt + (F.bmax_z - xl[2]) * F.l_idiratt);
+    const int j0 = F.wl ? 0 : j, j1 = F.wl ? F.nl : j + 1;
+    C sum = C{};
+    for (int jj = j0; jj < j1; ++jj) {
+        const double *lj = F.l + 3 * jj;
+        const double ph = F.lsign * F.kw * (lj[0] * xl[0] + lj[1] * xl[1] + lj[2] * xl[2]);
+        C e;
+        if constexpr (POL == P64) {
+            double s, co;
+            sincos(ph, &s, &co);
+            e = make_double2(co, s);
+        } else {
+            float s, co;
+            sincosf((float)reduce_2pi(ph), &s, &co);
+            e = make_float2(co, s);
+        }
+        if (F.wl) e = cmul(e, to_c<C>(F.wl[jj]));
+        sum.x += e.x;
+        sum.y += e.y;
+    }
+    if constexpr (POL == P64) {
+        const double a = exp(-at);
+        return make_double2(a * sum.x, a * sum.y);
+    } else {
+        const float a = expf(-(float)at);
+        return make_float2(a * sum.x, a * sum.y);
+    }
+}
 
 // One entry per (vertex, pass): pass 0 views from the first scatterer and
 // lights from the vertex (MCfieldFourierQuad.m:224-232 tt = 1), pass 1 the
@@ -107,7 +152,8 @@ __global__ void fq_entries_kernel(FqParams F, SingleRec S, int64_t scap, MultiRe
         double tz = 0.0;
         if (en.plane >= 0) tz = (F.gz[en.plane] + F.gz[en.plane + 1]) / 2;
         double sd, cd;
-        sincos(-F.kw * (-xv[2] + tz), &sd, &cd);  // exp(-2 pi i/lambda (-z + tz)) (line 272)
+        // exp(-2 pi i/lambda (-z + tz)) (MCfieldFourierQuad.m:272; OnWave: vsign for -1)
+        sincos(F.vsign_vertex * F.kw * (-xv[2] + tz), &sd, &cd);
         en.c0 = make_double2(s * (cp * cd - sp * sd), s * (cp * sd + sp * cd));
         out[k] = en;
         if (en.plane >= 0) atomicAdd(&counts[en.plane], 1);
@@ -164,7 +210,6 @@ fq_accum_kernel(FqParams F, const FqEntry *__restrict__ E, const int *__restrict
     const int r10 = (tile % nvt) * kFqTile, r20 = (tile / nvt) * kFqTile;
     const int plane = planes[blockIdx.y];
     const int e0 = offsets[plane], e1 = offsets[plane + 1];
-    const double *lj = F.l + 3 * j;
     C acc[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[q] = C{};
@@ -173,21 +218,7 @@ fq_accum_kernel(FqParams F, const FqEntry *__restrict__ E, const int *__restrict
         // per entry: the light factor exp(i k l.xl - sigt/2 * slab attenuation) (line 272)
         if (threadIdx.x < ne) {
             const FqEntry en = E[eb + threadIdx.x];
-            const double ph = F.kw * (lj[0] * en.xl[0] + lj[1] * en.xl[1] + lj[2] * en.xl[2]);
-            const double at = F.sigt_half * ((en.xl[2] - F.bmin_z) * F.l_diratt + (F.bmax_z - en.xl[2]) * F.l_idiratt);
-            C lf;
-            if constexpr (POL == P64) {
-                double s, co;
-                sincos(ph, &s, &co);
-                const double a = exp(-at);
-                lf = make_double2(a * co, a * s);
-            } else {
-                float s, co;
-                sincosf((float)reduce_2pi(ph), &s, &co);
-                const float a = expf(-(float)at);
-                lf = make_float2(a * co, a * s);
-            }
-            sc[threadIdx.x] = cmul(to_c<C>(en.c0), lf);
+            sc[threadIdx.x] = cmul(to_c<C>(en.c0), fq_light_factor<POL>(F, j, en.xl));
         }
         for (int idx = threadIdx.x; idx < kFqEB * 2 * kFqTile; idx += blockDim.x) {
             const int k = idx / (2 * kFqTile), m = idx % (2 * kFqTile);
@@ -269,14 +300,7 @@ fq_tc_rows_kernel(FqParams F, const FqEntry *__restrict__ E, const int2 *__restr
         int p1 = 0, p2 = 0;
         if ((int)threadIdx.x < bk.y) {
             const FqEntry en = E[bk.x + threadIdx.x];
-            const double *lj = F.l + 3 * light;
-            const double ph = F.kw * (lj[0] * en.xl[0] + lj[1] * en.xl[1] + lj[2] * en.xl[2]);
-            const double at =
-                F.sigt_half * ((en.xl[2] - F.bmin_z) * F.l_diratt + (F.bmax_z - en.xl[2]) * F.l_idiratt);
-            float sn, cs;
-            sincosf((float)reduce_2pi(ph), &sn, &cs);
-            const float amp = expf(-(float)at);
-            sv = cmul(to_c<float2>(en.c0), make_float2(amp * cs, amp * sn));
+            sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, light, en.xl));
             p1 = en.p1;
             p2 = en.p2;
         }

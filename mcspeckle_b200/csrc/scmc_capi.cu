@@ -1273,7 +1273,7 @@ void validate_fq(const scmc_fq_args *a)
 constexpr int64_t kFqTcEntries = (int64_t)1 << 18;
 constexpr int kFqTcPlanes = 2048;
 
-void fq_tc_batch(Ctx &c, const FqParams &F, const FqEntry *Es, const std::vector<int> &hcounts,
+void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
                  const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *T, const double2 *dzt,
                  double *U, bool split, cudaStream_t st)
 {
@@ -1326,7 +1326,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, const FqEntry *Es, const std::vector
         const CUtensorMap m_ahi = tc_map(ahi, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
         const CUtensorMap m_alo = tc_map(alo, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
         const CUtensorMap m_b = tc_map(bm, (uint64_t)K, (uint64_t)nv0, (uint64_t)K * 2, TC_BN);
-        for (int j = 0; j < F.nl; ++j) {
+        for (int j = 0; j < nl_out; ++j) {
             {
                 StageScope sc(ST_ROWS, st);
                 if (split)
@@ -1358,9 +1358,14 @@ void fq_tc_batch(Ctx &c, const FqParams &F, const FqEntry *Es, const std::vector
     }
 }
 
+// Wl == null: MCfieldFourierQuad.m.  Wl (nl complex, host): MCfieldFourierQuadOnWave.m,
+// which makes the pixel count's parity match the angular grid's (lines 97-99),
+// flips the sign of zexp0's phase (line 140), uses vsign in the light and
+// vertex phases and sums the weighted lights into one output (lines 278-302).
 template <int POL, typename AccT>
-void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
+void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaStream_t st)
 {
+    const int64_t nl_out = Wl ? 1 : a->nl;
     using R = typename std::conditional<POL == P64, double, float>::type;
     using Cx = typename cplx_t<R>::type;
     // geometry, as MCfieldFourierQuad.m:59-138
@@ -1376,7 +1381,8 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
         for (int k = 0; k < 3; ++k) unmeanl[k] = a->lmean0[k];
     const int64_t Nv = colon_count(-a->v_max, a->v_stp, a->v_max);
     const double box_stp = lambda / (a->v_max * 2 + a->v_stp);
-    const int64_t Nx = (int64_t)std::ceil(bw[0] / box_stp / 2) * 2 + 1;
+    int64_t Nx = (int64_t)std::ceil(bw[0] / box_stp / 2) * 2 + 1;
+    if (Wl && (((Nv - Nx) % 2) + 2) % 2 == 1) Nx += 1;  // MCfieldFourierQuadOnWave.m:97-99
     if (Nx > (int64_t)1 << 20) fail(SCMC_ERR_INVALID, "lateral pixel grid too large");
     const double box_w_n = Nx * box_stp, grow = (box_w_n - bw[0]) / 2;
     for (int k = 0; k < 2; ++k) {
@@ -1413,8 +1419,10 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
     for (int64_t q = 0; q < Nv * Nv; ++q) {
         const double zr = vzr[q], zi = vzi[q], av = std::hypot(zr, zi);
         const double dir = zr < 0 ? 1.0 / av : 0.0, idir = zr > 0 ? 1.0 / av : 0.0;
-        // zexp0 = -2 pi i/lambda vz vsign - sigt/2 (diratt - idiratt)
-        zexp0[q] = make_double2(twopi / lambda * zi * a->vsign - sigt / 2 * (dir - idir), -twopi / lambda * zr * a->vsign);
+        // zexp0 = -2 pi i/lambda vz vsign - sigt/2 (diratt - idiratt); OnWave: +2 pi i/lambda
+        const double zs = Wl ? -1.0 : 1.0;
+        zexp0[q] = make_double2(zs * twopi / lambda * zi * a->vsign - sigt / 2 * (dir - idir),
+                                -zs * twopi / lambda * zr * a->vsign);
         const double amp = std::exp(-sigt / 2 * (-bmin[2] * dir + bmax[2] * idir));
         const double sel = (zr < 0 ? -bmin[2] : 0.0) + (zr > 0 ? bmax[2] : 0.0);
         // exp(2 pi i/lambda * sel * vz)
@@ -1429,6 +1437,13 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
     F.nx = (int)Nx;
     F.nz = (int)Nz;
     F.nl = (int)a->nl;
+    if (Wl) {
+        F.lsign = a->vsign;
+        F.vsign_vertex = a->vsign;
+        double2 *dw = reinterpret_cast<double2 *>(c.wl.ensure(a->nl * sizeof(double2)));
+        CK(cudaMemcpyAsync(dw, Wl, a->nl * sizeof(double2), cudaMemcpyHostToDevice, st));
+        F.wl = dw;
+    }
     F.cbs = a->do_cbs;
     F.box_stp = box_stp;
     F.gx1 = bmin[0] + box_stp / 2;
@@ -1485,7 +1500,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
     W.pf0 = W.pf;
     W.key0 = (uint32_t)a->seed;
     W.key1 = (uint32_t)(a->seed >> 32);
-    const int64_t nout = Nv * Nv * a->nl;
+    const int64_t nout = Nv * Nv * nl_out;
     AccT *U = reinterpret_cast<AccT *>(c.acc_s.ensure(2 * nout * sizeof(AccT)));
     CK(cudaMemsetAsync(U, 0, 2 * nout * sizeof(AccT), st));
     int *counts = reinterpret_cast<int *>(c.fq_counts.ensure((Nz + 1) * sizeof(int)));
@@ -1542,13 +1557,13 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
             LAUNCHED();
         }
         if (use_tc) {
-            fq_tc_batch(c, F, Es, hcounts, hoff, hplanes, reinterpret_cast<const float2 *>(T), dzt,
+            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, reinterpret_cast<const float2 *>(T), dzt,
                         reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
             for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
                 const unsigned gy = (unsigned)std::min<size_t>(65535, hplanes.size() - p0);
-                dim3 grid((unsigned)(nvt * nvt * a->nl), gy);
+                dim3 grid((unsigned)(nvt * nvt * nl_out), gy);
                 StageScope sc(ST_CONTRACT, st);
                 fq_accum_kernel<POL, AccT><<<grid, 256, 0, st>>>(F, Es, offsets, planes + p0, T, dz, U);
                 CK(cudaGetLastError());
@@ -1562,18 +1577,18 @@ void fq_run(Ctx &c, const scmc_fq_args *a, double2 *d_u, cudaStream_t st)
     const double norm = total_vert > 0 ? std::sqrt(1.0 / (double)total_vert * V * sigt) : 0.0;  // lines 214, 302-303
     StageScope fin(ST_FINAL, st);
     fq_finalize_kernel<AccT><<<(int)std::max<int64_t>(1, std::min<int64_t>((nout + 255) / 256, 4096)), 256, 0, st>>>(
-        U, db, (int)Nv, (int)a->nl, norm, d_u, use_tc ? 1 : 0);
+        U, db, (int)Nv, (int)nl_out, norm, d_u, use_tc ? 1 : 0);
     CK(cudaGetLastError());
     LAUNCHED();
 }
 
-void fq_device_locked(Ctx &c, const scmc_fq_args *a, double *d_u, cudaStream_t st)
+void fq_device_locked(Ctx &c, const scmc_fq_args *a, double *d_u, cudaStream_t st, const double *Wl = nullptr)
 {
     CK(cudaSetDevice(a->device));
     double2 *u = reinterpret_cast<double2 *>(d_u);
-    if (a->precision == SCMC_PREC_FP64) fq_run<P64, double>(c, a, u, st);
-    else if (a->precision == SCMC_PREC_FP32) fq_run<P32, float>(c, a, u, st);
-    else fq_run<PMIX, double>(c, a, u, st);
+    if (a->precision == SCMC_PREC_FP64) fq_run<P64, double>(c, a, Wl, u, st);
+    else if (a->precision == SCMC_PREC_FP32) fq_run<P32, float>(c, a, Wl, u, st);
+    else fq_run<PMIX, double>(c, a, Wl, u, st);
 }
 
 #include "server.cuh"
@@ -1709,6 +1724,34 @@ int scmc_field_fourier_quad(const scmc_fq_args *args, double *u)
         const size_t bytes = (size_t)nv0 * nv0 * args->nl * 2 * sizeof(double);
         double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
         fq_device_locked(c, args, d, 0);
+        CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
+    });
+}
+
+int scmc_field_fourier_quad_onwave_device(const scmc_fq_args *args, const double *Wl, double *d_u, void *stream)
+{
+    return guarded([&] {
+        validate_fq(args);
+        if (!d_u || !Wl) fail(SCMC_ERR_INVALID, "null output or weights");
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        fq_device_locked(c, args, d_u, st, Wl);
+        CK(cudaStreamSynchronize(st));
+    });
+}
+
+int scmc_field_fourier_quad_onwave(const scmc_fq_args *args, const double *Wl, double *u)
+{
+    return guarded([&] {
+        validate_fq(args);
+        if (!u || !Wl) fail(SCMC_ERR_INVALID, "null output or weights");
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        const int64_t nv0 = colon_count(-args->v_max, args->v_stp, args->v_max);
+        const size_t bytes = (size_t)nv0 * nv0 * 2 * sizeof(double);
+        double *d = reinterpret_cast<double *>(c.out0.ensure(bytes));
+        fq_device_locked(c, args, d, 0, Wl);
         CK(cudaMemcpy(u, d, bytes, cudaMemcpyDeviceToHost));
     });
 }

@@ -96,3 +96,22 @@ def MCfieldFourierQuad(sigt, albedo, box_min, box_max, l, v_max, v_stp, maxItr, 
     """Speckle field on an angular grid by z-plane quadrature (MCfieldFourierQuad.m:1-303)."""
     return field_fourier_quad_from_args(fq_args(sigt, albedo, box_min, box_max, l, v_max, v_stp, maxItr, lambda_,
                                                 doCBS, smpFlg, lmean0, vsign, **gpu))
+
+
+def field_fourier_quad_onwave_from_args(h: FqHolder, Wl) -> np.ndarray:
+    a = h.args
+    w = np.ascontiguousarray(np.asarray(Wl, dtype=np.complex128).reshape(-1))
+    if w.size != a.nl:
+        raise MatlabStyleError("Wl needs one weight per light")
+    u = np.zeros(2 * h.nv0 * h.nv0)
+    dp = C.POINTER(C.c_double)
+    _lib.check(_lib.lib().scmc_field_fourier_quad_onwave(h.ref, w.view(np.float64).ctypes.data_as(dp),
+                                                         u.ctypes.data_as(dp)))
+    return u.view(np.complex128).reshape(h.nv0, h.nv0, order="F")
+
+
+def MCfieldFourierQuadOnWave(sigt, albedo, box_min, box_max, l, v_max, v_stp, maxItr, lambda_, doCBS, smpFlg,
+                             lmean0, Wl, vsign=-1, **gpu):
+    """The lights combined with complex weights Wl (MCfieldFourierQuadOnWave.m:1-337): Nv0 x Nv0."""
+    return field_fourier_quad_onwave_from_args(fq_args(sigt, albedo, box_min, box_max, l, v_max, v_stp, maxItr,
+                                                       lambda_, doCBS, smpFlg, lmean0, vsign, **gpu), Wl)

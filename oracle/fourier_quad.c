@@ -55,7 +55,15 @@ static int cmp_item(const void *p, const void *q)
     return (a->i < b->i) ? -1 : (a->i > b->i); /* stable, as MATLAB's sort */
 }
 
-int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double *u_out)
+/* Wl == NULL: MCfieldFourierQuad.m.  Wl != NULL: MCfieldFourierQuadOnWave.m,
+ * which differs in four places: the lateral pixel count is made to have the
+ * parity of the angular grid (lines 97-99), zexp0 has the opposite phase sign
+ * (line 140), the light term is twl = sum_j Wl_j exp(vsign 2 pi i/lambda
+ * l_j.x) times the slab attenuation atl (lines 278-295; see the note on
+ * which vertex twl reads), and the vertex
+ * phase is exp(vsign 2 pi i/lambda (-z1 + tz)) (line 302); the lights are
+ * summed into one output. */
+static int fq_core(const scmc_fq_args *a, const cplx *Wl, int as_written, oracle_rng_spec *rs, double *u_out)
 {
     const double lambda = a->lambda, sigt = a->sigt;
     const double PI = M_PI;
@@ -76,7 +84,8 @@ int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double
     for (int64_t k = 0; k < Nv; ++k) theta_v[k] = -v_max + (double)k * v_stp;
     /* lines 92-98: lateral pitch and the box padded to an odd pixel count */
     const double box_stp = lambda / (v_max * 2 + v_stp);
-    const int64_t Nx = (int64_t)ceil(bw[0] / box_stp / 2) * 2 + 1;
+    int64_t Nx = (int64_t)ceil(bw[0] / box_stp / 2) * 2 + 1;
+    if (Wl && (((Nv - Nx) % 2) + 2) % 2 == 1) Nx = Nx + 1; /* OnWave: mod(Nv - Nx, 2) == 1 */
     const double box_w_n = Nx * box_stp;
     const double grow = (box_w_n - bw[0]) / 2; /* box_w(1) for both x and y, as line 96-97 */
     for (int k = 0; k < 2; ++k) {
@@ -118,7 +127,8 @@ int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double
         double av = cabs(z);
         double diratt = (creal(z) < 0) ? 1.0 / av : 0.0;
         double idiratt = (creal(z) > 0) ? 1.0 / av : 0.0;
-        zexp0[q] = (-2 * PI * I / lambda) * z * vsign - sigt / 2 * (diratt - idiratt);
+        if (Wl) zexp0[q] = (2 * PI * I / lambda) * z * vsign - sigt / 2 * (diratt - idiratt);
+        else zexp0[q] = (-2 * PI * I / lambda) * z * vsign - sigt / 2 * (diratt - idiratt);
         cplx b1 = cexp(-sigt / 2 * (-bmin[2] * diratt + bmax[2] * idiratt));
         cplx ph = (-bmin[2] * (creal(z) < 0) * z + bmax[2] * (creal(z) > 0) * z);
         boxexp0[q] = b1 * cexp(2 * PI * I / lambda * ph);
@@ -144,7 +154,8 @@ int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double
         pi_ = realloc(pi_, sizeof(double) * cap);
     }
     const int64_t nl = a->nl;
-    cplx *u = calloc(Nv * Nv * nl, sizeof(cplx));
+    const int64_t nout = Wl ? 1 : nl; /* output planes */
+    cplx *u = calloc(Nv * Nv * nout, sizeof(cplx));
     if (rc == 0) {
         /* twiddles exp(-2 pi i m' P / M) for the centred, flipped, cropped DFT:
          * output r is FFT bin q = r + Nva_padd, flipped to M-1-q, centred by
@@ -186,7 +197,7 @@ int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double
                 zmax_ind = citr - 1;
                 if (zmax_ind < zmin_ind) continue;
                 double tz = (gz[j1 - 1] + gz[j1]) / 2;
-                for (int64_t j2 = 0; j2 < nl; ++j2) {
+                for (int64_t j2 = 0; j2 < nout; ++j2) {
                     const double *lj = a->l + 3 * j2;
                     memset(acc, 0, sizeof(cplx) * Nv * Nv);
                     for (int64_t e = zmin_ind - 1; e < zmax_ind; ++e) {
@@ -197,9 +208,28 @@ int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double
                         if (p1 > Nx) p1 = Nx;
                         if (p2 < 1) p2 = 1;
                         if (p2 > Nx) p2 = Nx;
-                        cplx w = sp[e] * cexp(-2 * PI * I / lambda * (-x1e[2] + tz)) *
-                                 cexp(2 * PI * I / lambda * (lj[0] * xe[0] + lj[1] * xe[1] + lj[2] * xe[2]) -
-                                      sigt / 2 * ((xe[2] - bmin[2]) * l_diratt + (bmax[2] - xe[2]) * l_idiratt));
+                        cplx w;
+                        if (Wl) {
+                            /* lines 282-292 evaluate twl at xL(:, 1:numel(jj)): the plane's
+                             * j3-th weight comes from the j3-th vertex of the whole
+                             * depth-sorted list, not from the plane's own vertex jj(j3).
+                             * as_written = 1 keeps that; 0 uses the plane's own vertex,
+                             * the formula of the commented-out line 279 (and of
+                             * MCfieldFourierQuad), which the GPU computes. */
+                            const double *xt = as_written ? sx + 3 * (e - (zmin_ind - 1)) : xe;
+                            cplx twl = 0.0;
+                            for (int64_t j = 0; j < nl; ++j) {
+                                const double *l = a->l + 3 * j;
+                                twl += Wl[j] * cexp(vsign * 2 * PI * I / lambda * (l[0] * xt[0] + l[1] * xt[1] + l[2] * xt[2]));
+                            }
+                            const double atl =
+                                exp(-sigt / 2 * ((xe[2] - bmin[2]) * l_diratt + (bmax[2] - xe[2]) * l_idiratt));
+                            w = sp[e] * cexp(vsign * 2 * PI * I / lambda * (-x1e[2] + tz)) * twl * atl;
+                        } else {
+                            w = sp[e] * cexp(-2 * PI * I / lambda * (-x1e[2] + tz)) *
+                                cexp(2 * PI * I / lambda * (lj[0] * xe[0] + lj[1] * xe[1] + lj[2] * xe[2]) -
+                                     sigt / 2 * ((xe[2] - bmin[2]) * l_diratt + (bmax[2] - xe[2]) * l_idiratt));
+                        }
                         for (int64_t r2 = 0; r2 < Nv; ++r2) {
                             cplx w2 = w * tw[r2 * Nx + (p2 - 1)];
                             for (int64_t r1 = 0; r1 < Nv; ++r1) acc[r1 + Nv * r2] += w2 * tw[r1 * Nx + (p1 - 1)];
@@ -214,11 +244,22 @@ int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double
         /* lines 291-303 */
         double V = bw[0] * bw[1] * bw[2];
         double f = sqrt(1.0 / (double)nvert * V * sigt);
-        for (int64_t j2 = 0; j2 < nl; ++j2)
+        for (int64_t j2 = 0; j2 < nout; ++j2)
             for (int64_t q = 0; q < Nv * Nv; ++q) u[Nv * Nv * j2 + q] = u[Nv * Nv * j2 + q] * boxexp0[q] * f;
-        memcpy(u_out, u, sizeof(cplx) * Nv * Nv * nl);
+        memcpy(u_out, u, sizeof(cplx) * Nv * Nv * nout);
     }
     free(u); free(xL); free(x1L); free(pr); free(pi_);
     free(theta_v); free(vz); free(gz); free(zexp0); free(boxexp0);
     return rc;
+}
+
+int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double *u_out)
+{
+    return fq_core(a, NULL, 0, rs, u_out);
+}
+
+int oracle_field_fourier_quad_onwave(const scmc_fq_args *a, const double *Wl, int32_t as_written,
+                                     oracle_rng_spec *rs, double *u_out)
+{
+    return fq_core(a, (const cplx *)Wl, as_written, rs, u_out);
 }

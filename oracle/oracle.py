@@ -60,6 +60,7 @@ def lib():
         _lib.oracle_cov_hetero.argtypes = [C.POINTER(HeteroArgs), C.POINTER(RngSpec), dp, dp, dp, C.c_int]
         _lib.oracle_field_hetero.argtypes = [C.POINTER(HeteroArgs), C.POINTER(RngSpec), dp]
         _lib.oracle_field_fourier_quad.argtypes = [C.POINTER(FqArgs), C.POINTER(RngSpec), dp]
+        _lib.oracle_field_fourier_quad_onwave.argtypes = [C.POINTER(FqArgs), dp, C.c_int32, C.POINTER(RngSpec), dp]
         _lib.oracle_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                               C.POINTER(C.c_uint32)]
         _lib.oracle_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
@@ -213,6 +214,20 @@ def field_fourier_quad(fa: FqArgs, rng: Rng, nv0: int) -> np.ndarray:
     u = np.zeros(2 * nv0 * nv0 * fa.nl)
     _check(lib().oracle_field_fourier_quad(C.byref(fa), C.byref(rng.spec), _dp(u)), "oracle_field_fourier_quad")
     return u.view(np.complex128).reshape(nv0, nv0, fa.nl, order="F")
+
+
+def field_fourier_quad_onwave(fa: FqArgs, Wl, rng: Rng, nv0: int, as_written: bool = False) -> np.ndarray:
+    """MCfieldFourierQuadOnWave on the oracle: nv0 x nv0 complex.  as_written:
+    the reference's lines 282-292 exactly (light weight of a plane's j3-th
+    vertex taken at the j3-th vertex of the whole sorted list)."""
+    w = np.ascontiguousarray(np.asarray(Wl, dtype=np.complex128).reshape(-1))
+    if w.size != fa.nl:
+        raise ValueError("Wl needs one weight per light")
+    u = np.zeros(2 * nv0 * nv0)
+    _check(lib().oracle_field_fourier_quad_onwave(C.byref(fa), _dp(w.view(np.float64)), int(bool(as_written)),
+                                                  C.byref(rng.spec), _dp(u)),
+           "oracle_field_fourier_quad_onwave")
+    return u.view(np.complex128).reshape(nv0, nv0, order="F")
 
 
 def cov_hetero(h, rng: Rng, threads: int = 1):

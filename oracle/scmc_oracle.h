@@ -60,6 +60,13 @@ int oracle_cov_from_records(const scmc_mc_args *a, int64_t n, const double *x,
 /* MCfieldFourierQuad.m:1-304 (isotropic walk, z-plane quadrature, lateral
  * gridding and a 2-D DFT per plane and light).  u: 2*nv0*nv0*nl doubles. */
 int oracle_field_fourier_quad(const scmc_fq_args *a, oracle_rng_spec *rs, double *u);
+/* MCfieldFourierQuadOnWave.m:1-337: the lights combined with weights Wl
+ * (2*nl doubles, interleaved) into one output.  u: 2*nv0*nv0 doubles.
+ * as_written = 1: the light weight of a plane's j3-th vertex is evaluated at
+ * the j3-th vertex of the whole depth-sorted list, as lines 282-292 do;
+ * 0: at the vertex itself (line 279's formula, the GPU's). */
+int oracle_field_fourier_quad_onwave(const scmc_fq_args *a, const double *Wl, int32_t as_written,
+                                     oracle_rng_spec *rs, double *u);
 
 /* MCCovHetro.m:1-276 (Ms, Mm, mean1) and MCsampleHetro.m:1-227 (u). */
 int oracle_cov_hetero(const scmc_hetero_args *a, oracle_rng_spec *rs, double *Ms, double *Mm, double *mean1,

@@ -218,6 +218,25 @@ class Gen:
                 "error": err}
         self.save(name, "fourier_quad", meta, arrays)
 
+    def fq_onwave_case(self, name, seed, *, sigt, albedo, box_min, box_max, l, v_max, v_stp, max_itr, lam, cbs,
+                       smp_flg, lmean0, Wl, vsign):
+        """MCfieldFourierQuadOnWave(..., lmean0, Wl, vsign): Wl as an Nl x 1 column, as its test passes it."""
+        it, ut, nt = self.interp(seed)
+        args = [M(float(sigt)), M(float(albedo)), M(np.reshape(box_min, (-1, 1)).astype(float)),
+                M(np.reshape(box_max, (-1, 1)).astype(float)), M(np.asarray(l, float)), M(float(v_max)),
+                M(float(v_stp)), M(float(max_itr)), M(float(lam)), M(bool(cbs)), M(float(smp_flg)),
+                M(np.zeros((0, 0))) if lmean0 is None else M(np.reshape(lmean0, (-1, 1)).astype(float)),
+                M(np.asarray(Wl, complex).reshape(-1, 1)), M(float(vsign))]
+        u = it.call("MCfieldFourierQuadOnWave", args, 1)[0]
+        arrays = {"u": np.asarray(u, dtype=complex), "utape": ut[:it.ui], "ntape": nt[:it.ni],
+                  "box_min": np.asarray(box_min, float), "box_max": np.asarray(box_max, float),
+                  "l": np.asarray(l, float), "Wl": np.asarray(Wl, complex).reshape(-1)}
+        if lmean0 is not None:
+            arrays["lmean0"] = np.asarray(lmean0, float)
+        meta = {"sigt": sigt, "albedo": albedo, "v_max": v_max, "v_stp": v_stp, "max_itr": max_itr, "lambda": lam,
+                "cbs": bool(cbs), "smp_flg": smp_flg, "vsign": vsign, "has_lmean0": lmean0 is not None}
+        self.save(name, "fq_onwave", meta, arrays)
+
     # -- MCCovHetro / MCsampleHetro ----------------------------------------------
     def hetero_case(self, name, func, seed, *, sigt, albedo, box_min, box_max, box_bin, l, v, is_ff_l, is_ff_v,
                     max_itr, lam, cbs, smp_flg, sct_type, ampfunc, ampfunc0=None, extra=None):
@@ -271,6 +290,22 @@ class Gen:
             msg = str(e)
         assert msg is not None, name
         self.save(name, "error", {"func": func, "error": msg}, {"dummy": np.zeros(1)})
+
+
+def fq_onwave_cases(g):
+    print("MCfieldFourierQuadOnWave")
+    wr = np.random.default_rng(19)
+    Lq = cap_dirs(3, 6, +1, 23)
+    W = wr.random(3) * np.exp(2j * np.pi * wr.random(3))
+    g.fq_onwave_case("fqow_wide_box_cbs_exp", 311, sigt=0.1, albedo=0.9, box_min=[-60, -60, 0], box_max=[60, 60, 20],
+                     l=Lq, v_max=0.2, v_stp=0.01, max_itr=20, lam=1.0, cbs=1, smp_flg=2, lmean0=None, Wl=W, vsign=-1)
+    g.fq_onwave_case("fqow_narrow_box_nocbs_unif", 312, sigt=0.15, albedo=0.8, box_min=[-10, -10, 0],
+                     box_max=[10, 10, 8], l=Lq, v_max=0.2, v_stp=0.01, max_itr=20, lam=1.0, cbs=0, smp_flg=1,
+                     lmean0=[0.0, 0.1, 1.0], Wl=W, vsign=1)
+    # even grid length: the parity fix (MCfieldFourierQuadOnWave.m:97-99) makes the padding integral
+    g.fq_onwave_case("fqow_even_grid_cbs", 313, sigt=0.1, albedo=0.9, box_min=[-10, -10, 0], box_max=[10, 10, 8],
+                     l=Lq[:, :2], v_max=0.195, v_stp=0.01, max_itr=10, lam=1.0, cbs=1, smp_flg=2, lmean0=None,
+                     Wl=W[:2], vsign=-1)
 
 
 def onwave_cases(g, common, box3, box2, L3, V3r, NFv, tab3d):
@@ -348,6 +383,8 @@ def main(ref):
               vsign=-1)
     g.fq_case("fq_even_grid_errors", 304, sigt=0.1, albedo=0.9, box_min=[-10, -10, 0], box_max=[10, 10, 8], l=Lq,
               v_max=0.195, v_stp=0.01, max_itr=5, lam=1.0, cbs=1, smp_flg=2, lmean0=None, vsign=-1)
+
+    fq_onwave_cases(g)
 
     print("hetero")
     g2 = np.random.default_rng(7)
@@ -439,5 +476,13 @@ if __name__ == "__main__":
     ref = args[0] if args else "/root/reference"
     if "--only-onwave" in sys.argv:
         only_onwave(ref)
+    elif "--only-fq-onwave" in sys.argv:
+        g = Gen(ref)
+        with open(os.path.join(HERE, "index.json")) as f:
+            g.index = [e for e in json.load(f) if e["kind"] != "fq_onwave"]
+        fq_onwave_cases(g)
+        with open(os.path.join(HERE, "index.json"), "w") as f:
+            json.dump(g.index, f, indent=1)
+        print(f"{len(g.index)} fixtures")
     else:
         main(ref)

@@ -1620,6 +1620,15 @@ def b_rem(it, args, nargout):
     return _elementwise(lambda x, y: np.where(y == 0, x, x - np.trunc(x / np.where(y == 0, 1, y)) * y), a, b)
 
 
+def b_num2str(it, args, nargout):
+    """num2str of a real scalar (only used here to build progress messages)."""
+    v = num(args[0]).reshape(-1)
+    if v.size == 1:
+        x = float(np.real(v[0]))
+        return MStr(str(int(x)) if x == int(x) else f"{x:.4g}")
+    return MStr(" ".join(f"{float(np.real(x)):.4g}" for x in v))
+
+
 def b_char(it, args, nargout):
     a = args[0]
     if isinstance(a, MStr):
@@ -1754,7 +1763,7 @@ BUILTINS = {
     "isscalar": b_isscalar, "isvector": b_isvector, "isreal": b_isreal, "isnumeric": b_isnumeric,
     "islogical": b_islogical, "isinf": b_isinf, "isnan": b_isnan, "isfield": b_isfield,
     "hist": b_hist, "strcmp": b_strcmp, "strncmpi": b_strncmpi, "char": b_char, "sinc": b_sinc, "null": b_null,
-    "logical": b_logical, "double": b_double,
+    "logical": b_logical, "double": b_double, "num2str": b_num2str,
     "deg2rad": lambda it, a, n: _as_float(a[0]) * (math.pi / 180.0),
     "rad2deg": lambda it, a, n: _as_float(a[0]) * (180.0 / math.pi),
     "plus": _binop_builtin("+"), "minus": _binop_builtin("-"), "times": _binop_builtin(".*"),

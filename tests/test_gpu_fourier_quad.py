@@ -104,3 +104,33 @@ def test_fourier_quad_tensor_cores_fp64_anchor(gpu, oracle_lib):
     u = FQ.field_fourier_quad_from_args(h)
     uo = oracle_lib.field_fourier_quad(h.args, oracle_lib.Rng.philox(), h.nv0)
     assert rel(u, uo) < 1e-10
+
+
+# MCfieldFourierQuadOnWave: the lights combined with complex weights Wl.
+def weights(n, seed=9):
+    g = np.random.default_rng(seed)
+    return g.random(n) * np.exp(2j * np.pi * g.random(n))
+
+
+OW_CASES = {k: FQ_CASES[k] for k in ("wide_cbs_exp", "narrow_nocbs_unif", "even_grid")}
+OW_CASES.update({k: TC_CASES[k] for k in ("tc_wide_cbs", "tc_even_grid")})
+
+
+@pytest.mark.parametrize("name", list(OW_CASES))
+def test_fourier_quad_onwave_fp64_matches_oracle(gpu, oracle_lib, name):
+    h = args_for(OW_CASES[name], "fp64")
+    W = weights(h.args.nl)
+    u = FQ.field_fourier_quad_onwave_from_args(h, W)
+    uo = oracle_lib.field_fourier_quad_onwave(h.args, W, oracle_lib.Rng.philox(), h.nv0)
+    assert u.shape == uo.shape == (h.nv0, h.nv0)
+    assert rel(u, uo) < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp16"])
+@pytest.mark.parametrize("name", list(OW_CASES))
+def test_fourier_quad_onwave_close_to_fp64(gpu, name, precision):
+    W = weights(2)
+    u64 = FQ.field_fourier_quad_onwave_from_args(args_for(OW_CASES[name], "fp64"), W)
+    u = FQ.field_fourier_quad_onwave_from_args(args_for(OW_CASES[name], precision), W)
+    assert np.isfinite(u).all()
+    assert rel(u, u64) < 1e-3

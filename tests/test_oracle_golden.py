@@ -271,3 +271,46 @@ def test_onwave_oracle_equals_field_times_weights(oracle_lib):
     u = O.field_onwave(h, arr["Wl"], O.Rng.philox())
     U = O.field(h, O.Rng.philox())
     assert relerr(u, U @ arr["Wl"].reshape(-1, 1)) < 1e-12
+
+
+FQOW_CASES = [e["name"] for e in INDEX if e["kind"] == "fq_onwave"]
+
+
+def test_fq_onwave_fixture_inventory():
+    assert len(FQOW_CASES) >= 3
+
+
+@pytest.mark.parametrize("name", FQOW_CASES)
+def test_fourier_quad_onwave_oracle_matches_reference(oracle_lib, name):
+    """MCfieldFourierQuadOnWave.m (weighted lights, its own phase conventions
+    and the pixel-count parity fix) vs the oracle on the same tapes."""
+    from mcspeckle_b200 import fourier_quad as FQ
+    meta, arr = load(name)
+    h = FQ.fq_args(meta["sigt"], meta["albedo"], arr["box_min"], arr["box_max"], arr["l"], meta["v_max"],
+                   meta["v_stp"], meta["max_itr"], meta["lambda"], meta["cbs"], meta["smp_flg"],
+                   arr["lmean0"] if meta["has_lmean0"] else None, meta["vsign"], seed=0, precision="fp64")
+    rng = oracle_lib.Rng.tape(arr["utape"], arr["ntape"])
+    u = oracle_lib.field_fourier_quad_onwave(h.args, arr["Wl"], rng, h.nv0, as_written=True)
+    assert u.shape == arr["u"].shape
+    assert relerr(u, arr["u"]) < RTOL
+    assert rng.spec.used_u == arr["utape"].size
+    assert rng.spec.used_n == arr["ntape"].size
+
+
+def test_fourier_quad_onwave_linear_in_weights(oracle_lib):
+    """On the same paths the OnWave field is linear in Wl: the sum over lights
+    of each light alone (weight 1) times its weight.  Holds for the formula the
+    GPU uses (each vertex's own light weight)."""
+    from mcspeckle_b200 import fourier_quad as FQ
+    meta, arr = load("fqow_wide_box_cbs_exp")
+    h = FQ.fq_args(meta["sigt"], meta["albedo"], arr["box_min"], arr["box_max"], arr["l"], meta["v_max"],
+                   meta["v_stp"], 15, meta["lambda"], meta["cbs"], meta["smp_flg"], None, -1.0, seed=3,
+                   precision="fp64")
+    W = arr["Wl"]
+    u = oracle_lib.field_fourier_quad_onwave(h.args, W, oracle_lib.Rng.philox(), h.nv0)
+    parts = 0
+    for j in range(W.size):
+        e = np.zeros(W.size, complex)
+        e[j] = 1.0
+        parts = parts + W[j] * oracle_lib.field_fourier_quad_onwave(h.args, e, oracle_lib.Rng.philox(), h.nv0)
+    assert relerr(u, parts) < 1e-10
