@@ -354,6 +354,36 @@ int scmc_server_stats_read(scmc_server *s, scmc_server_stats *out);
  * (SCMC_ERR_CANCELLED) and frees the server. */
 int scmc_server_destroy(scmc_server *s);
 
+/* ---------------------------------------------------------------------------
+ * Post-processing.
+ *
+ * rU = refocus(u, v, l, box_min, box_max, box_stp, lambda)    (refocus.m:1)
+ * The field of nv far-field views u (2*nv doubles) back-propagated onto the
+ * grid ndgrid(box_min(k):box_stp(k):box_max(k), ...) (dim 2 or 3, x fastest)
+ * with light direction l:  rU(p) = (sum_v conj(u_v) exp(-2 pi i/lambda
+ * v.p)) exp(2 pi i/lambda l.p).  v: dim x nv column-major.  rU: 2*N doubles,
+ * N = prod(dims) from scmc_refocus_grid.  as_written = 1 leaves the first
+ * grid point at 0 as the reference's chunk indices do (refocus.m:27).
+ * precision: SCMC_PREC_FP64 or SCMC_PREC_MIXED (phase reduced in FP64,
+ * sincos in FP32).
+ * ------------------------------------------------------------------------- */
+int scmc_refocus_grid(int32_t dim, const double *box_min, const double *box_max, const double *box_stp,
+                      int64_t *dims, int64_t *n);
+int scmc_refocus(const double *u, const double *v, int64_t nv, int32_t dim, const double *l, const double *box_min,
+                 const double *box_max, const double *box_stp, double lambda, int32_t as_written, int32_t precision,
+                 int32_t device, double *rU);
+
+/* Field samples from a covariance, as examples/samplingFromCovMatrix/
+ * samplingFromCovMatrix.m:47-64 does with mvnrnd: C is N x N complex
+ * (2*N*N doubles, column-major, index v + nv*l as scmc's C(:,:,l1,l2) blocks
+ * joined), Sigma = 0.5 [Re C, -Im C; Im C, Re C], sample t = g_t chol(Sigma)
+ * with g_t the 2N standard normals of the Philox normal stream (seed, path t)
+ * (scmc_philox_stream tag 1), z_t = s(1:N) + i s(N+1:2N).  Z: 2*N*n_samples
+ * doubles.  Cholesky in FP64 on the GPU.  A singular Sigma (a covariance of
+ * fewer events than 2N) returns SCMC_ERR_INVALID; mvnrnd's cholcov would
+ * fall back to an eigendecomposition there. */
+int scmc_sample_cov(const double *C, int64_t N, int64_t n_samples, uint64_t seed, int32_t device, double *Z);
+
 /* Library information and error reporting. */
 int scmc_abi_version(void);
 const char *scmc_last_error(void);

@@ -79,6 +79,10 @@ def lib():
         L.scmc_server_wait.argtypes = [vp, C.c_int64, C.c_int64, C.POINTER(_abi.RequestInfo)]
         L.scmc_server_stats_read.argtypes = [vp, C.POINTER(_abi.ServerStats)]
         L.scmc_server_destroy.argtypes = [vp]
+        L.scmc_refocus_grid.argtypes = [C.c_int32, dp, dp, dp, lp, lp]
+        L.scmc_refocus.argtypes = [dp, dp, C.c_int64, C.c_int32, dp, dp, dp, dp, C.c_double, C.c_int32, C.c_int32,
+                                   C.c_int32, dp]
+        L.scmc_sample_cov.argtypes = [dp, C.c_int64, C.c_int64, C.c_uint64, C.c_int32, dp]
         L.scmc_profile_enable.argtypes = [C.c_int32]
         L.scmc_profile_read.argtypes = [C.POINTER(_abi.StageTimes), C.c_int32]
         for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",
@@ -86,7 +90,7 @@ def lib():
                      "scmc_fq_grid_size", "scmc_field_fourier_quad", "scmc_field_fourier_quad_device",
                      "scmc_field_noalloc", "scmc_cov_hetero", "scmc_field_hetero", "scmc_cov_hetero_device",
                      "scmc_field_hetero_device", "scmc_field_onwave", "scmc_field_onwave_device", "scmc_field_fourier_quad_onwave",
-                     "scmc_field_fourier_quad_onwave_device", "scmc_server_create",
+                     "scmc_field_fourier_quad_onwave_device", "scmc_refocus_grid", "scmc_refocus", "scmc_sample_cov", "scmc_server_create",
                      "scmc_server_submit", "scmc_server_wait", "scmc_server_stats_read", "scmc_server_destroy"):
             getattr(L, name).restype = C.c_int
         _lib = L

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscmc_gpu.so")
 SOURCES = ["scmc_capi.cu"]
-HEADERS = ["common.cuh", "walk.cuh", "nee.cuh", "accum.cuh", "herk_tc.cuh", "field_tc.cuh", "fq.cuh", "onwave.cuh", "server.cuh", "hgrid.cuh", "../../include/scmc_gpu.h"]
+HEADERS = ["common.cuh", "walk.cuh", "nee.cuh", "accum.cuh", "herk_tc.cuh", "field_tc.cuh", "fq.cuh", "onwave.cuh", "postprocess.cuh", "server.cuh", "hgrid.cuh", "../../include/scmc_gpu.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -24,6 +24,7 @@
 #include "field_tc.cuh"
 #include "fq.cuh"
 #include "onwave.cuh"
+#include "postprocess.cuh"
 
 using namespace scmc;
 
@@ -1887,6 +1888,126 @@ int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, dou
         if (e == cudaSuccess) e = cudaMemcpy(out, d, n * sizeof(double), cudaMemcpyDeviceToHost);
         cudaFree(d);
         CK(e);
+    });
+}
+
+// ---------------------------------------------------------------------------
+// post-processing: refocus, samples from a covariance
+// ---------------------------------------------------------------------------
+static int64_t pp_colon(double a, double st, double b)
+{
+    if (st == 0 || (st > 0 && a > b) || (st < 0 && a < b)) return 0;
+    const double q = (b - a) / st;
+    return (int64_t)std::floor(q + 1e-10 * std::fmax(1.0, std::fabs(q))) + 1;
+}
+
+int scmc_refocus_grid(int32_t dim, const double *box_min, const double *box_max, const double *box_stp,
+                      int64_t *dims, int64_t *n)
+{
+    return guarded([&] {
+        if ((dim != 2 && dim != 3) || !box_min || !box_max || !box_stp || !dims || !n)
+            fail(SCMC_ERR_INVALID, "invalid refocus grid");
+        int64_t t = 1;
+        for (int k = 0; k < dim; ++k) {
+            dims[k] = pp_colon(box_min[k], box_stp[k], box_max[k]);
+            t *= dims[k];
+        }
+        *n = t;
+    });
+}
+
+int scmc_refocus(const double *u, const double *v, int64_t nv, int32_t dim, const double *l, const double *box_min,
+                 const double *box_max, const double *box_stp, double lambda, int32_t as_written, int32_t precision,
+                 int32_t device, double *rU)
+{
+    return guarded([&] {
+        if ((dim != 2 && dim != 3) || nv < 1 || !u || !v || !l || !box_min || !box_max || !box_stp || !rU)
+            fail(SCMC_ERR_INVALID, "invalid refocus arguments");
+        if (!(lambda > 0)) fail(SCMC_ERR_INVALID, "lambda must be positive");
+        if (precision != SCMC_PREC_FP64 && precision != SCMC_PREC_MIXED)
+            fail(SCMC_ERR_INVALID, "refocus runs in FP64 or MIXED precision");
+        RefocusGrid G{};
+        G.dim = dim;
+        int64_t N = 1;
+        for (int k = 0; k < 3; ++k) {
+            G.n[k] = k < dim ? pp_colon(box_min[k], box_stp[k], box_max[k]) : 1;
+            G.bmin[k] = k < dim ? box_min[k] : 0.0;
+            G.stp[k] = k < dim ? box_stp[k] : 0.0;
+            N *= G.n[k];
+        }
+        if (N < 1) fail(SCMC_ERR_INVALID, "empty refocus grid");
+        Ctx &c = context(device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        CK(cudaSetDevice(device));
+        double2 *du = reinterpret_cast<double2 *>(c.out1.ensure(nv * sizeof(double2)));
+        double *dv = reinterpret_cast<double *>(c.dirs_v.ensure(dim * nv * sizeof(double)));
+        double2 *dr = reinterpret_cast<double2 *>(c.out0.ensure(N * sizeof(double2)));
+        CK(cudaMemcpy(du, u, nv * sizeof(double2), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dv, v, dim * nv * sizeof(double), cudaMemcpyHostToDevice));
+        const double kw = 2 * SCMC_PI / lambda;
+        const double l2 = dim == 3 ? l[2] : 0.0;
+        const unsigned grid = (unsigned)((N + 255) / 256);
+        {
+            StageScope sc(ST_CONTRACT, 0);
+            if (precision == SCMC_PREC_MIXED)
+                refocus_kernel<true><<<grid, 256>>>(G, du, dv, nv, l[0], l[1], l2, kw, as_written, dr);
+            else
+                refocus_kernel<false><<<grid, 256>>>(G, du, dv, nv, l[0], l[1], l2, kw, as_written, dr);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        CK(cudaMemcpy(rU, dr, N * sizeof(double2), cudaMemcpyDeviceToHost));
+    });
+}
+
+int scmc_sample_cov(const double *C, int64_t N, int64_t n_samples, uint64_t seed, int32_t device, double *Z)
+{
+    return guarded([&] {
+        if (!C || !Z || N < 1 || n_samples < 0) fail(SCMC_ERR_INVALID, "invalid sampling arguments");
+        if (N > 32768) fail(SCMC_ERR_INVALID, "covariance too large to factorise (N <= 32768)");
+        if (n_samples == 0) return;
+        Ctx &c = context(device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        CK(cudaSetDevice(device));
+        const int64_t n = 2 * N;
+        double2 *dC = reinterpret_cast<double2 *>(c.acc_m.ensure(N * N * sizeof(double2)));
+        double *S = reinterpret_cast<double *>(c.acc_s.ensure(n * n * sizeof(double)));
+        double *g = reinterpret_cast<double *>(c.rows.ensure(n * n_samples * sizeof(double)));
+        double2 *dZ = reinterpret_cast<double2 *>(c.out0.ensure(N * n_samples * sizeof(double2)));
+        int *err = reinterpret_cast<int *>(c.err.ensure(sizeof(int)));
+        CK(cudaMemcpy(dC, C, N * N * sizeof(double2), cudaMemcpyHostToDevice));
+        CK(cudaMemset(err, 0, sizeof(int)));
+        const int sms = sm_count(device);
+        sigma_build_kernel<<<sms * 8, 256>>>(dC, N, S);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        {
+            StageScope sc(ST_CONTRACT, 0);
+            for (int64_t k0 = 0; k0 < n; k0 += kCholNB) {
+                const int nb = (int)std::min<int64_t>(kCholNB, n - k0);
+                chol_diag_kernel<<<1, 256>>>(S, n, k0, nb, err);
+                LAUNCHED();
+                const int64_t rest = n - k0 - nb;
+                if (rest <= 0) break;
+                chol_panel_kernel<<<(unsigned)((rest + 127) / 128), 128>>>(S, n, k0, nb);
+                LAUNCHED();
+                const int64_t nt = (rest + kCholNB - 1) / kCholNB;
+                chol_update_kernel<<<(unsigned)(nt * (nt + 1) / 2), 256>>>(S, n, k0, nb);
+                LAUNCHED();
+            }
+            CK(cudaGetLastError());
+        }
+        int herr = 0;
+        CK(cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) fail(SCMC_ERR_INVALID, "Sigma is not positive definite (a covariance of too few paths is singular)");
+        normals_kernel<<<sms * 8, 256>>>((uint32_t)seed, (uint32_t)(seed >> 32), n_samples, n, g);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        sample_product_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((N * n_samples + 255) / 256, sms * 32)),
+                                256>>>(S, N, n_samples, g, dZ);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        CK(cudaMemcpy(Z, dZ, N * n_samples * sizeof(double2), cudaMemcpyDeviceToHost));
     });
 }
 

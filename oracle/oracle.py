@@ -61,6 +61,10 @@ def lib():
         _lib.oracle_field_hetero.argtypes = [C.POINTER(HeteroArgs), C.POINTER(RngSpec), dp]
         _lib.oracle_field_fourier_quad.argtypes = [C.POINTER(FqArgs), C.POINTER(RngSpec), dp]
         _lib.oracle_field_fourier_quad_onwave.argtypes = [C.POINTER(FqArgs), dp, C.c_int32, C.POINTER(RngSpec), dp]
+        _lib.oracle_refocus_grid.argtypes = [C.c_int32, dp, dp, dp, lp]
+        _lib.oracle_refocus_grid.restype = C.c_int64
+        _lib.oracle_refocus.argtypes = [dp, dp, C.c_int64, C.c_int32, dp, dp, dp, dp, C.c_double, C.c_int32, dp]
+        _lib.oracle_sample_cov.argtypes = [dp, C.c_int64, C.c_int64, dp, dp]
         _lib.oracle_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                               C.POINTER(C.c_uint32)]
         _lib.oracle_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
@@ -246,3 +250,32 @@ def field_hetero(h, rng: Rng) -> np.ndarray:
     u = np.zeros(2 * h.nv * h.nl)
     _check(lib().oracle_field_hetero(C.byref(h.args), C.byref(rng.spec), _dp(u)), "oracle_field_hetero")
     return u.view(np.complex128).reshape(h.nv, h.nl, order="F")
+
+
+def refocus(u, v, l, box_min, box_max, box_stp, lambda_, as_written=True):
+    """refocus.m on the oracle: rU shaped like the reference's ndgrid."""
+    v = np.asarray(v, dtype=np.float64)
+    dim = v.shape[0]
+    f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))  # noqa: E731
+    bmin, bmax, bstp, lv = f(box_min), f(box_max), f(box_stp), f(l)
+    dims = np.zeros(3, dtype=np.int64)
+    n = lib().oracle_refocus_grid(dim, _dp(bmin), _dp(bmax), _dp(bstp), dims.ctypes.data_as(C.POINTER(C.c_int64)))
+    uc = np.ascontiguousarray(np.asarray(u, dtype=np.complex128).reshape(-1))
+    vc = np.ascontiguousarray(v.T)
+    out = np.zeros(2 * n)
+    _check(lib().oracle_refocus(_dp(uc.view(np.float64)), _dp(vc), v.shape[1], dim, _dp(lv), _dp(bmin), _dp(bmax),
+                                _dp(bstp), float(lambda_), int(bool(as_written)), _dp(out)), "oracle_refocus")
+    return out.view(np.complex128).reshape(tuple(dims[:dim]), order="F")
+
+
+def sample_cov(C_mat, normals):
+    """samplingFromCovMatrix.m:47-64 on the oracle: one complex N-vector per row of normals (2N each)."""
+    Cm = np.ascontiguousarray(np.asarray(C_mat, dtype=np.complex128).reshape(-1, order="F"))
+    N = int(round(np.sqrt(Cm.size)))
+    g = np.ascontiguousarray(np.asarray(normals, dtype=np.float64).reshape(-1, 2 * N))
+    Z = np.zeros(2 * N * g.shape[0])
+    rc = lib().oracle_sample_cov(_dp(Cm.view(np.float64)), N, g.shape[0], _dp(g), _dp(Z))
+    if rc == -1:
+        raise ValueError("Sigma is not positive definite")
+    _check(rc, "oracle_sample_cov")
+    return Z.view(np.complex128).reshape(N, g.shape[0], order="F")

@@ -73,6 +73,18 @@ int oracle_cov_hetero(const scmc_hetero_args *a, oracle_rng_spec *rs, double *Ms
                       int threads);
 int oracle_field_hetero(const scmc_hetero_args *a, oracle_rng_spec *rs, double *u);
 
+/* refocus.m:1-34: rU (2*N doubles, N grid points, x fastest).  v: dim x nv
+ * column-major directions, l: dim, u: 2*nv doubles.  as_written = 1 leaves
+ * the first grid point at 0, as the reference's chunk indices do. */
+int64_t oracle_refocus_grid(int32_t dim, const double *box_min, const double *box_max, const double *box_stp,
+                            int64_t *dims);
+int oracle_refocus(const double *u, const double *v, int64_t nv, int32_t dim, const double *l,
+                   const double *box_min, const double *box_max, const double *box_stp, double lambda,
+                   int32_t as_written, double *rU);
+/* samplingFromCovMatrix.m:47-64: Z (2*N*n_samples doubles) from C (2*N*N
+ * doubles) and normals (2N per sample).  -1 if Sigma is not positive definite. */
+int oracle_sample_cov(const double *C, int64_t N, int64_t n_samples, const double *normals, double *Z);
+
 /* Philox-4x32-10 (Salmon et al., SC'11): one block. */
 void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* The per-path streams (tag 0 uniform, tag 1 normal) of the walk. */

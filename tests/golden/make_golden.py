@@ -237,6 +237,18 @@ class Gen:
                 "cbs": bool(cbs), "smp_flg": smp_flg, "vsign": vsign, "has_lmean0": lmean0 is not None}
         self.save(name, "fq_onwave", meta, arrays)
 
+    # -- refocus ---------------------------------------------------------------
+    def refocus_case(self, name, *, u, v, l, box_min, box_max, box_stp, lam):
+        it, _, _ = self.interp(0)
+        rU = it.call("refocus", [M(np.asarray(u, complex).reshape(-1, 1)), M(np.asarray(v, float)),
+                                 M(np.asarray(l, float).reshape(-1, 1)), M(np.reshape(box_min, (-1, 1)).astype(float)),
+                                 M(np.reshape(box_max, (-1, 1)).astype(float)),
+                                 M(np.reshape(box_stp, (-1, 1)).astype(float)), M(float(lam))], 1)[0]
+        arrays = {"u": np.asarray(u, complex).reshape(-1), "v": np.asarray(v, float), "l": np.asarray(l, float),
+                  "box_min": np.asarray(box_min, float), "box_max": np.asarray(box_max, float),
+                  "box_stp": np.asarray(box_stp, float), "rU": np.asarray(rU, dtype=complex)}
+        self.save(name, "refocus", {"lambda": lam}, arrays)
+
     # -- MCCovHetro / MCsampleHetro ----------------------------------------------
     def hetero_case(self, name, func, seed, *, sigt, albedo, box_min, box_max, box_bin, l, v, is_ff_l, is_ff_v,
                     max_itr, lam, cbs, smp_flg, sct_type, ampfunc, ampfunc0=None, extra=None):
@@ -290,6 +302,18 @@ class Gen:
             msg = str(e)
         assert msg is not None, name
         self.save(name, "error", {"func": func, "error": msg}, {"dummy": np.zeros(1)})
+
+
+def refocus_cases(g):
+    print("refocus")
+    r = np.random.default_rng(29)
+    v3 = cap_dirs(7, 12, -1, 31)
+    u3 = r.normal(size=7) + 1j * r.normal(size=7)
+    g.refocus_case("refocus_3d", u=u3, v=v3, l=[0.0, 0.1, 1.0], box_min=[-3, -2, 0], box_max=[3, 2, 1.5],
+                   box_stp=[0.5, 0.4, 0.3], lam=1.0)
+    v2 = np.vstack([np.sin([3.0, 3.1, 3.3]), np.cos([3.0, 3.1, 3.3])])
+    g.refocus_case("refocus_2d", u=r.normal(size=3) + 1j * r.normal(size=3), v=v2, l=[0.05, 1.0],
+                   box_min=[-5, 0], box_max=[5, 4], box_stp=[0.25, 0.5], lam=0.8)
 
 
 def fq_onwave_cases(g):
@@ -385,6 +409,7 @@ def main(ref):
               v_max=0.195, v_stp=0.01, max_itr=5, lam=1.0, cbs=1, smp_flg=2, lmean0=None, vsign=-1)
 
     fq_onwave_cases(g)
+    refocus_cases(g)
 
     print("hetero")
     g2 = np.random.default_rng(7)
@@ -476,6 +501,14 @@ if __name__ == "__main__":
     ref = args[0] if args else "/root/reference"
     if "--only-onwave" in sys.argv:
         only_onwave(ref)
+    elif "--only-refocus" in sys.argv:
+        g = Gen(ref)
+        with open(os.path.join(HERE, "index.json")) as f:
+            g.index = [e for e in json.load(f) if e["kind"] != "refocus"]
+        refocus_cases(g)
+        with open(os.path.join(HERE, "index.json"), "w") as f:
+            json.dump(g.index, f, indent=1)
+        print(f"{len(g.index)} fixtures")
     elif "--only-fq-onwave" in sys.argv:
         g = Gen(ref)
         with open(os.path.join(HERE, "index.json")) as f:

@@ -314,3 +314,32 @@ def test_fourier_quad_onwave_linear_in_weights(oracle_lib):
         e[j] = 1.0
         parts = parts + W[j] * oracle_lib.field_fourier_quad_onwave(h.args, e, oracle_lib.Rng.philox(), h.nv0)
     assert relerr(u, parts) < 1e-10
+
+
+REFOCUS_CASES = [e["name"] for e in INDEX if e["kind"] == "refocus"]
+
+
+@pytest.mark.parametrize("name", REFOCUS_CASES)
+def test_refocus_oracle_matches_reference(oracle_lib, name):
+    """refocus.m run by the reference interpreter (first grid point left at 0
+    by its chunk indices) vs the oracle."""
+    meta, arr = load(name)
+    rU = oracle_lib.refocus(arr["u"], arr["v"], arr["l"], arr["box_min"], arr["box_max"], arr["box_stp"],
+                            meta["lambda"], as_written=True)
+    assert rU.shape == arr["rU"].shape
+    assert relerr(rU, arr["rU"]) < RTOL
+    assert arr["rU"].reshape(-1, order="F")[0] == 0
+
+
+def test_sample_cov_oracle_against_numpy(oracle_lib):
+    """samplingFromCovMatrix.m:47-64 with an independent Cholesky."""
+    g = np.random.default_rng(1)
+    N = 12
+    A = g.normal(size=(N, 3 * N)) + 1j * g.normal(size=(N, 3 * N))
+    C = A @ A.conj().T / (3 * N)
+    Sig = 0.5 * np.block([[C.real, -C.imag], [C.imag, C.real]])
+    R = np.linalg.cholesky(Sig).T
+    nm = g.normal(size=(4, 2 * N))
+    s = nm @ R
+    Z = oracle_lib.sample_cov(C, nm)
+    assert relerr(Z, (s[:, :N] + 1j * s[:, N:]).T) < 1e-12
