@@ -230,6 +230,16 @@ int scmc_export_records(const scmc_mc_args *args, int32_t want_phase, int64_t ca
                         double *x, double *ow, double *x1, double *w1, double *wpx,
                         double *xi, int32_t *plen, int64_t *path, int64_t *n_events);
 
+/* The field (MCfield.m:207-254 accumulation and normalisation) of n stored
+ * records in the layout above, on the GPU: records exported on one machine
+ * (and kept in the on-disk record format of mcspeckle_b200.formats) replay
+ * on another.  args supplies the lights, views, medium and normalisation
+ * (norm_itr, else max_itr); its walk-only fields are not used.  No
+ * counterpart in the reference (it never stores its paths). */
+int scmc_field_from_records(const scmc_mc_args *args, int64_t n, const double *x, const double *ow,
+                            const double *x1, const double *w1, const double *wpx, const double *xi,
+                            const int32_t *plen, const int64_t *path, double *u);
+
 /* Philox-4x32-10 uniform / normal streams of one path, as used by the walk:
  * n values of stream `tag` (0 uniform, 1 normal) of path `path` under `seed`.
  * Host memory.  Exposed so the random streams can be checked bit for bit. */

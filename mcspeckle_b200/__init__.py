@@ -10,11 +10,12 @@ from .interface import (HGScatter, boxArea, farFieldSource, invCDF, isotropicSca
 from .fourier_quad import MCfieldFourierQuad, MCfieldFourierQuadOnWave, fq_args
 from .hetero import MCCovHetro, MCsampleHetro, hetero_args
 from .mc import MCcov, MCfield, MCfieldOnWave, MatlabStyleError, export_records, mc_args, philox_stream, rng
+from .formats import load_amplitude_table, load_records, replay_field, save_records
 from .postprocess import refocus, sample_from_cov, united_cov
 from .scmc_api import ScmcInputError, scmc
 
 __all__ = [
-    "scmc", "refocus", "sample_from_cov", "united_cov", "MCfield", "MCcov", "MCfieldOnWave", "MCfieldFourierQuad", "MCfieldFourierQuadOnWave", "fq_args", "MCCovHetro", "MCsampleHetro", "hetero_args", "rng", "mc_args", "export_records", "philox_stream",
+    "scmc", "load_amplitude_table", "load_records", "replay_field", "save_records", "refocus", "sample_from_cov", "united_cov", "MCfield", "MCcov", "MCfieldOnWave", "MCfieldFourierQuad", "MCfieldFourierQuadOnWave", "fq_args", "MCCovHetro", "MCsampleHetro", "hetero_args", "rng", "mc_args", "export_records", "philox_stream",
     "boxArea", "farFieldSource", "nearFieldSource", "isotropicScatter", "HGScatter",
     "tabulatedAmplitudeScatter", "invCDF", "ScmcError", "ScmcInputError", "MatlabStyleError", "launch_count",
 ]

@@ -61,6 +61,7 @@ def lib():
         L.scmc_cov_device.argtypes = [mp, C.c_void_p, C.c_void_p, C.c_void_p]
         L.scmc_export_records.argtypes = [mp, C.c_int32, C.c_int64, dp, dp, dp, dp, dp, dp, ip, lp, lp]
         L.scmc_philox_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, dp]
+        L.scmc_field_from_records.argtypes = [mp, C.c_int64, dp, dp, dp, dp, dp, dp, ip, lp, dp]
         fq = C.POINTER(_abi.FqArgs)
         L.scmc_fq_grid_size.argtypes = [C.c_double, C.c_double, C.POINTER(C.c_int64)]
         L.scmc_field_fourier_quad.argtypes = [fq, dp]
@@ -90,7 +91,7 @@ def lib():
                      "scmc_fq_grid_size", "scmc_field_fourier_quad", "scmc_field_fourier_quad_device",
                      "scmc_field_noalloc", "scmc_cov_hetero", "scmc_field_hetero", "scmc_cov_hetero_device",
                      "scmc_field_hetero_device", "scmc_field_onwave", "scmc_field_onwave_device", "scmc_field_fourier_quad_onwave",
-                     "scmc_field_fourier_quad_onwave_device", "scmc_refocus_grid", "scmc_refocus", "scmc_sample_cov", "scmc_server_create",
+                     "scmc_field_fourier_quad_onwave_device", "scmc_refocus_grid", "scmc_refocus", "scmc_sample_cov", "scmc_field_from_records", "scmc_server_create",
                      "scmc_server_submit", "scmc_server_wait", "scmc_server_stats_read", "scmc_server_destroy"):
             getattr(L, name).restype = C.c_int
         _lib = L

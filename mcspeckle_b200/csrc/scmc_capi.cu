@@ -1892,6 +1892,128 @@ int scmc_philox_stream(uint64_t seed, uint64_t path, int32_t tag, int64_t n, dou
 }
 
 // ---------------------------------------------------------------------------
+// field from stored path records (replay on any machine)
+// ---------------------------------------------------------------------------
+int scmc_field_from_records(const scmc_mc_args *args, int64_t n, const double *x, const double *ow, const double *x1,
+                            const double *w1, const double *wpx, const double *xi, const int32_t *plen,
+                            const int64_t *path, double *u)
+{
+    return guarded([&] {
+        validate(args);
+        if (n < 0 || (n > 0 && (!x || !ow || !x1 || !w1 || !wpx || !xi || !plen || !path)) || !u)
+            fail(SCMC_ERR_INVALID, "invalid records");
+        // singles (pL == 1) index the paths; multis point at their path's single
+        std::unordered_map<int64_t, int32_t> first;
+        int64_t ns = 0, nm = 0;
+        for (int64_t e = 0; e < n; ++e) {
+            if (plen[e] == 1) {
+                if (!first.emplace(path[e], (int32_t)ns).second) fail(SCMC_ERR_INVALID, "a path has two first events");
+                ++ns;
+            } else if (plen[e] > 1) {
+                ++nm;
+            } else {
+                fail(SCMC_ERR_INVALID, "event with pL < 1");
+            }
+        }
+        if (ns > INT32_MAX) fail(SCMC_ERR_INVALID, "too many paths in one record set");
+        std::vector<double> sx1(3 * ns), sw1(3 * ns), swpx(ns), sxi(ns);
+        std::vector<int32_t> snev(ns, 1);
+        std::vector<double> mx(3 * std::max<int64_t>(nm, 1)), mow(3 * std::max<int64_t>(nm, 1)), mwpx(nm), mxi(nm);
+        std::vector<int32_t> mpath(nm), mplen(nm);
+        int64_t is = 0, im = 0;
+        for (int64_t e = 0; e < n; ++e) {
+            if (plen[e] == 1) {
+                for (int d = 0; d < 3; ++d) {
+                    sx1[d * ns + is] = x1[3 * e + d];
+                    sw1[d * ns + is] = w1[3 * e + d];
+                }
+                swpx[is] = wpx[e];
+                sxi[is] = xi[e];
+                ++is;
+            } else {
+                auto it = first.find(path[e]);
+                if (it == first.end()) fail(SCMC_ERR_INVALID, "a record's path has no first event");
+                for (int d = 0; d < 3; ++d) {
+                    mx[d * nm + im] = x[3 * e + d];
+                    mow[d * nm + im] = ow[3 * e + d];
+                }
+                mwpx[im] = wpx[e];
+                mxi[im] = xi[e];
+                mpath[im] = it->second;
+                mplen[im] = plen[e];
+                ++snev[it->second];
+                ++im;
+            }
+        }
+        Ctx &c = context(args->device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        CK(cudaSetDevice(args->device));
+        cudaStream_t st = 0;
+        Prepared P = prepare(c, args, 1, st);
+        const int64_t scap = std::max<int64_t>(ns, 1), mcap = std::max<int64_t>(nm, 1);
+        auto up = [&](DevBuf &b, const void *h, size_t bytes, size_t cap_bytes) {
+            b.ensure(cap_bytes);
+            if (bytes) CK(cudaMemcpy(b.p, h, bytes, cudaMemcpyHostToDevice));
+        };
+        up(c.s_x1, sx1.data(), 3 * ns * 8, 3 * scap * 8);
+        up(c.s_w1, sw1.data(), 3 * ns * 8, 3 * scap * 8);
+        up(c.s_wpx, swpx.data(), ns * 8, scap * 8);
+        up(c.s_xi, sxi.data(), ns * 8, scap * 8);
+        up(c.s_nev, snev.data(), ns * 4, scap * 4);
+        up(c.m_x, mx.data(), 3 * nm * 8, 3 * mcap * 8);
+        up(c.m_ow, mow.data(), 3 * nm * 8, 3 * mcap * 8);
+        up(c.m_wpx, mwpx.data(), nm * 8, mcap * 8);
+        up(c.m_xi, mxi.data(), nm * 8, mcap * 8);
+        up(c.m_path, mpath.data(), nm * 4, mcap * 4);
+        up(c.m_plen, mplen.data(), nm * 4, mcap * 4);
+        // strides of the uploaded layout; the walk re-sizes these if it needs more
+        c.scap = ns;
+        c.mcap = nm;
+        Batch B;
+        B.S = SingleRec{c.s_x1.as<double>(), c.s_w1.as<double>(), c.s_wpx.as<double>(), c.s_xi.as<double>(),
+                        c.s_nev.as<int32_t>()};
+        B.M = MultiRec{c.m_x.as<double>(), c.m_ow.as<double>(), c.m_wpx.as<double>(), c.m_xi.as<double>(),
+                       c.m_path.as<int32_t>(), c.m_plen.as<int32_t>()};
+        B.n_paths = ns;
+        B.n_multi = nm;
+        const int64_t nq = args->nv * args->nl;
+        double2 *d = reinterpret_cast<double2 *>(c.out0.ensure(nq * sizeof(double2)));
+        auto run = [&](auto dimc, auto polc, auto acc) {
+            constexpr int DIM = decltype(dimc)::value;
+            constexpr int POL = decltype(polc)::value;
+            using AccT = decltype(acc);
+            AccT *Us = reinterpret_cast<AccT *>(c.acc_s.ensure(2 * nq * sizeof(AccT)));
+            AccT *Um = reinterpret_cast<AccT *>(c.acc_m.ensure(2 * nq * sizeof(AccT)));
+            CK(cudaMemsetAsync(Us, 0, 2 * nq * sizeof(AccT), st));
+            CK(cudaMemsetAsync(Um, 0, 2 * nq * sizeof(AccT), st));
+            launch_field_accum<DIM, POL, true, AccT>(c, P, B, Us, ns, st);
+            launch_field_accum<DIM, POL, false, AccT>(c, P, B, Um, nm, st);
+            const double m = (double)(args->norm_itr > 0 ? args->norm_itr : args->max_itr);
+            const double norm = m > 0 ? std::sqrt(1.0 / m * P.volume * args->sigt) : 0.0;  // MCfield.m:253-254
+            field_finalize_kernel<DIM, AccT><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((nq + 255) / 256, 1024)),
+                                               256, 0, st>>>(P.Q, Us, Um, norm, d);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        };
+        using I3 = std::integral_constant<int, 3>;
+        using I2 = std::integral_constant<int, 2>;
+        using F64 = std::integral_constant<int, P64>;
+        using FMX = std::integral_constant<int, PMIX>;
+        using F32 = std::integral_constant<int, P32>;
+        if (args->dim == 3) {
+            if (args->precision == SCMC_PREC_FP64) run(I3{}, F64{}, double{});
+            else if (args->precision == SCMC_PREC_FP32) run(I3{}, F32{}, float{});
+            else run(I3{}, FMX{}, double{});
+        } else {
+            if (args->precision == SCMC_PREC_FP64) run(I2{}, F64{}, double{});
+            else if (args->precision == SCMC_PREC_FP32) run(I2{}, F32{}, float{});
+            else run(I2{}, FMX{}, double{});
+        }
+        CK(cudaMemcpy(u, d, nq * sizeof(double2), cudaMemcpyDeviceToHost));
+    });
+}
+
+// ---------------------------------------------------------------------------
 // post-processing: refocus, samples from a covariance
 // ---------------------------------------------------------------------------
 static int64_t pp_colon(double a, double st, double b)
