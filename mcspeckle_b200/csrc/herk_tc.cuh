@@ -322,30 +322,36 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
 }
 
 // ---------------------------------------------------------------------------
-// The same product on a CTA pair (cluster of 2, tcgen05 cta_group::2).
+// The covariance product on a CTA pair (cluster of 2, tcgen05 cta_group::2),
+// from split-complex ("planar") operands.
 //
-// A pair owns a 256 x 256 tile of D: CTA r loads its 128 rows of A and half
-// of the 256 B rows (B rows col0 + 128 r ..) into its own shared memory, and
-// the leader (rank 0) issues one M=256 N=256 K=16 MMA that reads both CTAs'
-// tiles; CTA r's TMEM holds D rows 128 r .. 128 r + 127.  Per SM and K block
-// that is 32 KB of TMA traffic (48 KB hi+lo) instead of 48 KB (64 KB) for the
-// single-CTA kernel at the same MMA work.  The loads are plain (no multicast);
-// their completion is counted on the leader's barrier.  The leader's MMA
-// commits arrive on both CTAs' barriers (commit multicast).  Every wait is
-// bounded as in herk_tc_kernel.
+// The rows are stored as two planes, Re T and Im T (N rows x K events each,
+// FP16, plus the low parts for hi+lo), half the bytes of the real-expanded
+// layout.  For complex rows i and columns j
+//     Re C_ij = Re t_i . Re t_j + Im t_i . Im t_j
+//     Im C_ij = Im t_i . Re t_j - Re t_i . Im t_j
+// so a pair that owns 256 complex rows x 256 complex columns keeps two
+// accumulators in TMEM (columns 0-255: Re C, 256-511: Im C) and issues four
+// M=256 N=256 K=16 MMAs per 16 events from four tiles of shared memory; the
+// minus sign is the MMA's negate-A bit.  CTA r loads the 128 A rows
+// crow0 + 128 r of both planes and B rows col0 + 128 r of both planes: 64 KB
+// per stage (96 KB hi+lo) for 4 x 128 x 256 x 64 multiply-adds per SM, twice
+// the work per loaded byte of a real-expanded tile.  The loads are plain (no
+// multicast); their completion is counted on the leader's barrier.  The
+// leader's MMA commits arrive on both CTAs' barriers (commit multicast).
+// Every wait is bounded as in herk_tc_kernel.
 // ---------------------------------------------------------------------------
 #ifndef SCMC_PAIR_STAGES_FP16
-#define SCMC_PAIR_STAGES_FP16 4
+#define SCMC_PAIR_STAGES_FP16 3
 #endif
+constexpr int TC2_TMEM_COLS = 512;  // Re C and Im C, 256 columns each
 template <bool SPLIT> struct Tc2Cfg {
-    static constexpr int A_BYTES = 128 * TC_BK * 2;   // this CTA's 128 rows of A
-    static constexpr int B_BYTES = 128 * TC_BK * 2;   // this CTA's half of B
-    static constexpr int STAGE_BYTES = (SPLIT ? 2 : 1) * A_BYTES + B_BYTES;
-    // 129 KB (FP16) / 145 KB (hi+lo) of ring, so a row-generation CTA of the
-    // next chunk (about 72 KB at 64 x 64) fits on the same SM beside it.
-    static constexpr int STAGES = SPLIT ? 3 : SCMC_PAIR_STAGES_FP16;
+    static constexpr int TILE = 128 * TC_BK * 2;  // 128 rows x 64 events of one plane
+    static constexpr int NA = SPLIT ? 4 : 2;      // A tiles: Re, Im (hi), Re, Im (lo)
+    static constexpr int STAGE_BYTES = (NA + 2) * TILE;
+    static constexpr int STAGES = SPLIT ? 2 : SCMC_PAIR_STAGES_FP16;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-    static constexpr int B_OFF = (SPLIT ? 2 : 1) * A_BYTES;
+    static constexpr int B_OFF = NA * TILE;  // then Re B, Im B
 };
 
 __device__ __forceinline__ uint32_t cluster_ctarank()
@@ -411,9 +417,10 @@ __device__ __forceinline__ void umma_commit_pair(uint64_t *bar)
 
 template <bool SPLIT>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
-herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
-                const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int kb_per_split,
-                int Mr, int N, double *__restrict__ D, int *__restrict__ err)
+herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant__ CUtensorMap tm_im,
+                const __grid_constant__ CUtensorMap tm_re_lo, const __grid_constant__ CUtensorMap tm_im_lo,
+                const int2 *__restrict__ tiles, int num_kb, int kb_per_split, int N, double *__restrict__ D,
+                int *__restrict__ err)
 {
     using Cfg = Tc2Cfg<SPLIT>;
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
@@ -432,10 +439,11 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
     const int kb0 = (int)blockIdx.y * kb_per_split;
     const int nkb = min(num_kb, kb0 + kb_per_split) - kb0;
     if (nkb <= 0) return;
+    const int Mr = 2 * N;
     D += (int64_t)blockIdx.y * Mr * N;
     const int2 tile = tiles[blockIdx.x >> 1];
-    const int arow0 = tile.x * 256 + (int)rank * 128;  // this CTA's A rows = its D rows
-    const int col0 = tile.y * 256;                     // the pair's D columns
+    const int crow0 = tile.x * 256 + (int)rank * 128;  // this CTA's complex rows
+    const int col0 = tile.y * 256;                     // the pair's complex columns
     const int brow0 = col0 + (int)rank * 128;          // this CTA's B rows
 
     if (threadIdx.x == 0) {
@@ -450,7 +458,7 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TC_TMEM_COLS)
+                     "r"(TC2_TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
     }
@@ -473,14 +481,21 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
             if (rank == 0) mbar_expect_tx(&full[s], 2 * Cfg::STAGE_BYTES);
             const uint32_t fb = full0 + (uint32_t)(s * sizeof(uint64_t));
             const int kx = (kb0 + kb) * TC_BK;
-            tma_load_2d_pair(st, &tm_ahi, kx, arow0, fb);
-            if (SPLIT) tma_load_2d_pair(st + Cfg::A_BYTES, &tm_alo, kx, arow0, fb);
-            tma_load_2d_pair(st + Cfg::B_OFF, &tm_b, kx, brow0, fb);
+            tma_load_2d_pair(st, &tm_re, kx, crow0, fb);
+            tma_load_2d_pair(st + Cfg::TILE, &tm_im, kx, crow0, fb);
+            if (SPLIT) {
+                tma_load_2d_pair(st + 2 * Cfg::TILE, &tm_re_lo, kx, crow0, fb);
+                tma_load_2d_pair(st + 3 * Cfg::TILE, &tm_im_lo, kx, crow0, fb);
+            }
+            tma_load_2d_pair(st + Cfg::B_OFF, &tm_re, kx, brow0, fb);
+            tma_load_2d_pair(st + Cfg::B_OFF + Cfg::TILE, &tm_im, kx, brow0, fb);
             *(volatile int *)issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0 && rank == 0) {
         // MMA issuer (leader only)
         constexpr uint32_t idesc = umma_idesc_f16(256, 256);
+        constexpr uint32_t idesc_neg = idesc | (1u << 13);  // negate A
+        const uint32_t t_re = tmem, t_im = tmem + 256;
         for (int kb = 0; kb < nkb; ++kb) {
             const int s = kb % Cfg::STAGES;
             if (!mbar_wait(&full[s], (kb / Cfg::STAGES) & 1)) {
@@ -489,14 +504,24 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
             }
             tc_fence_after();
             uint8_t *st = base + s * Cfg::STAGE_BYTES;
-            const uint64_t dh = umma_desc_sw128(st);
-            const uint64_t dl = umma_desc_sw128(st + Cfg::A_BYTES);
-            const uint64_t db = umma_desc_sw128(st + Cfg::B_OFF);
+            const uint64_t ar = umma_desc_sw128(st), ai = umma_desc_sw128(st + Cfg::TILE);
+            const uint64_t br = umma_desc_sw128(st + Cfg::B_OFF), bi = umma_desc_sw128(st + Cfg::B_OFF + Cfg::TILE);
 #pragma unroll
             for (int kk = 0; kk < TC_BK / 16; ++kk) {
                 const uint64_t adv = (uint64_t)(kk * 32) >> 4;
-                umma_f16_pair(tmem, dh + adv, db + adv, idesc, (kb | kk) != 0);
-                if (SPLIT) umma_f16_pair(tmem, dl + adv, db + adv, idesc, 1u);
+                const uint32_t first = (kb | kk) != 0;
+                umma_f16_pair(t_re, ar + adv, br + adv, idesc, first);
+                umma_f16_pair(t_im, ai + adv, br + adv, idesc, first);
+                umma_f16_pair(t_re, ai + adv, bi + adv, idesc, 1u);
+                umma_f16_pair(t_im, ar + adv, bi + adv, idesc_neg, 1u);
+                if (SPLIT) {
+                    const uint64_t lr = umma_desc_sw128(st + 2 * Cfg::TILE) + adv;
+                    const uint64_t li = umma_desc_sw128(st + 3 * Cfg::TILE) + adv;
+                    umma_f16_pair(t_re, lr, br + adv, idesc, 1u);
+                    umma_f16_pair(t_im, li, br + adv, idesc, 1u);
+                    umma_f16_pair(t_re, li, bi + adv, idesc, 1u);
+                    umma_f16_pair(t_im, lr, bi + adv, idesc_neg, 1u);
+                }
             }
             umma_commit_pair(&empty[s]);
         }
@@ -509,21 +534,24 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
     __syncthreads();
     const bool failed = !ok || *(volatile int *)abort_flag;
     if (!failed) {
-        // Epilogue: this CTA's 128 rows x 256 columns, TMEM -> smem transpose -> FP64 RMW.
+        // Epilogue: TMEM lane L = complex row crow0 + L; columns 0-255 -> D row
+        // 2 (crow0 + L) (Re), 256-511 -> row 2 (crow0 + L) + 1 (Im); smem
+        // transpose -> coalesced FP64 read-modify-write.
         float *ep = reinterpret_cast<float *>(base) + warp * 32 * 33;
         const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int c0 = 0; c0 < 256; c0 += 32) {
+        for (int c0 = 0; c0 < 512; c0 += 32) {
             uint32_t r[32];
             tmem_ld32(tbase + c0, r);
 #pragma unroll
             for (int j = 0; j < 32; ++j) ep[lane * 33 + j] = __uint_as_float(r[j]);
             __syncwarp();
-            const int n = col0 + c0 + lane;
+            const int part = c0 >> 8;
+            const int n = col0 + (c0 & 255) + lane;
 #pragma unroll 4
             for (int rr = 0; rr < 32; ++rr) {
-                const int R = arow0 + warp * 32 + rr;
-                if (R < Mr && n < N) {
-                    double *p = D + (int64_t)R * N + n;
+                const int i = crow0 + warp * 32 + rr;
+                if (i < N && n < N) {
+                    double *p = D + (int64_t)(2 * i + part) * N + n;
                     *p += (double)ep[rr * 33 + lane];
                 }
             }
@@ -535,7 +563,8 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
     cluster_sync_all();
     if (threadIdx.x == 0) {
         // After a failure anywhere in the pair, the leader waits (bounded) for
-        // every copy still in flight from either CTA before the pair exits.
+        // the pair's copies still in flight, which are counted on its
+        // barriers, before the pair exits.
         const int peer_abort = (int)ld_shared_cluster_u32(mapa_shared(smem_u32(abort_flag), rank ^ 1u));
         if (failed || peer_abort) {
             atomicExch(err, 1);
@@ -551,7 +580,7 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
     cluster_sync_all();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC2_TMEM_COLS) : "memory");
     }
 }
 
@@ -559,10 +588,13 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constan
 // Rows of one chunk in the split FP16 K-major layout.  One CTA per group of
 // 32 events; lane = event, so each row write is 32 consecutive half2 (128 B).
 // ---------------------------------------------------------------------------
-template <int DIM, bool SINGLE, bool SPLIT>
+// PLANAR (CTA-pair kernel): Re t_i and Im t_i in separate planes (rows of K
+// events), Ahi / Alo the Re planes and Ihi / Ilo the Im planes.
+template <int DIM, bool SINGLE, bool SPLIT, bool PLANAR>
 __global__ void __launch_bounds__(256)
 tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
-               int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo, const float2 *__restrict__ af_tab)
+               int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo, __half *__restrict__ Ihi,
+               __half *__restrict__ Ilo, const float2 *__restrict__ af_tab)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nv = Q.nv, nl = Q.nl;
@@ -616,8 +648,8 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
     // increments (no integer division per entry).
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float sc = ssc[lane];
-    const int64_t col = 2 * (g0 + lane);
-    const int64_t step = 16 * K;  // 8 views = 16 real rows
+    const int64_t col = (PLANAR ? 1 : 2) * (g0 + lane);
+    const int64_t step = (PLANAR ? 8 : 16) * K;  // 8 views
     const bool cbs = !SINGLE && Q.cbs;
     for (int lj = 0; lj < nl; ++lj) {
         float2 bl = sb[lj * 33 + lane], bl2 = sb2[lj * 33 + lane];
@@ -626,9 +658,10 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
         bl2.x *= sc;
         bl2.y *= sc;
         const int64_t i0 = (int64_t)nv * lj + warp;
-        __half *ph = Ahi + 2 * i0 * K + col;
-        __half *pl = Alo + 2 * i0 * K + col;
-        for (int vi = warp; vi < nv; vi += 8, ph += step, pl += step) {
+        const int64_t o0 = (PLANAR ? 1 : 2) * i0 * K + col;
+        __half *ph = Ahi + o0, *pl = Alo + o0;
+        __half *qh = PLANAR ? Ihi + o0 : nullptr, *ql = PLANAR ? Ilo + o0 : nullptr;
+        for (int vi = warp; vi < nv; vi += 8, ph += step, pl += step, qh += PLANAR ? step : 0, ql += PLANAR ? step : 0) {
             float2 t = cmul(sa[vi * 33 + lane], bl);
             if (SINGLE) {
                 const float2 af =
@@ -640,13 +673,25 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
                 t.y += t2.y;
             }
             const __half hr = __float2half_rn(t.x), hi = __float2half_rn(t.y);
-            *reinterpret_cast<__half2 *>(ph) = __halves2half2(hr, hi);
-            *reinterpret_cast<__half2 *>(ph + K) = __halves2half2(hi, __hneg(hr));
+            __half lr, li;
             if (SPLIT) {
-                const __half lr = __float2half_rn(t.x - __half2float(hr));
-                const __half li = __float2half_rn(t.y - __half2float(hi));
-                *reinterpret_cast<__half2 *>(pl) = __halves2half2(lr, li);
-                *reinterpret_cast<__half2 *>(pl + K) = __halves2half2(li, __hneg(lr));
+                lr = __float2half_rn(t.x - __half2float(hr));
+                li = __float2half_rn(t.y - __half2float(hi));
+            }
+            if (PLANAR) {
+                *ph = hr;
+                *qh = hi;
+                if (SPLIT) {
+                    *pl = lr;
+                    *ql = li;
+                }
+            } else {
+                *reinterpret_cast<__half2 *>(ph) = __halves2half2(hr, hi);
+                *reinterpret_cast<__half2 *>(ph + K) = __halves2half2(hi, __hneg(hr));
+                if (SPLIT) {
+                    *reinterpret_cast<__half2 *>(pl) = __halves2half2(lr, li);
+                    *reinterpret_cast<__half2 *>(pl + K) = __halves2half2(li, __hneg(lr));
+                }
             }
         }
     }
@@ -669,18 +714,22 @@ __global__ void af_table_kernel(NeeParams Q, float2 *__restrict__ tab)
 struct TcPlan {
     int N;
     bool split;
-    bool pair;  // CTA-pair kernel (256 x 256 tiles) instead of single-CTA 128 x 256
+    // CTA-pair kernel on planar operands (256 x 256 complex tiles) instead of
+    // the single-CTA kernel on real-expanded rows (128 real x 256 complex)
+    bool pair;
     int64_t events_per_chunk;
-    int64_t K;
+    int64_t K;  // halves per operand row: 2 x events (real-expanded), events (planar)
     std::vector<int2> tiles;
 };
 
 struct TcOperands {
-    __half *ahi, *alo;
+    __half *ahi, *alo;  // real-expanded rows; planar: the Re planes
+    __half *ihi, *ilo;  // planar: the Im planes
     int2 *tiles;
     int *err;
     float2 *af;
-    CUtensorMap m_ahi, m_alo, m_b, m_b_half;  // m_b_half: 128-row boxes of B for the CTA pair
+    CUtensorMap m_ahi, m_alo, m_b;  // planar: m_ahi / m_alo / m_ihi / m_ilo are 128-row boxes of the planes
+    CUtensorMap m_ihi, m_ilo;
     int n_tiles;
 };
 
@@ -689,15 +738,19 @@ inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30)
     TcPlan p;
     p.N = N;
     p.split = split;
-    // 8N (16N split) bytes of operand per event; keep a chunk's operands near chunk_bytes
-    int64_t e = (int64_t)chunk_bytes / ((split ? 16 : 8) * (int64_t)N);
-    e = std::max<int64_t>(32, std::min<int64_t>(e, 65536));
-    e = (e / 32) * 32;
+    // The pair kernel pays off once its 256 complex rows are mostly real rows.
+    p.pair = N >= 256;
+    // Operand bytes per event: 8N (16N hi+lo) real-expanded, 4N (8N) planar;
+    // keep a chunk's operands near chunk_bytes.  K blocks are 64 halves:
+    // 32 events real-expanded, 64 planar.
+    const int64_t per_event = (p.pair ? 4 : 8) * (split ? 2 : 1) * (int64_t)N;
+    const int64_t eb = p.pair ? 64 : 32;
+    int64_t e = (int64_t)chunk_bytes / per_event;
+    e = std::max<int64_t>(eb, std::min<int64_t>(e, 65536));
+    e = (e / eb) * eb;
     p.events_per_chunk = e;
-    p.K = 2 * e;
-    // The pair kernel pays off once a 256-row tile is mostly real rows.
-    p.pair = 2 * N >= 256;
-    const int bm_rows = p.pair ? 256 : TC_BM;  // real-expanded rows per tile
+    p.K = p.pair ? e : 2 * e;
+    const int bm_rows = p.pair ? 512 : TC_BM;  // real-expanded rows per tile
     const int n_tm = (2 * N + bm_rows - 1) / bm_rows;
     const int n_tn = (N + TC_BN - 1) / TC_BN;
     // Upper-triangle tiles (complex rows bm_rows/2 * tm .. against columns
@@ -714,10 +767,17 @@ inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30)
 
 inline size_t tc_align(size_t x) { return (x + 1023) & ~(size_t)1023; }
 
+// Bytes of one operand part: 2N real-expanded rows, or one N-row plane.
+inline size_t tc_part_bytes(const TcPlan &p)
+{
+    return tc_align((size_t)(p.pair ? 1 : 2) * p.N * p.K * sizeof(__half));
+}
+
+inline int tc_parts(const TcPlan &p) { return (p.split ? 2 : 1) * (p.pair ? 2 : 1); }
+
 inline size_t tc_operand_bytes(const TcPlan &p)
 {
-    size_t a = (size_t)2 * p.N * p.K * sizeof(__half);
-    return (p.split ? 2 : 1) * tc_align(a) + tc_align(p.tiles.size() * sizeof(int2)) + 1024 +
+    return tc_parts(p) * tc_part_bytes(p) + tc_align(p.tiles.size() * sizeof(int2)) + 1024 +
            tc_align((size_t)p.N * sizeof(float2));
 }
 
@@ -753,10 +813,13 @@ inline TcOperands tc_make_operands(const TcPlan &p, void *mem, cudaStream_t st)
 {
     TcOperands o{};
     char *b = reinterpret_cast<char *>(mem);
-    const size_t a = tc_align((size_t)2 * p.N * p.K * sizeof(__half));
-    const size_t na = p.split ? 2 : 1;
+    const size_t a = tc_part_bytes(p);
+    const size_t na = (size_t)tc_parts(p);
+    // parts: Re hi [, Re lo] (real-expanded: A hi [, A lo]), then planar Im hi [, Im lo]
     o.ahi = reinterpret_cast<__half *>(b);
     o.alo = p.split ? reinterpret_cast<__half *>(b + a) : o.ahi;
+    o.ihi = p.pair ? reinterpret_cast<__half *>(b + (p.split ? 2 : 1) * a) : nullptr;
+    o.ilo = p.pair ? (p.split ? reinterpret_cast<__half *>(b + 3 * a) : o.ihi) : nullptr;
     o.tiles = reinterpret_cast<int2 *>(b + na * a);
     o.err = reinterpret_cast<int *>(b + na * a + tc_align(p.tiles.size() * sizeof(int2)));
     o.af = reinterpret_cast<float2 *>(reinterpret_cast<char *>(o.err) + 1024);
@@ -765,10 +828,16 @@ inline TcOperands tc_make_operands(const TcPlan &p, void *mem, cudaStream_t st)
         cudaMemsetAsync(o.err, 0, sizeof(int), st) != cudaSuccess)
         throw std::runtime_error("tcgen05 operand set-up failed");
     const uint64_t K = (uint64_t)p.K;
-    o.m_ahi = tc_map(o.ahi, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
-    o.m_alo = tc_map(o.alo, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
-    o.m_b = tc_map(o.ahi, K, (uint64_t)p.N, 2 * K * 2, TC_BN);
-    o.m_b_half = tc_map(o.ahi, K, (uint64_t)p.N, 2 * K * 2, TC_BN / 2);
+    if (p.pair) {
+        o.m_ahi = tc_map(o.ahi, K, (uint64_t)p.N, K * 2, 128);
+        o.m_alo = tc_map(o.alo, K, (uint64_t)p.N, K * 2, 128);
+        o.m_ihi = tc_map(o.ihi, K, (uint64_t)p.N, K * 2, 128);
+        o.m_ilo = tc_map(o.ilo, K, (uint64_t)p.N, K * 2, 128);
+    } else {
+        o.m_ahi = tc_map(o.ahi, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
+        o.m_alo = tc_map(o.alo, K, 2 * (uint64_t)p.N, K * 2, TC_BM);
+        o.m_b = tc_map(o.ahi, K, (uint64_t)p.N, 2 * K * 2, TC_BN);
+    }
     return o;
 }
 
@@ -778,11 +847,14 @@ inline void tc_rows(const TcPlan &p, const TcOperands &o, const NeeParams &Q, co
 {
     const size_t smem = sizeof(float2) * 33 * 2 * (size_t)(Q.nv + Q.nl) + 32 * sizeof(float) +
                         32 * sizeof(EventView) + 64;
-    auto kern = tc_rows_kernel<DIM, SINGLE, SPLIT>;
+    auto kern = p.pair ? tc_rows_kernel<DIM, SINGLE, SPLIT, true> : tc_rows_kernel<DIM, SINGLE, SPLIT, false>;
     if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         throw std::runtime_error("too many lights/views for the tensor-core row kernel");
-    const int grid = (int)((n + 31) / 32);
-    kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, use_af_table ? o.af : nullptr);
+    // every column of the K blocks the product reads is written (zeros past n)
+    const int64_t eb = p.pair ? 64 : 32;
+    const int grid = (int)((n + eb - 1) / eb * (eb / 32));
+    kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, o.ihi, o.ilo,
+                                  use_af_table ? o.af : nullptr);
 }
 
 // D[ks][Mr][N] += A B^T over num_kb K-blocks, split ksplit ways along K.
@@ -826,12 +898,11 @@ inline void tc_gemm_planes_launch(const CUtensorMap &m_ahi, const CUtensorMap &m
         m_ahi, m_alo, m_b, tiles, 0, 0, Mr, N, nullptr, err, kranges, pe);
 }
 
-// D[ks][Mr][N] += A B^T on CTA pairs: tiles are 256 x 256 (pair rows x columns),
-// m_b_half has 128-row boxes.
+// D[ks][2N][N] += the planar pair product (Re C in even rows, Im C in odd
+// rows) over num_kb blocks of 64 events, split ksplit ways; tiles are 256 x 256
+// complex rows x columns.
 template <bool SPLIT>
-inline void tc_gemm2_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, const CUtensorMap &m_b_half,
-                            const int2 *tiles, int n_tiles, int num_kb, int ksplit, int Mr, int N, double *D, int *err,
-                            cudaStream_t st)
+inline void tc_gemm2_launch(const TcOperands &o, int num_kb, int ksplit, int N, double *D, cudaStream_t st)
 {
     static std::atomic<uint64_t> attr_set{0};
     int dev = 0;
@@ -844,18 +915,20 @@ inline void tc_gemm2_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, 
     }
     const int kb_per = (num_kb + ksplit - 1) / ksplit;
     const int ks = (num_kb + kb_per - 1) / kb_per;
-    herk_tc2_kernel<SPLIT><<<dim3(2u * (unsigned)n_tiles, (unsigned)ks), 128, Tc2Cfg<SPLIT>::SMEM_BYTES, st>>>(
-        m_ahi, m_alo, m_b_half, tiles, num_kb, kb_per, Mr, N, D, err);
+    herk_tc2_kernel<SPLIT><<<dim3(2u * (unsigned)o.n_tiles, (unsigned)ks), 128, Tc2Cfg<SPLIT>::SMEM_BYTES, st>>>(
+        o.m_ahi, o.m_ihi, o.m_alo, o.m_ilo, o.tiles, num_kb, kb_per, N, D, o.err);
 }
 
 template <bool SPLIT>
 inline void tc_herk_launch(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)
 {
-    const int num_kb = (int)((2 * n + TC_BK - 1) / TC_BK);
-    if (p.pair)
-        tc_gemm2_launch<SPLIT>(o.m_ahi, o.m_alo, o.m_b_half, o.tiles, o.n_tiles, num_kb, 1, 2 * p.N, p.N, D, o.err, st);
-    else
+    if (p.pair) {
+        const int num_kb = (int)((n + TC_BK - 1) / TC_BK);  // 64 events per block
+        tc_gemm2_launch<SPLIT>(o, num_kb, 1, p.N, D, st);
+    } else {
+        const int num_kb = (int)((2 * n + TC_BK - 1) / TC_BK);
         tc_gemm_launch<SPLIT>(o.m_ahi, o.m_alo, o.m_b, o.tiles, o.n_tiles, num_kb, 1, 2 * p.N, p.N, D, o.err, st);
+    }
 }
 
 inline void tc_herk(const TcPlan &p, const TcOperands &o, int64_t n, double *D, cudaStream_t st)

@@ -113,7 +113,7 @@ def test_mixed_and_fp32_close_to_fp64(gpu, case):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp16"])
-@pytest.mark.parametrize("nside_v,nside_l", [(4, 4), (8, 4), (5, 3), (8, 8)])
+@pytest.mark.parametrize("nside_v,nside_l", [(4, 4), (8, 4), (5, 3), (6, 5), (8, 8)])
 def test_tensor_core_cov_tiles(gpu, nside_v, nside_l, precision):
     """Mixed (tcgen05) vs FP64 covariance at sizes that exercise several
     tiles, partial tiles and the diagonal tiles of the Hermitian update."""
