@@ -301,14 +301,15 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
                     }
                 }
             } else {
-#pragma unroll 4
-                for (int rr = 0; rr < 32; ++rr) {
-                    const int R = row0 + warp * 32 + rr;
-                    if (R < Mr && n < N) {
-                        double *p = D + (int64_t)R * N + n;
-                        *p += (double)ep[rr * 33 + lane];
-                    }
-                }
+                // all 32 loads of the chunk in flight before the adds and stores
+                double *p = D + (int64_t)(row0 + warp * 32) * N + n;
+                const int rows = min(32, Mr - (row0 + warp * 32));
+                double v[32];
+#pragma unroll
+                for (int rr = 0; rr < 32; ++rr) v[rr] = (rr < rows && n < N) ? p[(int64_t)rr * N] : 0.0;
+#pragma unroll
+                for (int rr = 0; rr < 32; ++rr)
+                    if (rr < rows && n < N) p[(int64_t)rr * N] = v[rr] + (double)ep[rr * 33 + lane];
             }
             __syncwarp();
         }
@@ -547,14 +548,15 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
             __syncwarp();
             const int part = c0 >> 8;
             const int n = col0 + (c0 & 255) + lane;
-#pragma unroll 4
-            for (int rr = 0; rr < 32; ++rr) {
-                const int i = crow0 + warp * 32 + rr;
-                if (i < N && n < N) {
-                    double *p = D + (int64_t)(2 * i + part) * N + n;
-                    *p += (double)ep[rr * 33 + lane];
-                }
-            }
+            // all 32 loads of the chunk in flight before the adds and stores
+            double *p = D + (int64_t)(2 * (crow0 + warp * 32) + part) * N + n;
+            const int rows = min(32, N - (crow0 + warp * 32));
+            double v[32];
+#pragma unroll
+            for (int rr = 0; rr < 32; ++rr) v[rr] = (rr < rows && n < N) ? p[(int64_t)2 * rr * N] : 0.0;
+#pragma unroll
+            for (int rr = 0; rr < 32; ++rr)
+                if (rr < rows && n < N) p[(int64_t)2 * rr * N] = v[rr] + (double)ep[rr * 33 + lane];
             __syncwarp();
         }
     }
