@@ -64,7 +64,7 @@ template <typename A> struct acc_ptr;
 
 template <int DIM, int POL, bool SINGLE, typename AccT>
 __global__ void __launch_bounds__(kFieldThreads)
-field_accum_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_events,
+field_accum_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_events,
                    int tv, int tl, int n_vtiles, int64_t ev_per_cta, AccT *__restrict__ U, int field_phase,
                    int mean_mode = 0)
 {
@@ -174,7 +174,7 @@ field_accum_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t m
 
 // u = norm * (A o Us + Um), A = af(l.v) for far-field singles, else 1.
 template <int DIM, typename AccT>
-__global__ void field_finalize_kernel(NeeParams Q, const AccT *__restrict__ Us, const AccT *__restrict__ Um,
+__global__ void field_finalize_kernel(const __grid_constant__ NeeParams Q, const AccT *__restrict__ Us, const AccT *__restrict__ Um,
                                       double norm, double2 *__restrict__ u)
 {
     int64_t n = (int64_t)Q.nv * Q.nl;
@@ -194,7 +194,7 @@ __global__ void field_finalize_kernel(NeeParams Q, const AccT *__restrict__ Us, 
 // ---------------------------------------------------------------------------
 template <int DIM, int POL, bool SINGLE>
 __global__ void __launch_bounds__(256)
-cov_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e_begin,
+cov_rows_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e_begin,
                 int64_t n_ev, int eb, typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type *__restrict__ T)
 {
     using R = typename std::conditional<POL == P64, double, float>::type;

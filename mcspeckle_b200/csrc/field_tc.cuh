@@ -99,7 +99,7 @@ inline size_t field_tc_rows_smem()
 // lights.  SINGLE is used only for far-field lights and views.
 template <int DIM, bool SINGLE, bool SPLIT>
 __global__ void __launch_bounds__(256)
-field_tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
+field_tc_rows_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
                      int terms, int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo,
                      __half *__restrict__ Bm, int field_phase)
 {
@@ -204,7 +204,7 @@ field_tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t
 // far-field tensor-core sums, multiplied here by af(l.v); ds_slices == 0: the
 // singles are CUDA-core sums in complex layout (index 2(v + nv l)).
 template <int DIM>
-__global__ void field_tc_finalize_kernel(NeeParams Q, const double *__restrict__ Ds, int ds_slices,
+__global__ void field_tc_finalize_kernel(const __grid_constant__ NeeParams Q, const double *__restrict__ Ds, int ds_slices,
                                          const double *__restrict__ Dm, int dm_slices, double norm,
                                          double2 *__restrict__ u)
 {

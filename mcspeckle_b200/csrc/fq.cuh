@@ -108,7 +108,7 @@ __device__ __forceinline__ int fq_plane(const FqParams &F, double z)
 
 // Build the entries of a batch: singles are paths 0..n_paths-1, multis
 // follow.  counts[plane] is incremented for the counting sort.
-__global__ void fq_entries_kernel(FqParams F, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_paths,
+__global__ void fq_entries_kernel(const __grid_constant__ FqParams F, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_paths,
                                   int64_t n_multi, FqEntry *__restrict__ out, int *__restrict__ counts)
 {
     const int64_t nvert = n_paths + n_multi;
@@ -195,7 +195,7 @@ constexpr int kFqEB = 16;
 // One CTA: a 32 x 32 tile of (r1, r2) for light j and plane planes[blockIdx.y].
 template <int POL, typename AccT>
 __global__ void __launch_bounds__(256)
-fq_accum_kernel(FqParams F, const FqEntry *__restrict__ E, const int *__restrict__ offsets,
+fq_accum_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int *__restrict__ offsets,
                 const int *__restrict__ planes, const typename cplx_t<typename std::conditional<POL == P64, double, float>::type>::type *__restrict__ T,
                 const double2 *__restrict__ zexp0, AccT *__restrict__ U)
 {
@@ -288,7 +288,7 @@ fq_accum_kernel(FqParams F, const FqEntry *__restrict__ E, const int *__restrict
 // ---------------------------------------------------------------------------
 template <bool SPLIT>
 __global__ void __launch_bounds__(256)
-fq_tc_rows_kernel(FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk, int light,
+fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk, int light,
                   const float2 *__restrict__ T, int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo,
                   __half *__restrict__ Bm)
 {

@@ -587,28 +587,19 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
 }
 
 // ---------------------------------------------------------------------------
-// Rows of one chunk in the split FP16 K-major layout.  One CTA per group of
-// 32 events; lane = event, so each row write is 32 consecutive half2 (128 B).
+// Rows of one chunk in FP16 K-major layouts, one CTA per group of 32 events:
+// real-expanded rows (single-CTA kernel; lane = event, each row write is 32
+// consecutive half2, 128 B) or planar rows (CTA pair).
 // ---------------------------------------------------------------------------
-// PLANAR (CTA-pair kernel): Re t_i and Im t_i in separate planes (rows of K
-// events), Ahi / Alo the Re planes and Ihi / Ilo the Im planes.
-template <int DIM, bool SINGLE, bool SPLIT, bool PLANAR>
-__global__ void __launch_bounds__(256)
-tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
-               int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo, __half *__restrict__ Ihi,
-               __half *__restrict__ Ilo, const float2 *__restrict__ af_tab)
+// The per-event factors of 32 events (lane = event) in shared memory with row
+// stride `ld` float2: views a (sa) and a0 (sa0, CBS), lights b (sb) and b2
+// (sb2), the event scale sqrt(weight / px) (ssc) and the events (sev).
+template <int DIM, bool SINGLE>
+__device__ __forceinline__ void tc_rows_terms(const NeeParams &Q, const SingleRec &S, int64_t scap, const MultiRec &M,
+                                              int64_t mcap, int64_t e0, int64_t g0, int ne, int ld, float2 *sa,
+                                              float2 *sa0, float2 *sb, float2 *sb2, float *ssc, EventView *sev)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nv = Q.nv, nl = Q.nl;
-    float2 *sa = reinterpret_cast<float2 *>(smem_raw);  // [nv][33]
-    float2 *sa0 = sa + nv * 33;
-    float2 *sb = sa0 + nv * 33;                           // [nl][33]
-    float2 *sb2 = sb + nl * 33;
-    float *ssc = reinterpret_cast<float *>(sb2 + nl * 33);  // [32]
-    EventView *sev = reinterpret_cast<EventView *>(ssc + 32);
-
-    const int64_t g0 = (int64_t)blockIdx.x * 32;
-    const int ne = (int)max((int64_t)0, min((int64_t)32, n_ev - g0));
     if (threadIdx.x < 32) {
         EventView ev;
         if (threadIdx.x < ne) {
@@ -637,21 +628,40 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
             }
         }
         if (m < nv) {
-            sa[m * 33 + k] = p;
-            sa0[m * 33 + k] = q;
+            sa[m * ld + k] = p;
+            sa0[m * ld + k] = q;
         } else {
-            sb[(m - nv) * 33 + k] = p;
-            sb2[(m - nv) * 33 + k] = q;
+            sb[(m - nv) * ld + k] = p;
+            sb2[(m - nv) * ld + k] = q;
         }
     }
     __syncthreads();
+}
+
+template <int DIM, bool SINGLE, bool SPLIT>
+__global__ void __launch_bounds__(256)
+tc_rows_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
+               int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo, const float2 *__restrict__ af_tab)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nv = Q.nv, nl = Q.nl;
+    float2 *sa = reinterpret_cast<float2 *>(smem_raw);  // [nv][33]
+    float2 *sa0 = sa + nv * 33;
+    float2 *sb = sa0 + nv * 33;                           // [nl][33]
+    float2 *sb2 = sb + nl * 33;
+    float *ssc = reinterpret_cast<float *>(sb2 + nl * 33);  // [32]
+    EventView *sev = reinterpret_cast<EventView *>(ssc + 32);
+
+    const int64_t g0 = (int64_t)blockIdx.x * 32;
+    const int ne = (int)max((int64_t)0, min((int64_t)32, n_ev - g0));
+    tc_rows_terms<DIM, SINGLE>(Q, S, scap, M, mcap, e0, g0, ne, 33, sa, sa0, sb, sb2, ssc, sev);
     // t_i, i = v + nv*l: light-outer, view-inner, so the light factor (times
     // the event scale) is loaded once per light and rows advance by pointer
     // increments (no integer division per entry).
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float sc = ssc[lane];
-    const int64_t col = (PLANAR ? 1 : 2) * (g0 + lane);
-    const int64_t step = (PLANAR ? 8 : 16) * K;  // 8 views
+    const int64_t col = 2 * (g0 + lane);
+    const int64_t step = 16 * K;  // 8 views = 16 real rows
     const bool cbs = !SINGLE && Q.cbs;
     for (int lj = 0; lj < nl; ++lj) {
         float2 bl = sb[lj * 33 + lane], bl2 = sb2[lj * 33 + lane];
@@ -660,10 +670,9 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
         bl2.x *= sc;
         bl2.y *= sc;
         const int64_t i0 = (int64_t)nv * lj + warp;
-        const int64_t o0 = (PLANAR ? 1 : 2) * i0 * K + col;
-        __half *ph = Ahi + o0, *pl = Alo + o0;
-        __half *qh = PLANAR ? Ihi + o0 : nullptr, *ql = PLANAR ? Ilo + o0 : nullptr;
-        for (int vi = warp; vi < nv; vi += 8, ph += step, pl += step, qh += PLANAR ? step : 0, ql += PLANAR ? step : 0) {
+        __half *ph = Ahi + 2 * i0 * K + col;
+        __half *pl = Alo + 2 * i0 * K + col;
+        for (int vi = warp; vi < nv; vi += 8, ph += step, pl += step) {
             float2 t = cmul(sa[vi * 33 + lane], bl);
             if (SINGLE) {
                 const float2 af =
@@ -675,25 +684,86 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
                 t.y += t2.y;
             }
             const __half hr = __float2half_rn(t.x), hi = __float2half_rn(t.y);
-            __half lr, li;
+            *reinterpret_cast<__half2 *>(ph) = __halves2half2(hr, hi);
+            *reinterpret_cast<__half2 *>(ph + K) = __halves2half2(hi, __hneg(hr));
             if (SPLIT) {
-                lr = __float2half_rn(t.x - __half2float(hr));
-                li = __float2half_rn(t.y - __half2float(hi));
+                const __half lr = __float2half_rn(t.x - __half2float(hr));
+                const __half li = __float2half_rn(t.y - __half2float(hi));
+                *reinterpret_cast<__half2 *>(pl) = __halves2half2(lr, li);
+                *reinterpret_cast<__half2 *>(pl + K) = __halves2half2(li, __hneg(lr));
             }
-            if (PLANAR) {
-                *ph = hr;
-                *qh = hi;
-                if (SPLIT) {
-                    *pl = lr;
-                    *ql = li;
+        }
+    }
+}
+
+// Planar rows (CTA-pair kernel): Re t_i and Im t_i in separate planes, rows of
+// K events; Rhi / Rlo the Re planes, Ihi / Ilo the Im planes.  Lane = a pair
+// of adjacent events and half-warp = a view, so each thread reads both
+// events' factors with one 16-byte shared load, rounds them with one packed
+// conversion and writes one half2 per plane.
+template <int DIM, bool SINGLE, bool SPLIT>
+__global__ void __launch_bounds__(256)
+tc_rows_planar_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
+                      int64_t K, __half *__restrict__ Rhi, __half *__restrict__ Rlo, __half *__restrict__ Ihi,
+                      __half *__restrict__ Ilo, const float2 *__restrict__ af_tab)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nv = Q.nv, nl = Q.nl;
+    float2 *sa = reinterpret_cast<float2 *>(smem_raw);  // [nv][32]
+    float2 *sa0 = sa + nv * 32;
+    float2 *sb = sa0 + nv * 32;  // [nl][32]
+    float2 *sb2 = sb + nl * 32;
+    float *ssc = reinterpret_cast<float *>(sb2 + nl * 32);  // [32]
+    EventView *sev = reinterpret_cast<EventView *>(ssc + 32);
+
+    const int64_t g0 = (int64_t)blockIdx.x * 32;
+    const int ne = (int)max((int64_t)0, min((int64_t)32, n_ev - g0));
+    tc_rows_terms<DIM, SINGLE>(Q, S, scap, M, mcap, e0, g0, ne, 32, sa, sa0, sb, sb2, ssc, sev);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int h = lane >> 4, kp = lane & 15;  // view parity, event pair (events 2 kp, 2 kp + 1)
+    const float s0 = ssc[2 * kp], s1 = ssc[2 * kp + 1];
+    const float4 *sa4 = reinterpret_cast<const float4 *>(sa), *sa04 = reinterpret_cast<const float4 *>(sa0);
+    const float4 *sb4 = reinterpret_cast<const float4 *>(sb), *sb24 = reinterpret_cast<const float4 *>(sb2);
+    const int64_t col = g0 + 2 * kp;
+    const int64_t step = 16 * K;  // 16 views
+    const bool cbs = !SINGLE && Q.cbs;
+    for (int lj = 0; lj < nl; ++lj) {
+        float4 b = sb4[lj * 16 + kp], b2 = sb24[lj * 16 + kp];
+        b = make_float4(b.x * s0, b.y * s0, b.z * s1, b.w * s1);
+        b2 = make_float4(b2.x * s0, b2.y * s0, b2.z * s1, b2.w * s1);
+        const int v0 = 2 * warp + h;
+        const int64_t o0 = ((int64_t)nv * lj + v0) * K + col;
+        __half *pr = Rhi + o0, *pi = Ihi + o0, *qr = Rlo + o0, *qi = Ilo + o0;
+        for (int vi = v0; vi < nv; vi += 16, pr += step, pi += step, qr += step, qi += step) {
+            const float4 a = sa4[vi * 16 + kp];
+            float2 t0 = cmul(make_float2(a.x, a.y), make_float2(b.x, b.y));
+            float2 t1 = cmul(make_float2(a.z, a.w), make_float2(b.z, b.w));
+            if (SINGLE) {
+                float2 f0, f1;
+                if (af_tab) {
+                    f0 = f1 = af_tab[vi + nv * lj];
+                } else {
+                    f0 = to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[2 * kp].x1));
+                    f1 = to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[2 * kp + 1].x1));
                 }
-            } else {
-                *reinterpret_cast<__half2 *>(ph) = __halves2half2(hr, hi);
-                *reinterpret_cast<__half2 *>(ph + K) = __halves2half2(hi, __hneg(hr));
-                if (SPLIT) {
-                    *reinterpret_cast<__half2 *>(pl) = __halves2half2(lr, li);
-                    *reinterpret_cast<__half2 *>(pl + K) = __halves2half2(li, __hneg(lr));
-                }
+                t0 = cmul(t0, f0);
+                t1 = cmul(t1, f1);
+            } else if (cbs) {
+                const float4 a0 = sa04[vi * 16 + kp];
+                const float2 u0 = cmul(make_float2(a0.x, a0.y), make_float2(b2.x, b2.y));
+                const float2 u1 = cmul(make_float2(a0.z, a0.w), make_float2(b2.z, b2.w));
+                t0.x += u0.x;
+                t0.y += u0.y;
+                t1.x += u1.x;
+                t1.y += u1.y;
+            }
+            const __half2 re = __floats2half2_rn(t0.x, t1.x), im = __floats2half2_rn(t0.y, t1.y);
+            *reinterpret_cast<__half2 *>(pr) = re;
+            *reinterpret_cast<__half2 *>(pi) = im;
+            if (SPLIT) {
+                const float2 fr = __half22float2(re), fi = __half22float2(im);
+                *reinterpret_cast<__half2 *>(qr) = __floats2half2_rn(t0.x - fr.x, t1.x - fr.y);
+                *reinterpret_cast<__half2 *>(qi) = __floats2half2_rn(t0.y - fi.x, t1.y - fi.y);
             }
         }
     }
@@ -701,7 +771,7 @@ tc_rows_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
 
 // af(l_j . v_i) table for far-field single scattering, flattened i = v + nv*l.
 template <int DIM>
-__global__ void af_table_kernel(NeeParams Q, float2 *__restrict__ tab)
+__global__ void af_table_kernel(const __grid_constant__ NeeParams Q, float2 *__restrict__ tab)
 {
     const int N = Q.nv * Q.nl;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
@@ -849,14 +919,21 @@ inline void tc_rows(const TcPlan &p, const TcOperands &o, const NeeParams &Q, co
 {
     const size_t smem = sizeof(float2) * 33 * 2 * (size_t)(Q.nv + Q.nl) + 32 * sizeof(float) +
                         32 * sizeof(EventView) + 64;
-    auto kern = p.pair ? tc_rows_kernel<DIM, SINGLE, SPLIT, true> : tc_rows_kernel<DIM, SINGLE, SPLIT, false>;
-    if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        throw std::runtime_error("too many lights/views for the tensor-core row kernel");
-    // every column of the K blocks the product reads is written (zeros past n)
-    const int64_t eb = p.pair ? 64 : 32;
-    const int grid = (int)((n + eb - 1) / eb * (eb / 32));
-    kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, o.ihi, o.ilo,
-                                  use_af_table ? o.af : nullptr);
+    const float2 *af = use_af_table ? o.af : nullptr;
+    if (p.pair) {
+        auto kern = tc_rows_planar_kernel<DIM, SINGLE, SPLIT>;
+        if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            throw std::runtime_error("too many lights/views for the tensor-core row kernel");
+        // every column of the 64-event blocks the product reads is written (zeros past n)
+        const int grid = (int)((n + 63) / 64 * 2);
+        kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, o.ihi, o.ilo, af);
+    } else {
+        auto kern = tc_rows_kernel<DIM, SINGLE, SPLIT>;
+        if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            throw std::runtime_error("too many lights/views for the tensor-core row kernel");
+        const int grid = (int)((n + 31) / 32);
+        kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, af);
+    }
 }
 
 // D[ks][Mr][N] += A B^T over num_kb K-blocks, split ksplit ways along K.

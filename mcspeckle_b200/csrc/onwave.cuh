@@ -34,7 +34,7 @@ inline size_t onwave_smem(int nvc, int nl, size_t csize)
 
 template <int DIM, int POL, bool SINGLE>
 __global__ void __launch_bounds__(kOwWarps * 32)
-onwave_accum_kernel(NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_events,
+onwave_accum_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_events,
                     int64_t ev_per_cta, int nvc, const double2 *__restrict__ Wl, double2 *__restrict__ U)
 {
     using R = typename std::conditional<POL == P64, double, float>::type;

@@ -222,7 +222,7 @@ __device__ __forceinline__ bool path_advance(const WalkParams &P, PathRng &r, Wa
 
 // Pass 1: events per path.
 template <int DIM>
-__global__ void __launch_bounds__(128) walk_count_kernel(WalkParams P, int32_t *__restrict__ counts,
+__global__ void __launch_bounds__(128) walk_count_kernel(const __grid_constant__ WalkParams P, int32_t *__restrict__ counts,
                                                          unsigned long long *__restrict__ next_path,
                                                          int *__restrict__ err)
 {
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(128) walk_count_kernel(WalkParams P, int32_t *
 // Pass 2: records.  moff[p] = index of the first multiple-scattering record
 // of path p (exclusive scan of counts[p] - 1).
 template <int DIM>
-__global__ void __launch_bounds__(128) walk_record_kernel(WalkParams P, const int64_t *__restrict__ moff,
+__global__ void __launch_bounds__(128) walk_record_kernel(const __grid_constant__ WalkParams P, const int64_t *__restrict__ moff,
                                                           SingleRec S, int64_t scap, MultiRec M,
                                                           int64_t mcap, unsigned long long *__restrict__ next_path)
 {
