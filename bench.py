@@ -659,7 +659,7 @@ def main():
         flops_per_launch = prof["contract_flops"] / max(prof["contract_launches"], 1)
         achieved = flops_per_launch / (busy_per_launch_ms / 1000.0) / 1e12
         traffic = None
-        tf = os.path.join(ROOT, "profiles", "herk_tc_traffic.json")
+        tf = os.path.join(ROOT, "profiles", "herk_tc2_kernel_cov64x64_traffic.json")
         if os.path.exists(tf):
             with open(tf) as f:
                 tj = json.load(f)
@@ -714,7 +714,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "herk_tc_kernel", "peak_source": f"bf16_tflops_sustained ({peak_kind})",
+                         "kernel": "herk_tc2_kernel", "peak_source": f"bf16_tflops_sustained ({peak_kind})",
                          "flops_per_launch": flops_per_launch, "busy_ms_per_launch": busy_per_launch_ms,
                          "ms_per_launch_overlapped": per_launch_ms, "contract_busy_ms": prof["contract_busy_ms"],
                          "launches": prof["contract_launches"]},
