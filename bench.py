@@ -338,7 +338,8 @@ ACC_MASK = None  # entries excluded from the accuracy comparison of a workload
 
 def workload_spec(name):
     """(description, make(n, precision, seed, offset, norm) -> holder, device solve,
-    host solve, output doubles, oracle solve, dominant-kernel roofline kind)."""
+    host solve, output doubles, oracle solve, the tensor-core kernel whose
+    roofline is reported or None)."""
     from mcspeckle_b200 import _lib
     from mcspeckle_b200 import mc as MC
     from mcspeckle_b200 import fourier_quad as FQ
@@ -388,7 +389,7 @@ def workload_spec(name):
         return ("MCfieldFourierQuad, box 50x50x10 MFP (MFP 100 wavelengths), sigma_a 0.005 per MFP, plane wave "
                 "along +z, 256x256 angular grid (v_max 255/256, v_stp 1/128: 0.5-wavelength lateral pitch), CBS; "
                 "isotropic as the reference (HG g=0.9 and the point source are not built)",
-                make, dev, FQ.field_fourier_quad_from_args, [2 * 256 * 256], oracle, None)
+                make, dev, FQ.field_fourier_quad_from_args, [2 * 256 * 256], oracle, "herk_tc_kernel<PLANE>")
     if name == "hetero128":
         mfp = 10.0
         g = np.random.default_rng(4)
@@ -415,7 +416,7 @@ def workload_spec(name):
                 f"theta bins from 3 HG lobes g={[round(x, 3) for x in gs]} w={[round(x, 3) for x in ws]}, "
                 f"128 lights x 128 views (16x8 grids of +-5 deg), CBS",
                 make, dev, lambda h: H.cov_hetero_from_args(h)[:2], [2 * n2 * n2, 2 * n2 * n2, 2 * n2], oracle,
-                "tensor")
+                "herk_tc2_kernel")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -484,12 +485,12 @@ def run_workload(a):
     host(make(P, "fp32", seed))
     fp32_value = P / (time.perf_counter() - t32)
     roof = None
-    if bound == "tensor" and prof["contract_launches"]:
+    if bound is not None and prof["contract_launches"]:
         peaks, peak_kind = load_peaks()
         peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
         achieved = prof["contract_flops"] / (prof["contract_busy_ms"] / 1000.0) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "herk_tc2_kernel", "peak_source": f"bf16_tflops_sustained ({peak_kind})",
+                "traffic": None, "kernel": bound, "peak_source": f"bf16_tflops_sustained ({peak_kind})",
                 "flops": prof["contract_flops"], "contract_busy_ms": prof["contract_busy_ms"]}
     cpu = None
     if not a.no_cpu_baseline:

@@ -160,7 +160,7 @@ struct PlaneEpi {
     const double2 *zexp0;  // [r1][r2]
     const double *gz;      // plane boundaries
     const int *planes;     // plane of each slice (blockIdx.y)
-    double *U;             // [r1][r2] complex interleaved, this light
+    float *U;              // [r1][r2] complex interleaved FP32, this light
     int nv0;
 };
 
@@ -276,6 +276,7 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
             const int pl = pe.planes[blockIdx.y];
             tz = (pe.gz[pl] + pe.gz[pl + 1]) / 2;
         }
+        const bool vec4 = PLANE && !(pe.nv0 & 1);
         for (int c0 = 0; c0 < TC_BN; c0 += 32) {
             uint32_t r[32];
             tmem_ld32(tbase + c0, r);
@@ -284,20 +285,43 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
             __syncwarp();
             const int n = col0 + c0 + lane;
             if (PLANE) {
-#pragma unroll 2
+                // the chunk's 16 plane-factor exponents in flight together
+                double2 zc[16];
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int R = row0 + warp * 32 + 2 * m;
+                    zc[m] = (R < Mr && n < N) ? pe.zexp0[(int64_t)(R >> 1) * pe.nv0 + n] : make_double2(0.0, 0.0);
+                }
+#pragma unroll
                 for (int m = 0; m < 16; ++m) {
                     const int R = row0 + warp * 32 + 2 * m;  // even: Re row of complex row R / 2
-                    if (R < Mr && n < N) {
+                    const bool live = R < Mr && n < N;
+                    float vx = 0.f, vy = 0.f;
+                    int64_t q = 0;
+                    if (live) {
                         const int r1 = R >> 1;
                         const double re = (double)ep[(2 * m) * 33 + lane], im = (double)ep[(2 * m + 1) * 33 + lane];
-                        const int64_t q = (int64_t)r1 * pe.nv0 + n;
-                        const double2 z = pe.zexp0[q];
+                        q = (int64_t)r1 * pe.nv0 + n;
+                        const double2 z = zc[m];
                         float sn, cs;
                         __sincosf((float)reduce_2pi(z.y * tz), &sn, &cs);
                         const double mag = (double)expf((float)(z.x * tz));
                         const double fx = mag * cs, fy = mag * sn;
-                        atomicAdd(pe.U + 2 * q, fx * re - fy * im);
-                        atomicAdd(pe.U + 2 * q + 1, fx * im + fy * re);
+                        vx = (float)(fx * re - fy * im);
+                        vy = (float)(fx * im + fy * re);
+                    }
+                    // columns n, n + 1 (lanes 2i, 2i + 1) in one 16-byte atomic when
+                    // the row length is even (q even, so U + 2q is 16-byte aligned)
+                    const float wx = __shfl_down_sync(0xffffffffu, vx, 1), wy = __shfl_down_sync(0xffffffffu, vy, 1);
+                    if (live) {
+                        if (!vec4) {
+                            atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * q), make_float2(vx, vy));
+                        } else if (!(lane & 1)) {
+                            if (n + 1 < N)
+                                atomicAdd(reinterpret_cast<float4 *>(pe.U + 2 * q), make_float4(vx, vy, wx, wy));
+                            else
+                                atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * q), make_float2(vx, vy));
+                        }
                     }
                 }
             } else {
@@ -319,6 +343,251 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]),
+        "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]),
+        "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// The FourierQuad per-plane sums with the plane loop inside the CTA.
+//
+// A CTA owns one 128 x 256 tile (64 complex rows r1 as Re / Im real rows,
+// 256 columns r2) and a contiguous range of planes of a group (pranges[y]:
+// first plane slot, plane count; kranges[slot]: the plane's K blocks, which
+// are contiguous across slots).  TMEM columns 0-255 hold the current plane's
+// sum F_P (FP32), columns 256-511 the running sum  sum_P exp(zexp0 tz_P) F_P.
+// Warp 0 streams every K block of the range through the 4-stage ring, warp 1
+// issues the MMAs of one plane and commits acc_full, warps 4-7 (one TMEM lane
+// quarter each) multiply the plane's sum by its factor, add it into the
+// running sum and arrive on acc_empty, after which the next plane's MMAs
+// start; the producer keeps loading meanwhile.  The running sum is added into
+// U once per CTA.  The plane factor follows the PlaneEpi form: FP64 product
+// and reduction of the phase, FP32 sincos and exp.  Every wait is bounded.
+// ---------------------------------------------------------------------------
+template <bool SPLIT>
+__global__ void __launch_bounds__(256, 1)
+fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
+                    const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles,
+                    const int2 *__restrict__ kranges, const int2 *__restrict__ pranges, int Mr, int N,
+                    PlaneEpi pe, int *__restrict__ err)
+{
+    using Cfg = TcCfg<SPLIT>;
+    constexpr int S = Cfg::STAGES;
+    extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + S * Cfg::STAGE_BYTES);
+    uint64_t *empty = full + S;
+    uint64_t *acc_full = empty + S;
+    uint64_t *acc_empty = acc_full + 1;
+    uint64_t *done = acc_empty + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+    int *issued = abort_flag + 1;
+    int *ep_fail = issued + 1;  // written only by the epilogue warps
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int2 tile = tiles[blockIdx.x];
+    const int row0 = tile.x * TC_BM;
+    const int col0 = tile.y * TC_BN;
+    const int2 pr = pranges[blockIdx.y];  // the host makes every range non-empty
+    const int kb_first = kranges[pr.x].x;
+    const int2 klast = kranges[pr.x + pr.y - 1];
+    const int nkb = klast.x + klast.y - kb_first;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, 1);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        *issued = 0;
+        *ep_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(2 * TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer: every K block of the plane range
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % S;
+            if (kb >= S && !mbar_wait(&empty[s], ((kb / S) - 1) & 1)) {
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int *)abort_flag) break;
+            uint8_t *st = base + s * Cfg::STAGE_BYTES;
+            mbar_expect_tx(&full[s], Cfg::STAGE_BYTES);
+            const int kx = (kb_first + kb) * TC_BK;
+            tma_load_2d(st, &tm_ahi, kx, row0, &full[s]);
+            if (SPLIT) tma_load_2d(st + TC_A_BYTES, &tm_alo, kx, row0, &full[s]);
+            tma_load_2d(st + Cfg::B_OFF, &tm_b, kx, col0, &full[s]);
+            *(volatile int *)issued = kb + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer: one plane at a time into columns 0-255
+        constexpr uint32_t idesc = umma_idesc_f16(TC_BM, TC_BN);
+        int kb = 0;
+        bool ok = true;
+        for (int pi = 0; pi < pr.y && ok; ++pi) {
+            const int nk = kranges[pr.x + pi].y;
+            if (pi > 0) {
+                if (!mbar_wait(acc_empty, (pi - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+            }
+            for (int j = 0; j < nk; ++j, ++kb) {
+                const int s = kb % S;
+                if (!mbar_wait(&full[s], (kb / S) & 1)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint8_t *st = base + s * Cfg::STAGE_BYTES;
+                const uint64_t dh = umma_desc_sw128(st);
+                const uint64_t dl = umma_desc_sw128(st + TC_A_BYTES);
+                const uint64_t db = umma_desc_sw128(st + Cfg::B_OFF);
+#pragma unroll
+                for (int kk = 0; kk < TC_BK / 16; ++kk) {
+                    const uint64_t adv = (uint64_t)(kk * 32) >> 4;
+                    umma_f16(tmem, dh + adv, db + adv, idesc, (j | kk) != 0);
+                    if (SPLIT) umma_f16(tmem, dl + adv, db + adv, idesc, 1u);
+                }
+                umma_commit(&empty[s]);
+            }
+            if (ok) umma_commit(acc_full);
+        }
+        if (!ok) atomicExch(abort_flag, 1);
+        umma_commit(done);  // fires once every issued MMA has completed
+    } else if (warp >= 4) {
+        // plane epilogue: TMEM lane = real row row0 + 32 q + lane (Re rows even, Im rows odd)
+        const int q = warp - 4;
+        const uint32_t tacc = tmem + ((uint32_t)(q * 32) << 16), tsum = tacc + TC_TMEM_COLS;
+        const int R = row0 + q * 32 + lane;
+        const int r1 = R >> 1;
+        const bool re_row = !(lane & 1), row_ok = R < Mr;
+        const int jb = re_row ? 0 : 16;  // the pair's even lane forms the factors of columns 0-15, the odd 16-31
+        for (int pi = 0; pi < pr.y; ++pi) {
+            // the four warps agree on a timeout before leaving the loop, so
+            // that every named barrier below is reached by all of them
+            if (!__all_sync(0xffffffffu, mbar_wait(acc_full, pi & 1)) && lane == 0) atomicExch(ep_fail, 1);
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (*(volatile int *)ep_fail) {
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            tc_fence_after();
+            const int pl = pe.planes[pr.x + pi];
+            const double tz = (pe.gz[pl] + pe.gz[pl + 1]) / 2;
+            for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+                double2 zc[16];
+#pragma unroll
+                for (int t = 0; t < 16; ++t) {
+                    const int n = col0 + c0 + jb + t;
+                    zc[t] = (row_ok && n < N) ? pe.zexp0[(int64_t)r1 * pe.nv0 + n] : make_double2(0.0, 0.0);
+                }
+                uint32_t a[32], sm[32];
+                tmem_ld32(tacc + c0, a);
+                if (pi > 0) {
+                    tmem_ld32(tsum + c0, sm);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) sm[j] = 0u;
+                }
+#pragma unroll
+                for (int t = 0; t < 16; ++t) {
+                    float sn, cs;
+                    __sincosf((float)reduce_2pi(zc[t].y * tz), &sn, &cs);
+                    const float mag = expf((float)(zc[t].x * tz));
+                    const float fx = mag * cs, fy = mag * sn;
+                    const float ox = __shfl_xor_sync(0xffffffffu, fx, 1), oy = __shfl_xor_sync(0xffffffffu, fy, 1);
+                    // factor of column t and of column 16 + t
+                    const float gx0 = re_row ? fx : ox, gy0 = re_row ? fy : oy;
+                    const float gx1 = re_row ? ox : fx, gy1 = re_row ? oy : fy;
+                    const float a0 = __uint_as_float(a[t]), a1 = __uint_as_float(a[16 + t]);
+                    const float p0 = __shfl_xor_sync(0xffffffffu, a0, 1), p1 = __shfl_xor_sync(0xffffffffu, a1, 1);
+                    // Re row: Re(F P) = Fx Pre - Fy Pim; Im row: Im(F P) = Fx Pim + Fy Pre
+                    const float v0 = re_row ? gx0 * a0 - gy0 * p0 : gx0 * a0 + gy0 * p0;
+                    const float v1 = re_row ? gx1 * a1 - gy1 * p1 : gx1 * a1 + gy1 * p1;
+                    sm[t] = __float_as_uint(__uint_as_float(sm[t]) + v0);
+                    sm[16 + t] = __float_as_uint(__uint_as_float(sm[16 + t]) + v1);
+                }
+                tmem_st32(tsum + c0, sm);
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            tc_fence_before();
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (q == 0 && lane == 0) mbar_arrive(acc_empty);
+        }
+    }
+    __syncwarp();
+
+    const bool ok = mbar_wait(done, 0);
+    tc_fence_after();
+    __syncthreads();
+    const bool failed = !ok || *(volatile int *)abort_flag;
+    if (failed) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1);
+            // wait (bounded) for TMA copies this CTA still has in flight
+            const int n_issued = *(volatile int *)issued;
+            for (int kb = (n_issued > S ? n_issued - S : 0); kb < n_issued; ++kb)
+                (void)mbar_wait(&full[kb % S], (kb / S) & 1);
+        }
+    } else if (warp >= 4) {
+        // the running sum into U: (Re, Im) of column n from lanes 2i, 2i + 1
+        const int q = warp - 4;
+        const uint32_t tsum = tmem + ((uint32_t)(q * 32) << 16) + TC_TMEM_COLS;
+        const int R = row0 + q * 32 + lane;
+        const bool row_ok = R < Mr;
+        for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+            uint32_t sm[32];
+            tmem_ld32(tsum + c0, sm);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const float v = __uint_as_float(sm[j]);
+                const float w = __shfl_down_sync(0xffffffffu, v, 1);
+                const int n = col0 + c0 + j;
+                if (!(lane & 1) && row_ok && n < N)
+                    atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * ((int64_t)(R >> 1) * pe.nv0 + n)), make_float2(v, w));
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_TMEM_COLS)
+                     : "memory");
     }
 }
 
@@ -975,6 +1244,27 @@ inline void tc_gemm_planes_launch(const CUtensorMap &m_ahi, const CUtensorMap &m
     }
     herk_tc_kernel<SPLIT, true><<<dim3((unsigned)n_tiles, (unsigned)n_slices), 128, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
         m_ahi, m_alo, m_b, tiles, 0, 0, Mr, N, nullptr, err, kranges, pe);
+}
+
+// The plane-loop form: grid (tiles, plane ranges); pranges (device) holds
+// n_ranges (first plane slot, plane count) pairs, kranges the K blocks of
+// every plane slot, pe.planes the plane of every slot.
+template <bool SPLIT>
+inline void tc_gemm_plane_loop_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, const CUtensorMap &m_b,
+                                      const int2 *tiles, int n_tiles, const int2 *kranges, const int2 *pranges,
+                                      int n_ranges, int Mr, int N, const PlaneEpi &pe, int *err, cudaStream_t st)
+{
+    static std::atomic<uint64_t> attr_set{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
+    if (dev >= 64 || !((attr_set.load() >> dev) & 1)) {
+        if (cudaFuncSetAttribute(fq_planes_tc_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 TcCfg<SPLIT>::SMEM_BYTES) != cudaSuccess)
+            throw std::runtime_error("cannot reserve shared memory for the plane-loop tensor-core kernel");
+        if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
+    }
+    fq_planes_tc_kernel<SPLIT><<<dim3((unsigned)n_tiles, (unsigned)n_ranges), 256, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
+        m_ahi, m_alo, m_b, tiles, kranges, pranges, Mr, N, pe, err);
 }
 
 // D[ks][2N][N] += the planar pair product (Re C in even rows, Im C in odd

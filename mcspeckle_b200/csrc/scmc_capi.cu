@@ -1268,7 +1268,8 @@ void validate_fq(const scmc_fq_args *a)
 }
 
 // The per-plane DFT sums of one batch on tcgen05 (fq.cuh, tensor-core form),
-// added into U stored [light][r1][r2].  dzt: zexp0 stored [r1][r2].
+// added into U stored [light][r1][r2] in FP32 (each plane's sum is FP32 in
+// TMEM already; vector atomics of 16 bytes).  dzt: zexp0 stored [r1][r2].
 // Nonempty planes are taken in groups of at most kFqTcEntries padded entries
 // (operand memory) and kFqTcPlanes planes.
 constexpr int64_t kFqTcEntries = (int64_t)1 << 18;
@@ -1276,7 +1277,7 @@ constexpr int kFqTcPlanes = 2048;
 
 void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
                  const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *T, const double2 *dzt,
-                 double *U, bool split, cudaStream_t st)
+                 float *U, bool split, cudaStream_t st)
 {
     const int nv0 = F.nv0;
     const int Mr = 2 * nv0;
@@ -1302,9 +1303,26 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
             ++g1;
         }
         const int64_t K = 64 * nblk;
+        // plane ranges of about equal K blocks, about one CTA per SM over the tiles
+        std::vector<int2> prs;
+        {
+            const int want = std::max(1, std::min((int)gpl.size(), sm_count(c.device) / std::max(1, (int)tiles.size())));
+            const int64_t per = (nblk + want - 1) / want;
+            int first = 0;
+            int64_t acc = 0;
+            for (int i = 0; i < (int)gpl.size(); ++i) {
+                acc += kr[i].y;
+                if (acc >= per || i + 1 == (int)gpl.size()) {
+                    prs.push_back(make_int2(first, i - first + 1));
+                    first = i + 1;
+                    acc = 0;
+                }
+            }
+        }
         const size_t ab = tc_align((size_t)Mr * K * sizeof(__half)), bb = tc_align((size_t)nv0 * K * sizeof(__half));
         const size_t meta = tc_align(tiles.size() * sizeof(int2)) + tc_align(kr.size() * sizeof(int2)) +
-                            tc_align(blk.size() * sizeof(int2)) + tc_align(gpl.size() * sizeof(int)) + 1024;
+                            tc_align(blk.size() * sizeof(int2)) + tc_align(gpl.size() * sizeof(int)) +
+                            tc_align(prs.size() * sizeof(int2)) + 1024;
         char *mem = reinterpret_cast<char *>(c.tc_a.ensure((split ? 2 : 1) * ab + bb + meta));
         __half *ahi = reinterpret_cast<__half *>(mem);
         __half *alo = split ? reinterpret_cast<__half *>(mem + ab) : ahi;
@@ -1318,11 +1336,14 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
         q += tc_align(blk.size() * sizeof(int2));
         int *d_pl = reinterpret_cast<int *>(q);
         q += tc_align(gpl.size() * sizeof(int));
+        int2 *d_pr = reinterpret_cast<int2 *>(q);
+        q += tc_align(prs.size() * sizeof(int2));
         int *d_err = reinterpret_cast<int *>(q);
         CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(d_kr, kr.data(), kr.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(d_blk, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(d_pl, gpl.data(), gpl.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d_pr, prs.data(), prs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
         CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
         const CUtensorMap m_ahi = tc_map(ahi, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
         const CUtensorMap m_alo = tc_map(alo, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
@@ -1341,11 +1362,11 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
                 StageScope sc(ST_CONTRACT, st);
                 const PlaneEpi pe{dzt, F.gz, d_pl, U + 2 * (int64_t)nv0 * nv0 * j, nv0};
                 if (split)
-                    tc_gemm_planes_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, (int)gpl.size(),
-                                                Mr, nv0, pe, d_err, st);
+                    tc_gemm_plane_loop_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, d_pr,
+                                                    (int)prs.size(), Mr, nv0, pe, d_err, st);
                 else
-                    tc_gemm_planes_launch<false>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, (int)gpl.size(),
-                                                 Mr, nv0, pe, d_err, st);
+                    tc_gemm_plane_loop_launch<false>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, d_pr,
+                                                     (int)prs.size(), Mr, nv0, pe, d_err, st);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
@@ -1559,7 +1580,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
         }
         if (use_tc) {
             fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, reinterpret_cast<const float2 *>(T), dzt,
-                        reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, st);
+                        reinterpret_cast<float *>(U), a->precision == SCMC_PREC_MIXED, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
             for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
@@ -1577,8 +1598,12 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     const double V = bw[0] * bw[1] * bw[2];
     const double norm = total_vert > 0 ? std::sqrt(1.0 / (double)total_vert * V * sigt) : 0.0;  // lines 214, 302-303
     StageScope fin(ST_FINAL, st);
-    fq_finalize_kernel<AccT><<<(int)std::max<int64_t>(1, std::min<int64_t>((nout + 255) / 256, 4096)), 256, 0, st>>>(
-        U, db, (int)Nv, (int)nl_out, norm, d_u, use_tc ? 1 : 0);
+    const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((nout + 255) / 256, 4096));
+    if (use_tc)  // FP32 accumulator in U's memory, stored [light][r1][r2]
+        fq_finalize_kernel<float><<<fgrid, 256, 0, st>>>(reinterpret_cast<const float *>(U), db, (int)Nv, (int)nl_out,
+                                                         norm, d_u, 1);
+    else
+        fq_finalize_kernel<AccT><<<fgrid, 256, 0, st>>>(U, db, (int)Nv, (int)nl_out, norm, d_u, 0);
     CK(cudaGetLastError());
     LAUNCHED();
 }
