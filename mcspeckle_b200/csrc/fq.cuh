@@ -172,14 +172,16 @@ __global__ void fq_scatter_kernel(const FqEntry *__restrict__ in, int64_t n, con
 }
 
 // T[r][p] = exp(-2 pi i m'(r) P(p) / M): the centred DFT's twiddles at the
-// reference's cropped, flipped bins (see the file comment).
+// reference's cropped, flipped bins (see the file comment); stored [p][r]
+// when transposed.
 template <typename C>
-__global__ void fq_twiddle_kernel(int nv0, int nx, double M, double nx_pad, double nv_pad, C *__restrict__ T)
+__global__ void fq_twiddle_kernel(int nv0, int nx, double M, double nx_pad, double nv_pad, C *__restrict__ T,
+                                  int transposed)
 {
     const double c = floor(M / 2);
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < (int64_t)nv0 * nx;
          k += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(k / nx), p = (int)(k % nx);
+        const int r = transposed ? (int)(k % nv0) : (int)(k / nx), p = transposed ? (int)(k / nv0) : (int)(k % nx);
         const double m = (M - 1 - ((double)r + nv_pad)) - c;
         const double P = ((double)p + nx_pad) - c;
         const double t = fmod(m * P, M);
@@ -282,18 +284,21 @@ fq_accum_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ 
 // zero-padded), in the real expansion of the tensor-core field path
 //     A[2r1] = (Re a, -Im a), A[2r1+1] = (Im a, Re a), B[r2] = (Re b, Im b),
 // two K columns per entry, so one 64-column K block never spans two planes.
-// herk_tc_kernel computes F_P per plane (one grid row per plane) and its
-// epilogue multiplies by exp(zexp0 * tz_P) and adds into the output, which
-// for this form is stored [light][r1][r2] (r2 fastest).
+// fq_planes_tc_kernel (herk_tc.cuh) computes F_P plane after plane for a
+// range of planes per CTA, multiplies each by exp(zexp0 * tz_P) into a
+// running sum in TMEM and adds that sum into the output once; the output of
+// this form is stored [light][r1][r2] (r2 fastest) in FP32.
 // ---------------------------------------------------------------------------
 template <bool SPLIT>
 __global__ void __launch_bounds__(256)
-fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk, int light,
-                  const float2 *__restrict__ T, int64_t K, __half *__restrict__ Ahi, __half *__restrict__ Alo,
-                  __half *__restrict__ Bm)
+fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk,
+                  int light, const float2 *__restrict__ Tt, int64_t K, __half *__restrict__ Ahi,
+                  __half *__restrict__ Alo, __half *__restrict__ Bm)
 {
+    constexpr int RB = 64;  // twiddle rows staged per pass
     __shared__ float2 ss[32];
     __shared__ int sp1[32], sp2[32];
+    __shared__ float2 ta[RB][33], tb[RB][33];  // [r - r0][entry]
     const int2 bk = blk[blockIdx.x];  // (first entry, entries in this block)
     if (threadIdx.x < 32) {
         float2 sv = make_float2(0.f, 0.f);
@@ -308,31 +313,36 @@ fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict_
         sp1[threadIdx.x] = p1;
         sp2[threadIdx.x] = p2;
     }
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t col = 2 * ((int64_t)blockIdx.x * 32 + lane);
-    const float2 sv = ss[lane];
-    const int p1 = sp1[lane], p2 = sp2[lane];
-    const bool live = lane < bk.y;
-    for (int r = warp; r < F.nv0; r += 8) {
-        float2 av = make_float2(0.f, 0.f), bv = make_float2(0.f, 0.f);
-        if (live) {
-            av = cmul(sv, T[(int64_t)r * F.nx + p1]);
-            bv = T[(int64_t)r * F.nx + p2];
+    for (int r0 = 0; r0 < F.nv0; r0 += RB) {
+        __syncthreads();
+        // the entries' twiddle columns T[r0 .. r0 + RB)[p], contiguous in Tt
+        for (int idx = threadIdx.x; idx < 32 * RB; idx += blockDim.x) {
+            const int e = idx / RB, rr = idx % RB, r = r0 + rr;
+            const bool ok = e < bk.y && r < F.nv0;
+            ta[rr][e] = ok ? Tt[(int64_t)sp1[e] * F.nv0 + r] : make_float2(0.f, 0.f);
+            tb[rr][e] = ok ? Tt[(int64_t)sp2[e] * F.nv0 + r] : make_float2(0.f, 0.f);
         }
-        const __half hr = __float2half_rn(av.x), hi = __float2half_rn(av.y);
-        __half *e = Ahi + (int64_t)(2 * r) * K + col;
-        *reinterpret_cast<__half2 *>(e) = __halves2half2(hr, __hneg(hi));
-        *reinterpret_cast<__half2 *>(e + K) = __halves2half2(hi, hr);
-        if (SPLIT) {
-            const __half lr = __float2half_rn(av.x - __half2float(hr));
-            const __half li = __float2half_rn(av.y - __half2float(hi));
-            __half *o = Alo + (int64_t)(2 * r) * K + col;
-            *reinterpret_cast<__half2 *>(o) = __halves2half2(lr, __hneg(li));
-            *reinterpret_cast<__half2 *>(o + K) = __halves2half2(li, lr);
+        __syncthreads();
+        const float2 sv = ss[lane];
+        for (int rr = warp; rr < RB && r0 + rr < F.nv0; rr += 8) {
+            const int r = r0 + rr;
+            const float2 av = cmul(sv, ta[rr][lane]), bv = tb[rr][lane];
+            const __half hr = __float2half_rn(av.x), hi = __float2half_rn(av.y);
+            __half *e = Ahi + (int64_t)(2 * r) * K + col;
+            *reinterpret_cast<__half2 *>(e) = __halves2half2(hr, __hneg(hi));
+            *reinterpret_cast<__half2 *>(e + K) = __halves2half2(hi, hr);
+            if (SPLIT) {
+                const __half lr = __float2half_rn(av.x - __half2float(hr));
+                const __half li = __float2half_rn(av.y - __half2float(hi));
+                __half *o = Alo + (int64_t)(2 * r) * K + col;
+                *reinterpret_cast<__half2 *>(o) = __halves2half2(lr, __hneg(li));
+                *reinterpret_cast<__half2 *>(o + K) = __halves2half2(li, lr);
+            }
+            *reinterpret_cast<__half2 *>(Bm + (int64_t)r * K + col) =
+                __halves2half2(__float2half_rn(bv.x), __float2half_rn(bv.y));
         }
-        *reinterpret_cast<__half2 *>(Bm + (int64_t)r * K + col) =
-            __halves2half2(__float2half_rn(bv.x), __float2half_rn(bv.y));
     }
 }
 

@@ -149,33 +149,28 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// One 128 x 256 tile of D += (A_hi [+ A_lo]) B^T over num_kb K-blocks of 64.
-// Epilogue of the FourierQuad form (PLANE = true): instead of adding the tile
-// to a D slice, each complex element (real rows 2m, 2m+1 = Re, Im of row
-// r1 = m, column r2) is multiplied by the plane factor exp(zexp0 * tz) of the
-// slice's plane and added atomically into the output U, which is small enough
-// to stay in L2.  zexp0 and U are stored r2-fastest ([r1][r2]) so that a
-// warp's accesses (lane = r2) are contiguous.
+// The FourierQuad plane data of fq_planes_tc_kernel: zexp0 and U are stored
+// r2-fastest ([r1][r2]) so that a warp's accesses (consecutive r2) are
+// contiguous.
 struct PlaneEpi {
     const double2 *zexp0;  // [r1][r2]
     const double *gz;      // plane boundaries
-    const int *planes;     // plane of each slice (blockIdx.y)
+    const int *planes;     // plane of each plane slot
     float *U;              // [r1][r2] complex interleaved FP32, this light
     int nv0;
 };
 
-template <bool SPLIT, bool PLANE = false>
+// One 128 x 256 tile of D += (A_hi [+ A_lo]) B^T over num_kb K-blocks of 64.
+template <bool SPLIT>
 __global__ void __launch_bounds__(128, 1)
 herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
                const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int kb_per_split,
-               int Mr, int N, double *__restrict__ D, int *__restrict__ err, const int2 *__restrict__ kranges,
-               PlaneEpi pe)
+               int Mr, int N, double *__restrict__ D, int *__restrict__ err)
 {
     // split-K: blockIdx.y takes K-blocks [kb0, kb0 + nkb) and owns the slice
-    // D + blockIdx.y * Mr * N; the host makes every slice non-empty.  With
-    // kranges, slice y takes K-blocks [kranges[y].x, kranges[y].x + kranges[y].y).
-    const int kb0 = kranges ? kranges[blockIdx.y].x : (int)blockIdx.y * kb_per_split;
-    const int nkb = kranges ? kranges[blockIdx.y].y : min(num_kb, kb0 + kb_per_split) - kb0;
+    // D + blockIdx.y * Mr * N; the host makes every slice non-empty.
+    const int kb0 = (int)blockIdx.y * kb_per_split;
+    const int nkb = min(num_kb, kb0 + kb_per_split) - kb0;
     if (nkb <= 0) return;
     D += (int64_t)blockIdx.y * Mr * N;
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
@@ -271,12 +266,6 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
         // Epilogue: TMEM -> registers -> smem transpose -> coalesced FP64 RMW.
         float *ep = reinterpret_cast<float *>(base) + warp * 32 * 33;
         const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
-        double tz = 0.0;
-        if (PLANE) {
-            const int pl = pe.planes[blockIdx.y];
-            tz = (pe.gz[pl] + pe.gz[pl + 1]) / 2;
-        }
-        const bool vec4 = PLANE && !(pe.nv0 & 1);
         for (int c0 = 0; c0 < TC_BN; c0 += 32) {
             uint32_t r[32];
             tmem_ld32(tbase + c0, r);
@@ -284,57 +273,15 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
             for (int j = 0; j < 32; ++j) ep[lane * 33 + j] = __uint_as_float(r[j]);
             __syncwarp();
             const int n = col0 + c0 + lane;
-            if (PLANE) {
-                // the chunk's 16 plane-factor exponents in flight together
-                double2 zc[16];
+            // all 32 loads of the chunk in flight before the adds and stores
+            double *p = D + (int64_t)(row0 + warp * 32) * N + n;
+            const int rows = min(32, Mr - (row0 + warp * 32));
+            double v[32];
 #pragma unroll
-                for (int m = 0; m < 16; ++m) {
-                    const int R = row0 + warp * 32 + 2 * m;
-                    zc[m] = (R < Mr && n < N) ? pe.zexp0[(int64_t)(R >> 1) * pe.nv0 + n] : make_double2(0.0, 0.0);
-                }
+            for (int rr = 0; rr < 32; ++rr) v[rr] = (rr < rows && n < N) ? p[(int64_t)rr * N] : 0.0;
 #pragma unroll
-                for (int m = 0; m < 16; ++m) {
-                    const int R = row0 + warp * 32 + 2 * m;  // even: Re row of complex row R / 2
-                    const bool live = R < Mr && n < N;
-                    float vx = 0.f, vy = 0.f;
-                    int64_t q = 0;
-                    if (live) {
-                        const int r1 = R >> 1;
-                        const double re = (double)ep[(2 * m) * 33 + lane], im = (double)ep[(2 * m + 1) * 33 + lane];
-                        q = (int64_t)r1 * pe.nv0 + n;
-                        const double2 z = zc[m];
-                        float sn, cs;
-                        __sincosf((float)reduce_2pi(z.y * tz), &sn, &cs);
-                        const double mag = (double)expf((float)(z.x * tz));
-                        const double fx = mag * cs, fy = mag * sn;
-                        vx = (float)(fx * re - fy * im);
-                        vy = (float)(fx * im + fy * re);
-                    }
-                    // columns n, n + 1 (lanes 2i, 2i + 1) in one 16-byte atomic when
-                    // the row length is even (q even, so U + 2q is 16-byte aligned)
-                    const float wx = __shfl_down_sync(0xffffffffu, vx, 1), wy = __shfl_down_sync(0xffffffffu, vy, 1);
-                    if (live) {
-                        if (!vec4) {
-                            atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * q), make_float2(vx, vy));
-                        } else if (!(lane & 1)) {
-                            if (n + 1 < N)
-                                atomicAdd(reinterpret_cast<float4 *>(pe.U + 2 * q), make_float4(vx, vy, wx, wy));
-                            else
-                                atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * q), make_float2(vx, vy));
-                        }
-                    }
-                }
-            } else {
-                // all 32 loads of the chunk in flight before the adds and stores
-                double *p = D + (int64_t)(row0 + warp * 32) * N + n;
-                const int rows = min(32, Mr - (row0 + warp * 32));
-                double v[32];
-#pragma unroll
-                for (int rr = 0; rr < 32; ++rr) v[rr] = (rr < rows && n < N) ? p[(int64_t)rr * N] : 0.0;
-#pragma unroll
-                for (int rr = 0; rr < 32; ++rr)
-                    if (rr < rows && n < N) p[(int64_t)rr * N] = v[rr] + (double)ep[rr * 33 + lane];
-            }
+            for (int rr = 0; rr < 32; ++rr)
+                if (rr < rows && n < N) p[(int64_t)rr * N] = v[rr] + (double)ep[rr * 33 + lane];
             __syncwarp();
         }
     }
@@ -1223,27 +1170,7 @@ inline void tc_gemm_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, c
     const int kb_per = (num_kb + ksplit - 1) / ksplit;
     const int ks = (num_kb + kb_per - 1) / kb_per;  // every slice non-empty
     herk_tc_kernel<SPLIT><<<dim3((unsigned)n_tiles, (unsigned)ks), 128, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
-        m_ahi, m_alo, m_b, tiles, num_kb, kb_per, Mr, N, D, err, nullptr, PlaneEpi{});
-}
-
-// Slice y = A B^T over the K-blocks kranges[y] (device array of n_slices
-// (first, count) pairs), one slice per y, finished by the PlaneEpi epilogue.
-template <bool SPLIT>
-inline void tc_gemm_planes_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, const CUtensorMap &m_b,
-                                  const int2 *tiles, int n_tiles, const int2 *kranges, int n_slices, int Mr, int N,
-                                  const PlaneEpi &pe, int *err, cudaStream_t st)
-{
-    static std::atomic<uint64_t> attr_set{0};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
-    if (dev >= 64 || !((attr_set.load() >> dev) & 1)) {
-        if (cudaFuncSetAttribute(herk_tc_kernel<SPLIT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 TcCfg<SPLIT>::SMEM_BYTES) != cudaSuccess)
-            throw std::runtime_error("cannot reserve shared memory for the tensor-core kernel");
-        if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
-    }
-    herk_tc_kernel<SPLIT, true><<<dim3((unsigned)n_tiles, (unsigned)n_slices), 128, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
-        m_ahi, m_alo, m_b, tiles, 0, 0, Mr, N, nullptr, err, kranges, pe);
+        m_ahi, m_alo, m_b, tiles, num_kb, kb_per, Mr, N, D, err);
 }
 
 // The plane-loop form: grid (tiles, plane ranges); pranges (device) holds

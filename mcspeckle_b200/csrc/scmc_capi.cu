@@ -225,7 +225,7 @@ struct Ctx {
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
     DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl;
-    DevBuf fq_gz, fq_zexp, fq_zt, fq_box, fq_tw, fq_counts, fq_offsets, fq_cursor, fq_planes;
+    DevBuf fq_gz, fq_zexp, fq_zt, fq_box, fq_tw, fq_twt, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
     // Extra streams and events of the covariance pipeline: the walk and row
@@ -258,8 +258,8 @@ struct Ctx {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
                          &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl,
-                         &out1, &out2, &fq_gz, &fq_zexp, &fq_zt, &fq_box, &fq_tw, &fq_counts, &fq_offsets, &fq_cursor,
-                         &fq_planes};
+                         &out1, &out2, &fq_gz, &fq_zexp, &fq_zt, &fq_box, &fq_tw, &fq_twt, &fq_counts, &fq_offsets,
+                         &fq_cursor, &fq_planes};
         for (DevBuf *b : all) f(*b);
     }
     void set_stream_ordered(cudaStream_t st)
@@ -1269,14 +1269,14 @@ void validate_fq(const scmc_fq_args *a)
 
 // The per-plane DFT sums of one batch on tcgen05 (fq.cuh, tensor-core form),
 // added into U stored [light][r1][r2] in FP32 (each plane's sum is FP32 in
-// TMEM already; vector atomics of 16 bytes).  dzt: zexp0 stored [r1][r2].
+// TMEM already).  Tt: the twiddles stored [p][r]; dzt: zexp0 stored [r1][r2].
 // Nonempty planes are taken in groups of at most kFqTcEntries padded entries
 // (operand memory) and kFqTcPlanes planes.
 constexpr int64_t kFqTcEntries = (int64_t)1 << 18;
 constexpr int kFqTcPlanes = 2048;
 
 void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
-                 const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *T, const double2 *dzt,
+                 const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt, const double2 *dzt,
                  float *U, bool split, cudaStream_t st)
 {
     const int nv0 = F.nv0;
@@ -1352,9 +1352,9 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
             {
                 StageScope sc(ST_ROWS, st);
                 if (split)
-                    fq_tc_rows_kernel<true><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, T, K, ahi, alo, bm);
+                    fq_tc_rows_kernel<true><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, Tt, K, ahi, alo, bm);
                 else
-                    fq_tc_rows_kernel<false><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, T, K, ahi, alo, bm);
+                    fq_tc_rows_kernel<false><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, Tt, K, ahi, alo, bm);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
@@ -1493,12 +1493,22 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     CK(cudaMemcpyAsync(dl, a->l, 3 * a->nl * sizeof(double), cudaMemcpyHostToDevice, st));
     F.gz = dgz;
     F.l = dl;
+    // MIXED / FP16 with at least 64 angles per axis: the per-plane sums on tcgen05
+    const bool use_tc = POL == PMIX && (a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16) &&
+                        Nv >= 64;
+    // the tensor-core rows read the twiddles transposed, [p][r]
+    float2 *Tt = use_tc ? reinterpret_cast<float2 *>(c.fq_twt.ensure(Nv * Nx * sizeof(float2))) : nullptr;
     {
         StageScope sc(ST_ROWS, st);
-        fq_twiddle_kernel<Cx><<<std::max<int64_t>(1, std::min<int64_t>((Nv * Nx + 255) / 256, 4096)), 256, 0, st>>>(
-            (int)Nv, (int)Nx, M, nx_pad, nv_pad, T);
+        const int tg = (int)std::max<int64_t>(1, std::min<int64_t>((Nv * Nx + 255) / 256, 4096));
+        fq_twiddle_kernel<Cx><<<tg, 256, 0, st>>>((int)Nv, (int)Nx, M, nx_pad, nv_pad, T, 0);
         CK(cudaGetLastError());
         LAUNCHED();
+        if (use_tc) {
+            fq_twiddle_kernel<float2><<<tg, 256, 0, st>>>((int)Nv, (int)Nx, M, nx_pad, nv_pad, Tt, 1);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
     }
     // the walk: isotropic, phase per event, padded box (lines 146-213)
     WalkParams W{};
@@ -1534,9 +1544,6 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     const int sms = sm_count(c.device);
     int64_t total_vert = 0;
     const int passes = a->do_cbs ? 2 : 1;
-    // MIXED / FP16 with at least 64 angles per axis: the per-plane sums on tcgen05
-    const bool use_tc = POL == PMIX && (a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16) &&
-                        Nv >= 64;
     for (int64_t done = 0; done < a->max_itr;) {
         const int64_t nb = std::min<int64_t>(a->max_itr - done, (int64_t)1 << 18);
         W.path_base = a->path_offset + (uint64_t)done;
@@ -1579,8 +1586,8 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
             LAUNCHED();
         }
         if (use_tc) {
-            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, reinterpret_cast<const float2 *>(T), dzt,
-                        reinterpret_cast<float *>(U), a->precision == SCMC_PREC_MIXED, st);
+            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dzt, reinterpret_cast<float *>(U),
+                        a->precision == SCMC_PREC_MIXED, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
             for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
