@@ -35,6 +35,7 @@ struct HGrid {
     const double *alb;       // prod(nb) albedos or nullptr
     double alb_scalar;
     double bmin[3], bmax[3], bbin[3];
+    double ibbin[3];         // 1 / bbin (the attenuation march)
     int nb[3];
     double sigt_max;
     // first-scatter sampling

@@ -1136,6 +1136,7 @@ Prepared prepare_hetero(Ctx &c, const scmc_hetero_args *h, int want_phase, bool 
         g.bmin[k] = mc.box_min[k];
         g.bmax[k] = mc.box_max[k];
         g.bbin[k] = h->box_bin[k];
+        g.ibbin[k] = 1.0 / g.bbin[k];
         g.nb[k] = (int)std::llround((g.bmax[k] - g.bmin[k]) / g.bbin[k]);  // findBin.m:4
         if (g.nb[k] < 1) fail(SCMC_ERR_INVALID, "the box holds no voxel");
         nv *= g.nb[k];
