@@ -443,6 +443,18 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
         const int r1 = R >> 1;
         const bool re_row = !(lane & 1), row_ok = R < Mr;
         const int jb = re_row ? 0 : 16;  // the pair's even lane forms the factors of columns 0-15, the odd 16-31
+        // zexp0 does not depend on the plane: the next chunk's 16 values are
+        // loaded while the current chunk is processed (chunk 0 of the next
+        // plane while the plane's MMAs run)
+        double2 zn[16];
+        auto load_z = [&](int c0) {
+#pragma unroll
+            for (int t = 0; t < 16; ++t) {
+                const int n = col0 + c0 + jb + t;
+                zn[t] = (row_ok && n < N) ? pe.zexp0[(int64_t)r1 * pe.nv0 + n] : make_double2(0.0, 0.0);
+            }
+        };
+        load_z(0);
         for (int pi = 0; pi < pr.y; ++pi) {
             // the four warps agree on a timeout before leaving the loop, so
             // that every named barrier below is reached by all of them
@@ -458,10 +470,8 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
             for (int c0 = 0; c0 < TC_BN; c0 += 32) {
                 double2 zc[16];
 #pragma unroll
-                for (int t = 0; t < 16; ++t) {
-                    const int n = col0 + c0 + jb + t;
-                    zc[t] = (row_ok && n < N) ? pe.zexp0[(int64_t)r1 * pe.nv0 + n] : make_double2(0.0, 0.0);
-                }
+                for (int t = 0; t < 16; ++t) zc[t] = zn[t];
+                load_z(c0 + 32 < TC_BN ? c0 + 32 : 0);
                 uint32_t a[32], sm[32];
                 tmem_ld32(tacc + c0, a);
                 if (pi > 0) {
