@@ -149,11 +149,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// The FourierQuad plane data of fq_planes_tc_kernel: zexp0 and U are stored
-// r2-fastest ([r1][r2]) so that a warp's accesses (consecutive r2) are
-// contiguous.
+// The FourierQuad plane data of fq_planes_tc_kernel.  zexp0 is stored
+// r1-fastest ([r2][r1]): a warp's lanes hold 16 consecutive rows r1 at one
+// column, so its loads are contiguous.  U is stored [r1][r2].
 struct PlaneEpi {
-    const double2 *zexp0;  // [r1][r2]
+    const double2 *zexp0;  // [r2][r1]
     const double *gz;      // plane boundaries
     const int *planes;     // plane of each plane slot
     float *U;              // [r1][r2] complex interleaved FP32, this light
@@ -451,7 +451,7 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
 #pragma unroll
             for (int t = 0; t < 16; ++t) {
                 const int n = col0 + c0 + jb + t;
-                zn[t] = (row_ok && n < N) ? pe.zexp0[(int64_t)r1 * pe.nv0 + n] : make_double2(0.0, 0.0);
+                zn[t] = (row_ok && n < N) ? pe.zexp0[(int64_t)n * pe.nv0 + r1] : make_double2(0.0, 0.0);
             }
         };
         load_z(0);

@@ -225,7 +225,7 @@ struct Ctx {
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
     DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl;
-    DevBuf fq_gz, fq_zexp, fq_zt, fq_box, fq_tw, fq_twt, fq_counts, fq_offsets, fq_cursor, fq_planes;
+    DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_twt, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
     // Extra streams and events of the covariance pipeline: the walk and row
@@ -258,7 +258,7 @@ struct Ctx {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
                          &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl,
-                         &out1, &out2, &fq_gz, &fq_zexp, &fq_zt, &fq_box, &fq_tw, &fq_twt, &fq_counts, &fq_offsets,
+                         &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_twt, &fq_counts, &fq_offsets,
                          &fq_cursor, &fq_planes};
         for (DevBuf *b : all) f(*b);
     }
@@ -1270,14 +1270,14 @@ void validate_fq(const scmc_fq_args *a)
 
 // The per-plane DFT sums of one batch on tcgen05 (fq.cuh, tensor-core form),
 // added into U stored [light][r1][r2] in FP32 (each plane's sum is FP32 in
-// TMEM already).  Tt: the twiddles stored [p][r]; dzt: zexp0 stored [r1][r2].
+// TMEM already).  Tt: the twiddles stored [p][r]; dz: zexp0 stored [r2][r1].
 // Nonempty planes are taken in groups of at most kFqTcEntries padded entries
 // (operand memory) and kFqTcPlanes planes.
 constexpr int64_t kFqTcEntries = (int64_t)1 << 18;
 constexpr int kFqTcPlanes = 2048;
 
 void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
-                 const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt, const double2 *dzt,
+                 const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt, const double2 *dz,
                  float *U, bool split, cudaStream_t st)
 {
     const int nv0 = F.nv0;
@@ -1304,15 +1304,17 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
             ++g1;
         }
         const int64_t K = 64 * nblk;
-        // plane ranges of about equal K blocks, about one CTA per SM over the tiles
+        // plane ranges of about equal work, about one CTA per SM over the tiles;
+        // a plane costs its K blocks plus a fixed epilogue of about kFqPlaneCost
         std::vector<int2> prs;
         {
+            constexpr int64_t kFqPlaneCost = 4;
             const int want = std::max(1, std::min((int)gpl.size(), sm_count(c.device) / std::max(1, (int)tiles.size())));
-            const int64_t per = (nblk + want - 1) / want;
+            const int64_t per = (nblk + kFqPlaneCost * (int64_t)gpl.size() + want - 1) / want;
             int first = 0;
             int64_t acc = 0;
             for (int i = 0; i < (int)gpl.size(); ++i) {
-                acc += kr[i].y;
+                acc += kr[i].y + kFqPlaneCost;
                 if (acc >= per || i + 1 == (int)gpl.size()) {
                     prs.push_back(make_int2(first, i - first + 1));
                     first = i + 1;
@@ -1361,7 +1363,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
             }
             {
                 StageScope sc(ST_CONTRACT, st);
-                const PlaneEpi pe{dzt, F.gz, d_pl, U + 2 * (int64_t)nv0 * nv0 * j, nv0};
+                const PlaneEpi pe{dz, F.gz, d_pl, U + 2 * (int64_t)nv0 * nv0 * j, nv0};
                 if (split)
                     tc_gemm_plane_loop_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, d_pr,
                                                     (int)prs.size(), Mr, nv0, pe, d_err, st);
@@ -1484,12 +1486,6 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     Cx *T = reinterpret_cast<Cx *>(c.fq_tw.ensure(Nv * Nx * sizeof(Cx)));
     CK(cudaMemcpyAsync(dgz, gz.data(), Nz * sizeof(double), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dz, zexp0.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
-    // [r1][r2] copy of zexp0 for the tensor-core form
-    std::vector<double2> zexp0t(Nv * Nv);
-    for (int64_t r1 = 0; r1 < Nv; ++r1)
-        for (int64_t r2 = 0; r2 < Nv; ++r2) zexp0t[r2 + Nv * r1] = zexp0[r1 + Nv * r2];
-    double2 *dzt = reinterpret_cast<double2 *>(c.fq_zt.ensure(Nv * Nv * sizeof(double2)));
-    CK(cudaMemcpyAsync(dzt, zexp0t.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(db, boxexp0.data(), Nv * Nv * sizeof(double2), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dl, a->l, 3 * a->nl * sizeof(double), cudaMemcpyHostToDevice, st));
     F.gz = dgz;
@@ -1587,7 +1583,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
             LAUNCHED();
         }
         if (use_tc) {
-            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dzt, reinterpret_cast<float *>(U),
+            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, reinterpret_cast<float *>(U),
                         a->precision == SCMC_PREC_MIXED, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
