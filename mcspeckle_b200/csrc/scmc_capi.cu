@@ -1285,69 +1285,83 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
     std::vector<int2> tiles;
     for (int tn = 0; tn < (nv0 + TC_BN - 1) / TC_BN; ++tn)
         for (int tm = 0; tm < (Mr + TC_BM - 1) / TC_BM; ++tm) tiles.push_back(make_int2(tm, tn));
-    size_t g0 = 0;
-    while (g0 < hplanes.size()) {
+    // Every group's metadata is built first and uploaded in one copy, so the
+    // groups then run back to back with one synchronisation at the end.
+    struct Group {
+        int64_t nblk, blk0, kr0, pl0, pr0;
+        int n_pl, n_pr;
+        int64_t entries;
+    };
+    std::vector<Group> groups;
+    std::vector<int2> blk, kr, prs;
+    std::vector<int> gpl;
+    int64_t max_nblk = 0;
+    constexpr int64_t kFqPlaneCost = 4;  // a plane's epilogue, in K blocks, for balancing the plane ranges
+    const int want_max = std::max(1, sm_count(c.device) / std::max(1, (int)tiles.size()));
+    for (size_t g0 = 0; g0 < hplanes.size();) {
         // group [g0, g1): blocks of 32 entries per plane
-        std::vector<int2> blk, kr;
-        std::vector<int> gpl;
+        Group G{0, (int64_t)blk.size(), (int64_t)kr.size(), (int64_t)gpl.size(), (int64_t)prs.size(), 0, 0, 0};
         size_t g1 = g0;
-        int64_t nblk = 0;
-        while (g1 < hplanes.size() && (int)gpl.size() < kFqTcPlanes) {
+        while (g1 < hplanes.size() && G.n_pl < kFqTcPlanes) {
             const int p = hplanes[g1];
             const int cnt = hcounts[p];
             const int nb = (cnt + 31) / 32;
-            if (!gpl.empty() && (nblk + nb) * 32 > kFqTcEntries) break;
-            kr.push_back(make_int2((int)nblk, nb));
+            if (G.n_pl > 0 && (G.nblk + nb) * 32 > kFqTcEntries) break;
+            kr.push_back(make_int2((int)G.nblk, nb));
             for (int b = 0; b < nb; ++b) blk.push_back(make_int2(hoff[p] + 32 * b, std::min(32, cnt - 32 * b)));
             gpl.push_back(p);
-            nblk += nb;
+            G.nblk += nb;
+            G.entries += cnt;
+            ++G.n_pl;
             ++g1;
         }
-        const int64_t K = 64 * nblk;
-        // plane ranges of about equal work, about one CTA per SM over the tiles;
-        // a plane costs its K blocks plus a fixed epilogue of about kFqPlaneCost
-        std::vector<int2> prs;
-        {
-            constexpr int64_t kFqPlaneCost = 4;
-            const int want = std::max(1, std::min((int)gpl.size(), sm_count(c.device) / std::max(1, (int)tiles.size())));
-            const int64_t per = (nblk + kFqPlaneCost * (int64_t)gpl.size() + want - 1) / want;
-            int first = 0;
-            int64_t acc = 0;
-            for (int i = 0; i < (int)gpl.size(); ++i) {
-                acc += kr[i].y + kFqPlaneCost;
-                if (acc >= per || i + 1 == (int)gpl.size()) {
-                    prs.push_back(make_int2(first, i - first + 1));
-                    first = i + 1;
-                    acc = 0;
-                }
+        // plane ranges of about equal work (K blocks plus a fixed cost per
+        // plane), about one CTA per SM over the tiles
+        const int want = std::min(G.n_pl, want_max);
+        const int64_t per = (G.nblk + kFqPlaneCost * G.n_pl + want - 1) / want;
+        int first = 0;
+        int64_t acc = 0;
+        for (int i = 0; i < G.n_pl; ++i) {
+            acc += kr[G.kr0 + i].y + kFqPlaneCost;
+            if (acc >= per || i + 1 == G.n_pl) {
+                prs.push_back(make_int2(first, i - first + 1));
+                first = i + 1;
+                acc = 0;
             }
         }
-        const size_t ab = tc_align((size_t)Mr * K * sizeof(__half)), bb = tc_align((size_t)nv0 * K * sizeof(__half));
-        const size_t meta = tc_align(tiles.size() * sizeof(int2)) + tc_align(kr.size() * sizeof(int2)) +
-                            tc_align(blk.size() * sizeof(int2)) + tc_align(gpl.size() * sizeof(int)) +
-                            tc_align(prs.size() * sizeof(int2)) + 1024;
-        char *mem = reinterpret_cast<char *>(c.tc_a.ensure((split ? 2 : 1) * ab + bb + meta));
-        __half *ahi = reinterpret_cast<__half *>(mem);
-        __half *alo = split ? reinterpret_cast<__half *>(mem + ab) : ahi;
-        __half *bm = reinterpret_cast<__half *>(mem + (split ? 2 : 1) * ab);
-        char *q = mem + (split ? 2 : 1) * ab + bb;
-        int2 *d_tiles = reinterpret_cast<int2 *>(q);
-        q += tc_align(tiles.size() * sizeof(int2));
-        int2 *d_kr = reinterpret_cast<int2 *>(q);
-        q += tc_align(kr.size() * sizeof(int2));
-        int2 *d_blk = reinterpret_cast<int2 *>(q);
-        q += tc_align(blk.size() * sizeof(int2));
-        int *d_pl = reinterpret_cast<int *>(q);
-        q += tc_align(gpl.size() * sizeof(int));
-        int2 *d_pr = reinterpret_cast<int2 *>(q);
-        q += tc_align(prs.size() * sizeof(int2));
-        int *d_err = reinterpret_cast<int *>(q);
-        CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_kr, kr.data(), kr.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_blk, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_pl, gpl.data(), gpl.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d_pr, prs.data(), prs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-        CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+        G.n_pr = (int)(prs.size() - G.pr0);
+        max_nblk = std::max(max_nblk, G.nblk);
+        groups.push_back(G);
+        g0 = g1;
+    }
+    if (groups.empty()) return;
+    const int64_t Kmax = 64 * max_nblk;
+    const size_t ab = tc_align((size_t)Mr * Kmax * sizeof(__half)), bb = tc_align((size_t)nv0 * Kmax * sizeof(__half));
+    // metadata: tiles, blocks, K ranges, planes, plane ranges, error flag
+    const size_t o_tiles = 0, o_blk = o_tiles + tc_align(tiles.size() * sizeof(int2));
+    const size_t o_kr = o_blk + tc_align(blk.size() * sizeof(int2));
+    const size_t o_pl = o_kr + tc_align(kr.size() * sizeof(int2));
+    const size_t o_pr = o_pl + tc_align(gpl.size() * sizeof(int));
+    const size_t o_err = o_pr + tc_align(prs.size() * sizeof(int2));
+    const size_t meta = o_err + 1024;
+    char *mem = reinterpret_cast<char *>(c.tc_a.ensure((split ? 2 : 1) * ab + bb + meta));
+    __half *ahi = reinterpret_cast<__half *>(mem);
+    __half *alo = split ? reinterpret_cast<__half *>(mem + ab) : ahi;
+    __half *bm = reinterpret_cast<__half *>(mem + (split ? 2 : 1) * ab);
+    char *dmeta = mem + (split ? 2 : 1) * ab + bb;
+    std::vector<char> hmeta(o_err, 0);
+    std::memcpy(hmeta.data() + o_tiles, tiles.data(), tiles.size() * sizeof(int2));
+    std::memcpy(hmeta.data() + o_blk, blk.data(), blk.size() * sizeof(int2));
+    std::memcpy(hmeta.data() + o_kr, kr.data(), kr.size() * sizeof(int2));
+    std::memcpy(hmeta.data() + o_pl, gpl.data(), gpl.size() * sizeof(int));
+    std::memcpy(hmeta.data() + o_pr, prs.data(), prs.size() * sizeof(int2));
+    CK(cudaMemcpyAsync(dmeta, hmeta.data(), o_err, cudaMemcpyHostToDevice, st));
+    int2 *d_tiles = reinterpret_cast<int2 *>(dmeta + o_tiles), *d_blk = reinterpret_cast<int2 *>(dmeta + o_blk);
+    int2 *d_kr = reinterpret_cast<int2 *>(dmeta + o_kr), *d_pr = reinterpret_cast<int2 *>(dmeta + o_pr);
+    int *d_pl = reinterpret_cast<int *>(dmeta + o_pl), *d_err = reinterpret_cast<int *>(dmeta + o_err);
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    for (const Group &G : groups) {
+        const int64_t K = 64 * G.nblk;
         const CUtensorMap m_ahi = tc_map(ahi, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
         const CUtensorMap m_alo = tc_map(alo, (uint64_t)K, (uint64_t)Mr, (uint64_t)K * 2, TC_BM);
         const CUtensorMap m_b = tc_map(bm, (uint64_t)K, (uint64_t)nv0, (uint64_t)K * 2, TC_BN);
@@ -1355,32 +1369,33 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
             {
                 StageScope sc(ST_ROWS, st);
                 if (split)
-                    fq_tc_rows_kernel<true><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, Tt, K, ahi, alo, bm);
+                    fq_tc_rows_kernel<true><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K, ahi,
+                                                                                alo, bm);
                 else
-                    fq_tc_rows_kernel<false><<<(unsigned)nblk, 256, 0, st>>>(F, Es, d_blk, j, Tt, K, ahi, alo, bm);
+                    fq_tc_rows_kernel<false><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K, ahi,
+                                                                                 alo, bm);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
             {
                 StageScope sc(ST_CONTRACT, st);
-                const PlaneEpi pe{dz, F.gz, d_pl, U + 2 * (int64_t)nv0 * nv0 * j, nv0};
+                const PlaneEpi pe{dz, F.gz, d_pl + G.pl0, U + 2 * (int64_t)nv0 * nv0 * j, nv0};
                 if (split)
-                    tc_gemm_plane_loop_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, d_pr,
-                                                    (int)prs.size(), Mr, nv0, pe, d_err, st);
+                    tc_gemm_plane_loop_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr + G.kr0,
+                                                    d_pr + G.pr0, G.n_pr, Mr, nv0, pe, d_err, st);
                 else
-                    tc_gemm_plane_loop_launch<false>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr, d_pr,
-                                                     (int)prs.size(), Mr, nv0, pe, d_err, st);
+                    tc_gemm_plane_loop_launch<false>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr + G.kr0,
+                                                     d_pr + G.pr0, G.n_pr, Mr, nv0, pe, d_err, st);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
-            prof_count(0, 0, 8.0 * (double)nv0 * nv0 * (double)(hoff[gpl.back() + 1] - hoff[gpl.front()]));
+            prof_count(0, 0, 8.0 * (double)nv0 * nv0 * (double)G.entries);
         }
-        int herr = 0;
-        CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));  // the group's host vectors and operand memory are reused
-        if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
-        g0 = g1;
     }
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));  // the operand memory and metadata are reused by the next batch
+    if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
 }
 
 // Wl == null: MCfieldFourierQuad.m.  Wl (nl complex, host): MCfieldFourierQuadOnWave.m,
