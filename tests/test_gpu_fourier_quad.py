@@ -98,6 +98,25 @@ def test_fourier_quad_tensor_cores_close_to_fp64(gpu, name, precision):
     assert rel(u, u64) < 1e-3
 
 
+def test_fourier_quad_tensor_cores_several_plane_groups(gpu):
+    """More entries than one group of the tensor-core form holds (2^18), so a
+    batch's plane groups run back to back from one metadata upload."""
+    from mcspeckle_b200 import _lib
+    c = dict(TC_CASES["tc_wide_cbs"], n=150000)
+    u64 = FQ.field_fourier_quad_from_args(args_for(c, "fp64"))
+    h = args_for(c, "fp16")
+    _lib.profile_read(reset=True)
+    _lib.profile_enable(True)
+    try:
+        u = FQ.field_fourier_quad_from_args(h)
+    finally:
+        _lib.profile_enable(False)
+    prof = _lib.profile_read(reset=True)
+    entries = prof["contract_flops"] / (8.0 * h.nv0 * h.nv0)
+    assert entries > 2 ** 18
+    assert rel(u, u64) < 1e-3
+
+
 def test_fourier_quad_tensor_cores_fp64_anchor(gpu, oracle_lib):
     """The FP64 reference of the tensor-core tests is the oracle's estimator."""
     h = args_for(TC_CASES["tc_wide_cbs"], "fp64")
