@@ -568,8 +568,10 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
 // leader's MMA commits arrive on both CTAs' barriers (commit multicast).
 // Every wait is bounded as in herk_tc_kernel.
 // ---------------------------------------------------------------------------
+// Two 64 KB stages (FP16) leave room on the SM for a row-generation CTA of
+// the next chunk (about 72 KB at 64 x 64); three measured no faster.
 #ifndef SCMC_PAIR_STAGES_FP16
-#define SCMC_PAIR_STAGES_FP16 3
+#define SCMC_PAIR_STAGES_FP16 2
 #endif
 constexpr int TC2_TMEM_COLS = 512;  // Re C and Im C, 256 columns each
 template <bool SPLIT> struct Tc2Cfg {
