@@ -389,7 +389,7 @@ def workload_spec(name):
         return ("MCfieldFourierQuad, box 50x50x10 MFP (MFP 100 wavelengths), sigma_a 0.005 per MFP, plane wave "
                 "along +z, 256x256 angular grid (v_max 255/256, v_stp 1/128: 0.5-wavelength lateral pitch), CBS; "
                 "isotropic as the reference (HG g=0.9 and the point source are not built)",
-                make, dev, FQ.field_fourier_quad_from_args, [2 * 256 * 256], oracle, "herk_tc_kernel<PLANE>")
+                make, dev, FQ.field_fourier_quad_from_args, [2 * 256 * 256], oracle, "fq_planes_tc_kernel")
     if name == "hetero128":
         mfp = 10.0
         g = np.random.default_rng(4)
