@@ -134,18 +134,23 @@ int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream);
  * device memory while they call in: a process that reserved its GPU memory
  * budget up front, a real-time loop that must not take the allocator's locks
  * or let cudaFree synchronise the device, or a host thread on which
- * cudaMalloc / cudaFree are not allowed.  Same computation as
+ * cudaMalloc / cudaFree are not allowed.  Same estimator as
  * scmc_field_device, with every piece of device scratch in one fixed 32 MiB
  * array inside the library, which each GPU that loads the library holds
  * until the process exits.  No counterpart in the reference (MATLAB manages
  * memory for its callers).
  * d_u: device memory, 2*nv*nl doubles.  Limits: nv*nl <= 65536, tabulated
  * tables <= 16384 entries, and no single path longer than the scratch holds
- * (about 400k events); beyond them it returns SCMC_ERR_INVALID.  The first
- * call on a device looks up the array's device address, so make that call
- * before any stream capture.  All calls share the array and it keeps the
- * previous call's contents (each call clears what must start at zero); calls
- * whose work overlaps on the GPU race. */
+ * (about 400k events); beyond them it returns SCMC_ERR_INVALID.  The
+ * accumulation is always the CUDA-core one: in MIXED / FP16 mode with
+ * nv >= 64 and nl >= 32, where scmc_field_device uses tensor cores, the two
+ * agree within the mixed tolerance rather than bit for bit.  The first call on
+ * a device looks up the array's device address, so make that call before any
+ * stream capture.  All calls share the array and it keeps the previous call's
+ * contents (each call clears what must start at zero); two calls whose work
+ * overlapped on the GPU would race on it, so the library serialises the calls
+ * on one device and returns only after the call's work on `stream` has
+ * finished (on an error return too). */
 int scmc_field_noalloc(const scmc_mc_args *args, double *d_u, void *stream);
 
 /* ---------------------------------------------------------------------------

@@ -357,7 +357,11 @@ PhaseFn upload_pf(const scmc_phase_function &pf, DevBuf &amp, DevBuf &icdf, cuda
     return d;
 }
 
-Prepared prepare(Ctx &c, const scmc_mc_args *a, int want_phase, cudaStream_t st)
+// The host-side parameters of a solve (MCfield.m:71-110, MCcov.m:78-110):
+// everything except the device copies of the tables and directions, which
+// the caller places (prepare: allocated scratch; scmc_field_noalloc: the fixed
+// array) and then points W.pf / W.pf0 / Q.{l, v, vs, pf, pf0} at.
+Prepared host_params(const scmc_mc_args *a, int want_phase)
 {
     Prepared P{};
     const int dim = a->dim;
@@ -391,10 +395,63 @@ Prepared prepare(Ctx &c, const scmc_mc_args *a, int want_phase, cudaStream_t st)
     W.key0 = (uint32_t)a->seed;
     W.key1 = (uint32_t)(a->seed >> 32);
     W.max_events = a->max_events_per_path;
+    W.pf.sct_type = a->ampfunc.sct_type;
+    W.pf.g = a->ampfunc.g;
+    W.pf.table_n = a->ampfunc.table_n;
+    W.pf0 = W.pf;
+    if (a->has_ampfunc0) {
+        W.pf0.sct_type = a->ampfunc0.sct_type;
+        W.pf0.g = a->ampfunc0.g;
+        W.pf0.table_n = a->ampfunc0.table_n;
+    }
 
-    W.pf = upload_pf(a->ampfunc, c.tab0_amp, c.tab0_icdf, st);
-    if (a->has_ampfunc0) W.pf0 = upload_pf(a->ampfunc0, c.tab1_amp, c.tab1_icdf, st);
-    else W.pf0 = W.pf;
+    NeeParams &Q = P.Q;
+    Q.nv = (int)a->nv;
+    Q.nl = (int)a->nl;
+    Q.is_ff_l = a->is_ff_l;
+    Q.is_ff_v = a->is_ff_v;
+    Q.cbs = a->do_cbs;
+    Q.sigt_half = a->sigt / 2.0;
+    Q.kw = SCMC_PI * 2.0 / a->lambda;
+    Q.lambda = a->lambda;
+    for (int k = 0; k < 3; ++k) {
+        Q.box_min[k] = W.box_min[k];
+        Q.box_max[k] = W.box_max[k];
+        Q.meanl[k] = W.meanl[k];
+    }
+    nee_set_fbox(Q);
+    Q.has_pf0 = a->has_ampfunc0;
+    return P;
+}
+
+// Points the phase functions of P at their device tables (amp0/icdf0 for
+// ampfunc, amp1/icdf1 for ampfunc0; null where a function is not tabulated).
+void set_tables(Prepared &P, const scmc_mc_args *a, const double2 *amp0, const double *icdf0, const double2 *amp1,
+                const double *icdf1)
+{
+    if (a->ampfunc.sct_type == SCMC_SCT_TABULATED) {
+        P.W.pf.eval_amp = amp0;
+        P.W.pf.sample_icdf = icdf0;
+    }
+    if (a->has_ampfunc0) {
+        if (a->ampfunc0.sct_type == SCMC_SCT_TABULATED) {
+            P.W.pf0.eval_amp = amp1;
+            P.W.pf0.sample_icdf = icdf1;
+        }
+    } else {
+        P.W.pf0 = P.W.pf;
+    }
+    P.Q.pf = P.W.pf;
+    P.Q.pf0 = P.W.pf0;
+}
+
+Prepared prepare(Ctx &c, const scmc_mc_args *a, int want_phase, cudaStream_t st)
+{
+    Prepared P = host_params(a, want_phase);
+    const int dim = a->dim;
+    const PhaseFn d0 = upload_pf(a->ampfunc, c.tab0_amp, c.tab0_icdf, st);
+    const PhaseFn d1 = a->has_ampfunc0 ? upload_pf(a->ampfunc0, c.tab1_amp, c.tab1_icdf, st) : PhaseFn{};
+    set_tables(P, a, d0.eval_amp, d0.sample_icdf, d1.eval_amp, d1.sample_icdf);
 
     // directions as [n][3]
     std::vector<double> hl(3 * a->nl, 0.0), hv(3 * a->nv, 0.0), hvs(3 * a->nv, 0.0);
@@ -412,28 +469,9 @@ Prepared prepare(Ctx &c, const scmc_mc_args *a, int want_phase, cudaStream_t st)
     CK(cudaMemcpyAsync(c.dirs_l.p, hl.data(), hl.size() * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c.dirs_v.p, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(c.dirs_vs.p, hvs.data(), hvs.size() * 8, cudaMemcpyHostToDevice, st));
-
-    NeeParams &Q = P.Q;
-    Q.nv = (int)a->nv;
-    Q.nl = (int)a->nl;
-    Q.is_ff_l = a->is_ff_l;
-    Q.is_ff_v = a->is_ff_v;
-    Q.cbs = a->do_cbs;
-    Q.sigt_half = a->sigt / 2.0;
-    Q.kw = SCMC_PI * 2.0 / a->lambda;
-    Q.lambda = a->lambda;
-    for (int k = 0; k < 3; ++k) {
-        Q.box_min[k] = W.box_min[k];
-        Q.box_max[k] = W.box_max[k];
-        Q.meanl[k] = W.meanl[k];
-    }
-    nee_set_fbox(Q);
-    Q.l = c.dirs_l.as<double>();
-    Q.v = c.dirs_v.as<double>();
-    Q.vs = c.dirs_vs.as<double>();
-    Q.has_pf0 = a->has_ampfunc0;
-    Q.pf = W.pf;
-    Q.pf0 = W.pf0;
+    P.Q.l = c.dirs_l.as<double>();
+    P.Q.v = c.dirs_v.as<double>();
+    P.Q.vs = c.dirs_vs.as<double>();
     // the host copies above must complete before the vectors go out of scope
     CK(cudaStreamSynchronize(st));
     return P;
@@ -2185,19 +2223,24 @@ int scmc_sample_cov(const double *C, int64_t N, int64_t n_samples, uint64_t seed
 //
 // Some callers cannot allocate device memory while they call in: a host that
 // runs under a pre-reserved memory budget (a serving process that sized its
-// pools at start-up), a real-time caller that must not
-// take the allocator's locks, or an embedding runtime that forbids
-// cudaMalloc/cudaFree on its threads.  This entry point serves them: it calls
-// no cudaMalloc, cudaFree or allocating library routine; the caller passes
-// the inputs (host struct) and the output (device memory).
+// pools at start-up), a real-time caller that must not take the allocator's
+// locks or let cudaFree synchronise the device, or an embedding runtime that
+// forbids cudaMalloc/cudaFree on its threads.  This entry point serves them:
+// it calls no cudaMalloc, cudaFree or allocating library routine; the caller
+// passes the inputs (host struct) and the output (device memory).
 //
 // Limits (SCMC_ERR_INVALID beyond them): nv*nl <= 65536, each tabulated
 // table <= 16384 entries, and no single path may have more scattering events
 // than the scratch holds (~400k).  The scratch is 32 MiB per device and stays
 // resident in every GPU that loads the library until the process exits.
 // Every call shares it and it keeps the previous call's contents: the
-// accumulators and counters are cleared at the start of each call, and calls
-// whose work overlaps on the GPU (two host threads, or two streams) race.
+// accumulators and counters are cleared at the start of each call.  Two calls
+// whose work overlapped on the GPU would race on the array, so calls on one
+// device are serialised: a per-device lock is held until the call's work on
+// its stream has finished, on an error return too.  The accumulation is
+// always the CUDA-core one (field_accum_kernel); in MIXED / FP16 mode with
+// nv >= 64 and nl >= 32 scmc_field_device uses the tensor-core form instead,
+// so there the two agree to the mixed tolerance, not bit for bit.
 // The first call on a device looks up the array's device address
 // (cudaGetSymbolAddress) with that device current; make that first call
 // before any stream capture.
@@ -2207,18 +2250,14 @@ static __device__ __align__(256) unsigned char g_field_scratch[kFieldScratchByte
 
 namespace {
 
+constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-void *g_scratch_addr[64] = {};
-
-std::mutex &g_scratch_mu_call()
-{
-    static std::mutex m;
-    return m;
-}
+void *g_scratch_addr[kMaxDevices] = {};
+std::mutex g_scratch_call_mu[kMaxDevices];  // one per device: calls on different GPUs run concurrently
 
 unsigned char *field_scratch(int device)
 {
-    if (device < 0 || device >= 64) fail(SCMC_ERR_INVALID, "invalid device ordinal");
+    if (device < 0 || device >= kMaxDevices) fail(SCMC_ERR_INVALID, "invalid device ordinal");
     std::lock_guard<std::mutex> lk(g_scratch_mu);
     if (!g_scratch_addr[device]) {
         void *p = nullptr;
@@ -2253,22 +2292,23 @@ struct ScratchCarve {
     size_t left() const { return cap > off ? cap - off : 0; }
 };
 
-PhaseFn noalloc_pf(const scmc_phase_function &pf, ScratchCarve &sc, cudaStream_t st)
+constexpr int32_t kNoallocMaxTable = 16384;
+
+// A tabulated function's evalAmp / sampleIcdf copied into the scratch.
+void noalloc_table(const scmc_phase_function &pf, ScratchCarve &sc, cudaStream_t st, const double2 **amp,
+                   const double **icdf)
 {
-    PhaseFn d{};
-    d.sct_type = pf.sct_type;
-    d.g = pf.g;
-    d.table_n = pf.table_n;
-    if (pf.sct_type == SCMC_SCT_TABULATED) {
-        if (pf.table_n > 16384) fail(SCMC_ERR_INVALID, "scmc_field_noalloc: tabulated tables are limited to 16384 entries");
-        double2 *amp = sc.take<double2>(pf.table_n);
-        double *icdf = sc.take<double>(pf.table_n);
-        CK(cudaMemcpyAsync(amp, pf.eval_amp, pf.table_n * sizeof(double2), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(icdf, pf.sample_icdf, pf.table_n * sizeof(double), cudaMemcpyHostToDevice, st));
-        d.eval_amp = amp;
-        d.sample_icdf = icdf;
-    }
-    return d;
+    *amp = nullptr;
+    *icdf = nullptr;
+    if (pf.sct_type != SCMC_SCT_TABULATED) return;
+    if (pf.table_n > kNoallocMaxTable)
+        fail(SCMC_ERR_INVALID, "scmc_field_noalloc: tabulated tables are limited to 16384 entries");
+    double2 *a = sc.take<double2>(pf.table_n);
+    double *c = sc.take<double>(pf.table_n);
+    CK(cudaMemcpyAsync(a, pf.eval_amp, pf.table_n * sizeof(double2), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c, pf.sample_icdf, pf.table_n * sizeof(double), cudaMemcpyHostToDevice, st));
+    *amp = a;
+    *icdf = c;
 }
 
 template <int DIM, int POL, typename AccT>
@@ -2279,38 +2319,15 @@ void field_noalloc_run(const scmc_mc_args *a, double2 *d_u, cudaStream_t st)
     sc.cap = kFieldScratchBytes;
     const int nv = (int)a->nv, nl = (int)a->nl;
 
-    // parameters, as prepare() builds them, with the inputs placed in scratch
-    WalkParams W{};
-    W.dim = dim;
-    W.smp_flg = a->smp_flg;
-    W.has_pf0 = a->has_ampfunc0;
-    W.want_phase = 1;
-    W.sigt = a->sigt;
-    W.albedo = a->albedo;
-    double volume = 1.0;
-    for (int k = 0; k < 3; ++k) {
-        W.box_min[k] = k < dim ? a->box_min[k] : 0.0;
-        W.box_max[k] = k < dim ? a->box_max[k] : 0.0;
-        W.box_w[k] = W.box_max[k] - W.box_min[k];
-        if (k < dim) volume *= W.box_w[k];
-    }
-    double nrm = 0.0;
-    for (int k = 0; k < 3; ++k) {
-        double s = 0.0;
-        if (k < dim)
-            for (int64_t j = 0; j < a->nl; ++j) s += a->l[dim * j + k];
-        W.unmeanl[k] = k < dim ? (a->has_lmean0 ? a->lmean0[k] : s / (double)a->nl) : 0.0;
-        nrm += W.unmeanl[k] * W.unmeanl[k];
-    }
-    nrm = std::sqrt(nrm);
-    for (int k = 0; k < 3; ++k) W.meanl[k] = W.unmeanl[k] / nrm;
-    if (a->smp_flg == 2 && W.unmeanl[dim - 1] == 0.0)
-        fail(SCMC_ERR_INVALID, "exponential first-scatter sampling needs a mean light direction with a non-zero last component");
-    W.key0 = (uint32_t)a->seed;
-    W.key1 = (uint32_t)(a->seed >> 32);
-    W.max_events = a->max_events_per_path;
-    W.pf = noalloc_pf(a->ampfunc, sc, st);
-    W.pf0 = a->has_ampfunc0 ? noalloc_pf(a->ampfunc0, sc, st) : W.pf;
+    // parameters as prepare() builds them, with the inputs placed in scratch
+    Prepared P = host_params(a, 1);
+    const double2 *amp0, *amp1 = nullptr;
+    const double *icdf0, *icdf1 = nullptr;
+    noalloc_table(a->ampfunc, sc, st, &amp0, &icdf0);
+    if (a->has_ampfunc0) noalloc_table(a->ampfunc0, sc, st, &amp1, &icdf1);
+    set_tables(P, a, amp0, icdf0, amp1, icdf1);
+    WalkParams W = P.W;
+    const NeeParams &Q = P.Q;
 
     // raw dim x n inputs into scratch, then packed to [n][3] on the device
     double *raw_l = sc.take<double>((size_t)dim * nl), *raw_v = sc.take<double>((size_t)dim * nv);
@@ -2322,28 +2339,9 @@ void field_noalloc_run(const scmc_mc_args *a, double2 *d_u, cudaStream_t st)
     CK(cudaGetLastError());
     LAUNCHED();
     LAUNCHED();
-
-    NeeParams Q{};
-    Q.nv = nv;
-    Q.nl = nl;
-    Q.is_ff_l = a->is_ff_l;
-    Q.is_ff_v = a->is_ff_v;
-    Q.cbs = a->do_cbs;
-    Q.sigt_half = a->sigt / 2.0;
-    Q.kw = SCMC_PI * 2.0 / a->lambda;
-    Q.lambda = a->lambda;
-    for (int k = 0; k < 3; ++k) {
-        Q.box_min[k] = W.box_min[k];
-        Q.box_max[k] = W.box_max[k];
-        Q.meanl[k] = W.meanl[k];
-    }
-    nee_set_fbox(Q);
-    Q.l = dl;
-    Q.v = dv;
-    Q.vs = dvs;
-    Q.has_pf0 = a->has_ampfunc0;
-    Q.pf = W.pf;
-    Q.pf0 = W.pf0;
+    P.Q.l = dl;
+    P.Q.v = dv;
+    P.Q.vs = dvs;
 
     // accumulators, counters and the scan's temporary storage
     const int64_t n = (int64_t)nv * nl;
@@ -2435,7 +2433,7 @@ void field_noalloc_run(const scmc_mc_args *a, double2 *d_u, cudaStream_t st)
         done += nb;
     }
     const double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
-    const double norm = m > 0 ? std::sqrt(1.0 / m * volume * a->sigt) : 0.0;
+    const double norm = m > 0 ? std::sqrt(1.0 / m * P.volume * a->sigt) : 0.0;  // MCfield.m:253-254
     const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1024));
     field_finalize_kernel<DIM, AccT><<<fgrid, 256, 0, st>>>(Q, Us, Um, norm, d_u);
     CK(cudaGetLastError());
@@ -2453,21 +2451,29 @@ extern "C" int scmc_field_noalloc(const scmc_mc_args *args, double *d_u, void *s
             fail(SCMC_ERR_INVALID, "scmc_field_noalloc: nv*nl is limited to 65536 by its fixed scratch");
         int ndev = 0, major = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) fail(SCMC_ERR_NODEVICE, "no CUDA device visible");
-        if (args->device < 0 || args->device >= ndev) fail(SCMC_ERR_INVALID, "invalid device ordinal");
+        if (args->device < 0 || args->device >= ndev || args->device >= kMaxDevices)
+            fail(SCMC_ERR_INVALID, "invalid device ordinal");
         CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, args->device));
         if (major < 10) fail(SCMC_ERR_NODEVICE, "an sm_100 (Blackwell) device is required");
         CK(cudaSetDevice(args->device));
-        std::lock_guard<std::mutex> lk(g_scratch_mu_call());
+        std::lock_guard<std::mutex> lk(g_scratch_call_mu[args->device]);
         cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
         double2 *u = reinterpret_cast<double2 *>(d_u);
-        if (args->dim == 3) {
-            if (args->precision == SCMC_PREC_FP64) field_noalloc_run<3, P64, double>(args, u, st);
-            else if (args->precision == SCMC_PREC_FP32) field_noalloc_run<3, P32, float>(args, u, st);
-            else field_noalloc_run<3, PMIX, double>(args, u, st);
-        } else {
-            if (args->precision == SCMC_PREC_FP64) field_noalloc_run<2, P64, double>(args, u, st);
-            else if (args->precision == SCMC_PREC_FP32) field_noalloc_run<2, P32, float>(args, u, st);
-            else field_noalloc_run<2, PMIX, double>(args, u, st);
+        try {
+            if (args->dim == 3) {
+                if (args->precision == SCMC_PREC_FP64) field_noalloc_run<3, P64, double>(args, u, st);
+                else if (args->precision == SCMC_PREC_FP32) field_noalloc_run<3, P32, float>(args, u, st);
+                else field_noalloc_run<3, PMIX, double>(args, u, st);
+            } else {
+                if (args->precision == SCMC_PREC_FP64) field_noalloc_run<2, P64, double>(args, u, st);
+                else if (args->precision == SCMC_PREC_FP32) field_noalloc_run<2, P32, float>(args, u, st);
+                else field_noalloc_run<2, PMIX, double>(args, u, st);
+            }
+        } catch (...) {
+            // work this call already enqueued still uses the shared array:
+            // let it finish before the lock is released
+            (void)cudaStreamSynchronize(st);
+            throw;
         }
         CK(cudaStreamSynchronize(st));
     });

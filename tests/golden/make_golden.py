@@ -6,7 +6,8 @@ never copied) through the MATLAB-subset interpreter in mlite.py, with
 arguments, the consumed prefix of each tape and the outputs.  The oracle,
 fed the same tapes, must reproduce these outputs (tests/test_oracle_golden.py).
 
-Usage (in a container that has the reference tree):
+Usage (in a container that has the reference tree; the path is required,
+as an argument or in SCMC_REFERENCE_TREE):
     python tests/golden/make_golden.py /path/to/mcspeckle
 """
 from __future__ import annotations
@@ -498,7 +499,10 @@ def only_onwave(ref):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref = args[0] if args else "/root/reference"
+    ref = args[0] if args else os.environ.get("SCMC_REFERENCE_TREE")
+    if not ref:
+        sys.exit("usage: make_golden.py <path of the mcspeckle tree> [--only-...] "
+                 "(or set SCMC_REFERENCE_TREE)")
     if "--only-onwave" in sys.argv:
         only_onwave(ref)
     elif "--only-refocus" in sys.argv:
