@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define SCMC_ABI_VERSION 1
+#define SCMC_ABI_VERSION 2
 
 typedef enum {
     SCMC_OK = 0,
@@ -115,6 +115,15 @@ typedef struct {
     uint64_t path_offset;
     int32_t precision;
     int32_t device;
+    /* --- extensions (zero = the reference's isotropic plane-wave form) --- */
+    int32_t light_point;       /* 1: l holds point-source positions; each vertex's light factor is
+                                  evalphaseatt.m:10-16's near-field term (phase k|x - s|, attenuation
+                                  sigt/2 min(cubeDist, |x - s|), 1/(|x - s| + 0.01 lambda)) instead of the
+                                  plane wave of MCfieldFourierQuad.m:272 */
+    int32_t sct_type;          /* 0 or SCMC_SCT_ISOTROPIC: isotropic walk (MCfieldFourierQuad.m:208);
+                                  SCMC_SCT_HG: scattering directions sampled from HG(g) as
+                                  smpampfunc_general does (the call left commented out at line 208) */
+    double g;
 } scmc_fq_args;
 
 /* ---------------------------------------------------------------------------
@@ -404,6 +413,15 @@ int scmc_abi_version(void);
 const char *scmc_last_error(void);
 /* Kernel launches issued by this process since load (all entry points). */
 int64_t scmc_launch_count(void);
+
+/* Failure injection for the bounded device waits, for tests; no counterpart
+ * in the reference.  While on (process-wide), every tensor-core kernel
+ * (covariance, field, FourierQuad plane loop) issues no copy and its
+ * consumers wait 1 ms instead of 2 s, so each such launch gives up, flags
+ * its error, frees its tensor memory and returns, and the call reports
+ * SCMC_ERR_TIMEOUT.  Nothing is in flight when the waits give up, and the
+ * context stays usable: switch it off and the next call is correct. */
+int scmc_test_wait_fault(int32_t on);
 
 #ifdef __cplusplus
 }

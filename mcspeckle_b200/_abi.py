@@ -89,6 +89,9 @@ class FqArgs(C.Structure):
         ("path_offset", C.c_uint64),
         ("precision", C.c_int32),
         ("device", C.c_int32),
+        ("light_point", C.c_int32),
+        ("sct_type", C.c_int32),
+        ("g", C.c_double),
     ]
 
 

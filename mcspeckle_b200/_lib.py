@@ -85,6 +85,8 @@ def lib():
                                    C.c_int32, dp]
         L.scmc_sample_cov.argtypes = [dp, C.c_int64, C.c_int64, C.c_uint64, C.c_int32, dp]
         L.scmc_profile_enable.argtypes = [C.c_int32]
+        L.scmc_test_wait_fault.argtypes = [C.c_int32]
+        L.scmc_test_wait_fault.restype = C.c_int
         L.scmc_profile_read.argtypes = [C.POINTER(_abi.StageTimes), C.c_int32]
         for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",
                      "scmc_export_records", "scmc_philox_stream", "scmc_profile_enable", "scmc_profile_read",

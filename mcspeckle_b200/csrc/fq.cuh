@@ -37,10 +37,16 @@ struct FqParams {
     // MCfieldFourierQuadOnWave: lights combined with weights wl (nl of them)
     // into one output light; null for MCfieldFourierQuad
     const double2 *wl = nullptr;
+    // extension: l holds point-source positions and each vertex's light factor
+    // is evalphaseatt.m:10-16's near-field term, evaluated through phaseatt
+    // with the walk's (padded) box in `nf`
+    int light_point = 0;
+    NeeParams nf{};
 };
 
 // The light factor of an entry for output light j (MCfieldFourierQuad.m:272):
-// exp(i k l_j.xl - sigt/2 * slab attenuation); with weights
+// exp(i k l_j.xl - sigt/2 * slab attenuation); for a point source at l_j
+// (extension) the near-field evalphaseatt term; with weights
 // (MCfieldFourierQuadOnWave.m:278-302) sum_j wl_j exp(i vsign k l_j.xl) times
 // the same attenuation.  Phases are reduced mod 2 pi in FP64 outside P64.
 template <int POL>
@@ -52,6 +58,9 @@ fq_light_factor(const FqParams &F, int j, const double *xl)
     const double at = F.sigt_half * ((xl[2] - F.bmin_z) * F.l_diratt + (F.bmax_z - xl[2]) * F.l_idiratt);
     const int j0 = F.wl ? 0 : j, j1 = F.wl ? F.nl : j + 1;
     C sum = C{};
+    if (F.light_point) {  // one point source per output light (the OnWave form has none)
+        return phaseatt<3, POL>(xl, F.l + 3 * j, 0, F.nf);
+    }
     for (int jj = j0; jj < j1; ++jj) {
         const double *lj = F.l + 3 * jj;
         const double ph = F.lsign * F.kw * (lj[0] * xl[0] + lj[1] * xl[1] + lj[2] * xl[2]);

@@ -82,13 +82,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait: false after TC_WAIT_NS without the phase completing.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// Bounded wait: false after `limit` ns (TC_WAIT_NS by default) without the
+// phase completing.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned long long limit = TC_WAIT_NS)
 {
     if (mbar_try_wait(bar, parity)) return true;
     unsigned long long t0 = global_ns();
     while (!mbar_try_wait(bar, parity)) {
-        if (global_ns() - t0 > TC_WAIT_NS) return false;
+        if (global_ns() - t0 > limit) return false;
     }
     return true;
 }
@@ -149,23 +150,35 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// The FourierQuad plane data of fq_planes_tc_kernel.  zexp0 is stored
-// r1-fastest ([r2][r1]): a warp's lanes hold 16 consecutive rows r1 at one
-// column, so its loads are contiguous.  U is stored [r1][r2].
+// The FourierQuad plane data of fq_planes_tc_kernel.  zexp0 and rr are
+// stored r1-fastest ([r2][r1]): a warp's lanes hold 16 consecutive rows r1 at
+// one column, so its loads are contiguous.  U is stored [r1][r2].
 struct PlaneEpi {
-    const double2 *zexp0;  // [r2][r1]
+    const double2 *zexp0;  // [r2][r1]: the plane factor is exp(zexp0 * tz)
+    const float2 *rr;      // [r2][r1]: exp(zexp0 * 2 z_bin), the factor between planes P and P - 2
     const double *gz;      // plane boundaries
     const int *planes;     // plane of each plane slot
     float *U;              // [r1][r2] complex interleaved FP32, this light
     int nv0;
+    int n_uniform;         // planes 0 .. n_uniform-1 have centres bmin_z + (P + 1/2) z_bin
 };
+
+// Bounded waits can be made to run out on purpose (scmc_test_wait_fault):
+// the producer then issues no copy and the consumers wait only this long, so
+// the abort path runs with nothing in flight.
+constexpr unsigned long long TC_TEST_WAIT_NS = 1000000ull;  // 1 ms
+inline std::atomic<int> &tc_test_fault()
+{
+    static std::atomic<int> on{0};
+    return on;
+}
 
 // One 128 x 256 tile of D += (A_hi [+ A_lo]) B^T over num_kb K-blocks of 64.
 template <bool SPLIT>
 __global__ void __launch_bounds__(128, 1)
 herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
                const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles, int num_kb, int kb_per_split,
-               int Mr, int N, double *__restrict__ D, int *__restrict__ err)
+               int Mr, int N, double *__restrict__ D, int *__restrict__ err, int test_fault)
 {
     // split-K: blockIdx.y takes K-blocks [kb0, kb0 + nkb) and owns the slice
     // D + blockIdx.y * Mr * N; the host makes every slice non-empty.
@@ -208,9 +221,10 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
+    const unsigned long long wait_ns = test_fault ? TC_TEST_WAIT_NS : TC_WAIT_NS;
     if (warp == 0 && lane == 0) {
-        // TMA producer
-        for (int kb = 0; kb < nkb; ++kb) {
+        // TMA producer (none in a fault test)
+        for (int kb = 0; kb < (test_fault ? 0 : nkb); ++kb) {
             const int s = kb % TcCfg<SPLIT>::STAGES;
             if (kb >= TcCfg<SPLIT>::STAGES && !mbar_wait(&empty[s], ((kb / TcCfg<SPLIT>::STAGES) - 1) & 1)) {
                 atomicExch(abort_flag, 1);
@@ -230,7 +244,7 @@ herk_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant
         constexpr uint32_t idesc = umma_idesc_f16(TC_BM, TC_BN);
         for (int kb = 0; kb < nkb; ++kb) {
             const int s = kb % TcCfg<SPLIT>::STAGES;
-            if (!mbar_wait(&full[s], (kb / TcCfg<SPLIT>::STAGES) & 1)) {
+            if (!mbar_wait(&full[s], (kb / TcCfg<SPLIT>::STAGES) & 1, wait_ns)) {
                 atomicExch(abort_flag, 1);
                 break;
             }
@@ -315,24 +329,41 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32
 // The FourierQuad per-plane sums with the plane loop inside the CTA.
 //
 // A CTA owns one 128 x 256 tile (64 complex rows r1 as Re / Im real rows,
-// 256 columns r2) and a contiguous range of planes of a group (pranges[y]:
-// first plane slot, plane count; kranges[slot]: the plane's K blocks, which
-// are contiguous across slots).  TMEM columns 0-255 hold the current plane's
-// sum F_P (FP32), columns 256-511 the running sum  sum_P exp(zexp0 tz_P) F_P.
-// Warp 0 streams every K block of the range through the 4-stage ring, warp 1
-// issues the MMAs of one plane and commits acc_full, warps 4-7 (one TMEM lane
-// quarter each) multiply the plane's sum by its factor, add it into the
-// running sum and arrive on acc_empty, after which the next plane's MMAs
-// start; the producer keeps loading meanwhile.  The running sum is added into
-// U once per CTA.  The plane factor follows the PlaneEpi form: FP64 product
-// and reduction of the phase, FP32 sincos and exp.  Every wait is bounded.
+// 256 columns r2) and a contiguous range of plane slots of a group
+// (pranges[y]: first slot, slot count; kranges[slot]: the plane's K blocks,
+// contiguous across slots).  It needs  sum_P exp(zexp0 tz_P) F_P  over its
+// planes, F_P the plane's product A_P B_P^T.  The planes are walked from the
+// deepest down, alternately into two accumulators of 256 TMEM columns
+// (chain 0: slots 0, 2, 4, ... of the walk; chain 1: slots 1, 3, ...), each
+// summed Horner-wise: after plane P's MMAs, when the chain's next plane is
+// P - 2 (uniform planes, planes are 2 z_bin apart), the epilogue multiplies
+// the accumulator in place by rr = exp(zexp0 2 z_bin) in FP32 and the next
+// plane's MMAs add on top, so the chain holds sum_k rr^(m-k) F_(P_k).  When
+// the chain's next plane is not P - 2 (an empty plane, the last,
+// non-uniform plane, the end of the range) or the segment reached
+// kFqSegMax planes, the epilogue adds exp(zexp0 tz_P) times the
+// accumulator into U (factor with the phase product and reduction in FP64,
+// sincos and exp in FP32) and the chain's next MMA starts it afresh.  While
+// the epilogue works on one chain the MMAs of the other run.
+// Warp 0 issues the TMA loads of every K block in walk order through the
+// ring, warp 1 the MMAs, warps 4-7 (one TMEM lane quarter each) the
+// epilogue.  Every wait is bounded.
 // ---------------------------------------------------------------------------
+constexpr int kFqSegMax = 64;  // chain steps between FP64-seeded flushes
+
+// Whether a chain continues from plane p_hi (segment of seg_len planes so
+// far) to the chain's next plane p_lo.
+__device__ __forceinline__ bool fq_chain_continues(int p_hi, int p_lo, int seg_len, int n_uniform)
+{
+    return p_hi - p_lo == 2 && p_hi < n_uniform && seg_len < kFqSegMax;
+}
+
 template <bool SPLIT>
 __global__ void __launch_bounds__(256, 1)
 fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
                     const __grid_constant__ CUtensorMap tm_b, const int2 *__restrict__ tiles,
                     const int2 *__restrict__ kranges, const int2 *__restrict__ pranges, int Mr, int N,
-                    PlaneEpi pe, int *__restrict__ err)
+                    const __grid_constant__ PlaneEpi pe, int *__restrict__ err, int test_fault)
 {
     using Cfg = TcCfg<SPLIT>;
     constexpr int S = Cfg::STAGES;
@@ -340,9 +371,9 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
     uint64_t *full = reinterpret_cast<uint64_t *>(base + S * Cfg::STAGE_BYTES);
     uint64_t *empty = full + S;
-    uint64_t *acc_full = empty + S;
-    uint64_t *acc_empty = acc_full + 1;
-    uint64_t *done = acc_empty + 1;
+    uint64_t *acc_full = empty + S;   // [2], one per chain
+    uint64_t *acc_empty = acc_full + 2;
+    uint64_t *done = acc_empty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
     int *issued = abort_flag + 1;
@@ -353,17 +384,18 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
     const int row0 = tile.x * TC_BM;
     const int col0 = tile.y * TC_BN;
     const int2 pr = pranges[blockIdx.y];  // the host makes every range non-empty
-    const int kb_first = kranges[pr.x].x;
-    const int2 klast = kranges[pr.x + pr.y - 1];
-    const int nkb = klast.x + klast.y - kb_first;
+    const int last = pr.x + pr.y - 1;     // the walk goes from slot `last` down to pr.x
+    const unsigned long long wait_ns = test_fault ? TC_TEST_WAIT_NS : TC_WAIT_NS;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(acc_full, 1);
-        mbar_init(acc_empty, 1);
+        for (int c = 0; c < 2; ++c) {
+            mbar_init(&acc_full[c], 1);
+            mbar_init(&acc_empty[c], 1);
+        }
         mbar_init(done, 1);
         *abort_flag = 0;
         *issued = 0;
@@ -382,39 +414,56 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0 && lane == 0) {
-        // TMA producer: every K block of the plane range
-        for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb % S;
-            if (kb >= S && !mbar_wait(&empty[s], ((kb / S) - 1) & 1)) {
-                atomicExch(abort_flag, 1);
-                break;
+        // TMA producer: the K blocks of every plane, deepest plane first
+        int kb = 0;
+        bool stop = test_fault != 0;  // fault test: no copy is ever issued
+        for (int i = 0; i < pr.y && !stop; ++i) {
+            const int2 kr = kranges[last - i];
+            for (int j = 0; j < kr.y; ++j, ++kb) {
+                const int s = kb % S;
+                if (kb >= S && !mbar_wait(&empty[s], ((kb / S) - 1) & 1)) {
+                    atomicExch(abort_flag, 1);
+                    stop = true;
+                    break;
+                }
+                if (*(volatile int *)abort_flag) {
+                    stop = true;
+                    break;
+                }
+                uint8_t *st = base + s * Cfg::STAGE_BYTES;
+                mbar_expect_tx(&full[s], Cfg::STAGE_BYTES);
+                const int kx = (kr.x + j) * TC_BK;
+                tma_load_2d(st, &tm_ahi, kx, row0, &full[s]);
+                if (SPLIT) tma_load_2d(st + TC_A_BYTES, &tm_alo, kx, row0, &full[s]);
+                tma_load_2d(st + Cfg::B_OFF, &tm_b, kx, col0, &full[s]);
+                *(volatile int *)issued = kb + 1;
             }
-            if (*(volatile int *)abort_flag) break;
-            uint8_t *st = base + s * Cfg::STAGE_BYTES;
-            mbar_expect_tx(&full[s], Cfg::STAGE_BYTES);
-            const int kx = (kb_first + kb) * TC_BK;
-            tma_load_2d(st, &tm_ahi, kx, row0, &full[s]);
-            if (SPLIT) tma_load_2d(st + TC_A_BYTES, &tm_alo, kx, row0, &full[s]);
-            tma_load_2d(st + Cfg::B_OFF, &tm_b, kx, col0, &full[s]);
-            *(volatile int *)issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
-        // MMA issuer: one plane at a time into columns 0-255
+        // MMA issuer: plane slot i of the walk into chain i & 1
         constexpr uint32_t idesc = umma_idesc_f16(TC_BM, TC_BN);
         int kb = 0;
         bool ok = true;
-        for (int pi = 0; pi < pr.y && ok; ++pi) {
-            const int nk = kranges[pr.x + pi].y;
-            if (pi > 0) {
-                if (!mbar_wait(acc_empty, (pi - 1) & 1)) {
+        int prev[2] = {0, 0}, seg[2] = {0, 0};
+        for (int i = 0; i < pr.y && ok; ++i) {
+            const int c = i & 1;
+            const int slot = last - i;
+            const int P = pe.planes[slot];
+            const bool start = i < 2 || !fq_chain_continues(prev[c], P, seg[c], pe.n_uniform);
+            seg[c] = start ? 1 : seg[c] + 1;
+            prev[c] = P;
+            if (i >= 2) {  // the epilogue has released this chain's accumulator
+                if (!mbar_wait(&acc_empty[c], ((i >> 1) - 1) & 1, wait_ns)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
             }
+            const uint32_t tacc = tmem + (uint32_t)(c * TC_TMEM_COLS);
+            const int nk = kranges[slot].y;
             for (int j = 0; j < nk; ++j, ++kb) {
                 const int s = kb % S;
-                if (!mbar_wait(&full[s], (kb / S) & 1)) {
+                if (!mbar_wait(&full[s], (kb / S) & 1, wait_ns)) {
                     ok = false;
                     break;
                 }
@@ -426,84 +475,98 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
 #pragma unroll
                 for (int kk = 0; kk < TC_BK / 16; ++kk) {
                     const uint64_t adv = (uint64_t)(kk * 32) >> 4;
-                    umma_f16(tmem, dh + adv, db + adv, idesc, (j | kk) != 0);
-                    if (SPLIT) umma_f16(tmem, dl + adv, db + adv, idesc, 1u);
+                    umma_f16(tacc, dh + adv, db + adv, idesc, (start && j == 0 && kk == 0) ? 0u : 1u);
+                    if (SPLIT) umma_f16(tacc, dl + adv, db + adv, idesc, 1u);
                 }
                 umma_commit(&empty[s]);
             }
-            if (ok) umma_commit(acc_full);
+            if (ok) umma_commit(&acc_full[c]);
         }
         if (!ok) atomicExch(abort_flag, 1);
         umma_commit(done);  // fires once every issued MMA has completed
     } else if (warp >= 4) {
-        // plane epilogue: TMEM lane = real row row0 + 32 q + lane (Re rows even, Im rows odd)
+        // epilogue: TMEM lane = real row row0 + 32 q + lane (Re rows even, Im
+        // rows odd).  The lane pair (2i, 2i + 1) shares complex row r1: the
+        // even lane produces columns t, the odd lane columns 16 + t of each
+        // 32-column chunk, and they swap halves so each stores its own row.
         const int q = warp - 4;
-        const uint32_t tacc = tmem + ((uint32_t)(q * 32) << 16), tsum = tacc + TC_TMEM_COLS;
         const int R = row0 + q * 32 + lane;
         const int r1 = R >> 1;
-        const bool re_row = !(lane & 1), row_ok = R < Mr;
-        const int jb = re_row ? 0 : 16;  // the pair's even lane forms the factors of columns 0-15, the odd 16-31
-        // zexp0 does not depend on the plane: the next chunk's 16 values are
-        // loaded while the current chunk is processed (chunk 0 of the next
-        // plane while the plane's MMAs run)
-        double2 zn[16];
-        auto load_z = [&](int c0) {
-#pragma unroll
-            for (int t = 0; t < 16; ++t) {
-                const int n = col0 + c0 + jb + t;
-                zn[t] = (row_ok && n < N) ? pe.zexp0[(int64_t)n * pe.nv0 + r1] : make_double2(0.0, 0.0);
-            }
-        };
-        load_z(0);
-        for (int pi = 0; pi < pr.y; ++pi) {
+        const bool odd = lane & 1, row_ok = R < Mr;
+        const int jb = odd ? 16 : 0;
+        int prev[2] = {0, 0}, seg[2] = {0, 0};
+        for (int i = 0; i < pr.y; ++i) {
+            const int c = i & 1;
+            const int slot = last - i;
+            const int P = pe.planes[slot];
+            const bool start = i < 2 || !fq_chain_continues(prev[c], P, seg[c], pe.n_uniform);
+            seg[c] = start ? 1 : seg[c] + 1;
+            prev[c] = P;
+            const bool cont = i + 2 < pr.y && fq_chain_continues(P, pe.planes[slot - 2], seg[c], pe.n_uniform);
             // the four warps agree on a timeout before leaving the loop, so
             // that every named barrier below is reached by all of them
-            if (!__all_sync(0xffffffffu, mbar_wait(acc_full, pi & 1)) && lane == 0) atomicExch(ep_fail, 1);
+            if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[c], (i >> 1) & 1, wait_ns)) && lane == 0)
+                atomicExch(ep_fail, 1);
             asm volatile("bar.sync 1, 128;" ::: "memory");
             if (*(volatile int *)ep_fail) {
                 atomicExch(abort_flag, 1);
                 break;
             }
             tc_fence_after();
-            const int pl = pe.planes[pr.x + pi];
-            const double tz = (pe.gz[pl] + pe.gz[pl + 1]) / 2;
+            const uint32_t tacc = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * TC_TMEM_COLS);
+            const double tz = (pe.gz[P] + pe.gz[P + 1]) / 2;
             for (int c0 = 0; c0 < TC_BN; c0 += 32) {
-                double2 zc[16];
-#pragma unroll
-                for (int t = 0; t < 16; ++t) zc[t] = zn[t];
-                load_z(c0 + 32 < TC_BN ? c0 + 32 : 0);
-                uint32_t a[32], sm[32];
+                uint32_t a[32];
                 tmem_ld32(tacc + c0, a);
-                if (pi > 0) {
-                    tmem_ld32(tsum + c0, sm);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) sm[j] = 0u;
-                }
+                // this lane's column n = col0 + c0 + jb + t: its own value and
+                // the partner's (Re, Im) of the same complex element
+                float fx[16], fy[16];
 #pragma unroll
                 for (int t = 0; t < 16; ++t) {
-                    float sn, cs;
-                    __sincosf((float)reduce_2pi(zc[t].y * tz), &sn, &cs);
-                    const float mag = expf((float)(zc[t].x * tz));
-                    const float fx = mag * cs, fy = mag * sn;
-                    const float ox = __shfl_xor_sync(0xffffffffu, fx, 1), oy = __shfl_xor_sync(0xffffffffu, fy, 1);
-                    // factor of column t and of column 16 + t
-                    const float gx0 = re_row ? fx : ox, gy0 = re_row ? fy : oy;
-                    const float gx1 = re_row ? ox : fx, gy1 = re_row ? oy : fy;
-                    const float a0 = __uint_as_float(a[t]), a1 = __uint_as_float(a[16 + t]);
-                    const float p0 = __shfl_xor_sync(0xffffffffu, a0, 1), p1 = __shfl_xor_sync(0xffffffffu, a1, 1);
-                    // Re row: Re(F P) = Fx Pre - Fy Pim; Im row: Im(F P) = Fx Pim + Fy Pre
-                    const float v0 = re_row ? gx0 * a0 - gy0 * p0 : gx0 * a0 + gy0 * p0;
-                    const float v1 = re_row ? gx1 * a1 - gy1 * p1 : gx1 * a1 + gy1 * p1;
-                    sm[t] = __float_as_uint(__uint_as_float(sm[t]) + v0);
-                    sm[16 + t] = __float_as_uint(__uint_as_float(sm[16 + t]) + v1);
+                    const int n = col0 + c0 + jb + t;
+                    const bool ok = row_ok && n < N;
+                    if (cont) {
+                        const float2 f = ok ? pe.rr[(int64_t)n * pe.nv0 + r1] : make_float2(0.f, 0.f);
+                        fx[t] = f.x;
+                        fy[t] = f.y;
+                    } else {
+                        const double2 z = ok ? pe.zexp0[(int64_t)n * pe.nv0 + r1] : make_double2(0.0, 0.0);
+                        float sn, cs;
+                        __sincosf((float)reduce_2pi(z.y * tz), &sn, &cs);
+                        const float mag = ok ? expf((float)(z.x * tz)) : 0.f;
+                        fx[t] = mag * cs;
+                        fy[t] = mag * sn;
+                    }
                 }
-                tmem_st32(tsum + c0, sm);
+                uint32_t out[32];
+#pragma unroll
+                for (int t = 0; t < 16; ++t) {
+                    // even lane: element (r1, t) = (a[t], partner's a[t]);
+                    // odd lane: element (r1, 16 + t) = (partner's a[16 + t], a[16 + t])
+                    const float mine = __uint_as_float(odd ? a[16 + t] : a[t]);
+                    const float give = __uint_as_float(odd ? a[t] : a[16 + t]);
+                    const float got = __shfl_xor_sync(0xffffffffu, give, 1);
+                    const float re = odd ? got : mine, im = odd ? mine : got;
+                    const float vr = fx[t] * re - fy[t] * im, vi = fx[t] * im + fy[t] * re;
+                    if (cont) {
+                        // the chain continues: store back, even lane keeps the Re row, odd the Im row
+                        const float send = odd ? vr : vi;
+                        const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+                        out[t] = __float_as_uint(odd ? recv : vr);       // column t of this lane's row
+                        out[16 + t] = __float_as_uint(odd ? vi : recv);  // column 16 + t
+                    } else {
+                        const int n = col0 + c0 + jb + t;
+                        if (row_ok && n < N)
+                            atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * ((int64_t)r1 * pe.nv0 + n)),
+                                      make_float2(vr, vi));
+                    }
+                }
+                if (cont) tmem_st32(tacc + c0, out);
             }
-            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            if (cont) asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
             asm volatile("bar.sync 1, 128;" ::: "memory");
-            if (q == 0 && lane == 0) mbar_arrive(acc_empty);
+            if (q == 0 && lane == 0) mbar_arrive(&acc_empty[c]);
         }
     }
     __syncwarp();
@@ -512,32 +575,12 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
     tc_fence_after();
     __syncthreads();
     const bool failed = !ok || *(volatile int *)abort_flag;
-    if (failed) {
-        if (threadIdx.x == 0) {
-            atomicExch(err, 1);
-            // wait (bounded) for TMA copies this CTA still has in flight
-            const int n_issued = *(volatile int *)issued;
-            for (int kb = (n_issued > S ? n_issued - S : 0); kb < n_issued; ++kb)
-                (void)mbar_wait(&full[kb % S], (kb / S) & 1);
-        }
-    } else if (warp >= 4) {
-        // the running sum into U: (Re, Im) of column n from lanes 2i, 2i + 1
-        const int q = warp - 4;
-        const uint32_t tsum = tmem + ((uint32_t)(q * 32) << 16) + TC_TMEM_COLS;
-        const int R = row0 + q * 32 + lane;
-        const bool row_ok = R < Mr;
-        for (int c0 = 0; c0 < TC_BN; c0 += 32) {
-            uint32_t sm[32];
-            tmem_ld32(tsum + c0, sm);
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const float v = __uint_as_float(sm[j]);
-                const float w = __shfl_down_sync(0xffffffffu, v, 1);
-                const int n = col0 + c0 + j;
-                if (!(lane & 1) && row_ok && n < N)
-                    atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * ((int64_t)(R >> 1) * pe.nv0 + n)), make_float2(v, w));
-            }
-        }
+    if (failed && threadIdx.x == 0) {
+        atomicExch(err, 1);
+        // wait (bounded) for TMA copies this CTA still has in flight
+        const int n_issued = *(volatile int *)issued;
+        for (int kb = (n_issued > S ? n_issued - S : 0); kb < n_issued; ++kb)
+            (void)mbar_wait(&full[kb % S], (kb / S) & 1);
     }
     tc_fence_before();
     __syncthreads();
@@ -649,7 +692,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
 herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant__ CUtensorMap tm_im,
                 const __grid_constant__ CUtensorMap tm_re_lo, const __grid_constant__ CUtensorMap tm_im_lo,
                 const int2 *__restrict__ tiles, int num_kb, int kb_per_split, int N, double *__restrict__ D,
-                int *__restrict__ err)
+                int *__restrict__ err, int test_fault)
 {
     using Cfg = Tc2Cfg<SPLIT>;
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
@@ -696,10 +739,11 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
+    const unsigned long long wait_ns = test_fault ? TC_TEST_WAIT_NS : TC_WAIT_NS;
     if (warp == 0 && lane == 0) {
-        // TMA producer (both CTAs); completion counted on the leader's full[s]
+        // TMA producer (both CTAs; none in a fault test); completion counted on the leader's full[s]
         const uint32_t full0 = mapa_shared(smem_u32(&full[0]), 0);
-        for (int kb = 0; kb < nkb; ++kb) {
+        for (int kb = 0; kb < (test_fault ? 0 : nkb); ++kb) {
             const int s = kb % Cfg::STAGES;
             if (kb >= Cfg::STAGES && !mbar_wait(&empty[s], ((kb / Cfg::STAGES) - 1) & 1)) {
                 atomicExch(abort_flag, 1);
@@ -727,7 +771,7 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
         const uint32_t t_re = tmem, t_im = tmem + 256;
         for (int kb = 0; kb < nkb; ++kb) {
             const int s = kb % Cfg::STAGES;
-            if (!mbar_wait(&full[s], (kb / Cfg::STAGES) & 1)) {
+            if (!mbar_wait(&full[s], (kb / Cfg::STAGES) & 1, wait_ns)) {
                 atomicExch(abort_flag, 1);
                 break;
             }
@@ -1186,7 +1230,7 @@ inline void tc_gemm_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, c
     const int kb_per = (num_kb + ksplit - 1) / ksplit;
     const int ks = (num_kb + kb_per - 1) / kb_per;  // every slice non-empty
     herk_tc_kernel<SPLIT><<<dim3((unsigned)n_tiles, (unsigned)ks), 128, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
-        m_ahi, m_alo, m_b, tiles, num_kb, kb_per, Mr, N, D, err);
+        m_ahi, m_alo, m_b, tiles, num_kb, kb_per, Mr, N, D, err, tc_test_fault().load());
 }
 
 // The plane-loop form: grid (tiles, plane ranges); pranges (device) holds
@@ -1196,6 +1240,7 @@ template <bool SPLIT>
 inline void tc_gemm_plane_loop_launch(const CUtensorMap &m_ahi, const CUtensorMap &m_alo, const CUtensorMap &m_b,
                                       const int2 *tiles, int n_tiles, const int2 *kranges, const int2 *pranges,
                                       int n_ranges, int Mr, int N, const PlaneEpi &pe, int *err, cudaStream_t st)
+// slots of one range must be in increasing plane order; the kernel walks them from the last
 {
     static std::atomic<uint64_t> attr_set{0};
     int dev = 0;
@@ -1207,7 +1252,7 @@ inline void tc_gemm_plane_loop_launch(const CUtensorMap &m_ahi, const CUtensorMa
         if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
     }
     fq_planes_tc_kernel<SPLIT><<<dim3((unsigned)n_tiles, (unsigned)n_ranges), 256, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
-        m_ahi, m_alo, m_b, tiles, kranges, pranges, Mr, N, pe, err);
+        m_ahi, m_alo, m_b, tiles, kranges, pranges, Mr, N, pe, err, tc_test_fault().load());
 }
 
 // D[ks][2N][N] += the planar pair product (Re C in even rows, Im C in odd
@@ -1228,7 +1273,7 @@ inline void tc_gemm2_launch(const TcOperands &o, int num_kb, int ksplit, int N, 
     const int kb_per = (num_kb + ksplit - 1) / ksplit;
     const int ks = (num_kb + kb_per - 1) / kb_per;
     herk_tc2_kernel<SPLIT><<<dim3(2u * (unsigned)o.n_tiles, (unsigned)ks), 128, Tc2Cfg<SPLIT>::SMEM_BYTES, st>>>(
-        o.m_ahi, o.m_ihi, o.m_alo, o.m_ilo, o.tiles, num_kb, kb_per, N, D, o.err);
+        o.m_ahi, o.m_ihi, o.m_alo, o.m_ilo, o.tiles, num_kb, kb_per, N, D, o.err, tc_test_fault().load());
 }
 
 template <bool SPLIT>

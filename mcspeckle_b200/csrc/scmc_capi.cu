@@ -225,7 +225,7 @@ struct Ctx {
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
     DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl;
-    DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_twt, fq_counts, fq_offsets, fq_cursor, fq_planes;
+    DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_twt, fq_rr, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
     // Extra streams and events of the covariance pipeline: the walk and row
@@ -258,7 +258,7 @@ struct Ctx {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
                          &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl,
-                         &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_twt, &fq_counts, &fq_offsets,
+                         &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_twt, &fq_rr, &fq_counts, &fq_offsets,
                          &fq_cursor, &fq_planes};
         for (DevBuf *b : all) f(*b);
     }
@@ -1304,6 +1304,10 @@ void validate_fq(const scmc_fq_args *a)
     if (a->smp_flg != 1 && a->smp_flg != 2) fail(SCMC_ERR_INVALID, "smpFlg must be 1 or 2");
     if (a->precision < 0 || a->precision > 3) fail(SCMC_ERR_INVALID, "invalid precision mode");
     if (colon_count(-a->v_max, a->v_stp, a->v_max) > 4096) fail(SCMC_ERR_INVALID, "angular grid longer than 4096");
+    if (a->light_point != 0 && a->light_point != 1) fail(SCMC_ERR_INVALID, "light_point must be 0 or 1");
+    if (a->sct_type != 0 && a->sct_type != SCMC_SCT_ISOTROPIC && a->sct_type != SCMC_SCT_HG)
+        fail(SCMC_ERR_INVALID, "FourierQuad sct_type must be isotropic or HG");
+    if (a->sct_type == SCMC_SCT_HG && !(std::fabs(a->g) <= 1.0)) fail(SCMC_ERR_INVALID, "Invalid g input");
 }
 
 // The per-plane DFT sums of one batch on tcgen05 (fq.cuh, tensor-core form),
@@ -1311,12 +1315,12 @@ void validate_fq(const scmc_fq_args *a)
 // TMEM already).  Tt: the twiddles stored [p][r]; dz: zexp0 stored [r2][r1].
 // Nonempty planes are taken in groups of at most kFqTcEntries padded entries
 // (operand memory) and kFqTcPlanes planes.
-constexpr int64_t kFqTcEntries = (int64_t)1 << 18;
-constexpr int kFqTcPlanes = 2048;
+constexpr int64_t kFqTcEntries = (int64_t)1 << 20;
+constexpr int kFqTcPlanes = 16384;
 
 void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
                  const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt, const double2 *dz,
-                 float *U, bool split, cudaStream_t st)
+                 const float2 *rr, int n_uniform, float *U, bool split, cudaStream_t st)
 {
     const int nv0 = F.nv0;
     const int Mr = 2 * nv0;
@@ -1334,7 +1338,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
     std::vector<int2> blk, kr, prs;
     std::vector<int> gpl;
     int64_t max_nblk = 0;
-    constexpr int64_t kFqPlaneCost = 4;  // a plane's epilogue, in K blocks, for balancing the plane ranges
+    constexpr int64_t kFqPlaneCost = 1;  // a plane's epilogue step, in K blocks, for balancing the plane ranges
     const int want_max = std::max(1, sm_count(c.device) / std::max(1, (int)tiles.size()));
     for (size_t g0 = 0; g0 < hplanes.size();) {
         // group [g0, g1): blocks of 32 entries per plane
@@ -1417,7 +1421,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
             }
             {
                 StageScope sc(ST_CONTRACT, st);
-                const PlaneEpi pe{dz, F.gz, d_pl + G.pl0, U + 2 * (int64_t)nv0 * nv0 * j, nv0};
+                const PlaneEpi pe{dz, rr, F.gz, d_pl + G.pl0, U + 2 * (int64_t)nv0 * nv0 * j, nv0, n_uniform};
                 if (split)
                     tc_gemm_plane_loop_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr + G.kr0,
                                                     d_pr + G.pr0, G.n_pr, Mr, nv0, pe, d_err, st);
@@ -1508,6 +1512,13 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
         const double m = amp * std::exp(er);
         boxexp0[q] = make_double2(m * std::cos(ei), m * std::sin(ei));
     }
+    // the Horner ratio of the tensor-core form: exp(zexp0 * 2 z_bin), planes P and P - 2
+    std::vector<float2> rrh(Nv * Nv);
+    for (int64_t q = 0; q < Nv * Nv; ++q) {
+        const double m = std::exp(zexp0[q].x * 2 * z_bin), ph = zexp0[q].y * 2 * z_bin;
+        rrh[q] = make_float2((float)(m * std::cos(ph)), (float)(m * std::sin(ph)));
+    }
+    const int n_uniform = (int)(ng - 1);
     const double l_end = a->l[3 * (a->nl - 1) + 2];
 
     FqParams F{};
@@ -1515,6 +1526,19 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     F.nx = (int)Nx;
     F.nz = (int)Nz;
     F.nl = (int)a->nl;
+    if (Wl && a->light_point) fail(SCMC_ERR_INVALID, "point sources are not supported with light weights");
+    F.light_point = a->light_point;
+    if (a->light_point) {
+        NeeParams &Q = F.nf;
+        Q.sigt_half = sigt / 2;
+        Q.kw = twopi / lambda;
+        Q.lambda = lambda;
+        for (int k = 0; k < 3; ++k) {
+            Q.box_min[k] = bmin[k];  // the padded box the walk runs in
+            Q.box_max[k] = bmax[k];
+        }
+        nee_set_fbox(Q);
+    }
     if (Wl) {
         F.lsign = a->vsign;
         F.vsign_vertex = a->vsign;
@@ -1548,6 +1572,8 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
                         Nv >= 64;
     // the tensor-core rows read the twiddles transposed, [p][r]
     float2 *Tt = use_tc ? reinterpret_cast<float2 *>(c.fq_twt.ensure(Nv * Nx * sizeof(float2))) : nullptr;
+    float2 *drr = use_tc ? reinterpret_cast<float2 *>(c.fq_rr.ensure(Nv * Nv * sizeof(float2))) : nullptr;
+    if (use_tc) CK(cudaMemcpyAsync(drr, rrh.data(), Nv * Nv * sizeof(float2), cudaMemcpyHostToDevice, st));
     {
         StageScope sc(ST_ROWS, st);
         const int tg = (int)std::max<int64_t>(1, std::min<int64_t>((Nv * Nx + 255) / 256, 4096));
@@ -1579,7 +1605,11 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     nrm = std::sqrt(nrm);
     for (int k = 0; k < 3; ++k) W.meanl[k] = unmeanl[k] / nrm;
     W.pf.sct_type = SCMC_SCT_ISOTROPIC;
-    W.pf0 = W.pf;
+    W.pf0 = W.pf;  // the first direction stays isotropic (line 171)
+    if (a->sct_type == SCMC_SCT_HG) {  // extension: HG scattering directions (line 208's commented call)
+        W.pf.sct_type = SCMC_SCT_HG;
+        W.pf.g = a->g;
+    }
     W.key0 = (uint32_t)a->seed;
     W.key1 = (uint32_t)(a->seed >> 32);
     const int64_t nout = Nv * Nv * nl_out;
@@ -1595,7 +1625,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     int64_t total_vert = 0;
     const int passes = a->do_cbs ? 2 : 1;
     for (int64_t done = 0; done < a->max_itr;) {
-        const int64_t nb = std::min<int64_t>(a->max_itr - done, (int64_t)1 << 18);
+        const int64_t nb = std::min<int64_t>(a->max_itr - done, (int64_t)1 << 20);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
@@ -1636,8 +1666,8 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
             LAUNCHED();
         }
         if (use_tc) {
-            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, reinterpret_cast<float *>(U),
-                        a->precision == SCMC_PREC_MIXED, st);
+            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
+                        reinterpret_cast<float *>(U), a->precision == SCMC_PREC_MIXED, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
             for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
@@ -1692,6 +1722,12 @@ int scmc_abi_version(void) { return SCMC_ABI_VERSION; }
 const char *scmc_last_error(void) { return g_last_error.c_str(); }
 
 int64_t scmc_launch_count(void) { return g_launches.load(); }
+
+int scmc_test_wait_fault(int32_t on)
+{
+    tc_test_fault().store(on ? 1 : 0);
+    return SCMC_OK;
+}
 
 int scmc_field_device(const scmc_mc_args *args, double *d_u, void *stream)
 {

@@ -8,6 +8,7 @@ u is Nv0 x Nv0 x Nl complex on the angular grid -v_max:v_stp:v_max
 (uniform in sin(theta)).  The first-scatter direction defaults to +z
 (MCfieldFourierQuad.m:59-64), the walk is isotropic, and the normalisation
 counts vertices, as in the reference (MCfieldFourierQuad.m:214, 302-303).
+Keyword-only extensions (fq_args): point sources and HG scattering.
 
 The reference's FFT needs integer padding, which holds only for an odd grid
 length; for even lengths it stops.  The GPU evaluates the same centred-DFT
@@ -48,7 +49,14 @@ class FqHolder:
 
 
 def fq_args(sigt, albedo, box_min, box_max, l, v_max, v_stp, maxItr, lambda_, doCBS, smpFlg, lmean0=None,
-            vsign=-1, *, seed=None, precision=DEFAULT_PRECISION, device=0, path_offset=0) -> FqHolder:
+            vsign=-1, *, seed=None, precision=DEFAULT_PRECISION, device=0, path_offset=0, light_point=False,
+            hg_g=None) -> FqHolder:
+    """The C argument struct.  Two extensions beyond the reference, off by
+    default: light_point=True takes the columns of l as point-source
+    positions (the near-field light factor of evalphaseatt.m:10-16 instead of
+    the plane wave of MCfieldFourierQuad.m:272); hg_g=g samples the walk's
+    scattering directions from HG(g) (the smpampfunc_general call the
+    reference leaves commented out at line 208)."""
     bmin = np.asarray(box_min, dtype=float).reshape(-1)
     bmax = np.asarray(box_max, dtype=float).reshape(-1)
     if bmin.size != 3 or bmax.size != 3:
@@ -81,6 +89,12 @@ def fq_args(sigt, albedo, box_min, box_max, l, v_max, v_stp, maxItr, lambda_, do
     a.path_offset = int(path_offset)
     a.precision = _abi.PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     a.device = int(device)
+    a.light_point = int(bool(light_point))
+    if hg_g is not None:
+        if not abs(float(hg_g)) <= 1.0:
+            raise MatlabStyleError("Invalid g input")
+        a.sct_type = 3
+        a.g = float(hg_g)
     return FqHolder(a, [lc], grid_length(a.v_max, a.v_stp))
 
 

@@ -12,6 +12,14 @@
  * by exp(zexp0 * tz) and summed; finally multiplied by boxexp0 and normalised
  * by the VERTEX count (line 214).
  *
+ * Extensions (flagged in scmc_fq_args, not in the reference): HG(g) direction
+ * sampling in the walk (the smpampfunc_general call commented out at line
+ * 208; the first direction stays isotropic as at line 171, and the NEE terms
+ * keep the reference's isotropic couplings, because a view-side amplitude
+ * would depend on the output direction and could not be a per-vertex factor),
+ * and point sources: the light factor of line 272 replaced by the near-field
+ * branch of evalphaseatt.m:10-16.
+ *
  * The 2-D FFT is restated as the centred DFT it computes:
  *   X[q] = sum_p x[p] exp(-2 pi i (q - c)(p - c) / M),  c = floor(M/2),
  * followed by the flip q -> M-1-q and the crop of Nva_padd_size rows and
@@ -28,6 +36,8 @@ typedef double _Complex cplx;
 
 /* The walk and RNG live in scmc_oracle.c; this file reuses them through a
  * narrow internal interface. */
+cplx oracle_internal_evalphaseatt1(const double *x, const double *v, int is_ff, double sigt,
+                                   double lambda, const double *bmin, const double *bmax, int dim);
 int oracle_internal_fq_walk(const scmc_fq_args *a, const double *bmin, const double *bmax,
                             const double *unmeanl, oracle_rng_spec *rs, int64_t cap,
                             double *xL, double *x1L, double *pxr, double *pxi, int64_t *n_vert);
@@ -225,6 +235,11 @@ static int fq_core(const scmc_fq_args *a, const cplx *Wl, int as_written, oracle
                             const double atl =
                                 exp(-sigt / 2 * ((xe[2] - bmin[2]) * l_diratt + (bmax[2] - xe[2]) * l_idiratt));
                             w = sp[e] * cexp(vsign * 2 * PI * I / lambda * (-x1e[2] + tz)) * twl * atl;
+                        } else if (a->light_point) {
+                            /* extension: a point source at l_j, the near-field term of
+                             * evalphaseatt.m:10-16 (cubeDist in the padded box the walk uses) */
+                            w = sp[e] * cexp(-2 * PI * I / lambda * (-x1e[2] + tz)) *
+                                oracle_internal_evalphaseatt1(xe, lj, 0, sigt, lambda, bmin, bmax, 3);
                         } else {
                             w = sp[e] * cexp(-2 * PI * I / lambda * (-x1e[2] + tz)) *
                                 cexp(2 * PI * I / lambda * (lj[0] * xe[0] + lj[1] * xe[1] + lj[2] * xe[2]) -

@@ -164,6 +164,8 @@ static double cube_dist(const double *x, const double *vmin, const double *vmax,
 }
 
 /* evalphaseatt.m:1-21 for one direction / position v. */
+cplx oracle_internal_evalphaseatt1(const double *x, const double *v, int is_ff, double sigt,
+                                   double lambda, const double *bmin, const double *bmax, int dim);
 static cplx evalphaseatt1(const double *x, const double *v, int is_ff, double sigt,
                           double lambda, const double *bmin, const double *bmax, int dim)
 {
@@ -186,6 +188,12 @@ static cplx evalphaseatt1(const double *x, const double *v, int is_ff, double si
     double ph = (M_PI * 2.0 / lambda) * pv;
     double at = sigt / 2.0 * bdv;
     return exp(-at) * (cos(ph) + I * sin(ph)) * rv;
+}
+
+cplx oracle_internal_evalphaseatt1(const double *x, const double *v, int is_ff, double sigt,
+                                   double lambda, const double *bmin, const double *bmax, int dim)
+{
+    return evalphaseatt1(x, v, is_ff, sigt, lambda, bmin, bmax, dim);
 }
 
 /* evaluateHG.m:25-39 (cosineFlag = 1). */
@@ -817,7 +825,19 @@ int oracle_internal_fq_walk(const scmc_fq_args *a, const double *bmin, const dou
             } else {
                 weight = weight * a->albedo;
             }
-            randn_dir(dim, w, &r);
+            if (a->sct_type == SCMC_SCT_HG) {
+                /* extension: the smpampfunc_general(ow, sct_type, ampfunc) call that
+                 * MCfieldFourierQuad.m:208 leaves commented out, with HG(g) */
+                double ow[3];
+                memcpy(ow, w, sizeof ow);
+                scmc_phase_function pf;
+                memset(&pf, 0, sizeof pf);
+                pf.sct_type = SCMC_SCT_HG;
+                pf.g = a->g;
+                smpampfunc_general(ow, &pf, dim, w, &r);
+            } else {
+                randn_dir(dim, w, &r);
+            }
         }
         if (r.exhausted) { rc = -1; break; }
     }

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in declared_functions() if not hasattr(lib, n)]
     assert not missing, missing
     lib.scmc_abi_version.restype = ctypes.c_int
-    assert lib.scmc_abi_version() == 1
+    assert lib.scmc_abi_version() == 2
 
 
 def test_python_struct_matches_header_layout():
@@ -57,6 +57,7 @@ def test_serving_structs_match_header_layout():
     assert [f[0] for f in _abi.RequestInfo._fields_] == _header_fields("scmc_request_info")
     assert [f[0] for f in _abi.ServerStats._fields_] == _header_fields("scmc_server_stats")
     assert [f[0] for f in _abi.StageTimes._fields_] == _header_fields("scmc_stage_times")
+    assert [f[0].rstrip("_") for f in _abi.FqArgs._fields_] == [f.rstrip("_") for f in _header_fields("scmc_fq_args")]
 
 
 def test_server_create_without_gpu_fails_loudly():

@@ -51,7 +51,7 @@ def test_cov64_geometry_against_oracle(gpu, oracle_lib):
         assert rel(Ms + Mm, Mso + Mmo) < MIXED_TOL, prec
 
 
-@pytest.mark.parametrize("extended", [False], ids=["reference_form"])
+@pytest.mark.parametrize("extended", [False, True], ids=["reference_form", "hg09_point_source"])
 def test_fq256_geometry_against_oracle(gpu, oracle_lib, extended):
     h = WL.fq256_args(40, extended=extended, seed=78, precision="fp64")
     assert h.nv0 == 256

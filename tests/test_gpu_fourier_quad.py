@@ -99,10 +99,10 @@ def test_fourier_quad_tensor_cores_close_to_fp64(gpu, name, precision):
 
 
 def test_fourier_quad_tensor_cores_several_plane_groups(gpu):
-    """More entries than one group of the tensor-core form holds (2^18), so a
+    """More entries than one group of the tensor-core form holds (2^20), so a
     batch's plane groups run back to back from one metadata upload."""
     from mcspeckle_b200 import _lib
-    c = dict(TC_CASES["tc_wide_cbs"], n=150000)
+    c = dict(TC_CASES["tc_wide_cbs"], n=400000)
     u64 = FQ.field_fourier_quad_from_args(args_for(c, "fp64"))
     h = args_for(c, "fp16")
     _lib.profile_read(reset=True)
@@ -113,7 +113,7 @@ def test_fourier_quad_tensor_cores_several_plane_groups(gpu):
         _lib.profile_enable(False)
     prof = _lib.profile_read(reset=True)
     entries = prof["contract_flops"] / (8.0 * h.nv0 * h.nv0)
-    assert entries > 2 ** 18
+    assert entries > 2 ** 20
     assert rel(u, u64) < 1e-3
 
 
@@ -153,3 +153,57 @@ def test_fourier_quad_onwave_close_to_fp64(gpu, name, precision):
     u = FQ.field_fourier_quad_onwave_from_args(args_for(OW_CASES[name], precision), W)
     assert np.isfinite(u).all()
     assert rel(u, u64) < 1e-3
+
+
+# Extensions (not in the reference): point sources inside the medium (the
+# near-field light factor of evalphaseatt.m:10-16) and HG scattering in the
+# walk.  The oracle implements the same modes in FP64.
+EXT_CASES = {
+    "point_source_hg_cbs": (dict(FQ_CASES["wide_cbs_exp"], n=300), dict(light_point=True, hg_g=0.9)),
+    "point_source_iso_nocbs": (dict(FQ_CASES["narrow_nocbs_unif"], n=300), dict(light_point=True)),
+    "hg_plane_wave": (dict(FQ_CASES["wide_angles"], n=300), dict(hg_g=0.6)),
+    "tc_point_source_hg": (dict(TC_CASES["tc_wide_cbs"], n=250), dict(light_point=True, hg_g=0.9)),
+    "tc_hg_plane_wave": (dict(TC_CASES["tc_narrow_nocbs"], n=250), dict(hg_g=-0.4)),
+}
+
+
+def ext_args(name, precision):
+    c, ext = EXT_CASES[name]
+    if ext.get("light_point"):
+        # two sources inside the box, 2 and 5 wavelengths below its top face
+        bmin, bmax = np.array(c["box_min"], float), np.array(c["box_max"], float)
+        L = np.array([[0.0, 0.3 * bmax[0]], [0.0, -0.2 * bmax[1]], [bmin[2] + 2.0, bmin[2] + 5.0]])
+    else:
+        L = cap_dirs(2, 8, +1, 21)
+    return FQ.fq_args(c["sigt"], c["albedo"], c["box_min"], c["box_max"], L, c["v_max"], c["v_stp"], c["n"],
+                      c["lam"], c["cbs"], c["smp"], c["lmean0"], c["vsign"], seed=SEED + 1, precision=precision,
+                      **ext)
+
+
+@pytest.mark.parametrize("name", list(EXT_CASES))
+def test_fourier_quad_extensions_match_oracle(gpu, oracle_lib, name):
+    h = ext_args(name, "fp64")
+    u = FQ.field_fourier_quad_from_args(h)
+    uo = oracle_lib.field_fourier_quad(h.args, oracle_lib.Rng.philox(), h.nv0)
+    assert np.isfinite(uo).all() and np.linalg.norm(uo) > 0
+    assert rel(u, uo) < 1e-10
+    for precision in ("mixed", "fp16"):
+        um = FQ.field_fourier_quad_from_args(ext_args(name, precision))
+        assert rel(um, uo) < 1e-3, precision
+
+
+def test_fourier_quad_extensions_change_the_estimate(gpu):
+    """HG sampling and a point source give a different field than the
+    reference's isotropic plane-wave form on the same seed."""
+    h = ext_args("hg_plane_wave", "fp64")
+    u_hg = FQ.field_fourier_quad_from_args(h)
+    h.args.sct_type = 0
+    u_iso = FQ.field_fourier_quad_from_args(h)
+    assert rel(u_hg, u_iso) > 0.05
+
+
+def test_fourier_quad_point_source_with_weights_refused(gpu):
+    from mcspeckle_b200 import _lib
+    h = ext_args("point_source_iso_nocbs", "fp64")
+    with pytest.raises(_lib.ScmcError):
+        FQ.field_fourier_quad_onwave_from_args(h, weights(h.args.nl))
