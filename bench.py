@@ -1,20 +1,28 @@
 #!/usr/bin/env python
-"""Throughput of SCMC's Monte Carlo covariance path on B200.
+"""Throughput of SCMC's Monte Carlo speckle path on B200.
 
-Workload: the far-field covariance configuration - MCcov on a homogeneous box
-20 x 20 x 5 MFP (MFP = 10 wavelengths, wavelength 1), Henyey-Greenstein g=0.8,
-sigma_s = 1, sigma_a = 0.01 per MFP, 64 lights and 64 views on regular 8 x 8
+Headline workload (the one the metric is quoted on that fits one GPU): the
+far-field covariance - MCcov on a homogeneous box 20 x 20 x 5 MFP (MFP = 10
+wavelengths, wavelength 1), Henyey-Greenstein g=0.8, sigma_s = 1,
+sigma_a = 0.01 per MFP, 64 lights and 64 views on regular 8 x 8
 (sin theta_x, sin theta_y) grids spanning +-5 degrees about +z / -z
 (reflection, CBS on, exponential first-scatter sampling), 1e7 paths per GPU
 per step, full 64x64x64x64 complex covariance.  Synthetic: every input is
 generated from fixed seeds; each step walks a fresh Philox path range.
 
-One step = one MCcov solve of --paths paths on every GPU (mixed precision:
-tcgen05 FP16 hi+lo contraction, FP64 cross-chunk sums), plus for N>1 an
-NCCL sum of the partial Ms / Mm.  `value` = paths of all ranks / the max over
-ranks of the CUDA-event time of the K timed steps, outputs in HBM.  `e2e` =
-the same through the host-buffer C ABI call (scmc_cov: inputs from host,
-Ms / Mm copied back to host every step).
+One step = one MCcov solve of --paths paths on every GPU (default precision
+fp16: one FP16 tcgen05 product per term with FP32 accumulation, phases
+reduced in FP64, FP64 cross-chunk sums; --precision mixed runs the FP16
+hi+lo split), plus for N>1 an NCCL sum of the partial Ms / Mm.  `value` =
+paths of all ranks / the max over ranks of the CUDA-event time of the K
+timed steps, outputs in HBM.  `e2e` = the same through the host-buffer C ABI
+call (scmc_cov: inputs from host, Ms / Mm copied back to host every step).
+
+On one GPU the line also carries `workloads`: the other measured
+configurations (field16, fq256, hetero128), each with its own device-timed
+value, host-buffer e2e, roofline of its dominant kernel, error against the
+FP64 oracle on a small sample and the CPU oracle's rate; and `serving`, the
+served request stream.
 """
 from __future__ import annotations
 
@@ -33,171 +41,17 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from mcspeckle_b200 import workloads as WL  # noqa: E402
+
 METRIC = "MC paths/s at 1e-3 rel err vs FP64 (mixed vs FP32 GPU); p50/p99 request latency"
 UNIT = "paths/s"
-WORKLOAD = "MCcov far-field covariance, 64 lights x 64 views (8x8 grids, +-5 deg), HG g=0.8, box 20x20x5 MFP"
-
-
-def grid_dirs(n_side, half_deg, zsign):
-    s = math.sin(math.radians(half_deg))
-    g = np.linspace(-s, s, n_side)
-    sx, sy = np.meshgrid(g, g, indexing="ij")
-    sx, sy = sx.reshape(-1), sy.reshape(-1)
-    return np.stack([sx, sy, zsign * np.sqrt(1 - sx * sx - sy * sy)])
-
-
-def workload_args(n_paths):
-    mfp = 10.0
-    sigt = 1.01 / mfp          # sigma_s + sigma_a = (1 + 0.01) / MFP
-    albedo = 1.0 / 1.01
-    box_min = np.array([-100.0, -100.0, 0.0])
-    box_max = np.array([100.0, 100.0, 50.0])
-    l = grid_dirs(8, 5.0, +1.0)
-    v = grid_dirs(8, 5.0, -1.0)
-    return [sigt, albedo, box_min, box_max, l, v, 1, 1, int(n_paths), 1.0, True, 2, 3, 0.8]
+WORKLOAD = WL.COV64
+workload_args = WL.cov64_args
 
 
 # ---------------------------------------------------------------------------
-# served stream: uneven MCfield requests with Poisson arrivals
+# measurement helpers
 # ---------------------------------------------------------------------------
-SERVED_WORKLOAD = ("served MCfield stream: lights 1-256, views 1-1024, paths log-uniform; box 5-50 MFP "
-                   "(MFP 10 wavelengths, thickness 1/4 of the side), HG g~U(0,0.95), sigma_a~U(0,0.05), "
-                   "isotropic/HG/tabulated 1:2:1, far field, CBS, Poisson arrivals")
-
-
-def cap_dirs(n, half_deg, zsign, rng):
-    """n directions uniform on the solid-angle cap <= half_deg about zsign*z."""
-    c = rng.uniform(math.cos(math.radians(half_deg)), 1.0, n)
-    phi = rng.uniform(0, 2 * math.pi, n)
-    s = np.sqrt(1 - c * c)
-    return np.stack([s * np.cos(phi), s * np.sin(phi), zsign * c])
-
-
-def hg_table(g, n=1001):
-    """A tabulated phase function (tabulatedAmplitudeScatter of an HG lobe)."""
-    from mcspeckle_b200 import interface as I
-    th = np.linspace(0, 1, n) * np.pi
-    f = np.sqrt((1 - g * g) / (4 * np.pi * (1 + g * g - 2 * g * np.cos(th)) ** 1.5))
-    t = I.tabulatedAmplitudeScatter(th, f)["ampfunc"]
-    return {"evalAmp": t["evalAmp"], "sampleIcdf": t["sampleIcdf"]}
-
-
-def served_requests(n, seed=5, paths=(1e5, 1e8), nv_max=1024, nl_max=256, side_mfp=(5.0, 50.0)):
-    """The served stream: n MCfield requests with log-uniform sizes and budgets
-    and media drawn per request.  Returns dicts with the positional MCfield
-    arguments, the Philox key and the sizes."""
-    rng = np.random.default_rng(seed)
-
-    def logu(lo, hi):
-        return math.exp(rng.uniform(math.log(lo), math.log(hi)))
-
-    out = []
-    mfp = 10.0
-    for i in range(n):
-        nl = max(1, min(nl_max, int(round(logu(1, nl_max)))))
-        nv = max(1, min(nv_max, int(round(logu(1, nv_max)))))
-        n_paths = int(round(logu(*paths)))
-        side = logu(*side_mfp) * mfp
-        g = float(rng.uniform(0.0, 0.95))
-        sa = float(rng.uniform(0.0, 0.05))
-        kind = ["iso", "hg", "hg", "tab"][int(rng.integers(0, 4))]
-        sct, amp = {"iso": (1, 0), "hg": (3, g), "tab": (2, None)}[kind]
-        if kind == "tab":
-            amp = hg_table(g)
-        l = cap_dirs(nl, 10.0, +1.0, rng)
-        v = cap_dirs(nv, 10.0, -1.0, rng)
-        args = [(1.0 + sa) / mfp, 1.0 / (1.0 + sa), np.array([-side / 2, -side / 2, 0.0]),
-                np.array([side / 2, side / 2, side / 4]), l, v, 1, 1, n_paths, 1.0, True, 2, sct, amp]
-        out.append({"args": args, "seed": 0x5E4E0000 + i, "paths": n_paths, "nv": nv, "nl": nl, "scatter": kind})
-    return out
-
-
-def serve(reqs, slots=8, rate=None, precision="mixed", device=0, budget=80e9):
-    """Runs the requests through the request server.  rate None: all submitted
-    at once (closed batch); else Poisson arrivals at `rate` requests/s.
-    Returns per-request infos (server clock) and the results."""
-    from mcspeckle_b200 import mc as MC
-    from mcspeckle_b200.serving import Server
-    holders = [MC.mc_args(*r["args"], seed=r["seed"], precision=precision, device=device) for r in reqs]
-    gaps = np.random.default_rng(11).exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
-    arrive = np.cumsum(gaps) - gaps[0]
-    tickets = [None] * len(reqs)
-    with Server(device=device, slots=slots, hbm_budget=budget) as srv:
-        ready = threading.Event()
-
-        def submitter():
-            t0 = time.perf_counter()
-            for i, h in enumerate(holders):
-                dt = arrive[i] - (time.perf_counter() - t0)
-                if dt > 0:
-                    time.sleep(dt)
-                tickets[i] = srv.submit_field(h)
-                if i == 0:
-                    ready.set()
-            ready.set()
-
-        th = threading.Thread(target=submitter)
-        th.start()
-        infos, results = [], []
-        for i in range(len(reqs)):
-            while tickets[i] is None:
-                time.sleep(0.0005)
-            u, info = srv.wait(tickets[i])
-            infos.append(info)
-            results.append(u)
-        th.join()
-        stats = srv.stats()
-    return infos, results, stats
-
-
-def served_summary(reqs, infos):
-    lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
-    t0 = min(i["submit_ms"] for i in infos)
-    t1 = max(i["done_ms"] for i in infos)
-    paths = sum(r["paths"] for r in reqs)
-    busy = sum(i["device_ms"] for i in infos)
-    return {"requests": len(reqs), "paths": int(paths), "makespan_s": (t1 - t0) / 1000.0,
-            "paths_per_s": paths / ((t1 - t0) / 1000.0), "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
-            "sum_device_ms": busy}
-
-
-def run_served_leg(a, device):
-    """Served stream at reduced path budgets: closed batch (capacity), then
-    Poisson arrivals at 85% of that capacity (latency), then a plain FP32
-    one-request-at-a-time pass and the same requests served, on a prefix."""
-    from mcspeckle_b200 import mc as MC
-    lo, hi = a.served_paths_min, a.served_paths_max
-    reqs = served_requests(a.served_requests, paths=(lo, hi))
-    infos, _, st_closed = serve(reqs, slots=a.slots, device=device)
-    closed = served_summary(reqs, infos)
-    rate = 0.85 * len(reqs) / closed["makespan_s"]
-    infos, _, st_open = serve(reqs, slots=a.slots, rate=rate, device=device)
-    opened = served_summary(reqs, infos)
-    # plain FP32, one request at a time, on a prefix of the stream (bounded time)
-    t0 = time.perf_counter()
-    k = 0
-    while k < len(reqs) and time.perf_counter() - t0 < a.served_fp32_seconds:
-        r = reqs[k]
-        MC.field_from_args(MC.mc_args(*r["args"], seed=r["seed"], precision="fp32", device=device))
-        k += 1
-    fp32_s = time.perf_counter() - t0
-    prefix = reqs[:k]
-    infos_p, _, _ = serve(prefix, slots=a.slots, device=device)
-    served_prefix = served_summary(prefix, infos_p)
-    fp32_rate = sum(r["paths"] for r in prefix) / fp32_s
-    return {
-        "workload": SERVED_WORKLOAD, "requests": len(reqs), "paths_range": [lo, hi],
-        "path_budget_note": "config budgets 1e5-1e8 scaled to the stated range so the leg runs in about a minute",
-        "slots": a.slots, "hbm_budget_gb": 80, "precision": "mixed",
-        "closed_batch": closed, "poisson": dict(opened, offered_load=0.85, rate_per_s=rate),
-        "peak_reserved_gb": max(st_closed["peak_reserved_bytes"], st_open["peak_reserved_bytes"]) / 1e9,
-        "fp32_one_at_a_time": {"requests": k, "paths_per_s": fp32_rate, "seconds": fp32_s},
-        "served_same_prefix": {"requests": k, "paths_per_s": served_prefix["paths_per_s"]},
-        "speedup_vs_fp32_one_at_a_time": served_prefix["paths_per_s"] / fp32_rate,
-    }
-
-
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -205,6 +59,15 @@ def load_peaks():
             d = json.load(f)
         return d, "measured"
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def load_traffic(name):
+    """DRAM bytes per unit of work of a kernel, from a committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        return json.load(f)
 
 
 class ClockSampler:
@@ -228,6 +91,7 @@ class ClockSampler:
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+        return self
 
     def _read(self):
         for line in self.proc.stdout:
@@ -258,6 +122,20 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
                 "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def rel_err(x, ref, mask=None):
+    """Relative Frobenius error of x (array or tuple of arrays) against ref."""
+    x = x if isinstance(x, tuple) else (x,)
+    ref = ref if isinstance(ref, tuple) else (ref,)
+    num = den = 0.0
+    for xa, ra in zip(x, ref):
+        if mask is not None:
+            m = np.broadcast_to(mask, ra.shape)
+            xa, ra = xa[m], ra[m]
+        num += float(np.linalg.norm((xa - ra).ravel())) ** 2
+        den += float(np.linalg.norm(ra.ravel())) ** 2
+    return math.sqrt(num / den)
 
 
 def cpu_oracle_rate(args_fn, target_s=15.0, threads=None):
@@ -308,140 +186,225 @@ def run_reference(a):
 
 
 # ---------------------------------------------------------------------------
-# the other configurations, one JSON line each (`--workload`); the default line
-# above is the far-field covariance
+# served stream: uneven MCfield requests with Poisson arrivals
 # ---------------------------------------------------------------------------
-def grid_rect(nx, ny, half_deg, zsign):
-    """nx x ny directions on a regular (sin theta_x, sin theta_y) grid."""
-    s = math.sin(math.radians(half_deg))
-    sx, sy = np.meshgrid(np.linspace(-s, s, nx), np.linspace(-s, s, ny), indexing="ij")
-    sx, sy = sx.reshape(-1), sy.reshape(-1)
-    return np.stack([sx, sy, zsign * np.sqrt(1 - sx * sx - sy * sy)])
-
-
-def hg_mixture_table(n_bins, seed):
-    """Tabulated amplitude of a seeded mixture of 3 HG lobes (g in [-0.3, 0.95],
-    weights from Dirichlet(1,1,1)) on n_bins angles in [0, pi]."""
-    from mcspeckle_b200 import interface as I
-    g_rng = np.random.default_rng(seed)
-    gs = g_rng.uniform(-0.3, 0.95, 3)
-    w = g_rng.dirichlet([1.0, 1.0, 1.0])
-    th = np.linspace(0, 1, n_bins) * np.pi
-    c = np.cos(th)
-    pdf = sum(wk * (1 - gk * gk) / (4 * np.pi * (1 + gk * gk - 2 * gk * c) ** 1.5) for wk, gk in zip(w, gs))
-    t = I.tabulatedAmplitudeScatter(th, np.sqrt(pdf))["ampfunc"]
-    return {"evalAmp": t["evalAmp"], "sampleIcdf": t["sampleIcdf"]}, gs.tolist(), w.tolist()
-
-
-ACC_MASK = None  # entries excluded from the accuracy comparison of a workload
-
-
-def workload_spec(name):
-    """(description, make(n, precision, seed, offset, norm) -> holder, device solve,
-    host solve, output doubles, oracle solve, the tensor-core kernel whose
-    roofline is reported or None)."""
-    from mcspeckle_b200 import _lib
+def serve(reqs, slots=8, rate=None, precision="mixed", device=0, budget=80e9):
+    """Runs the requests through the request server.  rate None: all submitted
+    at once (closed batch); else Poisson arrivals at `rate` requests/s.
+    Returns per-request infos (server clock) and the results."""
     from mcspeckle_b200 import mc as MC
-    from mcspeckle_b200 import fourier_quad as FQ
-    from mcspeckle_b200 import hetero as H
-    L = _lib.lib()
-    if name == "field16":
-        rng = np.random.default_rng(0)
-        l16 = cap_dirs(16, 10.0, +1.0, rng)
-        v16 = cap_dirs(16, 10.0, -1.0, rng)
-        base = [0.1, 1.0, np.array([-100.0, -100.0, 0.0]), np.array([100.0, 100.0, 50.0]), l16, v16, 1, 1, 0,
-                1.0, True, 2, 1, 0]
+    from mcspeckle_b200.serving import Server
+    holders = [MC.mc_args(*r["args"], seed=r["seed"], precision=precision, device=device) for r in reqs]
+    gaps = np.random.default_rng(11).exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
+    arrive = np.cumsum(gaps) - gaps[0]
+    tickets = [None] * len(reqs)
+    with Server(device=device, slots=slots, hbm_budget=budget) as srv:
+        def submitter():
+            t0 = time.perf_counter()
+            for i, h in enumerate(holders):
+                dt = arrive[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets[i] = srv.submit_field(h)
 
-        def make(n, prec, seed, off=0, norm=0):
-            b = list(base)
-            b[8] = int(n)
-            return MC.mc_args(*b, seed=seed, precision=prec, path_offset=off, norm_itr=norm)
-
-        def dev(h, outs, stream):
-            _lib.check(L.scmc_field_device(h.ref, outs[0].data_ptr(), stream))
-
-        def oracle(h, O):
-            return O.field(h, O.Rng.philox())
-        return ("MCfield far field, 16 lights x 16 views within 10 deg of +z / -z, isotropic, box 20x20x5 MFP "
-                "(MFP 10 wavelengths), CBS, 1e5 paths per step", make, dev, MC.field_from_args, [2 * 16 * 16],
-                oracle, None)
-    if name == "fq256":
-        mfp = 100.0
-        base = dict(sigt=1.005 / mfp, albedo=1 / 1.005, box_min=[-25 * mfp, -25 * mfp, 0.0],
-                    box_max=[25 * mfp, 25 * mfp, 10 * mfp], l=np.array([[0.0], [0.0], [1.0]]),
-                    v_max=255.0 / 256.0, v_stp=1.0 / 128.0)
-
-        def make(n, prec, seed, off=0, norm=0):
-            return FQ.fq_args(base["sigt"], base["albedo"], base["box_min"], base["box_max"], base["l"],
-                              base["v_max"], base["v_stp"], int(n), 1.0, True, 2, None, -1, seed=seed,
-                              precision=prec, path_offset=off)
-
-        def dev(h, outs, stream):
-            _lib.check(L.scmc_field_fourier_quad_device(h.ref, outs[0].data_ptr(), stream))
-
-        def oracle(h, O):
-            return O.field_fourier_quad(h.args, O.Rng.philox(), h.nv0)
-        th = -base["v_max"] + np.arange(256) * base["v_stp"]
-        # accuracy over the propagating directions only: where vx^2 + vy^2 > 1 the
-        # reference's plane factor grows exponentially with depth (evanescent)
-        global ACC_MASK
-        ACC_MASK = (th[:, None] ** 2 + th[None, :] ** 2 < 1.0)[:, :, None]
-        return ("MCfieldFourierQuad, box 50x50x10 MFP (MFP 100 wavelengths), sigma_a 0.005 per MFP, plane wave "
-                "along +z, 256x256 angular grid (v_max 255/256, v_stp 1/128: 0.5-wavelength lateral pitch), CBS; "
-                "isotropic as the reference (HG g=0.9 and the point source are not built)",
-                make, dev, FQ.field_fourier_quad_from_args, [2 * 256 * 256], oracle, "fq_planes_tc_kernel")
-    if name == "hetero128":
-        mfp = 10.0
-        g = np.random.default_rng(4)
-        sig = np.exp(g.normal(0.0, 0.5, (128, 128, 128))) / mfp
-        table, gs, ws = hg_mixture_table(1024, 5)
-        bmin, bmax = np.array([-100.0, -100.0, 0.0]), np.array([100.0, 100.0, 50.0])
-        bbin = (bmax - bmin) / 128.0
-        l = grid_rect(16, 8, 5.0, +1.0)
-        v = grid_rect(16, 8, 5.0, -1.0)
-
-        def make(n, prec, seed, off=0, norm=0):
-            return H.hetero_args(True, sig, 1.0, bmin, bmax, bbin, l, v, 1, 1, int(n), 1.0, True, 2, 2, table,
-                                 seed=seed, precision=prec, path_offset=off, norm_itr=norm)
-
-        def dev(h, outs, stream):
-            _lib.check(L.scmc_cov_hetero_device(h.ref, outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(),
-                                                stream))
-
-        def oracle(h, O):
-            return O.cov_hetero(h, O.Rng.philox(), threads=os.cpu_count() or 1)[:2]
-        n2 = 128 * 128
-        return (f"MCCovHetro, sigma_s on a 128^3 grid log-normal(0, 0.5) per MFP (MFP 10 wavelengths, nearest "
-                f"voxel as the reference), box 20x20x5 MFP, Woodcock tracking, tabulated phase function on 1024 "
-                f"theta bins from 3 HG lobes g={[round(x, 3) for x in gs]} w={[round(x, 3) for x in ws]}, "
-                f"128 lights x 128 views (16x8 grids of +-5 deg), CBS",
-                make, dev, lambda h: H.cov_hetero_from_args(h)[:2], [2 * n2 * n2, 2 * n2 * n2, 2 * n2], oracle,
-                "herk_tc2_kernel")
-    raise SystemExit(f"unknown workload {name}")
+        th = threading.Thread(target=submitter)
+        th.start()
+        infos, results = [], []
+        for i in range(len(reqs)):
+            while tickets[i] is None:
+                time.sleep(0.0005)
+            u, info = srv.wait(tickets[i])
+            infos.append(info)
+            results.append(u)
+        th.join()
+        stats = srv.stats()
+    return infos, results, stats
 
 
-def run_workload(a):
-    """One JSON line for a non-default configuration, 1 GPU: device-timed
-    steps of fresh path ranges (outputs in HBM), the host-buffer call, stage
-    times, accuracy against FP64 on a smaller sample, the CPU oracle on a
-    bounded sample."""
+def served_summary(reqs, infos):
+    lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
+    t0 = min(i["submit_ms"] for i in infos)
+    t1 = max(i["done_ms"] for i in infos)
+    paths = sum(r["paths"] for r in reqs)
+    busy = sum(i["device_ms"] for i in infos)
+    out = {"requests": len(reqs), "paths": int(paths), "makespan_s": (t1 - t0) / 1000.0,
+           "paths_per_s": paths / ((t1 - t0) / 1000.0), "p50_ms": float(np.percentile(lat, 50)),
+           "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+           "sum_device_ms": busy}
+    # latency by request size (paths x (views + lights)): the small, medium and large thirds
+    size = np.array([r["paths"] * (r["nv"] + r["nl"]) for r in reqs], dtype=float)
+    if len(reqs) >= 6:
+        cuts = np.quantile(size, [1 / 3, 2 / 3])
+        buckets = {}
+        for name, sel in (("small", size <= cuts[0]), ("medium", (size > cuts[0]) & (size <= cuts[1])),
+                          ("large", size > cuts[1])):
+            if sel.any():
+                buckets[name] = {"requests": int(sel.sum()), "p50_ms": float(np.percentile(lat[sel], 50)),
+                                 "p99_ms": float(np.percentile(lat[sel], 99)),
+                                 "paths_range": [int(min(r["paths"] for r, s in zip(reqs, sel) if s)),
+                                                 int(max(r["paths"] for r, s in zip(reqs, sel) if s))]}
+        out["by_size"] = buckets
+    return out
+
+
+def run_served_leg(a, device):
+    """Served stream: closed batch (capacity), then Poisson arrivals at 85% of
+    that capacity (latency), then a plain FP32 one-request-at-a-time pass and
+    the same requests served, on a prefix."""
+    from mcspeckle_b200 import mc as MC
+    lo, hi = a.served_paths_min, a.served_paths_max
+    reqs = WL.served_requests(a.served_requests, paths=(lo, hi))
+    infos, _, st_closed = serve(reqs, slots=a.slots, device=device)
+    closed = served_summary(reqs, infos)
+    rate = 0.85 * len(reqs) / closed["makespan_s"]
+    infos, _, st_open = serve(reqs, slots=a.slots, rate=rate, device=device)
+    opened = served_summary(reqs, infos)
+    # plain FP32, one request at a time, on a prefix of the stream (bounded time)
+    t0 = time.perf_counter()
+    k = 0
+    while k < len(reqs) and time.perf_counter() - t0 < a.served_fp32_seconds:
+        r = reqs[k]
+        MC.field_from_args(MC.mc_args(*r["args"], seed=r["seed"], precision="fp32", device=device))
+        k += 1
+    fp32_s = time.perf_counter() - t0
+    prefix = reqs[:k]
+    infos_p, _, _ = serve(prefix, slots=a.slots, device=device)
+    served_prefix = served_summary(prefix, infos_p)
+    fp32_rate = sum(r["paths"] for r in prefix) / fp32_s
+    return {
+        "workload": WL.SERVED, "requests": len(reqs), "paths_range": [lo, hi],
+        "path_budget_note": f"the config's 10,000 requests at 1e5-1e8 paths run as {len(reqs)} requests at "
+                            f"{lo:.0e}-{hi:.0e} so the leg ends in minutes",
+        "slots": a.slots, "hbm_budget_gb": 80, "precision": "mixed",
+        "closed_batch": closed, "poisson": dict(opened, offered_load=0.85, rate_per_s=rate),
+        "peak_reserved_gb": max(st_closed["peak_reserved_bytes"], st_open["peak_reserved_bytes"]) / 1e9,
+        "fp32_one_at_a_time": {"requests": k, "paths_per_s": fp32_rate, "seconds": fp32_s},
+        "served_same_prefix": {"requests": k, "paths_per_s": served_prefix["paths_per_s"]},
+        "speedup_vs_fp32_one_at_a_time": served_prefix["paths_per_s"] / fp32_rate,
+    }
+
+
+# ---------------------------------------------------------------------------
+# the other configurations: field16, fq256, hetero128
+# ---------------------------------------------------------------------------
+class Leg:
+    """One configuration: how to build a solve, run it on the device and from
+    host buffers, its oracle, and the kernel whose roofline is reported."""
+
+    def __init__(self, name):
+        from mcspeckle_b200 import _lib
+        from mcspeckle_b200 import fourier_quad as FQ
+        from mcspeckle_b200 import hetero as H
+        from mcspeckle_b200 import mc as MC
+        L = _lib.lib()
+        self.name = name
+        self.mask = None
+        self.device_compare = False
+        if name == "field16":
+            self.desc = WL.FIELD16 + ", phases reduced in FP64, CUDA-core accumulation"
+            self.paths, self.acc_paths, self.cpu_paths = 1_000_000, 20_000, 4000
+            self.make = lambda n, p, seed, off=0, norm=0: MC.mc_args(*WL.field16_args(n), seed=seed, precision=p,
+                                                                     path_offset=off, norm_itr=norm)
+            self.sizes = [2 * 16 * 16]
+            self.dev = lambda h, outs, st: _lib.check(L.scmc_field_device(h.ref, outs[0].data_ptr(), st))
+            self.host = MC.field_from_args
+            self.oracle = lambda h, O: O.field(h, O.Rng.philox())
+            self.kernel, self.bound, self.stage = "field_accum_kernel", "fp32", "rows"
+            self.traffic_file, self.unit_name = "field_accum_kernel_field16_traffic.json", "event"
+            self.h2d = 2 * 16 * 3 * 8
+            self.cpu_threads = 1
+        elif name == "fq256":
+            self.desc = WL.fq256_desc(True)
+            self.paths, self.acc_paths, self.cpu_paths = 10_000_000, 40, 40
+            self.make = lambda n, p, seed, off=0, norm=0: WL.fq256_args(n, extended=True, seed=seed, precision=p,
+                                                                        path_offset=off)
+            self.sizes = [2 * 256 * 256]
+            self.dev = lambda h, outs, st: _lib.check(L.scmc_field_fourier_quad_device(h.ref, outs[0].data_ptr(), st))
+            self.host = FQ.field_fourier_quad_from_args
+            self.oracle = lambda h, O: O.field_fourier_quad(h.args, O.Rng.philox(), h.nv0)
+            self.mask = WL.fq256_propagating()
+            self.kernel, self.bound, self.stage = "fq_planes_tc_kernel", "tensor", "contract"
+            self.traffic_file, self.unit_name = "fq_planes_tc_kernel_fq256_traffic.json", "entry"
+            self.h2d = 3 * 8 + 256 * 256 * 16 * 2
+            self.cpu_threads = 1
+        elif name == "hetero128":
+            self.desc = WL.hetero128_desc()
+            self.paths, self.acc_paths, self.cpu_paths = 100_000, 8, 8
+            self.make = lambda n, p, seed, off=0, norm=0: WL.hetero128_args(n, seed=seed, precision=p,
+                                                                            path_offset=off, norm_itr=norm)
+            n2 = 128 * 128
+            self.sizes = [2 * n2 * n2, 2 * n2 * n2, 2 * n2]
+            self.dev = lambda h, outs, st: _lib.check(L.scmc_cov_hetero_device(
+                h.ref, outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(), st))
+            self.host = lambda h: H.cov_hetero_from_args(h)[:2]
+            self.oracle = lambda h, O: O.cov_hetero(h, O.Rng.philox(), threads=os.cpu_count() or 1)[:2]
+            self.kernel, self.bound, self.stage = "herk_tc2_kernel", "tensor", "contract"
+            self.traffic_file, self.unit_name = "herk_tc2_kernel_hetero128_traffic.json", "event"
+            self.h2d = 128 ** 3 * 8 + 2 * 128 * 3 * 8 + 1024 * 24
+            self.cpu_threads = os.cpu_count() or 1
+            self.device_compare = True
+        else:
+            raise SystemExit(f"unknown workload {name}")
+
+
+def _device_rel(outs, ref_dev):
+    num = den = 0.0
+    step = 1 << 27
+    for x, r in zip(outs, ref_dev):
+        for k in range(0, r.numel(), step):
+            rr = r[k:k + step]
+            num += float(((x[k:k + step] - rr) ** 2).sum())
+            den += float((rr ** 2).sum())
+    return math.sqrt(num / den)
+
+
+def leg_accuracy(leg, precisions, O):
+    """Error of each precision against the FP64 oracle on the same paths
+    (a small sample; the oracle runs outside every timed region)."""
+    import torch
+    na = leg.acc_paths
+    ho = leg.make(na, "fp64", 7)
+    ref = leg.oracle(ho, O)
+    out = {"paths": na, "tol": 1e-3, "reference": "FP64 oracle (C restatement of the reference) on the same "
+                                                   "Philox paths"}
+    if leg.mask is not None:
+        out["mask"] = "propagating directions (vx^2 + vy^2 < 1)"
+    if leg.device_compare:
+        ref_dev = [torch.from_numpy(x.reshape(-1, order="F").view(np.float64)).cuda() for x in ref]
+        del ref
+        for p in precisions:
+            outs = [torch.empty(n, dtype=torch.float64, device="cuda") for n in leg.sizes]
+            leg.dev(leg.make(na, p, 7), outs, torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            out[f"rel_err_{p}_vs_oracle"] = _device_rel(outs[:len(ref_dev)], ref_dev)
+            del outs
+        del ref_dev
+        torch.cuda.empty_cache()
+    else:
+        for p in precisions:
+            out[f"rel_err_{p}_vs_oracle"] = rel_err(leg.host(leg.make(na, p, 7)), ref, leg.mask)
+    return out
+
+
+def run_leg(leg, a, prec, peaks, peak_kind):
+    """Device-timed steps of fresh path ranges (outputs in HBM), the
+    host-buffer call, the roofline of the dominant kernel, accuracy against
+    the oracle, plain FP32 and the CPU oracle."""
     import torch
     from mcspeckle_b200 import _lib
-    desc, make, dev, host, sizes, oracle_fn, bound = workload_spec(a.workload)
-    prec = a.precision
-    P = int(a.paths if a.paths is not None else {"field16": 1e5, "fq256": 1e5, "hetero128": 2e4}[a.workload])
+    from oracle import oracle as O
+    O.build()
+    P = int(a.leg_paths.get(leg.name, leg.paths))
     stream = torch.cuda.current_stream()
-    outs = [torch.zeros(n, dtype=torch.float64, device="cuda") for n in sizes]
-    seed = 0
+    outs = [torch.zeros(n, dtype=torch.float64, device="cuda") for n in leg.sizes]
 
     def step(i):
-        dev(make(P, prec, seed, off=i * P, norm=P), outs, stream.cuda_stream)
+        leg.dev(leg.make(P, prec, 0, off=i * P, norm=P), outs, stream.cuda_stream)
 
     for i in range(a.warmup):
         step(i)
     torch.cuda.synchronize()
-    clocks = ClockSampler(0)
-    clocks.start()
+    clocks = ClockSampler(0).start()
     _lib.profile_read(reset=True)
     _lib.profile_enable(True)
     l0 = _lib.launch_count()
@@ -457,67 +420,97 @@ def run_workload(a):
     _lib.profile_enable(False)
     prof = _lib.profile_read(reset=True)
     clk = clocks.stop()
+    del outs
+    torch.cuda.empty_cache()
     value = P * a.steps / (ms / 1000.0)
-    # e2e: the host-buffer call (results copied to host every step)
+    # e2e: the host-buffer call (inputs from host, results copied back every step)
+    ke = max(1, min(a.steps, a.leg_e2e_steps))
     t0 = time.perf_counter()
-    for i in range(a.steps):
-        host(make(P, prec, seed, off=(a.warmup + a.steps + i) * P, norm=P))
-    e2e = P * a.steps / (time.perf_counter() - t0)
-    # accuracy on a smaller sample, same paths in every precision
-    na = int(a.accuracy_paths if a.accuracy_paths is not None else
-             {"field16": 1e5, "fq256": 2e4, "hetero128": 1e3}[a.workload])
-    ref = host(make(na, "fp64", 7))
-    ref = ref if isinstance(ref, tuple) else (ref,)
-
-    def rel(x):
-        x = x if isinstance(x, tuple) else (x,)
-        num = den = 0.0
-        for xa, ra in zip(x, ref):
-            m = np.isfinite(ra) if ACC_MASK is None else np.broadcast_to(ACC_MASK, ra.shape)
-            num += float(np.linalg.norm((xa - ra)[m])) ** 2
-            den += float(np.linalg.norm(ra[m])) ** 2
-        return math.sqrt(num / den)
-    acc = {"paths": na, "tol": 1e-3}
-    for pz in ("mixed", "fp16", "fp32"):
-        acc[f"rel_err_{pz}_vs_fp64"] = rel(host(make(na, pz, 7)))
-    # plain FP32 GPU, one solve, same paths as one timed step
-    t32 = time.perf_counter()
-    host(make(P, "fp32", seed))
-    fp32_value = P / (time.perf_counter() - t32)
+    for i in range(ke):
+        leg.host(leg.make(P, prec, 0, off=(a.warmup + a.steps + i) * P, norm=P))
+    e2e = P * ke / (time.perf_counter() - t0)
+    # roofline of the dominant kernel over its busy time (launches on several
+    # streams overlap; each instant counts once)
     roof = None
-    if bound is not None and prof["contract_launches"]:
-        peaks, peak_kind = load_peaks()
-        peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
-        achieved = prof["contract_flops"] / (prof["contract_busy_ms"] / 1000.0) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "kernel": bound, "peak_source": f"bf16_tflops_sustained ({peak_kind})",
-                "flops": prof["contract_flops"], "contract_busy_ms": prof["contract_busy_ms"]}
+    busy = prof[f"{leg.stage}_busy_ms"]
+    if busy > 0:
+        tj = load_traffic(leg.traffic_file)
+        if leg.bound == "tensor":
+            work = prof["contract_flops"]
+            peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+            peak_src = f"bf16_tflops_sustained ({peak_kind})"
+            units = work / (8.0 * 256 * 256) if leg.name == "fq256" else work / (4.0 * 16384 * 16385)
+        else:
+            # CUDA-core field accumulation: 8 nv nl flops per event and term
+            # (single events 1 term, multiple-scattering events 2 with CBS)
+            ev = prof["events"]
+            paths = prof["paths"]
+            work = 8.0 * 16 * 16 * (paths + 2.0 * (ev - paths))
+            units = ev
+            sms = torch.cuda.get_device_properties(0).multi_processor_count
+            mhz = clk.get("sm_max_mhz") or 1965.0
+            peak = sms * 128 * 2 * mhz * 1e6 / 1e12
+            peak_src = f"nominal FP32 FMA peak ({sms} SMs x 128 lanes x 2 flops x {mhz:.0f} MHz)"
+        n_launch = max(prof[f"{leg.stage}_launches"], 1)
+        achieved = work / (busy / 1000.0) / 1e12
+        traffic = None
+        if tj is not None:
+            traffic = tj[f"dram_bytes_per_{leg.unit_name}"] * units / n_launch
+        roof = {"bound": leg.bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": leg.kernel, "peak_source": peak_src,
+                "flops_per_launch": work / n_launch, "busy_ms_per_launch": busy / n_launch, "launches": n_launch,
+                f"{leg.unit_name}s_per_launch": units / n_launch,
+                "traffic_source": f"profiles/{leg.traffic_file}" if tj is not None else None}
+    acc = leg_accuracy(leg, [prec] + [p for p in ("mixed", "fp16", "fp32") if p != prec], O)
+    # plain FP32 GPU on a smaller sample, and the same sample in the line's precision
+    n32 = max(1, P // 10)
+    t32 = time.perf_counter()
+    leg.host(leg.make(n32, "fp32", 0))
+    fp32_value = n32 / (time.perf_counter() - t32)
+    tp = time.perf_counter()
+    leg.host(leg.make(n32, prec, 0))
+    same_value = n32 / (time.perf_counter() - tp)
     cpu = None
     if not a.no_cpu_baseline:
-        from oracle import oracle as O
-        O.build()
-        n = {"field16": 2000, "fq256": 20, "hetero128": 16}[a.workload]
-        h = make(n, "fp64", 99)
+        n = leg.cpu_paths
+        h = leg.make(n, "fp64", 99)
         tc = time.perf_counter()
-        oracle_fn(h, O)
+        r = leg.oracle(h, O)
         dt = time.perf_counter() - tc
-        thr = (os.cpu_count() or 1) if a.workload == "hetero128" else 1
-        cpu = {"value": n / dt, "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": f"{n} paths of the workload in {dt:.1f} s (FP64 oracle, {thr} thread(s))"}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": prec, "data": "synthetic",
-            "config": {"workload": a.workload, "description": desc, "paths_per_step": P, "precision": prec},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": None,
-                    "d2h_bytes_per_step": int(sum(sizes) * 8)},
+        del r
+        cpu = {"value": n / dt, "unit": UNIT, "cores": leg.cpu_threads, "kind": "port",
+               "sample": f"{n} paths of the workload in {dt:.1f} s (FP64 oracle, {leg.cpu_threads} thread(s))"}
+    return {"workload": leg.name, "description": leg.desc, "value": value, "unit": UNIT, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "paths_per_step": P, "precision": prec,
+            "e2e": {"value": e2e, "unit": UNIT, "steps": ke, "h2d_bytes_per_step": int(leg.h2d),
+                    "d2h_bytes_per_step": int(sum(leg.sizes[:2]) * 8)},
             "gpu_launches": int(launches), "roofline": roof,
             "stages_ms": {k: prof[k] for k in ("walk_ms", "rows_ms", "contract_ms", "finalize_ms",
                                                "contract_busy_ms", "rows_busy_ms")},
-            "accuracy": acc, "fp32_gpu": {"paths": P, "value": fp32_value}, "cpu_baseline": cpu, "clocks": clk}
+            "accuracy": acc,
+            "fp32_gpu": {"paths": n32, "value": fp32_value, f"{prec}_same_sample": same_value,
+                         f"speedup_{prec}_over_fp32": same_value / fp32_value},
+            "cpu_baseline": cpu, "clocks": clk}
+
+
+def run_workload(a):
+    """--workload NAME: one configuration's leg alone, as one JSON line."""
+    peaks, kind = load_peaks()
+    r = run_leg(Leg(a.workload), a, a.precision, peaks, kind)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": a.precision, "data": "synthetic",
+            "config": {"workload": a.workload, "description": r["description"], "paths_per_step": r["paths_per_step"],
+                       "precision": a.precision},
+            **{k: r[k] for k in ("e2e", "gpu_launches", "roofline", "stages_ms", "accuracy", "fp32_gpu",
+                                 "cpu_baseline", "clocks")}}
     print(json.dumps(line), flush=True)
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the headline: far-field covariance, 64 x 64
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -525,23 +518,29 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--paths", type=float, default=None, help="paths per GPU per step (cov64: 1e7)")
-    ap.add_argument("--accuracy-paths", type=float, default=None, help="(cov64: 1e5)")
+    ap.add_argument("--accuracy-paths", type=float, default=1e5,
+                    help="cov64: regenerated paths for the error against the GPU's FP64 mode")
+    ap.add_argument("--oracle-paths", type=int, default=100, help="cov64: paths for the error against the oracle")
     ap.add_argument("--fp32-paths", type=float, default=1e5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp16", choices=["mixed", "fp16"],
                     help="mixed: FP16 hi+lo split (2 tensor products); fp16: one FP16 product")
-    ap.add_argument("--served-requests", type=int, default=200)
-    ap.add_argument("--served-paths-min", type=float, default=1e4)
-    ap.add_argument("--served-paths-max", type=float, default=1e7)
+    ap.add_argument("--served-requests", type=int, default=60)
+    ap.add_argument("--served-paths-min", type=float, default=1e5)
+    ap.add_argument("--served-paths-max", type=float, default=1e8)
     ap.add_argument("--served-fp32-seconds", type=float, default=20.0)
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--legs", default="field16,fq256,hetero128",
+                    help="configurations measured beside the headline on one GPU ('' for none)")
+    ap.add_argument("--leg-paths", default="", help="per-leg path budgets, e.g. fq256=1e6,hetero128=2e4")
+    ap.add_argument("--leg-e2e-steps", type=int, default=3)
     ap.add_argument("--workload", default="cov64", choices=["cov64", "field16", "fq256", "hetero128"],
-                    help="cov64: the far-field covariance (the default line); the others print one line of "
-                         "their own (1 GPU): field16, fq256, hetero128")
+                    help="cov64: the default line; the others print one line of their own (1 GPU)")
     a = ap.parse_args()
+    a.leg_paths = {k: int(float(v)) for k, v in (kv.split("=") for kv in a.leg_paths.split(",") if kv)}
     if a.impl == "reference":
         return run_reference(a)
     if a.workload != "cov64":
@@ -549,7 +548,6 @@ def main():
         torch.cuda.set_device(0)
         return run_workload(a)
     a.paths = 1e7 if a.paths is None else a.paths
-    a.accuracy_paths = 1e5 if a.accuracy_paths is None else a.accuracy_paths
 
     import torch
     import torch.distributed as dist
@@ -596,8 +594,7 @@ def main():
     barrier()
 
     # timed region (device-resident outputs)
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks = ClockSampler(local).start()
     _lib.profile_read(reset=True)
     _lib.profile_enable(True)
     l0 = _lib.launch_count()
@@ -649,6 +646,7 @@ def main():
 
     line = None
     if rank == 0:
+        del host_Ms, host_Mm
         peaks, peak_kind = load_peaks()
         peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
         # Consecutive contraction launches run on two streams and overlap, so
@@ -660,42 +658,50 @@ def main():
         flops_per_launch = prof["contract_flops"] / max(prof["contract_launches"], 1)
         achieved = flops_per_launch / (busy_per_launch_ms / 1000.0) / 1e12
         traffic = None
-        tf = os.path.join(ROOT, "profiles", "herk_tc2_kernel_cov64x64_traffic.json")
-        if os.path.exists(tf):
-            with open(tf) as f:
-                tj = json.load(f)
+        tj = load_traffic("herk_tc2_kernel_cov64x64_traffic.json")
+        if tj is not None:
             # bytes per event measured by ncu, scaled to this run's events per launch
             ev_per_launch = flops_per_launch / (4.0 * N * (N + 1))
             traffic = tj["dram_bytes_per_event"] * ev_per_launch
-        # accuracy on regenerated paths: mixed and plain FP32 against FP64
+        # accuracy on regenerated paths against the GPU's FP64 mode (1e5 paths)
+        # and against the FP64 oracle (a small sample)
         na = int(a.accuracy_paths)
-        ha = MC.mc_args(*workload_args(na), seed=seed, precision="fp64", device=local)
-        M64 = MC.cov_from_args(ha)
-        Mmx = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision=a.precision, device=local))
         other = "fp16" if a.precision == "mixed" else "mixed"
-        Moth = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision=other, device=local))
+        M64 = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision="fp64", device=local))
+        acc = {"paths": na, "tol": 1e-3, "norm": "Frobenius of (Ms, Mm)"}
+        for p in (a.precision, other, "fp32"):
+            acc[f"rel_err_{p}_vs_fp64"] = rel_err(
+                MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision=p, device=local)), M64)
+        del M64
+        from oracle import oracle as O
+        O.build()
+        no = int(a.oracle_paths)
+        ho = MC.mc_args(*workload_args(no), seed=seed, precision="fp64", device=local)
+        Mo = O.cov(ho, O.Rng.philox(), threads=os.cpu_count() or 1)
+        acc["oracle_paths"] = no
+        acc["rel_err_fp64_vs_oracle"] = rel_err(MC.cov_from_args(ho), Mo)
+        for p in (a.precision, other):
+            acc[f"rel_err_{p}_vs_oracle"] = rel_err(
+                MC.cov_from_args(MC.mc_args(*workload_args(no), seed=seed, precision=p, device=local)), Mo)
+        del Mo
+        # the 5x comparison: plain FP32 GPU and both tensor-core precisions on the same sample
+        nf = int(a.fp32_paths)
         t32 = time.perf_counter()
-        M32 = MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision="fp32",
-                                          device=local))
+        MC.cov_from_args(MC.mc_args(*workload_args(nf), seed=seed, precision="fp32", device=local))
         fp32_s = time.perf_counter() - t32
-        if int(a.fp32_paths) != na:
-            M32 = MC.cov_from_args(MC.mc_args(*workload_args(na), seed=seed, precision="fp32", device=local))
-        C64 = M64[0] + M64[1]
-
-        def rel(x, y):
-            return float(np.linalg.norm((x - y).ravel()) / np.linalg.norm(y.ravel()))
-
-        err_mixed = rel(Mmx[0] + Mmx[1], C64)
-        err_fp32 = rel(M32[0] + M32[1], C64)
-        err_other = rel(Moth[0] + Moth[1], C64)
         tmx = time.perf_counter()
-        MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision=a.precision,
-                                    device=local))
-        mixed_small_s = time.perf_counter() - tmx
+        MC.cov_from_args(MC.mc_args(*workload_args(nf), seed=seed, precision=a.precision, device=local))
+        prec_small_s = time.perf_counter() - tmx
         tot = time.perf_counter()
-        MC.cov_from_args(MC.mc_args(*workload_args(int(a.fp32_paths)), seed=seed, precision=other, device=local))
+        MC.cov_from_args(MC.mc_args(*workload_args(nf), seed=seed, precision=other, device=local))
         other_small_s = time.perf_counter() - tot
-        served = None if a.no_served else run_served_leg(a, local)
+        legs = None
+        if world == 1 and a.legs:
+            legs = {}
+            for name in a.legs.split(","):
+                legs[name] = run_leg(Leg(name), a, a.precision, peaks, peak_kind)
+                torch.cuda.empty_cache()
+        served = None if (a.no_served or world > 1) else run_served_leg(a, local)
         cpu = None
         if not a.no_cpu_baseline:
             rate, n, dt, thr = cpu_oracle_rate(workload_args, target_s=a.cpu_seconds)
@@ -722,14 +728,11 @@ def main():
             "stages_ms": {"walk": prof["walk_ms"], "rows": prof["rows_ms"], "contract": prof["contract_ms"],
                           "finalize": prof["finalize_ms"], "contract_busy": prof["contract_busy_ms"],
                           "rows_busy": prof["rows_busy_ms"], "timed_region": ms_max},
-            "accuracy": {"paths": na, f"rel_err_{a.precision}_vs_fp64": err_mixed,
-                         f"rel_err_{other}_vs_fp64": err_other, "rel_err_fp32_vs_fp64": err_fp32,
-                         "tol": 1e-3, "norm": "Frobenius of C = Ms + Mm"},
-            "other_precision": {"precision": other, "paths": int(a.fp32_paths),
-                                "value": int(a.fp32_paths) / other_small_s},
-            "fp32_gpu": {"paths": int(a.fp32_paths), "value": int(a.fp32_paths) / fp32_s,
-                         "mixed_same_sample": int(a.fp32_paths) / mixed_small_s,
-                         "speedup_mixed_over_fp32": (int(a.fp32_paths) / mixed_small_s) / (int(a.fp32_paths) / fp32_s)},
+            "accuracy": acc,
+            "other_precision": {"precision": other, "paths": nf, "value": nf / other_small_s},
+            "fp32_gpu": {"paths": nf, "value": nf / fp32_s, f"{a.precision}_same_sample": nf / prec_small_s,
+                         f"speedup_{a.precision}_over_fp32": fp32_s / prec_small_s},
+            "workloads": legs,
             "serving": served,
             "cpu_baseline": cpu,
             "clocks": clk,

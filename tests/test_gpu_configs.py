@@ -39,7 +39,7 @@ def rel(a, b, mask=None):
 
 
 def test_cov64_geometry_against_oracle(gpu, oracle_lib):
-    args = WL.cov64_args(200)
+    args = WL.cov64_args(100)
     ho = MC.mc_args(*args, seed=77, precision="fp64")
     Mso, Mmo = oracle_lib.cov(ho, oracle_lib.Rng.philox(), threads=THREADS)
     Ms, Mm = MC.cov_from_args(ho)
