@@ -408,6 +408,22 @@ int scmc_refocus(const double *u, const double *v, int64_t nv, int32_t dim, cons
  * fall back to an eigendecomposition there. */
 int scmc_sample_cov(const double *C, int64_t N, int64_t n_samples, uint64_t seed, int32_t device, double *Z);
 
+/* The memory-effect view of a covariance (config: 64 x 64 covariance on
+ * 8 x 8 angular grids).  C1 (+ C2 when not NULL, e.g. Ms + Mm) is
+ * nv x nv x nl x nl complex as scmc_cov writes it, with the views on an
+ * nvx x nvy grid and the lights on an nlx x nly grid (flat index x fastest).
+ * R(dv, dl) = the mean of C(v1, v2, l1, l2) over all entries with view offset
+ * v1 - v2 = dv and light offset l1 - l2 = dl: the diagonal means that
+ * examples/memoryEffectMeasurements/memoryEffectMeasurements.m:72-86 takes
+ * one pair of directions at a time.  R: complex FP32 (2 floats each),
+ * (2nvx-1)(2nvy-1) view offsets fastest, then (2nlx-1)(2nly-1) light
+ * offsets; offset (dx, dy) at index (dx + nx - 1) + (2nx - 1)(dy + ny - 1).
+ * _device: C1, C2, R in device memory, work on `stream`. */
+int scmc_cov_offsets(const double *C1, const double *C2, int32_t nvx, int32_t nvy, int32_t nlx, int32_t nly,
+                     float *R, int32_t device);
+int scmc_cov_offsets_device(const double *d_C1, const double *d_C2, int32_t nvx, int32_t nvy, int32_t nlx,
+                            int32_t nly, float *d_R, int32_t device, void *stream);
+
 /* Library information and error reporting. */
 int scmc_abi_version(void);
 const char *scmc_last_error(void);

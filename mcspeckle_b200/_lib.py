@@ -85,6 +85,12 @@ def lib():
                                    C.c_int32, dp]
         L.scmc_sample_cov.argtypes = [dp, C.c_int64, C.c_int64, C.c_uint64, C.c_int32, dp]
         L.scmc_profile_enable.argtypes = [C.c_int32]
+        fp = C.POINTER(C.c_float)
+        L.scmc_cov_offsets.argtypes = [dp, dp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, fp, C.c_int32]
+        L.scmc_cov_offsets_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                              C.c_void_p, C.c_int32, C.c_void_p]
+        L.scmc_cov_offsets.restype = C.c_int
+        L.scmc_cov_offsets_device.restype = C.c_int
         L.scmc_test_wait_fault.argtypes = [C.c_int32]
         L.scmc_test_wait_fault.restype = C.c_int
         L.scmc_profile_read.argtypes = [C.POINTER(_abi.StageTimes), C.c_int32]

@@ -233,4 +233,69 @@ __global__ void sample_product_kernel(const double *__restrict__ S, int64_t N, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// Memory-effect view of a covariance.  C(v1, v2, l1, l2) (v1 fastest, the
+// scmc layout) with the views on an nvx x nvy grid and the lights on an
+// nlx x nly grid (flat index x fastest) is reduced to the mean over all
+// entries with the same view offset v1 - v2 and light offset l1 - l2:
+//   R(dv, dl) = 1/(n(dv) n(dl)) sum_{v1 - v2 = dv, l1 - l2 = dl} C(v1, v2, l1, l2),
+// n(d) = (nx - |dx|)(ny - |dy|) the number of pairs with offset d, stored
+// with offset index (dx + nx - 1) + (2 nx - 1)(dy + ny - 1), view offset
+// fastest, complex FP32.  examples/memoryEffectMeasurements/
+// memoryEffectMeasurements.m:72-86 takes such means along diagonals of C.
+// One CTA per light pair (l1, l2): its nv x nv block is contiguous, so the
+// reads are coalesced; block sums per view offset collect in shared memory
+// (FP64) and are added once into the FP64 sums of (view offset, light offset).
+// Every element of C is read once: the kernel is HBM bound.
+// ---------------------------------------------------------------------------
+struct OffsetGrid {
+    int nvx, nvy, nlx, nly;
+};
+
+__global__ void __launch_bounds__(256) offsets_sum_kernel(const double2 *__restrict__ C1,
+                                                          const double2 *__restrict__ C2, OffsetGrid g,
+                                                          double2 *__restrict__ sums)
+{
+    extern __shared__ double2 part[];  // one per view offset
+    const int nv = g.nvx * g.nvy, nl = g.nlx * g.nly;
+    const int ovx = 2 * g.nvx - 1, nvo = ovx * (2 * g.nvy - 1), olx = 2 * g.nlx - 1;
+    for (int o = threadIdx.x; o < nvo; o += blockDim.x) part[o] = make_double2(0.0, 0.0);
+    __syncthreads();
+    const int l1 = blockIdx.x % nl, l2 = blockIdx.x / nl;
+    const int64_t base = (int64_t)nv * nv * blockIdx.x;  // (l1, l2) block, l1 fastest
+    for (int64_t k = threadIdx.x; k < (int64_t)nv * nv; k += blockDim.x) {
+        const int v1 = (int)(k % nv), v2 = (int)(k / nv);
+        double2 c = C1[base + k];
+        if (C2) {
+            const double2 d = C2[base + k];
+            c.x += d.x;
+            c.y += d.y;
+        }
+        const int dx = v1 % g.nvx - v2 % g.nvx, dy = v1 / g.nvx - v2 / g.nvx;
+        const int o = (dx + g.nvx - 1) + ovx * (dy + g.nvy - 1);
+        atomicAdd(&part[o].x, c.x);
+        atomicAdd(&part[o].y, c.y);
+    }
+    __syncthreads();
+    const int ldx = l1 % g.nlx - l2 % g.nlx, ldy = l1 / g.nlx - l2 / g.nlx;
+    const int lo = (ldx + g.nlx - 1) + olx * (ldy + g.nly - 1);
+    for (int o = threadIdx.x; o < nvo; o += blockDim.x) {
+        atomicAdd(&sums[(int64_t)lo * nvo + o].x, part[o].x);
+        atomicAdd(&sums[(int64_t)lo * nvo + o].y, part[o].y);
+    }
+}
+
+__global__ void offsets_finalize_kernel(const double2 *__restrict__ sums, OffsetGrid g, float2 *__restrict__ R)
+{
+    const int ovx = 2 * g.nvx - 1, nvo = ovx * (2 * g.nvy - 1), olx = 2 * g.nlx - 1;
+    const int64_t n = (int64_t)nvo * olx * (2 * g.nly - 1);
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int o = (int)(k % nvo), lo = (int)(k / nvo);
+        const int dvx = o % ovx - (g.nvx - 1), dvy = o / ovx - (g.nvy - 1);
+        const int dlx = lo % olx - (g.nlx - 1), dly = lo / olx - (g.nly - 1);
+        const double cnt = (double)(g.nvx - abs(dvx)) * (g.nvy - abs(dvy)) * (g.nlx - abs(dlx)) * (g.nly - abs(dly));
+        R[k] = make_float2((float)(sums[k].x / cnt), (float)(sums[k].y / cnt));
+    }
+}
+
 }  // namespace scmc

@@ -224,7 +224,7 @@ struct Ctx {
     DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
-    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl;
+    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl, offs;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_twt, fq_rr, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
@@ -257,7 +257,7 @@ struct Ctx {
     {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
-                         &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl,
+                         &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl, &offs,
                          &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_twt, &fq_rr, &fq_counts, &fq_offsets,
                          &fq_cursor, &fq_planes};
         for (DevBuf *b : all) f(*b);
@@ -2248,6 +2248,77 @@ int scmc_sample_cov(const double *C, int64_t N, int64_t n_samples, uint64_t seed
         CK(cudaGetLastError());
         LAUNCHED();
         CK(cudaMemcpy(Z, dZ, N * n_samples * sizeof(double2), cudaMemcpyDeviceToHost));
+    });
+}
+
+// ---------------------------------------------------------------------------
+// memory-effect view: means of a covariance over equal view / light offsets
+// ---------------------------------------------------------------------------
+static void offsets_run(Ctx &c, const double *d_C1, const double *d_C2, const OffsetGrid &g, float *d_R,
+                        cudaStream_t st)
+{
+    const int nv = g.nvx * g.nvy, nl = g.nlx * g.nly;
+    const int64_t nvo = (int64_t)(2 * g.nvx - 1) * (2 * g.nvy - 1);
+    const int64_t nlo = (int64_t)(2 * g.nlx - 1) * (2 * g.nly - 1);
+    const size_t smem = (size_t)nvo * sizeof(double2);
+    if (smem > 200 * 1024) fail(SCMC_ERR_INVALID, "view grid too large for the offset reduction");
+    double2 *sums = reinterpret_cast<double2 *>(c.offs.ensure((size_t)nvo * nlo * sizeof(double2)));
+    CK(cudaMemsetAsync(sums, 0, (size_t)nvo * nlo * sizeof(double2), st));
+    if (smem > 48 * 1024)
+        CK(cudaFuncSetAttribute(offsets_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    {
+        StageScope sc(ST_FINAL, st);
+        offsets_sum_kernel<<<(unsigned)((int64_t)nl * nl), 256, smem, st>>>(
+            reinterpret_cast<const double2 *>(d_C1), reinterpret_cast<const double2 *>(d_C2), g, sums);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        offsets_finalize_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((nvo * nlo + 255) / 256, 4096)), 256, 0,
+                                  st>>>(sums, g, reinterpret_cast<float2 *>(d_R));
+        CK(cudaGetLastError());
+        LAUNCHED();
+    }
+    (void)nv;
+}
+
+static OffsetGrid offsets_grid(int32_t nvx, int32_t nvy, int32_t nlx, int32_t nly)
+{
+    if (nvx < 1 || nvy < 1 || nlx < 1 || nly < 1) fail(SCMC_ERR_INVALID, "grid sizes must be positive");
+    if ((int64_t)nvx * nvy > 65536 || (int64_t)nlx * nly > 65536) fail(SCMC_ERR_INVALID, "grid too large");
+    return OffsetGrid{nvx, nvy, nlx, nly};
+}
+
+int scmc_cov_offsets_device(const double *d_C1, const double *d_C2, int32_t nvx, int32_t nvy, int32_t nlx,
+                            int32_t nly, float *d_R, int32_t device, void *stream)
+{
+    return guarded([&] {
+        if (!d_C1 || !d_R) fail(SCMC_ERR_INVALID, "null covariance or output");
+        const OffsetGrid g = offsets_grid(nvx, nvy, nlx, nly);
+        Ctx &c = context(device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        CK(cudaSetDevice(device));
+        offsets_run(c, d_C1, d_C2, g, d_R, reinterpret_cast<cudaStream_t>(stream));
+    });
+}
+
+int scmc_cov_offsets(const double *C1, const double *C2, int32_t nvx, int32_t nvy, int32_t nlx, int32_t nly,
+                     float *R, int32_t device)
+{
+    return guarded([&] {
+        if (!C1 || !R) fail(SCMC_ERR_INVALID, "null covariance or output");
+        const OffsetGrid g = offsets_grid(nvx, nvy, nlx, nly);
+        Ctx &c = context(device);
+        std::lock_guard<std::mutex> lk(c.mu);
+        CK(cudaSetDevice(device));
+        const int64_t nv = (int64_t)nvx * nvy, nl = (int64_t)nlx * nly;
+        const size_t cb = (size_t)nv * nv * nl * nl * sizeof(double2);
+        const int64_t nout = (int64_t)(2 * nvx - 1) * (2 * nvy - 1) * (2 * nlx - 1) * (2 * nly - 1);
+        double *d1 = reinterpret_cast<double *>(c.acc_s.ensure(cb));
+        double *d2 = C2 ? reinterpret_cast<double *>(c.acc_m.ensure(cb)) : nullptr;
+        float *dR = reinterpret_cast<float *>(c.out0.ensure((size_t)nout * sizeof(float2)));
+        CK(cudaMemcpy(d1, C1, cb, cudaMemcpyHostToDevice));
+        if (C2) CK(cudaMemcpy(d2, C2, cb, cudaMemcpyHostToDevice));
+        offsets_run(c, d1, d2, g, dR, 0);
+        CK(cudaMemcpy(R, dR, (size_t)nout * sizeof(float2), cudaMemcpyDeviceToHost));
     });
 }
 

@@ -72,3 +72,54 @@ def sample_from_cov(Cmat, n_samples=1, seed=0, *, device=0):
     if shape4:
         return z.reshape(Cm.shape[0], Cm.shape[2], int(n_samples), order="F")
     return z
+
+
+def memory_effect_offsets(C1, C2=None, *, views_grid, lights_grid, device=0):
+    """The memory-effect view of scmc's covariance C(v1, v2, l1, l2) (+ C2,
+    e.g. Ms + Mm): the mean over all entries with the same view offset
+    v1 - v2 and light offset l1 - l2 on the views' (nvx, nvy) and the lights'
+    (nlx, nly) grids (flat index x fastest), the diagonal means that
+    examples/memoryEffectMeasurements/memoryEffectMeasurements.m:72-86 takes.
+    Returns complex64 R[dvx, dvy, dlx, dly], offset d at index d + n - 1."""
+    nvx, nvy = (int(x) for x in views_grid)
+    nlx, nly = (int(x) for x in lights_grid)
+    c1 = np.ascontiguousarray(np.asarray(C1, dtype=np.complex128).reshape(-1, order="F"))
+    if c1.size != (nvx * nvy) ** 2 * (nlx * nly) ** 2:
+        raise ValueError("C does not match the grids")
+    c2 = None
+    if C2 is not None:
+        c2 = np.ascontiguousarray(np.asarray(C2, dtype=np.complex128).reshape(-1, order="F"))
+        if c2.size != c1.size:
+            raise ValueError("C1 and C2 differ in size")
+    shape = (2 * nvx - 1, 2 * nvy - 1, 2 * nlx - 1, 2 * nly - 1)
+    out = np.zeros(2 * int(np.prod(shape)), dtype=np.float32)
+    _lib.check(_lib.lib().scmc_cov_offsets(c1.view(np.float64).ctypes.data_as(_dp),
+                                           None if c2 is None else c2.view(np.float64).ctypes.data_as(_dp),
+                                           nvx, nvy, nlx, nly, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                           int(device)))
+    return out.view(np.complex64).reshape(shape, order="F")
+
+
+def memory_effect_offsets_numpy(Cmat, views_grid, lights_grid):
+    """The same reduction in NumPy (FP64), for checks."""
+    nvx, nvy = views_grid
+    nlx, nly = lights_grid
+    Cm = np.asarray(Cmat).reshape(nvx, nvy, nvx, nvy, nlx, nly, nlx, nly, order="F")
+    R = np.zeros((2 * nvx - 1, 2 * nvy - 1, 2 * nlx - 1, 2 * nly - 1), dtype=np.complex128)
+    cnt = np.zeros(R.shape)
+    ix = np.arange(nvx)
+    iy = np.arange(nvy)
+    jx = np.arange(nlx)
+    jy = np.arange(nly)
+    dvx = (ix[:, None] - ix[None, :]) + nvx - 1      # (v1x, v2x)
+    dvy = (iy[:, None] - iy[None, :]) + nvy - 1
+    dlx = (jx[:, None] - jx[None, :]) + nlx - 1
+    dly = (jy[:, None] - jy[None, :]) + nly - 1
+    a = dvx[:, None, :, None, None, None, None, None]
+    b = dvy[None, :, None, :, None, None, None, None]
+    c = dlx[None, None, None, None, :, None, :, None]
+    d = dly[None, None, None, None, None, :, None, :]
+    A, B, Cc, D = np.broadcast_arrays(a, b, c, d)
+    np.add.at(R, (A.ravel(), B.ravel(), Cc.ravel(), D.ravel()), Cm.ravel())
+    np.add.at(cnt, (A.ravel(), B.ravel(), Cc.ravel(), D.ravel()), 1.0)
+    return R / cnt

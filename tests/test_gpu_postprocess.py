@@ -95,3 +95,49 @@ def test_sample_cov_singular_is_an_error(gpu):
     C[0, 0] = 1.0
     with pytest.raises(_lib.ScmcError):
         PP.sample_from_cov(C, 1, 0)
+
+
+def test_memory_effect_offsets_match_numpy(gpu):
+    """The offset-mean reduction (memoryEffectMeasurements.m:72-86) on the GPU
+    against NumPy: a random covariance on uneven grids, and Ms + Mm of the
+    64 x 64 covariance configuration (8 x 8 view and light grids)."""
+    from mcspeckle_b200 import mc as MC
+    from mcspeckle_b200 import postprocess as PP
+    from mcspeckle_b200 import workloads as WL
+    g = np.random.default_rng(3)
+    nvx, nvy, nlx, nly = 3, 5, 4, 2
+    nv, nl = nvx * nvy, nlx * nly
+    A = g.normal(size=(nv, nv, nl, nl)) + 1j * g.normal(size=(nv, nv, nl, nl))
+    B = g.normal(size=A.shape) + 1j * g.normal(size=A.shape)
+    R = PP.memory_effect_offsets(A, B, views_grid=(nvx, nvy), lights_grid=(nlx, nly))
+    Rn = PP.memory_effect_offsets_numpy(A + B, (nvx, nvy), (nlx, nly))
+    assert R.dtype == np.complex64 and R.shape == Rn.shape
+    assert np.linalg.norm(R - Rn) / np.linalg.norm(Rn) < 1e-6
+    # the configuration's own geometry (grid_rect flattens x-major: ix * 8 + iy, so
+    # the grid's fast axis is its y axis)
+    Ms, Mm = MC.cov_from_args(MC.mc_args(*WL.cov64_args(2000), seed=5, precision="fp16"))
+    R = PP.memory_effect_offsets(Ms, Mm, views_grid=(8, 8), lights_grid=(8, 8))
+    Rn = PP.memory_effect_offsets_numpy(Ms + Mm, (8, 8), (8, 8))
+    assert R.shape == (15, 15, 15, 15)
+    assert np.linalg.norm(R - Rn) / np.linalg.norm(Rn) < 1e-6
+    # zero offset: the mean of the diagonal intensities is real and positive
+    assert abs(Rn[7, 7, 7, 7].imag) < 1e-9 * abs(Rn[7, 7, 7, 7]) and Rn[7, 7, 7, 7].real > 0
+
+
+def test_memory_effect_offsets_device_entry(gpu):
+    import torch
+
+    from mcspeckle_b200 import _lib
+    from mcspeckle_b200 import postprocess as PP
+    g = np.random.default_rng(4)
+    nvx, nvy, nlx, nly = 4, 4, 2, 2
+    nv, nl = 16, 4
+    A = g.normal(size=(nv, nv, nl, nl)) + 1j * g.normal(size=(nv, nv, nl, nl))
+    dA = torch.from_numpy(np.ascontiguousarray(A.reshape(-1, order="F")).view(np.float64)).cuda()
+    nout = 7 * 7 * 3 * 3
+    dR = torch.zeros(2 * nout, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib().scmc_cov_offsets_device(dA.data_ptr(), None, nvx, nvy, nlx, nly, dR.data_ptr(), 0, None))
+    torch.cuda.synchronize()
+    R = dR.cpu().numpy().view(np.complex64).reshape(7, 7, 3, 3, order="F")
+    Rn = PP.memory_effect_offsets_numpy(A, (nvx, nvy), (nlx, nly))
+    assert np.linalg.norm(R - Rn) / np.linalg.norm(Rn) < 1e-6
