@@ -60,6 +60,9 @@ typedef struct {
     int32_t table_n;           /* length of the tabulated tables */
     const double *eval_amp;    /* 2*table_n doubles: interleaved complex evalAmp */
     const double *sample_icdf; /* table_n doubles: sampleIcdf (angles) */
+    int32_t table_in_cos;      /* extension, 3-D only: 0 = the reference's tables on angle bins
+                                  (evalAmp at theta_i = i pi/(n-1), sampleIcdf angles); 1 = on cos(theta)
+                                  bins: evalAmp at cos_i = 1 - 2i/(n-1), sampleIcdf holds cosines */
 } scmc_phase_function;
 
 /* Positional arguments of MCfield / MCcov (MCfield.m:1, MCcov.m:1) plus the
@@ -219,6 +222,11 @@ typedef struct {
     int32_t has_lrad;           /* 17th argument of MCCovHetro (plane launch radius) */
     double lrad;
     double null_basis[6];
+    int32_t trilinear;          /* extension: 0 = the reference's nearest voxel (findBin.m); 1 = sigt
+                                   interpolated trilinearly between voxel centres (clamped at the faces)
+                                   in the Woodcock acceptance, the attenuation integral (exact per
+                                   piece between voxel-centre planes) and the first-scatter weight;
+                                   per-voxel albedo stays nearest */
 } scmc_hetero_args;
 
 int scmc_cov_hetero(const scmc_hetero_args *args, double *Ms, double *Mm, double *mean1);

@@ -34,6 +34,7 @@ class PhaseFunction(C.Structure):
         ("table_n", C.c_int32),
         ("eval_amp", _dp),
         ("sample_icdf", _dp),
+        ("table_in_cos", C.c_int32),
     ]
 
 
@@ -104,6 +105,7 @@ class HeteroArgs(C.Structure):
         ("has_lrad", C.c_int32),
         ("lrad", C.c_double),
         ("null_basis", C.c_double * 6),
+        ("trilinear", C.c_int32),
     ]
 
 
@@ -183,7 +185,9 @@ class ScatterSpec:
     """One (sct_type, ampfunc) pair in C form.
 
     `ampfunc` is 0 (isotropic), a scalar g (HG) or a mapping with the
-    `evalAmp` and `sampleIcdf` tables of tabulatedAmplitudeScatter.m:78-99.
+    `evalAmp` and `sampleIcdf` tables of tabulatedAmplitudeScatter.m:78-99
+    (with `cosBins` true: tables on cos(theta) bins, the extension of
+    interface.tabulatedAmplitudeScatterCos).
     """
 
     def __init__(self, sct_type: int, ampfunc):
@@ -191,6 +195,7 @@ class ScatterSpec:
         self.g = 0.0
         self.eval_amp = None
         self.sample_icdf = None
+        self.cos_bins = 0
         if self.sct_type == SCT_HG:
             self.g = float(np.asarray(ampfunc).reshape(-1)[0])
         elif self.sct_type == SCT_TABULATED:
@@ -200,6 +205,10 @@ class ScatterSpec:
                 raise ValueError("tabulated ampfunc needs evalAmp and sampleIcdf of equal length >= 2")
             self.eval_amp = np.ascontiguousarray(ea.view(np.float64))
             self.sample_icdf = np.ascontiguousarray(ic)
+            try:
+                self.cos_bins = int(bool(np.asarray(_field(ampfunc, "cosBins")).reshape(-1)[0]))
+            except (KeyError, AttributeError, TypeError, IndexError):
+                self.cos_bins = 0
         elif self.sct_type != SCT_ISOTROPIC:
             raise ValueError("sct_type must be 1, 2 or 3")
 
@@ -210,6 +219,7 @@ class ScatterSpec:
             pf.table_n = self.sample_icdf.size
             pf.eval_amp = _ptr(self.eval_amp)
             pf.sample_icdf = _ptr(self.sample_icdf)
+            pf.table_in_cos = self.cos_bins
         else:
             pf.table_n = 0
 

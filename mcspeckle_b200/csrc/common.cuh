@@ -25,7 +25,8 @@ struct PhaseFn {
     double g;
     int table_n;
     const double2 *eval_amp;   // table_n complex (evalAmp)
-    const double *sample_icdf; // table_n angles (sampleIcdf)
+    const double *sample_icdf; // table_n angles (sampleIcdf), or cosines with cos_bins
+    int cos_bins;              // tables on cos(theta) bins (extension) instead of angle bins
 };
 
 // Voxel medium of MCCovHetro.m / MCsampleHetro.m (device functions in hgrid.cuh).
@@ -46,6 +47,7 @@ struct HGrid {
     double inv_V;            // px = 1/V, V = sum(sigt) prod(box_bin)
     double lrad;
     double basis[6];         // null(meanl'), dim x (dim-1) column-major
+    int trilinear;           // extension: sigt trilinear between voxel centres
 };
 
 // Everything the walk needs, passed by value.
@@ -181,6 +183,15 @@ __device__ __forceinline__ double evaluate_hg(double c, double g)
     return (1.0 / 2.0 / SCMC_PI) * ((1.0 - g * g) / den);
 }
 
+// Nearest entry of a table on cos(theta) bins cos_i = 1 - 2i/(n-1) (the
+// extension; evaluated in FP64 in every precision mode so all modes read the
+// same entry).
+__device__ __forceinline__ int tab_cos_index(double cc, int n)
+{
+    long long idx = (long long)mround((1.0 - cc) * 0.5 * (double)(n - 1));
+    return (int)(idx < 0 ? 0 : (idx > n - 1 ? n - 1 : idx));
+}
+
 // evalampfunc_general.m:1-19 / evalampfunc_amplitude.m:1-9.
 template <int DIM>
 __device__ __forceinline__ double2 evalampfunc(double c, const PhaseFn &pf)
@@ -190,6 +201,7 @@ __device__ __forceinline__ double2 evalampfunc(double c, const PhaseFn &pf)
     }
     if (pf.sct_type == 2) {
         double cc = fmin(fmax(c, -1.0), 1.0);
+        if (pf.cos_bins) return pf.eval_amp[tab_cos_index(cc, pf.table_n)];
         double ang = acos(cc);
         double span = (DIM == 2) ? 2.0 * SCMC_PI : SCMC_PI;
         long long idx = (long long)mround(ang * (double)(pf.table_n - 1) / span);
@@ -262,7 +274,7 @@ __device__ __forceinline__ void smpampfunc_general(const double *ow, const Phase
         double stp = 1.0 / (double)(pf.table_n - 1);
         long long i = (long long)mround(r.rand() / stp);
         i = i > pf.table_n - 1 ? pf.table_n - 1 : i;
-        c = cos(pf.sample_icdf[i]);
+        c = pf.cos_bins ? pf.sample_icdf[i] : cos(pf.sample_icdf[i]);
     } else {
         c = sample_hg<DIM>(pf.g, r);
     }

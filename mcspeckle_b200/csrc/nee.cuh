@@ -236,6 +236,10 @@ amp_eval(double c, const PhaseFn &pf)
         if (pf.sct_type == 1) return make_float2((float)(1.0 / sqrt((DIM == 3 ? 4.0 : 2.0) * SCMC_PI)), 0.f);
         if (pf.sct_type == 2) {
             const double cc = fmin(fmax(c, -1.0), 1.0);
+            if (pf.cos_bins) {
+                const double2 t = pf.eval_amp[tab_cos_index(cc, pf.table_n)];
+                return make_float2((float)t.x, (float)t.y);
+            }
             float ang;
             if (cc >= 0.0) ang = 2.f * asinf(sqrtf((float)(0.5 * (1.0 - cc))));
             else ang = (float)SCMC_PI - 2.f * asinf(sqrtf((float)(0.5 * (1.0 + cc))));

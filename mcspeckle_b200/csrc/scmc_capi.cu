@@ -311,6 +311,7 @@ void validate_pf(const scmc_phase_function &pf, const char *name)
     if (pf.sct_type == SCMC_SCT_TABULATED && (pf.table_n < 2 || !pf.eval_amp || !pf.sample_icdf))
         fail(SCMC_ERR_INVALID, std::string("tabulated ") + name + " needs evalAmp and sampleIcdf tables");
     if (pf.sct_type == SCMC_SCT_HG && !(std::fabs(pf.g) <= 1.0)) fail(SCMC_ERR_INVALID, "Invalid g input");
+    if (pf.table_in_cos != 0 && pf.table_in_cos != 1) fail(SCMC_ERR_INVALID, "table_in_cos must be 0 or 1");
 }
 
 void validate(const scmc_mc_args *a)
@@ -328,6 +329,8 @@ void validate(const scmc_mc_args *a)
         if (!(a->box_max[k] >= a->box_min[k])) fail(SCMC_ERR_INVALID, "Invalid box size");
     validate_pf(a->ampfunc, "ampfunc");
     if (a->has_ampfunc0) validate_pf(a->ampfunc0, "ampfunc0");
+    if (a->dim != 3 && (a->ampfunc.table_in_cos || (a->has_ampfunc0 && a->ampfunc0.table_in_cos)))
+        fail(SCMC_ERR_INVALID, "tables on cos(theta) bins are 3-D only");
 }
 
 // ---------------------------------------------------------------------------
@@ -345,6 +348,7 @@ PhaseFn upload_pf(const scmc_phase_function &pf, DevBuf &amp, DevBuf &icdf, cuda
     d.sct_type = pf.sct_type;
     d.g = pf.g;
     d.table_n = pf.table_n;
+    d.cos_bins = pf.table_in_cos;
     if (pf.sct_type == SCMC_SCT_TABULATED) {
         size_t n = (size_t)pf.table_n;
         amp.ensure(n * sizeof(double2));
@@ -398,11 +402,13 @@ Prepared host_params(const scmc_mc_args *a, int want_phase)
     W.pf.sct_type = a->ampfunc.sct_type;
     W.pf.g = a->ampfunc.g;
     W.pf.table_n = a->ampfunc.table_n;
+    W.pf.cos_bins = a->ampfunc.table_in_cos;
     W.pf0 = W.pf;
     if (a->has_ampfunc0) {
         W.pf0.sct_type = a->ampfunc0.sct_type;
         W.pf0.g = a->ampfunc0.g;
         W.pf0.table_n = a->ampfunc0.table_n;
+        W.pf0.cos_bins = a->ampfunc0.table_in_cos;
     }
 
     NeeParams &Q = P.Q;
@@ -1203,6 +1209,8 @@ Prepared prepare_hetero(Ctx &c, const scmc_hetero_args *h, int want_phase, bool 
     g.cdf_step = (hi - lo) / (double)g.n_icdf;
     g.inv_V = 1.0 / (ssum * vb);  // px = 1/V, V = sum(sigt) prod(box_bin)
     g.lrad = h->has_lrad ? h->lrad : std::sqrt(diag);
+    if (h->trilinear != 0 && h->trilinear != 1) fail(SCMC_ERR_INVALID, "trilinear must be 0 or 1");
+    g.trilinear = h->trilinear;
     for (int k = 0; k < 6; ++k) g.basis[k] = h->null_basis[k];
     HeteroBufs &hb = g_hbufs[c.device];
     double *dsig = reinterpret_cast<double *>(hb.sigt.ensure(nv * sizeof(double)));

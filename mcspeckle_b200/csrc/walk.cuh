@@ -54,8 +54,8 @@ __device__ __forceinline__ double hg_woodcock(const HGrid &g, const double *x, c
 #pragma unroll
         for (int k = 0; k < DIM; ++k) nx[k] = x[k] + d * v[k];
         if (hg_outside(g, nx)) break;
-        const int64_t bi = hg_find_bin(g, nx, nullptr, nullptr);
-        if (r.rand() <= (g.sigt[bi] / g.sigt_max)) break;
+        const double sg = g.trilinear ? hg_sigma_tri<DIM>(g, nx) : g.sigt[hg_find_bin(g, nx, nullptr, nullptr)];
+        if (r.rand() <= (sg / g.sigt_max)) break;
     }
     return d;
 }
@@ -93,6 +93,12 @@ __device__ __forceinline__ bool hg_first_scatter(const WalkParams &P, PathRng &r
             s.x[k] = r.rand() * g.bbin[k] + bmn;
         }
         s.px = g.inv_V;
+        if (g.trilinear) {
+            // the voxel pick samples sigma_nearest(x) / V; the medium is
+            // sigma_trilinear: px carries their ratio (a zero trilinear
+            // sigma gives px = inf, a weight of 0)
+            s.px = g.inv_V * g.sigt[hg_find_bin(g, s.x, nullptr, nullptr)] / hg_sigma_tri<DIM>(g, s.x);
+        }
         return !hg_outside(g, s.x);
     }
     // expSmpXHetro.m:1-31: launch from a plane across meanl, enter the box,

@@ -49,7 +49,10 @@ class HeteroHolder:
 def hetero_args(cov: bool, sigt, albedo, box_min, box_max, box_bin, l, v, is_ff_l, is_ff_v, maxItr, lambda_,
                 doCBS, smpFlg, sct_type, ampfunc, ampfunc0=_MISSING, extra=_MISSING, *, seed=None,
                 precision=DEFAULT_PRECISION, device=0, path_offset=0, norm_itr=0, max_events_per_path=0,
-                basis=None) -> HeteroHolder:
+                basis=None, trilinear=False) -> HeteroHolder:
+    """The C argument struct.  trilinear=True (an extension, off by default)
+    interpolates sigt trilinearly between voxel centres instead of the
+    reference's nearest voxel (findBin.m)."""
     bmin = np.asarray(box_min, dtype=float).reshape(-1)
     bmax = np.asarray(box_max, dtype=float).reshape(-1)
     bbin = np.asarray(box_bin, dtype=float).reshape(-1)
@@ -94,6 +97,7 @@ def hetero_args(cov: bool, sigt, albedo, box_min, box_max, box_bin, l, v, is_ff_
     if lrad is not None:
         a.has_lrad = 1
         a.lrad = lrad
+    a.trilinear = int(bool(trilinear))
     # meanl as the reference forms it (MCCovHetro.m:38-39, MCsampleHetro.m:35-41)
     um = lmean0 if lmean0 is not None else L.mean(axis=1)
     meanl = um / np.linalg.norm(um)

@@ -215,3 +215,34 @@ def tabulatedAmplitudeScatter(theta, f, *albedo):
     amp["evalAmp"] = amp["evalPdf"] ** 0.5 * np.exp(1j * np.angle(fv))
     s["ampfunc"] = amp
     return s
+
+
+def tabulatedAmplitudeScatterCos(cs, f, *albedo):
+    """Extension (3-D): a measured amplitude f tabulated on cos(theta) bins
+    cs = 1 - 2i/(n-1), i = 0 .. n-1 (forward first), the form of the
+    tabulated phase function of the heterogeneous configuration.  Built as
+    tabulatedAmplitudeScatter.m:75-99 builds the angle-bin tables, with the
+    measure dOmega = 2 pi dcos: cross section 4 pi mean(|f|^2), sampling pdf
+    |f|^2 / sum |f|^2 over the bins, the inverse CDF by the nearest-grid
+    search of invCDF.m returning the bin's cosine, evalAmp = sqrt(|f|^2 / cs)
+    with f's phase.  The tables carry cosBins = True."""
+    if len(albedo) > 1:
+        raise InterfaceError("Too many input arguments.")
+    c = np.asarray(cs, dtype=float).reshape(-1)
+    fv = np.asarray(f).reshape(-1)
+    n = c.size
+    if fv.size != n or n < 2:
+        raise InterfaceError("cs and f must have same elements number")
+    if not np.allclose(c, 1.0 - 2.0 * np.arange(n) / (n - 1), rtol=0, atol=1e-12):
+        raise InterfaceError("cs must be the bins 1 - 2i/(n-1)")
+    a2 = np.abs(fv) ** 2
+    amp = {"cosBins": True, "cs_bins": c.copy(), "cs": float(np.mean(a2)) * 4 * math.pi}
+    amp["samplePdf"] = a2 / np.sum(a2)
+    amp["sampleCdf"] = np.cumsum(amp["samplePdf"])
+    grid = np.arange(n) * (1.0 / (n - 1))
+    idx = np.array([np.argmin(np.abs(amp["sampleCdf"] - grid[j])) for j in range(n)])
+    amp["sampleIcdf"] = c[idx]
+    amp["evalPdf"] = a2 / amp["cs"]
+    amp["evalAmp"] = amp["evalPdf"] ** 0.5 * np.exp(1j * np.angle(fv))
+    return {"albedo": _scalar(albedo[0]) if albedo else 1.0, "type": "scatter", "function": "tabulated", "D": 3,
+            "ampfunc": amp}

@@ -16,7 +16,9 @@ parity tests.  Every random choice comes from a fixed seed.
              plane-wave form, or HG g = 0.9 with a point source 2 MFP deep.
   hetero128  MCCovHetro, sigma_s on a 128^3 grid, log-normal(0, 0.5) per MFP,
              box 20 x 20 x 5 MFP, tabulated phase function on 1024 bins from a
-             seeded mixture of 3 HG lobes, 128 lights x 128 views.
+             seeded mixture of 3 HG lobes, 128 lights x 128 views; trilinear
+             sigma and cos(theta) bins as the configuration states them, or
+             the reference's nearest voxel and angle bins.
   served     uneven MCfield requests (lights 1-256, views 1-1024, log-uniform
              path budgets, media drawn per request).
 """
@@ -52,16 +54,23 @@ def hg_table(g, n=1001):
     return {"evalAmp": t["evalAmp"], "sampleIcdf": t["sampleIcdf"]}
 
 
-def hg_mixture_table(n_bins, seed):
+def hg_mixture_table(n_bins, seed, cos_bins=False):
     """Tabulated amplitude of a seeded mixture of 3 HG lobes (g in [-0.3, 0.95],
-    weights from Dirichlet(1,1,1)) on n_bins angles in [0, pi]."""
+    weights from Dirichlet(1,1,1)) on n_bins angles in [0, pi] (the
+    reference's tables), or on n_bins cos(theta) bins (the extension)."""
     from . import interface as I
     g_rng = np.random.default_rng(seed)
     gs = g_rng.uniform(-0.3, 0.95, 3)
     w = g_rng.dirichlet([1.0, 1.0, 1.0])
-    th = np.linspace(0, 1, n_bins) * np.pi
-    c = np.cos(th)
+    if cos_bins:
+        c = 1.0 - 2.0 * np.arange(n_bins) / (n_bins - 1)
+    else:
+        th = np.linspace(0, 1, n_bins) * np.pi
+        c = np.cos(th)
     pdf = sum(wk * (1 - gk * gk) / (4 * np.pi * (1 + gk * gk - 2 * gk * c) ** 1.5) for wk, gk in zip(w, gs))
+    if cos_bins:
+        t = I.tabulatedAmplitudeScatterCos(c, np.sqrt(pdf))["ampfunc"]
+        return {"evalAmp": t["evalAmp"], "sampleIcdf": t["sampleIcdf"], "cosBins": True}, gs.tolist(), w.tolist()
     t = I.tabulatedAmplitudeScatter(th, np.sqrt(pdf))["ampfunc"]
     return {"evalAmp": t["evalAmp"], "sampleIcdf": t["sampleIcdf"]}, gs.tolist(), w.tolist()
 
@@ -137,34 +146,41 @@ def fq256_propagating():
 _HGRID = {}
 
 
-def hetero128_medium():
-    """(sigma grid 128^3, tabulated table, lobe g's, lobe weights); cached."""
-    if "m" not in _HGRID:
+def hetero128_medium(extended=False):
+    """(sigma grid 128^3, tabulated table, lobe g's, lobe weights); cached.
+    extended: the table on cos(theta) bins instead of angle bins."""
+    key = "ext" if extended else "ref"
+    if key not in _HGRID:
         mfp = 10.0
         g = np.random.default_rng(4)
         sig = np.exp(g.normal(0.0, 0.5, (128, 128, 128))) / mfp
-        table, gs, ws = hg_mixture_table(1024, 5)
-        _HGRID["m"] = (sig, table, gs, ws)
-    return _HGRID["m"]
+        table, gs, ws = hg_mixture_table(1024, 5, cos_bins=extended)
+        _HGRID[key] = (sig, table, gs, ws)
+    return _HGRID[key]
 
 
-def hetero128_desc():
-    _, _, gs, ws = hetero128_medium()
-    return (f"MCCovHetro, sigma_s on a 128^3 grid log-normal(0, 0.5) per MFP (MFP 10 wavelengths, nearest voxel as "
-            f"the reference), box 20x20x5 MFP, Woodcock tracking, tabulated phase function on 1024 theta bins from "
-            f"3 HG lobes g={[round(x, 3) for x in gs]} w={[round(x, 3) for x in ws]}, 128 lights x 128 views (16x8 "
-            f"grids of +-5 deg), CBS")
+def hetero128_desc(extended=True):
+    _, _, gs, ws = hetero128_medium(extended)
+    lookup = "trilinear between voxel centres" if extended else "nearest voxel as the reference"
+    bins = "cos(theta)" if extended else "theta"
+    return (f"MCCovHetro, sigma_s on a 128^3 grid log-normal(0, 0.5) per MFP (MFP 10 wavelengths, {lookup}), box "
+            f"20x20x5 MFP, Woodcock tracking, tabulated phase function on 1024 {bins} bins from 3 HG lobes "
+            f"g={[round(x, 3) for x in gs]} w={[round(x, 3) for x in ws]}, 128 lights x 128 views (16x8 grids of "
+            f"+-5 deg), CBS")
 
 
-def hetero128_args(n, *, seed, precision, path_offset=0, norm_itr=0):
+def hetero128_args(n, *, seed, precision, path_offset=0, norm_itr=0, extended=True):
+    """extended: trilinear sigma and the cos(theta)-bin table (the
+    configuration as stated); False: the reference's nearest voxel and angle
+    bins."""
     from . import hetero as H
-    sig, table, _, _ = hetero128_medium()
+    sig, table, _, _ = hetero128_medium(extended)
     bmin, bmax = np.array([-100.0, -100.0, 0.0]), np.array([100.0, 100.0, 50.0])
     bbin = (bmax - bmin) / 128.0
     l = grid_rect(16, 8, 5.0, +1.0)
     v = grid_rect(16, 8, 5.0, -1.0)
     return H.hetero_args(True, sig, 1.0, bmin, bmax, bbin, l, v, 1, 1, int(n), 1.0, True, 2, 2, table, seed=seed,
-                         precision=precision, path_offset=path_offset, norm_itr=norm_itr)
+                         precision=precision, path_offset=path_offset, norm_itr=norm_itr, trilinear=extended)
 
 
 # ---------------------------------------------------------------------------

@@ -212,6 +212,12 @@ static cplx evalampfunc(double c, const scmc_phase_function *pf, int dim)
         return 1.0 / sqrt(pow(2.0, dim - 1) * M_PI);
     case SCMC_SCT_TABULATED: {
         double cc = c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
+        if (pf->table_in_cos) { /* extension: cos(theta) bins cos_i = 1 - 2i/(n-1) */
+            int64_t i = (int64_t)mround((1.0 - cc) * 0.5 * (double)(pf->table_n - 1));
+            if (i < 0) i = 0;
+            if (i > pf->table_n - 1) i = pf->table_n - 1;
+            return pf->eval_amp[2 * i] + I * pf->eval_amp[2 * i + 1];
+        }
         double ang = acos(cc);
         int n = pf->table_n;
         double span = (dim == 2) ? 2.0 * M_PI : M_PI;
@@ -288,7 +294,9 @@ static void smpampfunc_general(const double *ow, const scmc_phase_function *pf, 
                                double *w, rng_t *r)
 {
     if (pf->sct_type == SCMC_SCT_ISOTROPIC) { randn_dir(dim, w, r); return; }
-    double c = (pf->sct_type == SCMC_SCT_TABULATED) ? cos(smpampfunc(pf, r)) : sample_hg(pf->g, dim, r);
+    double c = (pf->sct_type == SCMC_SCT_TABULATED)
+                   ? (pf->table_in_cos ? smpampfunc(pf, r) : cos(smpampfunc(pf, r)))  /* cos bins: icdf holds cosines */
+                   : sample_hg(pf->g, dim, r);
     rotate_by_theta(ow, c, dim, w, r);
 }
 
@@ -860,6 +868,7 @@ typedef struct {
     int64_t nb[3];
     double sigt_max;
     int bad;  /* a voxel march ran away (guard) */
+    int trilinear; /* extension: sigt trilinear between voxel centres */
 } grid_t;
 
 static void grid_init(grid_t *g, const scmc_hetero_args *a)
@@ -879,6 +888,7 @@ static void grid_init(grid_t *g, const scmc_hetero_args *a)
     }
     g->sigt_max = -INFINITY;
     for (int64_t i = 0; i < n; ++i) g->sigt_max = fmax(g->sigt_max, g->sigt[i]);
+    g->trilinear = a->trilinear;
 }
 
 static int64_t grid_count(const grid_t *g)
@@ -933,6 +943,70 @@ static double cube_dist_exit(const double *x, const double *vmin, const double *
     return d;
 }
 
+/* Extension: sigma interpolated trilinearly between the voxel centres
+ * bmin + (i + 1/2) bbin, clamped to the outer centres. */
+static double sigma_tri(const grid_t *g, const double *x)
+{
+    int64_t i0[3] = {0, 0, 0};
+    double f[3] = {0, 0, 0};
+    for (int k = 0; k < g->dim; ++k) {
+        double u = (x[k] - g->bmin[k]) / g->bbin[k] - 0.5;
+        if (u < 0) u = 0;
+        if (u > (double)(g->nb[k] - 1)) u = (double)(g->nb[k] - 1);
+        int64_t i = (int64_t)floor(u);
+        if (i > g->nb[k] - 2) i = g->nb[k] - 2;
+        if (i < 0) i = 0;
+        i0[k] = i;
+        f[k] = g->nb[k] > 1 ? u - (double)i : 0.0;
+    }
+    double s = 0.0;
+    for (int c = 0; c < (1 << g->dim); ++c) {
+        int64_t idx = 0, stride = 1;
+        double w = 1.0;
+        for (int k = 0; k < g->dim; ++k) {
+            int b = (c >> k) & 1;
+            idx += ((g->nb[k] > 1) ? i0[k] + b : 0) * stride;
+            stride *= g->nb[k];
+            w *= b ? f[k] : 1.0 - f[k];
+        }
+        if (w != 0.0) s += w * g->sigt[idx];
+    }
+    return s;
+}
+
+/* Extension: the optical depth of the trilinear sigma from x along m over
+ * min(nd, distance to the box), cut at every voxel-centre plane crossing;
+ * sigma is a cubic in t on each piece and Simpson's rule is exact there. */
+static double optical_depth_tri(const grid_t *g, const double *x, const double *m, double nd)
+{
+    const int dim = g->dim;
+    double tend = INFINITY, tn[3], dt[3];
+    for (int k = 0; k < dim; ++k) {
+        if (m[k] > 0) tend = fmin(tend, (g->bmax[k] - x[k]) / m[k]);
+        else if (m[k] < 0) tend = fmin(tend, (x[k] - g->bmin[k]) / -m[k]);
+        double u = (x[k] - g->bmin[k]) / g->bbin[k] - 0.5;
+        if (m[k] > 0) { tn[k] = (floor(u) + 1.0 - u) * g->bbin[k] / m[k]; dt[k] = g->bbin[k] / m[k]; }
+        else if (m[k] < 0) { tn[k] = (u - (ceil(u) - 1.0)) * g->bbin[k] / -m[k]; dt[k] = g->bbin[k] / -m[k]; }
+        else { tn[k] = INFINITY; dt[k] = INFINITY; }
+    }
+    tend = fmax(fmin(tend, nd), 0.0);
+    double t0 = 0.0, s0 = sigma_tri(g, x), tau = 0.0, p[3] = {0, 0, 0};
+    while (t0 < tend) {
+        double t1 = tend;
+        for (int k = 0; k < dim; ++k) t1 = fmin(t1, tn[k]);
+        for (int k = 0; k < dim; ++k) if (tn[k] <= t1) tn[k] += dt[k];
+        double tm = 0.5 * (t0 + t1);
+        for (int k = 0; k < dim; ++k) p[k] = x[k] + tm * m[k];
+        double sm = sigma_tri(g, p);
+        for (int k = 0; k < dim; ++k) p[k] = x[k] + t1 * m[k];
+        double s1 = sigma_tri(g, p);
+        tau += (t1 - t0) / 6.0 * (s0 + 4.0 * sm + s1);
+        t0 = t1;
+        s0 = s1;
+    }
+    return tau;
+}
+
 /* evalphaseattHetro.m:1-52 for one direction / position. */
 static cplx phaseatt_hetero(grid_t *g, const double *x, const double *v, int is_ff, double lambda)
 {
@@ -954,6 +1028,11 @@ static cplx phaseatt_hetero(grid_t *g, const double *x, const double *v, int is_
     double m[3], nx[3], bmn[3], bmx[3];
     for (int k = 0; k < dim; ++k) { m[k] = -dir[k]; nx[k] = x[k]; }
     double bdv = 0.0, wbdv = 0.0;
+    if (g->trilinear) {
+        wbdv = optical_depth_tri(g, x, m, nd);
+        double ph = (M_PI * 2.0 / lambda) * pv;
+        return exp(-(1.0 / 2.0 * wbdv)) * (cos(ph) + I * sin(ph)) * rv;
+    }
     for (int guard = 0; guard < 1000000; ++guard) {
         int64_t bi = find_bin(g, nx, bmn, bmx);
         double dd = cube_dist_exit(nx, bmn, bmx, m, dim, nx);
@@ -980,8 +1059,8 @@ static double smp_woodcock(grid_t *g, const double *x, const double *v, rng_t *r
         d = d - log(1 - rand_u(r)) / g->sigt_max;
         for (int k = 0; k < g->dim; ++k) nx[k] = x[k] + d * v[k];
         if (outside(g, nx)) break;
-        int64_t bi = find_bin(g, nx, NULL, NULL);
-        if (rand_u(r) <= (g->sigt[bi] / g->sigt_max)) break;
+        double sg = g->trilinear ? sigma_tri(g, nx) : g->sigt[find_bin(g, nx, NULL, NULL)];
+        if (rand_u(r) <= (sg / g->sigt_max)) break;
         if (r->exhausted) break;
     }
     return d;
@@ -1110,6 +1189,8 @@ static int hetero_walk(const scmc_hetero_args *a, oracle_rng_spec *rs, hsink_t *
                 x[k] = rand_u(&r) * g.bbin[k] + bmn;
             }
             px = 1.0 / V;
+            /* extension: voxel pick density sigma_nearest / V, medium sigma_trilinear */
+            if (g.trilinear) px = g.sigt[find_bin(&g, x, NULL, NULL)] / (V * sigma_tri(&g, x));
         } else {
             if (exp_smp_x_hetero(&g, c.meanl, lrad, a->null_basis, x, &px, &r) != 0) {
                 if (r.exhausted) { rc = -1; break; }

@@ -87,12 +87,13 @@ def _rel_dev(x, ref):
     return (num / den) ** 0.5
 
 
-def test_hetero128_geometry_against_oracle(gpu, oracle_lib):
+@pytest.mark.parametrize("extended", [False, True], ids=["reference_form", "trilinear_cos_bins"])
+def test_hetero128_geometry_against_oracle(gpu, oracle_lib, extended):
     """The covariance outputs are 2 x 4.3 GB: the oracle's are moved to the
     device once and compared there, chunk by chunk."""
     import torch
 
-    h = WL.hetero128_args(8, seed=79, precision="fp64")
+    h = WL.hetero128_args(8, seed=79, precision="fp64", extended=extended)
     Mso, Mmo, m1o = oracle_lib.cov_hetero(h, oracle_lib.Rng.philox(), threads=THREADS)
     ref = [torch.from_numpy(x.reshape(-1, order="F").view(np.float64)).cuda() for x in (Mso, Mmo, m1o)]
     del Mso, Mmo
@@ -101,7 +102,7 @@ def test_hetero128_geometry_against_oracle(gpu, oracle_lib):
         assert _rel_dev(g, r) < FP64_TOL
     del got
     for prec in ("fp16", "mixed"):
-        got = _device_cov_hetero(WL.hetero128_args(8, seed=79, precision=prec))
+        got = _device_cov_hetero(WL.hetero128_args(8, seed=79, precision=prec, extended=extended))
         for g, r in zip(got[:2], ref[:2]):
             assert _rel_dev(g, r) < MIXED_TOL, prec
         del got
