@@ -66,6 +66,7 @@ struct WalkParams {
     int64_t max_events;        // 0 = unlimited
     int hetero;                // voxel medium (Woodcock flights, voxel albedo)
     HGrid hg;
+    int any_order;             // records may be written in any order (one-pass walk); 0 keeps path order
 };
 
 // ---------------------------------------------------------------------------

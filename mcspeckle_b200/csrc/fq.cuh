@@ -298,12 +298,38 @@ fq_accum_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ 
 // running sum in TMEM and adds that sum into the output once; the output of
 // this form is stored [light][r1][r2] (r2 fastest) in FP32.
 // ---------------------------------------------------------------------------
+// The entry scales s_e(j) of a plane group can span many decades (a point
+// source: 1/r and the attenuation), and FP16 keeps its relative precision
+// only above 2^-14.  The group's operands are therefore scaled by a power of
+// two 2^(13 - e), e the exponent of max |s_e| (exact in FP16 and FP32), which
+// the plane loop undoes when it adds a chain into U (fq_scale_exponent,
+// herk_tc.cuh).  fq_scale_kernel finds max |s_e| (as the ordered bits of a
+// non-negative float).
+__global__ void __launch_bounds__(256)
+fq_scale_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk,
+                int64_t nblk, int light, unsigned *__restrict__ max_bits)
+{
+    float m = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nblk * 32; i += (int64_t)gridDim.x * blockDim.x) {
+        const int2 bk = blk[i >> 5];
+        const int t = (int)(i & 31);
+        if (t < bk.y) {
+            const FqEntry en = E[bk.x + t];
+            const float2 sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, light, en.xl));
+            m = fmaxf(m, fmaxf(fabsf(sv.x), fabsf(sv.y)));
+        }
+    }
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && isfinite(m)) atomicMax(max_bits, __float_as_uint(m));
+}
+
 template <bool SPLIT>
 __global__ void __launch_bounds__(256)
 fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk,
                   int light, const float2 *__restrict__ Tt, int64_t K, __half *__restrict__ Ahi,
-                  __half *__restrict__ Alo, __half *__restrict__ Bm)
+                  __half *__restrict__ Alo, __half *__restrict__ Bm, const unsigned *__restrict__ max_bits)
 {
+    const float scale = ldexpf(1.f, fq_scale_exponent(max_bits));
     constexpr int RB = 64;  // twiddle rows staged per pass
     __shared__ float2 ss[32];
     __shared__ int sp1[32], sp2[32];
@@ -315,6 +341,8 @@ fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict_
         if ((int)threadIdx.x < bk.y) {
             const FqEntry en = E[bk.x + threadIdx.x];
             sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, light, en.xl));
+            sv.x *= scale;
+            sv.y *= scale;
             p1 = en.p1;
             p2 = en.p2;
         }

@@ -161,7 +161,16 @@ struct PlaneEpi {
     float *U;              // [r1][r2] complex interleaved FP32, this light
     int nv0;
     int n_uniform;         // planes 0 .. n_uniform-1 have centres bmin_z + (P + 1/2) z_bin
+    const unsigned *max_bits;  // the group's operand scale (fq_scale_exponent); the flush undoes it
 };
+
+// The exponent of the power-of-two operand scale of a FourierQuad plane
+// group: max |s_e| maps into [2^13, 2^14), well inside FP16's normal range.
+__device__ __forceinline__ int fq_scale_exponent(const unsigned *max_bits)
+{
+    const float m = __uint_as_float(*max_bits);
+    return m > 0.f ? 13 - ilogbf(m) : 0;
+}
 
 // Bounded waits can be made to run out on purpose (scmc_test_wait_fault):
 // the producer then issues no copy and the consumers wait only this long, so
@@ -515,6 +524,7 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
             tc_fence_after();
             const uint32_t tacc = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * TC_TMEM_COLS);
             const double tz = (pe.gz[P] + pe.gz[P + 1]) / 2;
+            const float unscale = ldexpf(1.f, -fq_scale_exponent(pe.max_bits));
             for (int c0 = 0; c0 < TC_BN; c0 += 32) {
                 uint32_t a[32];
                 tmem_ld32(tacc + c0, a);
@@ -533,7 +543,7 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
                         const double2 z = ok ? pe.zexp0[(int64_t)n * pe.nv0 + r1] : make_double2(0.0, 0.0);
                         float sn, cs;
                         __sincosf((float)reduce_2pi(z.y * tz), &sn, &cs);
-                        const float mag = ok ? expf((float)(z.x * tz)) : 0.f;
+                        const float mag = ok ? expf((float)(z.x * tz)) * unscale : 0.f;
                         fx[t] = mag * cs;
                         fy[t] = mag * sn;
                     }

@@ -227,6 +227,7 @@ struct Ctx {
     DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl, offs;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_twt, fq_rr, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
+    double multi_per_path = 8.0;  // multiple-scattering events per path seen so far (one-pass capacity)
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
     // Extra streams and events of the covariance pipeline: the walk and row
     // generation run on `aux`, contractions alternate between the caller's
@@ -399,6 +400,9 @@ Prepared host_params(const scmc_mc_args *a, int want_phase)
     W.key0 = (uint32_t)a->seed;
     W.key1 = (uint32_t)(a->seed >> 32);
     W.max_events = a->max_events_per_path;
+    // the reduced-precision modes walk once and take the records in any order;
+    // FP64 (parity) keeps the two passes and path order
+    W.any_order = a->precision != SCMC_PREC_FP64;
     W.pf.sct_type = a->ampfunc.sct_type;
     W.pf.g = a->ampfunc.g;
     W.pf.table_n = a->ampfunc.table_n;
@@ -508,9 +512,92 @@ struct Batch {
     int64_t n_paths = 0, n_multi = 0;
 };
 
+void ensure_single_records(Ctx &c, int64_t n_paths)
+{
+    if (c.scap >= n_paths) return;
+    const int64_t cap = n_paths;
+    c.s_x1.ensure(3 * cap * 8);
+    c.s_w1.ensure(3 * cap * 8);
+    c.s_wpx.ensure(cap * 8);
+    c.s_xi.ensure(cap * 8);
+    c.s_nev.ensure(cap * 4);
+    c.scap = cap;
+}
+
+void ensure_multi_records(Ctx &c, int64_t n_multi)
+{
+    if (c.mcap >= std::max<int64_t>(n_multi, 1)) return;
+    const int64_t cap = std::max<int64_t>(n_multi + n_multi / 4, 1024);
+    c.m_x.ensure(3 * cap * 8);
+    c.m_ow.ensure(3 * cap * 8);
+    c.m_wpx.ensure(cap * 8);
+    c.m_xi.ensure(cap * 8);
+    c.m_path.ensure(cap * 4);
+    c.m_plen.ensure(cap * 4);
+    c.mcap = cap;
+}
+
+void batch_views(Ctx &c, int64_t n_paths, int64_t n_multi, Batch &B)
+{
+    B.S = SingleRec{c.s_x1.as<double>(), c.s_w1.as<double>(), c.s_wpx.as<double>(), c.s_xi.as<double>(),
+                    c.s_nev.as<int32_t>()};
+    B.M = MultiRec{c.m_x.as<double>(), c.m_ow.as<double>(), c.m_wpx.as<double>(), c.m_xi.as<double>(),
+                   c.m_path.as<int32_t>(), c.m_plen.as<int32_t>()};
+    B.n_paths = n_paths;
+    B.n_multi = n_multi;
+}
+
+// One walk pass writing records in any order (reduced-precision modes): the
+// multiple-scattering capacity comes from the events per path of earlier
+// batches; a batch with more events than that is walked again with room for
+// all of them.
+template <int DIM>
+void walk_batch_onepass(Ctx &c, WalkParams W, int64_t n_paths, cudaStream_t st, Batch &B)
+{
+    const int sms = sm_count(c.device);
+    const int threads = 128;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n_paths + threads - 1) / threads, (int64_t)sms * 8));
+    W.n_paths = n_paths;
+    ensure_single_records(c, n_paths);
+    ensure_multi_records(c, (int64_t)((double)n_paths * c.multi_per_path * 1.15) + 1024);
+    c.ctr.ensure(2 * sizeof(unsigned long long));
+    c.err.ensure(sizeof(int));
+    unsigned long long *ctr = c.ctr.as<unsigned long long>();
+    for (int attempt = 0;; ++attempt) {
+        batch_views(c, n_paths, 0, B);
+        CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+        CK(cudaMemsetAsync(c.err.p, 0, sizeof(int), st));
+        {
+            StageScope sc(ST_WALK, st);
+            walk_onepass_kernel<DIM><<<grid, threads, 0, st>>>(W, B.S, c.scap, B.M, c.mcap, ctr, c.err.as<int>());
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        unsigned long long n_multi = 0;
+        int herr = 0;
+        CK(cudaMemcpyAsync(&n_multi, ctr + 1, sizeof(n_multi), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&herr, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr) fail(SCMC_ERR_LIMIT, "a path exceeded max_events_per_path");
+        const double ratio = (double)n_multi / (double)std::max<int64_t>(n_paths, 1);
+        c.multi_per_path = std::max(ratio, 0.5 * c.multi_per_path);
+        if ((int64_t)n_multi <= c.mcap) {
+            batch_views(c, n_paths, (int64_t)n_multi, B);
+            prof_count(n_paths, n_paths + (int64_t)n_multi, 0.0);
+            return;
+        }
+        if (attempt > 0) fail(SCMC_ERR_CUDA, "one-pass walk: record count changed between two walks of a batch");
+        ensure_multi_records(c, (int64_t)n_multi);
+    }
+}
+
 template <int DIM>
 void walk_batch_dim(Ctx &c, WalkParams W, int64_t n_paths, cudaStream_t st, Batch &B)
 {
+    if (W.any_order) {
+        walk_batch_onepass<DIM>(c, W, n_paths, st, B);
+        return;
+    }
     const int sms = sm_count(c.device);
     const int threads = 128;
     int grid = (int)std::min<int64_t>((n_paths + threads - 1) / threads, (int64_t)sms * 8);
@@ -549,31 +636,9 @@ void walk_batch_dim(Ctx &c, WalkParams W, int64_t n_paths, cudaStream_t st, Batc
     const int64_t n_multi = last[0] + last[1];
 
     // record storage
-    if (c.scap < n_paths) {
-        int64_t cap = n_paths;
-        c.s_x1.ensure(3 * cap * 8);
-        c.s_w1.ensure(3 * cap * 8);
-        c.s_wpx.ensure(cap * 8);
-        c.s_xi.ensure(cap * 8);
-        c.s_nev.ensure(cap * 4);
-        c.scap = cap;
-    }
-    if (c.mcap < std::max<int64_t>(n_multi, 1)) {
-        int64_t cap = std::max<int64_t>(n_multi + n_multi / 4, 1024);
-        c.m_x.ensure(3 * cap * 8);
-        c.m_ow.ensure(3 * cap * 8);
-        c.m_wpx.ensure(cap * 8);
-        c.m_xi.ensure(cap * 8);
-        c.m_path.ensure(cap * 4);
-        c.m_plen.ensure(cap * 4);
-        c.mcap = cap;
-    }
-    B.S = SingleRec{c.s_x1.as<double>(), c.s_w1.as<double>(), c.s_wpx.as<double>(), c.s_xi.as<double>(),
-                    c.s_nev.as<int32_t>()};
-    B.M = MultiRec{c.m_x.as<double>(), c.m_ow.as<double>(), c.m_wpx.as<double>(), c.m_xi.as<double>(),
-                   c.m_path.as<int32_t>(), c.m_plen.as<int32_t>()};
-    B.n_paths = n_paths;
-    B.n_multi = n_multi;
+    ensure_single_records(c, n_paths);
+    ensure_multi_records(c, n_multi);
+    batch_views(c, n_paths, n_multi, B);
     CK(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), st));
     {
         StageScope sc(ST_WALK, st);
@@ -1093,6 +1158,7 @@ void export_records(const scmc_mc_args *a, int want_phase, int64_t capacity, dou
     cudaStream_t st = 0;
     Prepared P = prepare(c, a, want_phase, st);
     WalkParams W = P.W;
+    W.any_order = 0;  // the export is in path order
     int64_t total = 0;
     std::vector<Batch> dummy;
     // first pass: count all events
@@ -1393,6 +1459,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
     const size_t o_pl = o_kr + tc_align(kr.size() * sizeof(int2));
     const size_t o_pr = o_pl + tc_align(gpl.size() * sizeof(int));
     const size_t o_err = o_pr + tc_align(prs.size() * sizeof(int2));
+    const size_t o_max = o_err + 256;  // the group's max |s_e| bits (reset per group and light)
     const size_t meta = o_err + 1024;
     char *mem = reinterpret_cast<char *>(c.tc_a.ensure((split ? 2 : 1) * ab + bb + meta));
     __half *ahi = reinterpret_cast<__half *>(mem);
@@ -1409,6 +1476,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
     int2 *d_tiles = reinterpret_cast<int2 *>(dmeta + o_tiles), *d_blk = reinterpret_cast<int2 *>(dmeta + o_blk);
     int2 *d_kr = reinterpret_cast<int2 *>(dmeta + o_kr), *d_pr = reinterpret_cast<int2 *>(dmeta + o_pr);
     int *d_pl = reinterpret_cast<int *>(dmeta + o_pl), *d_err = reinterpret_cast<int *>(dmeta + o_err);
+    unsigned *d_max = reinterpret_cast<unsigned *>(dmeta + o_max);
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     for (const Group &G : groups) {
         const int64_t K = 64 * G.nblk;
@@ -1418,18 +1486,24 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
         for (int j = 0; j < nl_out; ++j) {
             {
                 StageScope sc(ST_ROWS, st);
+                CK(cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
+                fq_scale_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((G.nblk * 32 + 255) / 256,
+                                                                                   (int64_t)sm_count(c.device) * 8)),
+                                  256, 0, st>>>(F, Es, d_blk + G.blk0, G.nblk, j, d_max);
+                CK(cudaGetLastError());
+                LAUNCHED();
                 if (split)
                     fq_tc_rows_kernel<true><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K, ahi,
-                                                                                alo, bm);
+                                                                                alo, bm, d_max);
                 else
                     fq_tc_rows_kernel<false><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K, ahi,
-                                                                                 alo, bm);
+                                                                                 alo, bm, d_max);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
             {
                 StageScope sc(ST_CONTRACT, st);
-                const PlaneEpi pe{dz, rr, F.gz, d_pl + G.pl0, U + 2 * (int64_t)nv0 * nv0 * j, nv0, n_uniform};
+                const PlaneEpi pe{dz, rr, F.gz, d_pl + G.pl0, U + 2 * (int64_t)nv0 * nv0 * j, nv0, n_uniform, d_max};
                 if (split)
                     tc_gemm_plane_loop_launch<true>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr + G.kr0,
                                                     d_pr + G.pr0, G.n_pr, Mr, nv0, pe, d_err, st);
@@ -1620,6 +1694,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     }
     W.key0 = (uint32_t)a->seed;
     W.key1 = (uint32_t)(a->seed >> 32);
+    W.any_order = a->precision != SCMC_PREC_FP64;
     const int64_t nout = Nv * Nv * nl_out;
     AccT *U = reinterpret_cast<AccT *>(c.acc_s.ensure(2 * nout * sizeof(AccT)));
     CK(cudaMemsetAsync(U, 0, 2 * nout * sizeof(AccT), st));

@@ -309,4 +309,89 @@ __global__ void __launch_bounds__(128) walk_record_kernel(const __grid_constant_
     }
 }
 
+// One pass for the reduced-precision modes: each lane walks paths taken from
+// an atomic counter and writes its records as it goes.  A path's single
+// record sits at its own index; the multiple-scattering records of a warp's
+// lanes at one step get consecutive slots from one atomicAdd by the warp
+// (ballot, popc), so the records are in no fixed order (every consumer reads
+// an event's path from M.path).  slots[0] counts paths handed out, slots[1]
+// the multiple-scattering events; records past mcap are counted but not
+// written, and the host then walks the batch again with room for all of
+// them (Philox regenerates the same paths).
+template <int DIM>
+__global__ void __launch_bounds__(128) walk_onepass_kernel(const __grid_constant__ WalkParams P, SingleRec S,
+                                                           int64_t scap, MultiRec M, int64_t mcap,
+                                                           unsigned long long *__restrict__ slots,
+                                                           int *__restrict__ err)
+{
+    PathRng r;
+    WalkState s;
+    int64_t p = -1;
+    bool active = true;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        if (active && p < 0) {
+            p = (int64_t)atomicAdd(&slots[0], 1ull);
+            if (p >= P.n_paths) {
+                active = false;
+                p = -1;
+            } else {
+                r.init(P.key0, P.key1, P.path_base + (uint64_t)p);
+                path_init<DIM>(P, r, s);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    S.x1[k * scap + p] = s.x[k];
+                    S.w1[k * scap + p] = s.w[k];
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        bool multi = false;
+        double xi = 0.0, wpx = 0.0;
+        if (active) {
+            ++s.pL;
+            xi = P.want_phase ? r.rand() : 0.0;
+            wpx = s.weight / s.px;
+            if (s.pL == 1) {
+                S.wpx[p] = wpx;
+                S.xi[p] = xi;
+            } else {
+                multi = true;
+            }
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, multi);
+        if (mask) {
+            const int leader = __ffs(mask) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(&slots[1], (unsigned long long)__popc(mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (multi) {
+                const int64_t e = (int64_t)base + __popc(mask & ((1u << lane) - 1u));
+                if (e < mcap) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        M.x[k * mcap + e] = s.x[k];
+                        M.ow[k * mcap + e] = s.ow[k];
+                    }
+                    M.wpx[e] = wpx;
+                    M.xi[e] = xi;
+                    M.path[e] = (int32_t)p;
+                    M.plen[e] = s.pL;
+                }
+            }
+        }
+        if (active) {
+            bool alive = path_advance<DIM>(P, r, s);
+            if (alive && P.max_events > 0 && s.pL >= P.max_events) {
+                atomicExch(err, 1);
+                alive = false;
+            }
+            if (!alive) {
+                S.nev[p] = s.pL;
+                p = -1;
+            }
+        }
+    }
+}
+
 }  // namespace scmc

@@ -4,22 +4,25 @@ MCcov solves on worker slots with their own streams and scratch.
 Each request's result must be the same alone (scmc_field / scmc_cov on the
 library's default context) and in the mix (on a server slot, overlapping
 other requests): every path draws from its own Philox stream and every
-accumulator is private, so only the order of FP64 atomic sums may differ
-(tolerance 1e-12 relative).  Also: admission never reserves more than the
+accumulator is private, so only the order of sums may differ: of FP64 atomic
+sums in FP64 mode (tolerance 1e-12 relative), and in the reduced precisions
+also the order in which the one-pass walk writes its records, which decides
+which events share an FP32 tensor-core chunk (tolerance 1e-6).  Also: admission never reserves more than the
 HBM budget, oversize requests are refused, a failing request does not disturb
 the others, and destroying the server cancels what is still queued.
 """
 import numpy as np
 import pytest
 
-import bench
 from mcspeckle_b200 import _abi, _lib
+from mcspeckle_b200 import workloads as WL
 from mcspeckle_b200 import mc as MC
 from mcspeckle_b200.serving import Server
 
 pytestmark = pytest.mark.gpu
 
 SAME_TOL = 1e-12
+SAME_TOL_MIXED = 1e-6
 
 
 def rel(a, b):
@@ -27,7 +30,7 @@ def rel(a, b):
 
 
 def small_stream(n=24, seed=3):
-    return bench.served_requests(n, seed=seed, paths=(200, 3000), nv_max=160, nl_max=64, side_mfp=(5.0, 12.0))
+    return WL.served_requests(n, seed=seed, paths=(200, 3000), nv_max=160, nl_max=64, side_mfp=(5.0, 12.0))
 
 
 def holder(r, precision="mixed"):
@@ -51,7 +54,7 @@ def test_same_alone_and_in_the_mix(gpu, precision):
     for r, (u, info) in zip(reqs, mixed):
         alone = MC.field_from_args(holder(r, precision))
         assert u.shape == alone.shape == (r["nv"], r["nl"])
-        assert rel(u, alone) < SAME_TOL
+        assert rel(u, alone) < (SAME_TOL if precision == "fp64" else SAME_TOL_MIXED)
         assert info["status"] == 0 and info["finished"] == 1
         assert info["done_ms"] >= info["start_ms"] >= info["submit_ms"]
         assert info["peak_bytes"] <= info["reserved_bytes"]
@@ -59,9 +62,9 @@ def test_same_alone_and_in_the_mix(gpu, precision):
 
 def test_cov_requests_in_the_mix(gpu):
     reqs = small_stream(6, seed=9)
-    cov_args = bench.workload_args(400)
-    cov_args[4] = bench.grid_dirs(4, 5.0, +1.0)
-    cov_args[5] = bench.grid_dirs(4, 5.0, -1.0)
+    cov_args = WL.cov64_args(400)
+    cov_args[4] = WL.grid_rect(4, 4, 5.0, +1.0)
+    cov_args[5] = WL.grid_rect(4, 4, 5.0, -1.0)
     hc = MC.mc_args(*cov_args, seed=77, precision="mixed")
     with Server(slots=3) as srv:
         tf = [srv.submit_field(holder(r)) for r in reqs[:3]]
@@ -70,9 +73,9 @@ def test_cov_requests_in_the_mix(gpu):
         (Ms, Mm), info = srv.wait(tc)
         fields = [srv.wait(t)[0] for t in tf]
     Ms0, Mm0 = MC.cov_from_args(hc)
-    assert rel(Ms, Ms0) < SAME_TOL and rel(Mm, Mm0) < SAME_TOL
+    assert rel(Ms, Ms0) < SAME_TOL_MIXED and rel(Mm, Mm0) < SAME_TOL_MIXED
     for r, u in zip(reqs, fields):
-        assert rel(u, MC.field_from_args(holder(r))) < SAME_TOL
+        assert rel(u, MC.field_from_args(holder(r))) < SAME_TOL_MIXED
 
 
 def test_budget_admission(gpu):
@@ -98,7 +101,7 @@ def test_budget_admission(gpu):
 
 
 def test_oversize_request_refused(gpu):
-    cov_args = bench.workload_args(100)
+    cov_args = WL.cov64_args(100)
     h = MC.mc_args(*cov_args, seed=1, precision="mixed")  # 64x64 cov: ~1 GB of accumulators
     with Server(slots=2, hbm_budget=2e8) as srv:
         with pytest.raises(_lib.ScmcError) as ei:
@@ -120,8 +123,8 @@ def test_failing_request_isolated(gpu):
         u2, _ = srv.wait(t_ok2)
         st = srv.stats()
     assert st["failed"] == 1 and st["completed"] == 2
-    assert rel(u1, MC.field_from_args(holder(reqs[1]))) < SAME_TOL
-    assert rel(u2, MC.field_from_args(holder(reqs[2]))) < SAME_TOL
+    assert rel(u1, MC.field_from_args(holder(reqs[1]))) < SAME_TOL_MIXED
+    assert rel(u2, MC.field_from_args(holder(reqs[2]))) < SAME_TOL_MIXED
 
 
 def test_poll_and_destroy_with_queue(gpu):
@@ -133,4 +136,4 @@ def test_poll_and_destroy_with_queue(gpu):
     u0, info0 = srv.wait(tickets[0])
     assert info0["finished"] == 1
     srv.close()  # runs the admitted request to completion, cancels the queue
-    assert rel(u0, MC.field_from_args(holder(reqs[0]))) < SAME_TOL
+    assert rel(u0, MC.field_from_args(holder(reqs[0]))) < SAME_TOL_MIXED
