@@ -432,6 +432,39 @@ int scmc_cov_offsets(const double *C1, const double *C2, int32_t nvx, int32_t nv
 int scmc_cov_offsets_device(const double *d_C1, const double *d_C2, int32_t nvx, int32_t nvy, int32_t nlx,
                             int32_t nly, float *d_R, int32_t device, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Tuning.  Launch parameters the project's autotuner (mcspeckle_b200.autotune)
+ * chooses per (kind, precision, size) by timing candidates on the GPU; no
+ * counterpart in the reference.  An entry applies to solves of its kind and
+ * precision whose size n lies in [n_lo, n_hi] (n = nv*nl for field and cov,
+ * nv0*nv0 for FourierQuad); the last matching entry wins, and a 0 field keeps
+ * the built-in choice.  The library reads entries, at its first use, from the
+ * file named by SCMC_TUNING_FILE, else from scmc_tuning.txt beside the
+ * library; scmc_tuning_load reads another file.  File lines:
+ *   kind precision n_lo n_hi path_batch chunk_events stages ksplit group_entries
+ * with kind field | cov | fq and precision fp64 | mixed | fp32 | fp16; '#'
+ * starts a comment.  The covariance's chunk is capped where its FP32 tensor
+ * sums would exceed the mixed tolerance (65536 events FP16, 32768 hi+lo).
+ * ------------------------------------------------------------------------- */
+enum { SCMC_TUNE_FIELD = 0, SCMC_TUNE_COV = 1, SCMC_TUNE_FQ = 2 };
+
+typedef struct {
+    int32_t kind;            /* SCMC_TUNE_* */
+    int32_t precision;       /* SCMC_PREC_* */
+    int64_t n_lo, n_hi;
+    int64_t path_batch;      /* paths walked per batch (built-in: 2^20) */
+    int64_t chunk_events;    /* events per tensor-core chunk (built-in: from 1-2 GiB of operands) */
+    int32_t stages;          /* CTA-pair pipeline stages, 2 or 3 (3: FP16 covariance only) */
+    int32_t ksplit;          /* split-K slices of the tensor-core field (built-in: fill the SMs) */
+    int64_t group_entries;   /* FourierQuad entries per plane group (built-in: 2^20) */
+} scmc_tuning;
+
+int scmc_tuning_set(const scmc_tuning *t);
+int scmc_tuning_clear(void);
+int scmc_tuning_load(const char *path);
+/* The resolved parameters (built-in defaults filled in) for one solve shape. */
+int scmc_tuning_get(int32_t kind, int32_t precision, int64_t n, scmc_tuning *out);
+
 /* Library information and error reporting. */
 int scmc_abi_version(void);
 const char *scmc_last_error(void);

@@ -96,6 +96,23 @@ class FqArgs(C.Structure):
     ]
 
 
+SCMC_TUNE_FIELD, SCMC_TUNE_COV, SCMC_TUNE_FQ = 0, 1, 2
+
+
+class Tuning(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("precision", C.c_int32),
+        ("n_lo", C.c_int64),
+        ("n_hi", C.c_int64),
+        ("path_batch", C.c_int64),
+        ("chunk_events", C.c_int64),
+        ("stages", C.c_int32),
+        ("ksplit", C.c_int32),
+        ("group_entries", C.c_int64),
+    ]
+
+
 class HeteroArgs(C.Structure):
     _fields_ = [
         ("mc", McArgs),

@@ -92,6 +92,11 @@ def lib():
         L.scmc_cov_offsets.restype = C.c_int
         L.scmc_cov_offsets_device.restype = C.c_int
         L.scmc_test_wait_fault.argtypes = [C.c_int32]
+        L.scmc_tuning_set.argtypes = [C.POINTER(_abi.Tuning)]
+        L.scmc_tuning_load.argtypes = [C.c_char_p]
+        L.scmc_tuning_get.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.POINTER(_abi.Tuning)]
+        for name in ("scmc_tuning_set", "scmc_tuning_clear", "scmc_tuning_load", "scmc_tuning_get"):
+            getattr(L, name).restype = C.c_int
         L.scmc_test_wait_fault.restype = C.c_int
         L.scmc_profile_read.argtypes = [C.POINTER(_abi.StageTimes), C.c_int32]
         for name in ("scmc_field", "scmc_field_device", "scmc_cov", "scmc_cov_device",

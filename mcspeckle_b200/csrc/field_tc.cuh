@@ -33,7 +33,8 @@ struct FieldTcOps {
 
 // sms: multiprocessors; the K split fills them when the output has few tiles.
 // chunk_bytes bounds the operand memory of one chunk of events.
-inline FieldTcPlan field_tc_plan(int nv, int nl, int terms, bool split, int sms, size_t chunk_bytes = (size_t)1 << 30)
+inline FieldTcPlan field_tc_plan(int nv, int nl, int terms, bool split, int sms, size_t chunk_bytes = (size_t)1 << 30,
+                                 int ksplit = 0)
 {
     FieldTcPlan p;
     p.nv = nv;
@@ -52,6 +53,7 @@ inline FieldTcPlan field_tc_plan(int nv, int nl, int terms, bool split, int sms,
         for (int tm = 0; tm < n_tm; ++tm) p.tiles.push_back(make_int2(tm, tn));
     const int nt = (int)p.tiles.size();
     p.ksplit = std::max(1, std::min(sms / std::max(nt, 1), (int)(p.K / TC_BK / 8)));
+    if (ksplit > 0) p.ksplit = std::max(1, std::min(ksplit, (int)(p.K / TC_BK)));
     return p;
 }
 

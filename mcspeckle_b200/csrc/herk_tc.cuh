@@ -622,16 +622,14 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
 // Every wait is bounded as in herk_tc_kernel.
 // ---------------------------------------------------------------------------
 // Two 64 KB stages (FP16) leave room on the SM for a row-generation CTA of
-// the next chunk (about 72 KB at 64 x 64); three measured no faster.
-#ifndef SCMC_PAIR_STAGES_FP16
-#define SCMC_PAIR_STAGES_FP16 2
-#endif
+// the next chunk (about 72 KB at 64 x 64); three (FP16 only: 193 KB) are the
+// autotuner's alternative.
 constexpr int TC2_TMEM_COLS = 512;  // Re C and Im C, 256 columns each
-template <bool SPLIT> struct Tc2Cfg {
+template <bool SPLIT, int NSTAGES = 2> struct Tc2Cfg {
     static constexpr int TILE = 128 * TC_BK * 2;  // 128 rows x 64 events of one plane
     static constexpr int NA = SPLIT ? 4 : 2;      // A tiles: Re, Im (hi), Re, Im (lo)
     static constexpr int STAGE_BYTES = (NA + 2) * TILE;
-    static constexpr int STAGES = SPLIT ? 2 : SCMC_PAIR_STAGES_FP16;
+    static constexpr int STAGES = NSTAGES;
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
     static constexpr int B_OFF = NA * TILE;  // then Re B, Im B
 };
@@ -697,14 +695,14 @@ __device__ __forceinline__ void umma_commit_pair(uint64_t *bar)
         : "memory");
 }
 
-template <bool SPLIT>
+template <bool SPLIT, int NSTAGES>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(128, 1)
 herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant__ CUtensorMap tm_im,
                 const __grid_constant__ CUtensorMap tm_re_lo, const __grid_constant__ CUtensorMap tm_im_lo,
                 const int2 *__restrict__ tiles, int num_kb, int kb_per_split, int N, double *__restrict__ D,
                 int *__restrict__ err, int test_fault)
 {
-    using Cfg = Tc2Cfg<SPLIT>;
+    using Cfg = Tc2Cfg<SPLIT, NSTAGES>;
     extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
     uint64_t *full = reinterpret_cast<uint64_t *>(base + Cfg::STAGES * Cfg::STAGE_BYTES);
@@ -1074,6 +1072,7 @@ struct TcPlan {
     int64_t events_per_chunk;
     int64_t K;  // halves per operand row: 2 x events (real-expanded), events (planar)
     std::vector<int2> tiles;
+    int stages = 2;  // pipeline stages of the CTA-pair kernel
 };
 
 struct TcOperands {
@@ -1087,11 +1086,13 @@ struct TcOperands {
     int n_tiles;
 };
 
-inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30)
+inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30, int64_t chunk_events = 0,
+                      int stages = 0)
 {
     TcPlan p;
     p.N = N;
     p.split = split;
+    p.stages = (!split && stages == 3) ? 3 : 2;
     // The pair kernel pays off once its 256 complex rows are mostly real rows.
     p.pair = N >= 256;
     // Operand bytes per event: 8N (16N hi+lo) real-expanded, 4N (8N) planar;
@@ -1103,7 +1104,7 @@ inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30)
     // 65536 events, 2.9e-4 at 32768 on the 64 x 64 covariance); the hi+lo
     // split keeps chunks of at most 32768 events to stay the accurate mode.
     const int64_t e_max = split ? 32768 : 65536;
-    int64_t e = (int64_t)chunk_bytes / per_event;
+    int64_t e = chunk_events > 0 ? chunk_events : (int64_t)chunk_bytes / per_event;
     e = std::max<int64_t>(eb, std::min<int64_t>(e, e_max));
     e = (e / eb) * eb;
     p.events_per_chunk = e;
@@ -1268,22 +1269,34 @@ inline void tc_gemm_plane_loop_launch(const CUtensorMap &m_ahi, const CUtensorMa
 // D[ks][2N][N] += the planar pair product (Re C in even rows, Im C in odd
 // rows) over num_kb blocks of 64 events, split ksplit ways; tiles are 256 x 256
 // complex rows x columns.
-template <bool SPLIT>
-inline void tc_gemm2_launch(const TcOperands &o, int num_kb, int ksplit, int N, double *D, cudaStream_t st)
+template <bool SPLIT, int NSTAGES>
+inline void tc_gemm2_launch_stages(const TcOperands &o, int num_kb, int ksplit, int N, double *D, cudaStream_t st)
 {
+    using Cfg = Tc2Cfg<SPLIT, NSTAGES>;
     static std::atomic<uint64_t> attr_set{0};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
     if (dev >= 64 || !((attr_set.load() >> dev) & 1)) {
-        if (cudaFuncSetAttribute(herk_tc2_kernel<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 Tc2Cfg<SPLIT>::SMEM_BYTES) != cudaSuccess)
+        if (cudaFuncSetAttribute(herk_tc2_kernel<SPLIT, NSTAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg::SMEM_BYTES) != cudaSuccess)
             throw std::runtime_error("cannot reserve shared memory for the CTA-pair tensor-core kernel");
         if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
     }
     const int kb_per = (num_kb + ksplit - 1) / ksplit;
     const int ks = (num_kb + kb_per - 1) / kb_per;
-    herk_tc2_kernel<SPLIT><<<dim3(2u * (unsigned)o.n_tiles, (unsigned)ks), 128, Tc2Cfg<SPLIT>::SMEM_BYTES, st>>>(
+    herk_tc2_kernel<SPLIT, NSTAGES><<<dim3(2u * (unsigned)o.n_tiles, (unsigned)ks), 128, Cfg::SMEM_BYTES, st>>>(
         o.m_ahi, o.m_ihi, o.m_alo, o.m_ilo, o.tiles, num_kb, kb_per, N, D, o.err, tc_test_fault().load());
+}
+
+// D[ks][2N][N] += the planar pair product (Re C in even rows, Im C in odd
+// rows) over num_kb blocks of 64 events, split ksplit ways; tiles are 256 x 256
+// complex rows x columns.  stages: 2, or 3 for the FP16 product.
+template <bool SPLIT>
+inline void tc_gemm2_launch(const TcOperands &o, int num_kb, int ksplit, int N, double *D, cudaStream_t st,
+                            int stages = 2)
+{
+    if (!SPLIT && stages == 3) tc_gemm2_launch_stages<false, 3>(o, num_kb, ksplit, N, D, st);
+    else tc_gemm2_launch_stages<SPLIT, 2>(o, num_kb, ksplit, N, D, st);
 }
 
 template <bool SPLIT>
@@ -1291,7 +1304,7 @@ inline void tc_herk_launch(const TcPlan &p, const TcOperands &o, int64_t n, doub
 {
     if (p.pair) {
         const int num_kb = (int)((n + TC_BK - 1) / TC_BK);  // 64 events per block
-        tc_gemm2_launch<SPLIT>(o, num_kb, 1, p.N, D, st);
+        tc_gemm2_launch<SPLIT>(o, num_kb, 1, p.N, D, st, p.stages);
     } else {
         const int num_kb = (int)((2 * n + TC_BK - 1) / TC_BK);
         tc_gemm_launch<SPLIT>(o.m_ahi, o.m_alo, o.m_b, o.tiles, o.n_tiles, num_kb, 1, 2 * p.N, p.N, D, o.err, st);

@@ -3,6 +3,7 @@
 // declared in include/scmc_gpu.h.
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <atomic>
@@ -13,7 +14,10 @@
 #include <thread>
 #include <unordered_map>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <sstream>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -182,6 +186,100 @@ int guarded(F &&f)
         g_last_error = "unknown error";
         return SCMC_ERR_CUDA;
     }
+}
+
+// ---------------------------------------------------------------------------
+// tuning table (scmc_tuning_*): launch parameters per (kind, precision, size)
+// ---------------------------------------------------------------------------
+std::mutex g_tune_mu;
+std::vector<scmc_tuning> g_tune;
+bool g_tune_loaded = false;
+
+void tuning_parse_file(const char *path, bool must_exist)
+{
+    std::ifstream f(path);
+    if (!f) {
+        if (must_exist) fail(SCMC_ERR_INVALID, std::string("cannot read tuning file ") + path);
+        return;
+    }
+    std::vector<scmc_tuning> add;
+    std::string line;
+    int lineno = 0;
+    while (std::getline(f, line)) {
+        ++lineno;
+        const size_t h = line.find('#');
+        if (h != std::string::npos) line.resize(h);
+        std::istringstream is(line);
+        std::string kind, prec;
+        if (!(is >> kind)) continue;
+        scmc_tuning t{};
+        long long nlo = 0, nhi = 0, pb = 0, ce = 0, ge = 0;
+        int st = 0, ks = 0;
+        if (!(is >> prec >> nlo >> nhi >> pb >> ce >> st >> ks >> ge))
+            fail(SCMC_ERR_INVALID, std::string("tuning file ") + path + ": bad line " + std::to_string(lineno));
+        if (kind == "field") t.kind = SCMC_TUNE_FIELD;
+        else if (kind == "cov") t.kind = SCMC_TUNE_COV;
+        else if (kind == "fq") t.kind = SCMC_TUNE_FQ;
+        else fail(SCMC_ERR_INVALID, std::string("tuning file ") + path + ": unknown kind " + kind);
+        if (prec == "fp64") t.precision = SCMC_PREC_FP64;
+        else if (prec == "mixed") t.precision = SCMC_PREC_MIXED;
+        else if (prec == "fp32") t.precision = SCMC_PREC_FP32;
+        else if (prec == "fp16") t.precision = SCMC_PREC_FP16;
+        else fail(SCMC_ERR_INVALID, std::string("tuning file ") + path + ": unknown precision " + prec);
+        t.n_lo = nlo;
+        t.n_hi = nhi;
+        t.path_batch = pb;
+        t.chunk_events = ce;
+        t.stages = st;
+        t.ksplit = ks;
+        t.group_entries = ge;
+        add.push_back(t);
+    }
+    g_tune.insert(g_tune.end(), add.begin(), add.end());
+}
+
+// At the first use: SCMC_TUNING_FILE, else scmc_tuning.txt beside the library.
+void tuning_autoload_locked()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    if (const char *env = std::getenv("SCMC_TUNING_FILE")) {
+        tuning_parse_file(env, true);
+        return;
+    }
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void *>(&tuning_parse_file), &info) && info.dli_fname) {
+        std::string p(info.dli_fname);
+        const size_t slash = p.rfind('/');
+        p = (slash == std::string::npos ? std::string(".") : p.substr(0, slash)) + "/scmc_tuning.txt";
+        tuning_parse_file(p.c_str(), false);
+    }
+}
+
+scmc_tuning tuning_for(int kind, int precision, int64_t n)
+{
+    scmc_tuning r{};
+    r.kind = kind;
+    r.precision = precision;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tuning_autoload_locked();
+        for (const scmc_tuning &t : g_tune)
+            if (t.kind == kind && t.precision == precision && n >= t.n_lo && n <= t.n_hi) {
+                r.n_lo = t.n_lo;
+                r.n_hi = t.n_hi;
+                if (t.path_batch > 0) r.path_batch = t.path_batch;
+                if (t.chunk_events > 0) r.chunk_events = t.chunk_events;
+                if (t.stages > 0) r.stages = t.stages;
+                if (t.ksplit > 0) r.ksplit = t.ksplit;
+                if (t.group_entries > 0) r.group_entries = t.group_entries;
+            }
+    }
+    if (r.path_batch <= 0) r.path_batch = (int64_t)1 << 20;
+    if (r.stages != 3) r.stages = 2;
+    if (r.group_entries <= 0) r.group_entries = (int64_t)1 << 20;
+    r.group_entries = std::max<int64_t>(r.group_entries, 4096);
+    return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -655,7 +753,10 @@ void walk_batch(Ctx &c, const WalkParams &W, int64_t n_paths, cudaStream_t st, B
     else walk_batch_dim<2>(c, W, n_paths, st, B);
 }
 
-int64_t path_batch_size(int64_t remaining) { return std::min<int64_t>(remaining, (int64_t)1 << 20); }
+int64_t path_batch_size(int64_t remaining, int64_t limit = (int64_t)1 << 20)
+{
+    return std::min<int64_t>(remaining, std::max<int64_t>(limit, 1));
+}
 
 // ---------------------------------------------------------------------------
 // field
@@ -702,7 +803,8 @@ void field_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u
     const int nv = (int)a->nv, nl = (int)a->nl;
     const bool split = a->precision == SCMC_PREC_MIXED;
     const int terms_m = a->do_cbs ? 2 : 1;
-    const FieldTcPlan plan = field_tc_plan(nv, nl, terms_m, split, sm_count(c.device), c.tc_chunk_bytes);
+    const scmc_tuning T = tuning_for(SCMC_TUNE_FIELD, a->precision, (int64_t)nv * nl);
+    const FieldTcPlan plan = field_tc_plan(nv, nl, terms_m, split, sm_count(c.device), c.tc_chunk_bytes, T.ksplit);
     const bool ffff = a->is_ff_l && a->is_ff_v;
     const size_t slice = (size_t)2 * nv * nl;
     const size_t d_bytes = (size_t)plan.ksplit * slice * sizeof(double);
@@ -716,7 +818,7 @@ void field_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u
     const int phase = P.W.want_phase;
     WalkParams W = P.W;
     for (int64_t done = 0; done < a->max_itr;) {
-        int64_t nb = path_batch_size(a->max_itr - done);
+        int64_t nb = path_batch_size(a->max_itr - done, T.path_batch);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
@@ -785,13 +887,14 @@ void field_run(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_u, c
         return;
     }
     const int64_t n = a->nv * a->nl;
+    const scmc_tuning T = tuning_for(SCMC_TUNE_FIELD, a->precision, n);
     AccT *Us = reinterpret_cast<AccT *>(c.acc_s.ensure(2 * n * sizeof(AccT)));
     AccT *Um = reinterpret_cast<AccT *>(c.acc_m.ensure(2 * n * sizeof(AccT)));
     CK(cudaMemsetAsync(Us, 0, 2 * n * sizeof(AccT), st));
     CK(cudaMemsetAsync(Um, 0, 2 * n * sizeof(AccT), st));
     WalkParams W = P.W;
     for (int64_t done = 0; done < a->max_itr;) {
-        int64_t nb = path_batch_size(a->max_itr - done);
+        int64_t nb = path_batch_size(a->max_itr - done, T.path_batch);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
@@ -847,9 +950,10 @@ void onwave_run(Ctx &c, const scmc_mc_args *a, const Prepared &P, const double2 
         CK(cudaFuncSetAttribute(km, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
     const int sms = sm_count(c.device);
+    const scmc_tuning T = tuning_for(SCMC_TUNE_FIELD, a->precision, (int64_t)nv * nl);
     WalkParams W = P.W;
     for (int64_t done = 0; done < a->max_itr;) {
-        int64_t nb = path_batch_size(a->max_itr - done);
+        int64_t nb = path_batch_size(a->max_itr - done, T.path_batch);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
@@ -960,9 +1064,10 @@ void cov_run_cc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     CK(cudaMemsetAsync(Cm, 0, acc_bytes, st));
     int64_t chunk = std::max<int64_t>(64, std::min<int64_t>(8192, ((int64_t)256 << 20) / ((int64_t)N * sizeof(C))));
     void *T = c.rows.ensure((size_t)chunk * N * sizeof(C));
+    const scmc_tuning tune = tuning_for(SCMC_TUNE_COV, a->precision, N);
     WalkParams W = P.W;
     for (int64_t done = 0; done < a->max_itr;) {
-        int64_t nb = path_batch_size(a->max_itr - done);
+        int64_t nb = path_batch_size(a->max_itr - done, tune.path_batch);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
@@ -1007,7 +1112,8 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     // and the tail wave of one contraction overlaps the head of the next.
     // Three operand buffers: rows of chunk i reuse the buffer of chunk i-3.
     const int N = (int)(a->nv * a->nl);
-    TcPlan plan = tc_plan(N, a->precision == SCMC_PREC_MIXED, c.tc_chunk_bytes);
+    const scmc_tuning T = tuning_for(SCMC_TUNE_COV, a->precision, N);
+    TcPlan plan = tc_plan(N, a->precision == SCMC_PREC_MIXED, c.tc_chunk_bytes, T.chunk_events, T.stages);
     const size_t acc_bytes = (size_t)2 * N * N * sizeof(double);
     double *Ds0 = reinterpret_cast<double *>(c.acc_s.ensure(2 * acc_bytes));
     double *Dm0 = reinterpret_cast<double *>(c.acc_m.ensure(2 * acc_bytes));
@@ -1038,7 +1144,7 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
     int64_t chunk_id = 0;
     WalkParams W = P.W;
     for (int64_t done = 0; done < a->max_itr;) {
-        int64_t nb = path_batch_size(a->max_itr - done);
+        int64_t nb = path_batch_size(a->max_itr - done, T.path_batch);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, rs, B);  // after the previous batch's rows (same stream)
@@ -1387,14 +1493,13 @@ void validate_fq(const scmc_fq_args *a)
 // The per-plane DFT sums of one batch on tcgen05 (fq.cuh, tensor-core form),
 // added into U stored [light][r1][r2] in FP32 (each plane's sum is FP32 in
 // TMEM already).  Tt: the twiddles stored [p][r]; dz: zexp0 stored [r2][r1].
-// Nonempty planes are taken in groups of at most kFqTcEntries padded entries
-// (operand memory) and kFqTcPlanes planes.
-constexpr int64_t kFqTcEntries = (int64_t)1 << 20;
+// Nonempty planes are taken in groups of at most group_entries padded entries
+// (operand memory; tuned, 2^20 built in) and kFqTcPlanes planes.
 constexpr int kFqTcPlanes = 16384;
 
 void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
                  const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt, const double2 *dz,
-                 const float2 *rr, int n_uniform, float *U, bool split, cudaStream_t st)
+                 const float2 *rr, int n_uniform, float *U, bool split, int64_t group_entries, cudaStream_t st)
 {
     const int nv0 = F.nv0;
     const int Mr = 2 * nv0;
@@ -1422,7 +1527,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
             const int p = hplanes[g1];
             const int cnt = hcounts[p];
             const int nb = (cnt + 31) / 32;
-            if (G.n_pl > 0 && (G.nblk + nb) * 32 > kFqTcEntries) break;
+            if (G.n_pl > 0 && (G.nblk + nb) * 32 > group_entries) break;
             kr.push_back(make_int2((int)G.nblk, nb));
             for (int b = 0; b < nb; ++b) blk.push_back(make_int2(hoff[p] + 32 * b, std::min(32, cnt - 32 * b)));
             gpl.push_back(p);
@@ -1705,10 +1810,11 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     std::vector<int> hcounts(Nz + 1);
     std::vector<int> hplanes;
     const int sms = sm_count(c.device);
+    const scmc_tuning tune = tuning_for(SCMC_TUNE_FQ, a->precision, Nv * Nv);
     int64_t total_vert = 0;
     const int passes = a->do_cbs ? 2 : 1;
     for (int64_t done = 0; done < a->max_itr;) {
-        const int64_t nb = std::min<int64_t>(a->max_itr - done, (int64_t)1 << 20);
+        const int64_t nb = path_batch_size(a->max_itr - done, tune.path_batch);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
         walk_batch(c, W, nb, st, B);
@@ -1750,7 +1856,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
         }
         if (use_tc) {
             fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
-                        reinterpret_cast<float *>(U), a->precision == SCMC_PREC_MIXED, st);
+                        reinterpret_cast<float *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
             for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
@@ -1805,6 +1911,46 @@ int scmc_abi_version(void) { return SCMC_ABI_VERSION; }
 const char *scmc_last_error(void) { return g_last_error.c_str(); }
 
 int64_t scmc_launch_count(void) { return g_launches.load(); }
+
+int scmc_tuning_set(const scmc_tuning *t)
+{
+    return guarded([&] {
+        if (!t) fail(SCMC_ERR_INVALID, "null tuning entry");
+        if (t->kind < SCMC_TUNE_FIELD || t->kind > SCMC_TUNE_FQ) fail(SCMC_ERR_INVALID, "invalid tuning kind");
+        if (t->precision < 0 || t->precision > 3) fail(SCMC_ERR_INVALID, "invalid precision mode");
+        if (t->stages != 0 && t->stages != 2 && t->stages != 3) fail(SCMC_ERR_INVALID, "stages must be 2 or 3");
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        tuning_autoload_locked();
+        g_tune.push_back(*t);
+    });
+}
+
+int scmc_tuning_clear(void)
+{
+    return guarded([&] {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune.clear();
+        g_tune_loaded = true;  // cleared on purpose: do not load the default file later
+    });
+}
+
+int scmc_tuning_load(const char *path)
+{
+    return guarded([&] {
+        if (!path) fail(SCMC_ERR_INVALID, "null path");
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_loaded = true;
+        tuning_parse_file(path, true);
+    });
+}
+
+int scmc_tuning_get(int32_t kind, int32_t precision, int64_t n, scmc_tuning *out)
+{
+    return guarded([&] {
+        if (!out) fail(SCMC_ERR_INVALID, "null output");
+        *out = tuning_for(kind, precision, n);
+    });
+}
 
 int scmc_test_wait_fault(int32_t on)
 {

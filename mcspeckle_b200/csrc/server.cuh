@@ -57,7 +57,8 @@ struct Request {
 // known only after the walk, and the server tracks the real footprint.
 int64_t request_estimate(int kind, const scmc_mc_args &a, int sms, size_t chunk_bytes)
 {
-    const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(a.max_itr, (int64_t)1 << 20));
+    const scmc_tuning T = tuning_for(kind == SCMC_REQ_FIELD ? SCMC_TUNE_FIELD : SCMC_TUNE_COV, a.precision, a.nv * a.nl);
+    const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(a.max_itr, T.path_batch));
     const double depth = a.sigt * (a.box_max[a.dim - 1] - a.box_min[a.dim - 1]);
     const double ev = 4.0 + 2.0 * std::max(depth, 1.0);
     double walk = (double)nb * (4 + 8 + 8 + 68) + (double)nb * ev * 1.25 * 72;
@@ -67,7 +68,7 @@ int64_t request_estimate(int kind, const scmc_mc_args &a, int sms, size_t chunk_
         const bool tc = use_field_tc(&a);
         if (tc) {
             FieldTcPlan p = field_tc_plan((int)a.nv, (int)a.nl, a.do_cbs ? 2 : 1, a.precision == SCMC_PREC_MIXED, sms,
-                                          chunk_bytes);
+                                          chunk_bytes, T.ksplit);
             acc = (double)field_tc_bytes(p) + 2.0 * p.ksplit * 2 * nv * nl * 8;
         } else {
             acc = 2.0 * 2 * nv * nl * 8;
@@ -80,7 +81,9 @@ int64_t request_estimate(int kind, const scmc_mc_args &a, int sms, size_t chunk_
         // operand buffers; CUDA-core path: one accumulator each and a row buffer;
         // both: device copies of Ms, Mm
         acc = (tc ? 4.0 : 2.0) * 2 * N * N * 8 + 2.0 * 2 * N * N * 8;
-        if (tc) acc += 3.0 * (double)tc_operand_bytes(tc_plan((int)N, a.precision == SCMC_PREC_MIXED, chunk_bytes));
+        if (tc)
+            acc += 3.0 * (double)tc_operand_bytes(
+                                 tc_plan((int)N, a.precision == SCMC_PREC_MIXED, chunk_bytes, T.chunk_events, T.stages));
         else acc += 256.0 * (1 << 20);
     }
     // every scratch buffer is allocated 1/8 above its request (DevBuf::ensure)
