@@ -329,9 +329,14 @@ int scmc_profile_read(scmc_stage_times *out, int32_t reset);
  *
  * The server owns n_slots worker slots, each with its own CUDA stream and
  * scratch memory (stream-ordered allocations).  A submitted request waits in
- * a FIFO queue until a slot is free and its estimated device memory fits the
- * HBM budget next to the requests already running; then it runs on that
- * slot's stream, so requests on different slots overlap on the device.  The
+ * the queue until a slot is free and its estimated device memory fits the
+ * HBM budget next to the requests already running (oldest first; a request
+ * that does not fit is passed by younger ones a bounded number of times);
+ * then it runs on that slot's stream, so requests on different slots overlap
+ * on the device.  Small field requests on the CUDA-core accumulation (up to
+ * 2^20 paths, same dimension and precision class) are packed: up to 64 run
+ * as one walk, one accumulation and one finalisation launch per round of
+ * 2^20 paths.  The
  * output arrays stay owned by the caller and must stay valid until
  * scmc_server_wait has reported the request finished.  A request's result does
  * not depend on what else runs: each path draws from its own Philox stream
@@ -352,8 +357,9 @@ typedef struct {
     double done_ms;         /* result copied to the caller's arrays */
     double device_ms;       /* CUDA-event time on the slot stream, first to last launch */
     int64_t reserved_bytes; /* device memory reserved against the budget */
-    int64_t peak_bytes;     /* device memory the slot actually held for it */
+    int64_t peak_bytes;     /* device memory the slot actually held for it (for a pack: the pack) */
     int64_t paths;          /* max_itr of the request */
+    int32_t packed;         /* requests that shared its launches (1: it ran alone) */
 } scmc_request_info;
 
 typedef struct {

@@ -166,6 +166,7 @@ class RequestInfo(C.Structure):
         ("reserved_bytes", C.c_int64),
         ("peak_bytes", C.c_int64),
         ("paths", C.c_int64),
+        ("packed", C.c_int32),
     ]
 
     def as_dict(self):

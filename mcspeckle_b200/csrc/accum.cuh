@@ -62,11 +62,13 @@ constexpr int kFieldMaxTile = 1024;
 
 template <typename A> struct acc_ptr;
 
+// One CTA's share of the field sum: a tv x tl tile (`tile`) of views and
+// lights over the events [e_begin, e_end) (path indices for singles, record
+// indices for multiple scattering), added into U.
 template <int DIM, int POL, bool SINGLE, typename AccT>
-__global__ void __launch_bounds__(kFieldThreads)
-field_accum_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_events,
-                   int tv, int tl, int n_vtiles, int64_t ev_per_cta, AccT *__restrict__ U, int field_phase,
-                   int mean_mode = 0)
+__device__ __forceinline__ void field_accum_body(const NeeParams &Q, const SingleRec &S, int64_t scap, const MultiRec &M,
+                                                 int64_t mcap, int64_t e_begin, int64_t e_end, int tile, int tv, int tl,
+                                                 int n_vtiles, AccT *__restrict__ U, int field_phase, int mean_mode)
 {
     using R = typename std::conditional<POL == P64, double, float>::type;
     using C = typename cplx_t<R>::type;
@@ -78,13 +80,10 @@ field_accum_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t sca
     C *ssc = sb2 + kFieldEB * tl;                       // [EB] scale
     EventView *sev = reinterpret_cast<EventView *>(ssc + kFieldEB);  // [EB]
 
-    const int tile = blockIdx.x;
     const int v0 = (tile % n_vtiles) * tv;
     const int l0 = (tile / n_vtiles) * tl;
     const int nvt = min(tv, Q.nv - v0);
     const int nlt = min(tl, Q.nl - l0);
-    const int64_t e_begin = (int64_t)blockIdx.y * ev_per_cta;
-    const int64_t e_end = min(n_events, e_begin + ev_per_cta);
     const int nq = tv * tl;
     const int near_single = SINGLE && !(Q.is_ff_l && Q.is_ff_v);
 
@@ -172,21 +171,83 @@ field_accum_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t sca
     }
 }
 
+template <int DIM, int POL, bool SINGLE, typename AccT>
+__global__ void __launch_bounds__(kFieldThreads)
+field_accum_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_events,
+                   int tv, int tl, int n_vtiles, int64_t ev_per_cta, AccT *__restrict__ U, int field_phase,
+                   int mean_mode = 0)
+{
+    const int64_t e_begin = (int64_t)blockIdx.y * ev_per_cta;
+    const int64_t e_end = min(n_events, e_begin + ev_per_cta);
+    field_accum_body<DIM, POL, SINGLE, AccT>(Q, S, scap, M, mcap, e_begin, e_end, (int)blockIdx.x, tv, tl, n_vtiles, U,
+                                             field_phase, mean_mode);
+}
+
+// Many field requests in one launch (the request server's packs): CTA b
+// takes job jobs[b] - request, tile, event range, singles or multiple
+// scattering - with that request's NEE parameters and accumulators.
+struct PackJob {
+    int req, tile, single, pad;
+    int64_t e_begin, e_end;
+};
+struct PackTiling {
+    int tv, tl, n_vtiles, pad;
+    int64_t acc_s, acc_m;  // offsets (AccT units) of the request's accumulators in the pack's arena
+};
+
+template <int DIM, int POL, typename AccT>
+__global__ void __launch_bounds__(kFieldThreads)
+field_accum_packed_kernel(const NeeParams *__restrict__ Qs, const PackTiling *__restrict__ tiling,
+                          const PackJob *__restrict__ jobs, SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
+                          AccT *__restrict__ arena)
+{
+    const PackJob j = jobs[blockIdx.x];
+    const PackTiling t = tiling[j.req];
+    const NeeParams &Q = Qs[j.req];
+    if (j.single)
+        field_accum_body<DIM, POL, true, AccT>(Q, S, scap, M, mcap, j.e_begin, j.e_end, j.tile, t.tv, t.tl, t.n_vtiles,
+                                               arena + t.acc_s, 1, 0);
+    else
+        field_accum_body<DIM, POL, false, AccT>(Q, S, scap, M, mcap, j.e_begin, j.e_end, j.tile, t.tv, t.tl,
+                                                t.n_vtiles, arena + t.acc_m, 1, 0);
+}
+
 // u = norm * (A o Us + Um), A = af(l.v) for far-field singles, else 1.
+template <int DIM, typename AccT>
+__device__ __forceinline__ void field_finalize_at(const NeeParams &Q, const AccT *__restrict__ Us,
+                                                  const AccT *__restrict__ Um, double norm, double2 *__restrict__ u,
+                                                  int64_t q)
+{
+    int i = (int)(q % Q.nv), j = (int)(q / Q.nv);
+    double2 s = make_double2((double)Us[2 * q], (double)Us[2 * q + 1]);
+    if (Q.is_ff_l && Q.is_ff_v) {
+        double2 af = evalampfunc<DIM>(dot3<DIM>(Q.l + 3 * j, Q.v + 3 * i), Q.pf);
+        s = cmul(af, s);
+    }
+    u[q] = make_double2(norm * (s.x + (double)Um[2 * q]), norm * (s.y + (double)Um[2 * q + 1]));
+}
+
 template <int DIM, typename AccT>
 __global__ void field_finalize_kernel(const __grid_constant__ NeeParams Q, const AccT *__restrict__ Us, const AccT *__restrict__ Um,
                                       double norm, double2 *__restrict__ u)
 {
     int64_t n = (int64_t)Q.nv * Q.nl;
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-        int i = (int)(q % Q.nv), j = (int)(q / Q.nv);
-        double2 s = make_double2((double)Us[2 * q], (double)Us[2 * q + 1]);
-        if (Q.is_ff_l && Q.is_ff_v) {
-            double2 af = evalampfunc<DIM>(dot3<DIM>(Q.l + 3 * j, Q.v + 3 * i), Q.pf);
-            s = cmul(af, s);
-        }
-        u[q] = make_double2(norm * (s.x + (double)Um[2 * q]), norm * (s.y + (double)Um[2 * q + 1]));
-    }
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        field_finalize_at<DIM, AccT>(Q, Us, Um, norm, u, q);
+}
+
+// The finalisation of a pack: blockIdx.y = request, its output at outs[r].
+template <int DIM, typename AccT>
+__global__ void field_finalize_packed_kernel(const NeeParams *__restrict__ Qs, const PackTiling *__restrict__ tiling,
+                                             const AccT *__restrict__ arena, const double *__restrict__ norms,
+                                             double2 *const *__restrict__ outs)
+{
+    const int r = blockIdx.y;
+    const NeeParams &Q = Qs[r];
+    const PackTiling t = tiling[r];
+    const int64_t n = (int64_t)Q.nv * Q.nl;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        field_finalize_at<DIM, AccT>(Q, arena + t.acc_s, arena + t.acc_m, norms[r], outs[r], q);
 }
 
 // ---------------------------------------------------------------------------

@@ -322,7 +322,7 @@ struct Ctx {
     DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
-    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl, offs;
+    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl, offs, mcap_bounds;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_twt, fq_rr, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     double multi_per_path = 8.0;  // multiple-scattering events per path seen so far (one-pass capacity)
@@ -357,6 +357,7 @@ struct Ctx {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
                          &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl, &offs,
+                         &mcap_bounds,
                          &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_twt, &fq_rr, &fq_counts, &fq_offsets,
                          &fq_cursor, &fq_planes};
         for (DevBuf *b : all) f(*b);
@@ -1891,6 +1892,269 @@ void fq_device_locked(Ctx &c, const scmc_fq_args *a, double *d_u, cudaStream_t s
     if (a->precision == SCMC_PREC_FP64) fq_run<P64, double>(c, a, Wl, u, st);
     else if (a->precision == SCMC_PREC_FP32) fq_run<P32, float>(c, a, Wl, u, st);
     else fq_run<PMIX, double>(c, a, Wl, u, st);
+}
+
+// ---------------------------------------------------------------------------
+// packs of field requests (the request server): many small MCfield solves of
+// one dimension and precision class, all on the CUDA-core accumulation, run
+// as one walk, one accumulation and one finalisation launch per round of up
+// to 2^20 paths instead of a launch sequence each.
+// ---------------------------------------------------------------------------
+struct PackItem {
+    const scmc_mc_args *a;
+    double *d_u;  // device output, 2*nv*nl doubles
+};
+
+__global__ void pack_bounds_kernel(const int64_t *__restrict__ moff, const int64_t *__restrict__ mcnt,
+                                   const int64_t *__restrict__ prefix, int n_req, int64_t n_paths,
+                                   int64_t *__restrict__ out)
+{
+    const int64_t total = n_paths > 0 ? moff[n_paths - 1] + mcnt[n_paths - 1] : 0;
+    for (int r = threadIdx.x; r <= n_req; r += blockDim.x) out[r] = prefix[r] < n_paths ? moff[prefix[r]] : total;
+}
+
+// Host staging of the pack's read-only inputs (directions, tables), uploaded in one copy.
+struct PackStage {
+    std::vector<char> bytes;
+    size_t put(const void *src, size_t n)
+    {
+        const size_t off = (bytes.size() + 255) & ~(size_t)255;
+        bytes.resize(off + n);
+        if (n) std::memcpy(bytes.data() + off, src, n);
+        return off;
+    }
+};
+
+template <int DIM, int POL, typename AccT>
+void field_pack_run(Ctx &c, const std::vector<PackItem> &items, cudaStream_t st)
+{
+    const int K = (int)items.size();
+    const int sms = sm_count(c.device);
+    std::vector<Prepared> P(K);
+    std::vector<PackTiling> tiling(K);
+    PackStage sg;
+    struct Offs {
+        size_t l, v, vs, a0, i0, a1, i1;
+    };
+    std::vector<Offs> off(K);
+    int64_t arena = 0;
+    size_t smem = 0;
+    using R = typename std::conditional<POL == P64, double, float>::type;
+    using Cx = typename cplx_t<R>::type;
+    for (int k = 0; k < K; ++k) {
+        const scmc_mc_args *a = items[k].a;
+        P[k] = host_params(a, 1);
+        std::vector<double> hl(3 * a->nl, 0.0), hv(3 * a->nv, 0.0), hvs(3 * a->nv, 0.0);
+        const double ff_sign = a->is_ff_v ? -1.0 : 1.0;  // MCfield.m:106
+        for (int64_t j = 0; j < a->nl; ++j)
+            for (int d = 0; d < DIM; ++d) hl[3 * j + d] = a->l[DIM * j + d];
+        for (int64_t i = 0; i < a->nv; ++i)
+            for (int d = 0; d < DIM; ++d) {
+                hv[3 * i + d] = a->v[DIM * i + d];
+                hvs[3 * i + d] = ff_sign * a->v[DIM * i + d];
+            }
+        Offs &o = off[k];
+        o.l = sg.put(hl.data(), hl.size() * 8);
+        o.v = sg.put(hv.data(), hv.size() * 8);
+        o.vs = sg.put(hvs.data(), hvs.size() * 8);
+        o.a0 = o.i0 = o.a1 = o.i1 = (size_t)-1;
+        if (a->ampfunc.sct_type == SCMC_SCT_TABULATED) {
+            o.a0 = sg.put(a->ampfunc.eval_amp, (size_t)a->ampfunc.table_n * sizeof(double2));
+            o.i0 = sg.put(a->ampfunc.sample_icdf, (size_t)a->ampfunc.table_n * sizeof(double));
+        }
+        if (a->has_ampfunc0 && a->ampfunc0.sct_type == SCMC_SCT_TABULATED) {
+            o.a1 = sg.put(a->ampfunc0.eval_amp, (size_t)a->ampfunc0.table_n * sizeof(double2));
+            o.i1 = sg.put(a->ampfunc0.sample_icdf, (size_t)a->ampfunc0.table_n * sizeof(double));
+        }
+        PackTiling &t = tiling[k];
+        const int nv = (int)a->nv, nl = (int)a->nl;
+        t.tv = std::min(nv, 32);
+        t.tl = std::min(nl, 32);
+        while (t.tv * t.tl > kFieldMaxTile) t.tl /= 2;
+        t.n_vtiles = (nv + t.tv - 1) / t.tv;
+        t.acc_s = arena;
+        t.acc_m = arena + 2 * (int64_t)nv * nl;
+        arena += 4 * (int64_t)nv * nl;
+        smem = std::max(smem, sizeof(Cx) * (2 * kFieldEB * (t.tv + t.tl) + kFieldEB) + sizeof(EventView) * kFieldEB + 16);
+    }
+    char *din = reinterpret_cast<char *>(c.wl.ensure(sg.bytes.size() + 256));
+    CK(cudaMemcpyAsync(din, sg.bytes.data(), sg.bytes.size(), cudaMemcpyHostToDevice, st));
+    auto dptr = [&](size_t o) { return o == (size_t)-1 ? nullptr : din + o; };
+    for (int k = 0; k < K; ++k) {
+        const Offs &o = off[k];
+        set_tables(P[k], items[k].a, reinterpret_cast<const double2 *>(dptr(o.a0)),
+                   reinterpret_cast<const double *>(dptr(o.i0)), reinterpret_cast<const double2 *>(dptr(o.a1)),
+                   reinterpret_cast<const double *>(dptr(o.i1)));
+        P[k].Q.l = reinterpret_cast<const double *>(din + o.l);
+        P[k].Q.v = reinterpret_cast<const double *>(din + o.v);
+        P[k].Q.vs = reinterpret_cast<const double *>(din + o.vs);
+        P[k].W.any_order = 0;
+    }
+    AccT *acc = reinterpret_cast<AccT *>(c.acc_s.ensure((size_t)arena * sizeof(AccT)));
+    CK(cudaMemsetAsync(acc, 0, (size_t)arena * sizeof(AccT), st));
+    // per-pack device tables: NEE parameters, tiling, outputs, norms (fixed), then per round the walk
+    // parameters, path prefix and jobs
+    std::vector<NeeParams> hQ(K);
+    std::vector<double> norms(K);
+    std::vector<double2 *> outs(K);
+    for (int k = 0; k < K; ++k) {
+        const scmc_mc_args *a = items[k].a;
+        hQ[k] = P[k].Q;
+        const double m = (double)(a->norm_itr > 0 ? a->norm_itr : a->max_itr);
+        norms[k] = m > 0 ? std::sqrt(1.0 / m * P[k].volume * a->sigt) : 0.0;  // MCfield.m:253-254
+        outs[k] = reinterpret_cast<double2 *>(items[k].d_u);
+    }
+    PackStage fixed;
+    const size_t oQ = fixed.put(hQ.data(), hQ.size() * sizeof(NeeParams));
+    const size_t oT = fixed.put(tiling.data(), tiling.size() * sizeof(PackTiling));
+    const size_t oN = fixed.put(norms.data(), norms.size() * sizeof(double));
+    const size_t oO = fixed.put(outs.data(), outs.size() * sizeof(double2 *));
+    char *dfix = reinterpret_cast<char *>(c.tiles.ensure(fixed.bytes.size() + 256));
+    CK(cudaMemcpyAsync(dfix, fixed.bytes.data(), fixed.bytes.size(), cudaMemcpyHostToDevice, st));
+    const NeeParams *dQ = reinterpret_cast<const NeeParams *>(dfix + oQ);
+    const PackTiling *dT = reinterpret_cast<const PackTiling *>(dfix + oT);
+    auto kacc = field_accum_packed_kernel<DIM, POL, AccT>;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kacc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+    std::vector<int64_t> done(K, 0);
+    const int64_t round_paths = (int64_t)1 << 20;
+    for (;;) {
+        // this round: every unfinished request gets an equal share of the round's paths
+        int open = 0;
+        for (int k = 0; k < K; ++k) open += done[k] < items[k].a->max_itr;
+        if (!open) break;
+        std::vector<WalkParams> hW(K);
+        std::vector<int64_t> prefix(K + 1, 0);
+        const int64_t share = std::max<int64_t>(1, round_paths / open);
+        for (int k = 0; k < K; ++k) {
+            const int64_t take = std::min<int64_t>(items[k].a->max_itr - done[k], share);
+            hW[k] = P[k].W;
+            hW[k].path_base = items[k].a->path_offset + (uint64_t)done[k];
+            hW[k].n_paths = take;
+            prefix[k + 1] = prefix[k] + take;
+        }
+        const int64_t n = prefix[K];
+        PackStage rs;
+        const size_t oW = rs.put(hW.data(), hW.size() * sizeof(WalkParams));
+        const size_t oP = rs.put(prefix.data(), prefix.size() * sizeof(int64_t));
+        char *drs = reinterpret_cast<char *>(c.out2.ensure(rs.bytes.size() + 256));
+        CK(cudaMemcpyAsync(drs, rs.bytes.data(), rs.bytes.size(), cudaMemcpyHostToDevice, st));
+        const WalkParams *dW = reinterpret_cast<const WalkParams *>(drs + oW);
+        const int64_t *dP = reinterpret_cast<const int64_t *>(drs + oP);
+        // pass 1: events per path, offsets of the multiple-scattering records
+        c.counts.ensure(n * sizeof(int32_t));
+        c.mcnt.ensure(n * sizeof(int64_t));
+        c.moff.ensure((n + 1) * sizeof(int64_t));
+        c.ctr.ensure(2 * sizeof(unsigned long long));
+        c.err.ensure(sizeof(int));
+        int64_t *dbounds = reinterpret_cast<int64_t *>(c.mcap_bounds.ensure((K + 1) * sizeof(int64_t)));
+        unsigned long long *ctr = c.ctr.as<unsigned long long>();
+        CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+        CK(cudaMemsetAsync(c.err.p, 0, sizeof(int), st));
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 127) / 128, (int64_t)sms * 8));
+        {
+            StageScope sc(ST_WALK, st);
+            walk_count_packed_kernel<DIM><<<grid, 128, 0, st>>>(dW, dP, K, n, c.counts.as<int32_t>(), ctr, c.err.as<int>());
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        count_to_multi_kernel<<<std::max(1, std::min(sms * 4, (int)((n + 255) / 256))), 256, 0, st>>>(
+            c.counts.as<int32_t>(), n, c.mcnt.as<int64_t>());
+        CK(cudaGetLastError());
+        LAUNCHED();
+        size_t tmp = 0;
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, c.mcnt.as<int64_t>(), c.moff.as<int64_t>(), n, st));
+        c.scan_tmp.ensure(tmp);
+        CK(cub::DeviceScan::ExclusiveSum(c.scan_tmp.p, tmp, c.mcnt.as<int64_t>(), c.moff.as<int64_t>(), n, st));
+        LAUNCHED();
+        pack_bounds_kernel<<<1, 256, 0, st>>>(c.moff.as<int64_t>(), c.mcnt.as<int64_t>(), dP, K, n, dbounds);
+        CK(cudaGetLastError());
+        LAUNCHED();
+        std::vector<int64_t> mb(K + 1);
+        int herr = 0;
+        CK(cudaMemcpyAsync(mb.data(), dbounds, (K + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&herr, c.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr) fail(SCMC_ERR_LIMIT, "a path exceeded max_events_per_path");
+        const int64_t n_multi = mb[K];
+        // pass 2: records
+        ensure_single_records(c, n);
+        ensure_multi_records(c, n_multi);
+        Batch B;
+        batch_views(c, n, n_multi, B);
+        CK(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), st));
+        {
+            StageScope sc(ST_WALK, st);
+            walk_record_packed_kernel<DIM><<<grid, 128, 0, st>>>(dW, dP, K, n, c.moff.as<int64_t>(), B.S, c.scap, B.M,
+                                                                 c.mcap, ctr + 1);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        prof_count(n, n + n_multi, 0.0);
+        // one accumulation launch: jobs of (request, tile, event range, singles / multis)
+        std::vector<PackJob> jobs;
+        for (int k = 0; k < K; ++k) {
+            const PackTiling &t = tiling[k];
+            const int tiles = t.n_vtiles * (int)((items[k].a->nl + t.tl - 1) / t.tl);
+            for (int single = 1; single >= 0; --single) {
+                const int64_t e0 = single ? prefix[k] : mb[k], e1 = single ? prefix[k + 1] : mb[k + 1];
+                const int64_t ne = e1 - e0;
+                if (ne <= 0) continue;
+                const int64_t ranges = std::max<int64_t>(1, (int64_t)sms * 6 / std::max(1, tiles * K));
+                const int64_t per = std::max<int64_t>((int64_t)kFieldEB * 4, (ne + ranges - 1) / ranges);
+                for (int tile = 0; tile < tiles; ++tile)
+                    for (int64_t e = e0; e < e1; e += per)
+                        jobs.push_back(PackJob{k, tile, single, 0, e, std::min(e1, e + per)});
+            }
+        }
+        if (!jobs.empty()) {
+            PackJob *dj = reinterpret_cast<PackJob *>(c.fq_planes.ensure(jobs.size() * sizeof(PackJob)));
+            CK(cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(PackJob), cudaMemcpyHostToDevice, st));
+            StageScope sc(ST_ROWS, st);
+            kacc<<<(unsigned)jobs.size(), kFieldThreads, smem, st>>>(dQ, dT, dj, B.S, c.scap, B.M, c.mcap, acc);
+            CK(cudaGetLastError());
+            LAUNCHED();
+        }
+        CK(cudaStreamSynchronize(st));  // the host vectors of this round go out of scope
+        for (int k = 0; k < K; ++k) done[k] += prefix[k + 1] - prefix[k];
+    }
+    int64_t nmax = 0;
+    for (int k = 0; k < K; ++k) nmax = std::max<int64_t>(nmax, items[k].a->nv * items[k].a->nl);
+    StageScope fin(ST_FINAL, st);
+    field_finalize_packed_kernel<DIM, AccT><<<dim3((unsigned)std::max<int64_t>(1, std::min<int64_t>((nmax + 255) / 256, 64)),
+                                                   (unsigned)K),
+                                              256, 0, st>>>(dQ, dT, acc, reinterpret_cast<const double *>(dfix + oN),
+                                                            reinterpret_cast<double2 *const *>(dfix + oO));
+    CK(cudaGetLastError());
+    LAUNCHED();
+    CK(cudaStreamSynchronize(st));
+}
+
+// A pack's items must share dim and precision class and take the CUDA-core
+// accumulation (use_field_tc false).
+void field_pack_device(Ctx &c, const std::vector<PackItem> &items, cudaStream_t st)
+{
+    if (items.empty()) return;
+    const scmc_mc_args *a = items[0].a;
+    CK(cudaSetDevice(a->device));
+    const bool mix = a->precision == SCMC_PREC_MIXED || a->precision == SCMC_PREC_FP16;
+    if (a->dim == 3) {
+        if (a->precision == SCMC_PREC_FP64) field_pack_run<3, P64, double>(c, items, st);
+        else if (mix) field_pack_run<3, PMIX, double>(c, items, st);
+        else field_pack_run<3, P32, float>(c, items, st);
+    } else {
+        if (a->precision == SCMC_PREC_FP64) field_pack_run<2, P64, double>(c, items, st);
+        else if (mix) field_pack_run<2, PMIX, double>(c, items, st);
+        else field_pack_run<2, P32, float>(c, items, st);
+    }
+}
+
+// The precision class a request packs with (-1: never packed).
+int pack_class(int kind, const scmc_mc_args &a, int64_t max_paths)
+{
+    if (kind != SCMC_REQ_FIELD || a.max_itr > max_paths || a.max_itr < 1 || use_field_tc(&a)) return -1;
+    const int pol = a.precision == SCMC_PREC_FP64 ? 0 : (a.precision == SCMC_PREC_FP32 ? 2 : 1);
+    return a.dim * 4 + pol;
 }
 
 #include "server.cuh"

@@ -3,11 +3,18 @@
 //
 // Continuous batching of MCfield / MCcov solves: n_slots worker threads, each
 // with its own CUDA stream and its own scratch context (stream-ordered
-// allocations, released after every request).  The queue is FIFO: its head is
-// admitted as soon as a slot is idle and the head's memory estimate fits the
-// HBM budget beside the reservations of the requests already running.  The
-// estimate is an upper bound from the request's sizes and expected events per
-// path; each request's real footprint is reported beside its reservation.
+// allocations, released after every request).  Admission: a slot that falls
+// idle takes the oldest request whose memory estimate fits the HBM budget
+// beside the reservations of the requests already running; a request that
+// does not fit may be passed by younger ones at most kMaxPassed times, after
+// which nothing is admitted before it (no starvation).  The estimate is an
+// upper bound from the request's sizes and expected events per path; each
+// request's real footprint is reported beside its reservation.  Small field
+// requests on the CUDA-core accumulation (up to kPackPaths paths, same
+// dimension and precision class) are packed: the slot takes up to kPackMax of
+// them from the queue and runs them as one walk, one accumulation and one
+// finalisation launch per round (field_pack_device); if a pack fails, its
+// requests are rerun one by one so that a failure stays with its request.
 // Requests on different slots share the device: their kernels interleave and
 // overlap.
 // The standard headers it needs (<chrono>, <condition_variable>, <deque>,
@@ -49,7 +56,14 @@ struct Request {
     int slot = -1, status = SCMC_OK, finished = 0;
     std::string message;
     double submit_ms = 0, start_ms = 0, done_ms = 0, device_ms = 0;
+    int passed = 0;   // times a younger request was admitted before it
+    int packed = 0;   // requests in the pack it ran in (1: alone)
 };
+
+constexpr int kMaxPassed = 16;
+constexpr int kPackMax = 64;
+constexpr int64_t kPackPaths = (int64_t)1 << 20;       // per request
+constexpr int64_t kPackTotalPaths = (int64_t)1 << 23;  // per pack
 
 // Device memory a request will hold on its slot, from its sizes.  The walk
 // term uses the expected events per path of a slab sigt*thickness optical
@@ -120,6 +134,49 @@ struct Server {
         for (int s = 0; s < n_slots; ++s) workers.emplace_back([this, s] { worker(s); });
     }
 
+    // The queue index of the request to admit next, if any fits: the oldest
+    // that fits the budget, younger ones passing an older one that does not fit
+    // at most kMaxPassed times.  Called with mu held.
+    bool admissible(size_t &pick)
+    {
+        for (size_t i = 0; i < queue.size(); ++i) {
+            if (reserved + queue[i]->estimate <= budget) {
+                pick = i;
+                return true;
+            }
+            if (queue[i]->passed >= kMaxPassed) return false;  // its turn: wait for room
+        }
+        return false;
+    }
+
+    // Runs a pack of small field requests as one walk / accumulate / finalise
+    // launch sequence per round and copies each result out.
+    void run_pack(Ctx &c, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, std::vector<Request *> &batch)
+    {
+        size_t total = 0;
+        for (Request *r : batch) total += (size_t)r->args.a.nv * r->args.a.nl * 2;
+        CK(cudaEventRecord(e0, st));
+        double *d = reinterpret_cast<double *>(c.out0.ensure(total * sizeof(double)));
+        std::vector<PackItem> items;
+        size_t o = 0;
+        for (Request *r : batch) {
+            items.push_back(PackItem{&r->args.a, d + o});
+            o += (size_t)r->args.a.nv * r->args.a.nl * 2;
+        }
+        field_pack_device(c, items, st);
+        o = 0;
+        for (Request *r : batch) {
+            const size_t n = (size_t)r->args.a.nv * r->args.a.nl * 2;
+            CK(cudaMemcpyAsync(r->out0, d + o, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            o += n;
+        }
+        CK(cudaEventRecord(e1, st));
+        CK(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        for (Request *r : batch) r->device_ms = ms;
+    }
+
     // Runs one request on a slot's stream and copies its result out.
     void run(Ctx &c, cudaStream_t st, cudaEvent_t e0, cudaEvent_t e1, Request &r)
     {
@@ -159,34 +216,78 @@ struct Server {
         }
         c.set_stream_ordered(st);
         for (;;) {
-            Request *r = nullptr;
+            std::vector<Request *> batch;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] {
-                    return stopping || (!queue.empty() && reserved + queue.front()->estimate <= budget);
-                });
+                size_t pick = 0;
+                cv_work.wait(lk, [&] { return stopping || admissible(pick); });
                 if (stopping) break;  // shutdown has cancelled the queue
-                r = queue.front();
-                queue.pop_front();
-                r->slot = s;
-                r->reserved = r->estimate;
-                r->start_ms = now_ms();
-                reserved += r->reserved;
+                Request *r = queue[pick];
+                for (size_t i = 0; i < pick; ++i) ++queue[i]->passed;
+                queue.erase(queue.begin() + (std::ptrdiff_t)pick);
+                batch.push_back(r);
+                // a small CUDA-core field request takes others of its class along
+                const int cls = pack_class(r->kind, r->args.a, kPackPaths);
+                int64_t paths = r->args.a.max_itr, res = reserved + r->estimate;
+                if (cls >= 0) {
+                    for (size_t i = 0; i < queue.size() && (int)batch.size() < kPackMax;) {
+                        Request *q = queue[i];
+                        if (pack_class(q->kind, q->args.a, kPackPaths) == cls && paths + q->args.a.max_itr <= kPackTotalPaths &&
+                            res + q->estimate <= budget) {
+                            paths += q->args.a.max_itr;
+                            res += q->estimate;
+                            batch.push_back(q);
+                            queue.erase(queue.begin() + (std::ptrdiff_t)i);
+                        } else {
+                            ++i;
+                        }
+                    }
+                }
+                const double t = now_ms();
+                for (Request *q : batch) {
+                    q->slot = s;
+                    q->reserved = q->estimate;
+                    q->start_ms = t;
+                    q->packed = (int)batch.size();
+                    reserved += q->reserved;
+                }
                 peak_reserved = std::max(peak_reserved, reserved);
                 ++busy;
             }
-            int status = SCMC_OK;
-            std::string msg;
-            try {
-                run(c, st, e0, e1, *r);
-            } catch (const ScmcError &e) {
-                status = e.code;
-                msg = e.msg;
-            } catch (const std::exception &e) {
-                status = SCMC_ERR_CUDA;
-                msg = e.what();
+            std::vector<int> status(batch.size(), SCMC_OK);
+            std::vector<std::string> msg(batch.size());
+            auto attempt = [&](auto &&fn, size_t k) {
+                try {
+                    fn();
+                } catch (const ScmcError &e) {
+                    status[k] = e.code;
+                    msg[k] = e.msg;
+                } catch (const std::exception &e) {
+                    status[k] = SCMC_ERR_CUDA;
+                    msg[k] = e.what();
+                }
+            };
+            if (batch.size() == 1) {
+                attempt([&] { run(c, st, e0, e1, *batch[0]); }, 0);
+            } else {
+                attempt([&] { run_pack(c, st, e0, e1, batch); }, 0);
+                if (status[0] != SCMC_OK) {  // rerun one by one: a failure stays with its request
+                    try {
+                        cudaStreamSynchronize(st);
+                        c.release_all();
+                    } catch (...) {
+                    }
+                    for (size_t k = 0; k < batch.size(); ++k) {
+                        status[k] = SCMC_OK;
+                        msg[k].clear();
+                        batch[k]->packed = 1;
+                        attempt([&] { run(c, st, e0, e1, *batch[k]); }, k);
+                    }
+                } else {
+                    for (size_t k = 1; k < batch.size(); ++k) status[k] = SCMC_OK;
+                }
             }
-            const int64_t held = (int64_t)c.held();  // what the slot allocated for this request
+            const int64_t held = (int64_t)c.held();  // what the slot allocated for this request or pack
             try {
                 c.release_all();
                 cudaStreamSynchronize(st);
@@ -194,19 +295,23 @@ struct Server {
             }
             {
                 std::lock_guard<std::mutex> lk(mu);
-                r->peak = held;
-                reserved -= r->reserved;
-                r->status = status;
-                r->message = msg;
-                r->done_ms = now_ms();
-                r->finished = 1;
-                --busy;
-                if (status == SCMC_OK) {
-                    ++completed;
-                    paths_completed += r->args.a.max_itr;
-                } else {
-                    ++failed;
+                const double t = now_ms();
+                for (size_t k = 0; k < batch.size(); ++k) {
+                    Request *r = batch[k];
+                    r->peak = held;
+                    reserved -= r->reserved;
+                    r->status = status[k];
+                    r->message = msg[k];
+                    r->done_ms = t;
+                    r->finished = 1;
+                    if (status[k] == SCMC_OK) {
+                        ++completed;
+                        paths_completed += r->args.a.max_itr;
+                    } else {
+                        ++failed;
+                    }
                 }
+                --busy;
             }
             cv_done.notify_all();
             cv_work.notify_all();
@@ -232,6 +337,7 @@ struct Server {
         o->reserved_bytes = r.reserved ? r.reserved : r.estimate;
         o->peak_bytes = r.peak;
         o->paths = r.args.a.max_itr;
+        o->packed = r.packed;
     }
 
     void shutdown()

@@ -394,4 +394,111 @@ __global__ void __launch_bounds__(128) walk_onepass_kernel(const __grid_constant
     }
 }
 
+// ---------------------------------------------------------------------------
+// Packs of requests (the request server): the paths of n requests are one
+// index range, request r owning [prefix[r], prefix[r + 1]); path g of request
+// r is that request's path path_base + g - prefix[r] under its own Philox key
+// and medium.  Two passes as for one request, so each request's records are
+// contiguous (its multiple-scattering records follow moff[prefix[r]]).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int pack_request(const int64_t *__restrict__ prefix, int n, int64_t g)
+{
+    int lo = 0, hi = n - 1;  // the last r with prefix[r] <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) walk_count_packed_kernel(const WalkParams *__restrict__ Ps,
+                                                                const int64_t *__restrict__ prefix, int n_req,
+                                                                int64_t n_paths, int32_t *__restrict__ counts,
+                                                                unsigned long long *__restrict__ next_path,
+                                                                int *__restrict__ err)
+{
+    PathRng r;
+    WalkState s;
+    int64_t p = -1;
+    const WalkParams *P = Ps;
+    int n = 0;
+    for (;;) {
+        if (p < 0) {
+            p = (int64_t)atomicAdd(next_path, 1ull);
+            if (p >= n_paths) break;
+            const int q = pack_request(prefix, n_req, p);
+            P = Ps + q;
+            r.init(P->key0, P->key1, P->path_base + (uint64_t)(p - prefix[q]));
+            path_init<DIM>(*P, r, s);
+            n = 0;
+        }
+        ++n;
+        if (P->want_phase) (void)r.rand();
+        bool alive = path_advance<DIM>(*P, r, s);
+        if (alive && P->max_events > 0 && n >= P->max_events) {
+            atomicExch(err, 1);
+            alive = false;
+        }
+        if (!alive) {
+            counts[p] = n;
+            p = -1;
+        }
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) walk_record_packed_kernel(const WalkParams *__restrict__ Ps,
+                                                                 const int64_t *__restrict__ prefix, int n_req,
+                                                                 int64_t n_paths, const int64_t *__restrict__ moff,
+                                                                 SingleRec S, int64_t scap, MultiRec M, int64_t mcap,
+                                                                 unsigned long long *__restrict__ next_path)
+{
+    PathRng r;
+    WalkState s;
+    int64_t p = -1, mo = 0;
+    const WalkParams *P = Ps;
+    for (;;) {
+        if (p < 0) {
+            p = (int64_t)atomicAdd(next_path, 1ull);
+            if (p >= n_paths) break;
+            const int q = pack_request(prefix, n_req, p);
+            P = Ps + q;
+            r.init(P->key0, P->key1, P->path_base + (uint64_t)(p - prefix[q]));
+            path_init<DIM>(*P, r, s);
+            mo = moff[p];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                S.x1[k * scap + p] = s.x[k];
+                S.w1[k * scap + p] = s.w[k];
+            }
+        }
+        ++s.pL;
+        const double xi = P->want_phase ? r.rand() : 0.0;
+        const double wpx = s.weight / s.px;
+        if (s.pL == 1) {
+            S.wpx[p] = wpx;
+            S.xi[p] = xi;
+        } else {
+            const int64_t e = mo + (s.pL - 2);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                M.x[k * mcap + e] = s.x[k];
+                M.ow[k * mcap + e] = s.ow[k];
+            }
+            M.wpx[e] = wpx;
+            M.xi[e] = xi;
+            M.path[e] = (int32_t)p;
+            M.plen[e] = s.pL;
+        }
+        bool alive = path_advance<DIM>(*P, r, s);
+        if (alive && P->max_events > 0 && s.pL >= P->max_events) alive = false;
+        if (!alive) {
+            S.nev[p] = s.pL;
+            p = -1;
+        }
+    }
+}
+
 }  // namespace scmc

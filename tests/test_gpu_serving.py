@@ -137,3 +137,46 @@ def test_poll_and_destroy_with_queue(gpu):
     assert info0["finished"] == 1
     srv.close()  # runs the admitted request to completion, cancels the queue
     assert rel(u0, MC.field_from_args(holder(reqs[0]))) < SAME_TOL_MIXED
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_small_requests_are_packed(gpu, precision):
+    """Small CUDA-core field requests submitted together run in packs (one walk,
+    accumulation and finalisation per round for many requests), with the same
+    results as alone; a tensor-core-size request and a 2-D one run on their own."""
+    reqs = WL.served_requests(40, seed=21, paths=(300, 5000), nv_max=48, nl_max=24, side_mfp=(5.0, 12.0))
+    with Server(slots=2) as srv:
+        tickets = [srv.submit_field(holder(r, precision)) for r in reqs]
+        out = [srv.wait(t) for t in tickets]
+        st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    sizes = [info["packed"] for _, info in out]
+    assert max(sizes) > 4  # many requests shared their launches
+    for r, (u, info) in zip(reqs, out):
+        alone = MC.field_from_args(holder(r, precision))
+        assert rel(u, alone) < (SAME_TOL if precision == "fp64" else SAME_TOL_MIXED)
+
+
+def test_large_head_does_not_block_small_requests(gpu):
+    """With a budget that holds one large request and a few small ones, a large
+    request waiting at the head of the queue is passed by small ones (a bounded
+    number of times) and still completes."""
+    big = WL.served_requests(1, seed=31, paths=(20000, 20001), nv_max=1024, nl_max=256)[0]
+    big["args"][4] = WL.cap_dirs(200, 10.0, +1.0, np.random.default_rng(1))
+    big["args"][5] = WL.cap_dirs(900, 10.0, -1.0, np.random.default_rng(2))
+    small = WL.served_requests(12, seed=32, paths=(500, 2000), nv_max=16, nl_max=8)
+    with Server(slots=1) as srv:  # the reservation of each request alone
+        est_big = srv.wait(srv.submit_field(holder(big)))[1]["reserved_bytes"]
+        est_small = max(srv.wait(srv.submit_field(holder(r)))[1]["reserved_bytes"] for r in small)
+    budget = est_big + 3 * est_small
+    with Server(slots=3, hbm_budget=budget) as srv:
+        first = srv.submit_field(holder(big))      # occupies most of the budget
+        t_big = srv.submit_field(holder(big))      # does not fit beside the first
+        ts = [srv.submit_field(holder(r)) for r in small]
+        res_small = [srv.wait(t) for t in ts]
+        u_big, info_big = srv.wait(t_big)
+        srv.wait(first)
+    assert any(info["start_ms"] < info_big["start_ms"] for _, info in res_small)
+    for r, (u, _) in zip(small, res_small):
+        assert rel(u, MC.field_from_args(holder(r))) < SAME_TOL_MIXED
+    assert rel(u_big, MC.field_from_args(holder(big))) < SAME_TOL_MIXED
