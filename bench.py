@@ -424,11 +424,13 @@ def run_leg(leg, a, prec, peaks, peak_kind):
     torch.cuda.empty_cache()
     value = P * a.steps / (ms / 1000.0)
     # e2e: the host-buffer call (inputs from host, results copied back every step)
-    ke = max(1, min(a.steps, a.leg_e2e_steps))
-    t0 = time.perf_counter()
-    for i in range(ke):
-        leg.host(leg.make(P, prec, 0, off=(a.warmup + a.steps + i) * P, norm=P))
-    e2e = P * ke / (time.perf_counter() - t0)
+    ke = min(a.steps, a.leg_e2e_steps)
+    e2e = None
+    if ke > 0:
+        t0 = time.perf_counter()
+        for i in range(ke):
+            leg.host(leg.make(P, prec, 0, off=(a.warmup + a.steps + i) * P, norm=P))
+        e2e = P * ke / (time.perf_counter() - t0)
     # roofline of the dominant kernel over its busy time (launches on several
     # streams overlap; each instant counts once)
     roof = None
@@ -461,15 +463,19 @@ def run_leg(leg, a, prec, peaks, peak_kind):
                 "flops_per_launch": work / n_launch, "busy_ms_per_launch": busy / n_launch, "launches": n_launch,
                 f"{leg.unit_name}s_per_launch": units / n_launch,
                 "traffic_source": f"profiles/{leg.traffic_file}" if tj is not None else None}
-    acc = leg_accuracy(leg, [prec] + [p for p in ("mixed", "fp16", "fp32") if p != prec], O)
+    acc = None if a.no_accuracy else leg_accuracy(leg, [prec] + [p for p in ("mixed", "fp16", "fp32") if p != prec], O)
     # plain FP32 GPU on a smaller sample, and the same sample in the line's precision
     n32 = max(1, P // 10)
-    t32 = time.perf_counter()
-    leg.host(leg.make(n32, "fp32", 0))
-    fp32_value = n32 / (time.perf_counter() - t32)
-    tp = time.perf_counter()
-    leg.host(leg.make(n32, prec, 0))
-    same_value = n32 / (time.perf_counter() - tp)
+    fp32 = None
+    if not a.no_fp32:
+        t32 = time.perf_counter()
+        leg.host(leg.make(n32, "fp32", 0))
+        fp32_value = n32 / (time.perf_counter() - t32)
+        tp = time.perf_counter()
+        leg.host(leg.make(n32, prec, 0))
+        same_value = n32 / (time.perf_counter() - tp)
+        fp32 = {"paths": n32, "value": fp32_value, f"{prec}_same_sample": same_value,
+                f"speedup_{prec}_over_fp32": same_value / fp32_value}
     cpu = None
     if not a.no_cpu_baseline:
         n = leg.cpu_paths
@@ -482,15 +488,12 @@ def run_leg(leg, a, prec, peaks, peak_kind):
                "sample": f"{n} paths of the workload in {dt:.1f} s (FP64 oracle, {leg.cpu_threads} thread(s))"}
     return {"workload": leg.name, "description": leg.desc, "value": value, "unit": UNIT, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "paths_per_step": P, "precision": prec,
-            "e2e": {"value": e2e, "unit": UNIT, "steps": ke, "h2d_bytes_per_step": int(leg.h2d),
-                    "d2h_bytes_per_step": int(sum(leg.sizes[:2]) * 8)},
+            "e2e": None if e2e is None else {"value": e2e, "unit": UNIT, "steps": ke, "h2d_bytes_per_step": int(leg.h2d),
+                                             "d2h_bytes_per_step": int(sum(leg.sizes[:2]) * 8)},
             "gpu_launches": int(launches), "roofline": roof,
             "stages_ms": {k: prof[k] for k in ("walk_ms", "rows_ms", "contract_ms", "finalize_ms",
                                                "contract_busy_ms", "rows_busy_ms")},
-            "accuracy": acc,
-            "fp32_gpu": {"paths": n32, "value": fp32_value, f"{prec}_same_sample": same_value,
-                         f"speedup_{prec}_over_fp32": same_value / fp32_value},
-            "cpu_baseline": cpu, "clocks": clk}
+            "accuracy": acc, "fp32_gpu": fp32, "cpu_baseline": cpu, "clocks": clk}
 
 
 def run_workload(a):
@@ -536,7 +539,9 @@ def main():
     ap.add_argument("--legs", default="field16,fq256,hetero128",
                     help="configurations measured beside the headline on one GPU ('' for none)")
     ap.add_argument("--leg-paths", default="", help="per-leg path budgets, e.g. fq256=1e6,hetero128=2e4")
-    ap.add_argument("--leg-e2e-steps", type=int, default=3)
+    ap.add_argument("--leg-e2e-steps", type=int, default=3, help="host-buffer solves per leg (0: none)")
+    ap.add_argument("--no-accuracy", action="store_true", help="legs: skip the oracle comparison (profiling runs)")
+    ap.add_argument("--no-fp32", action="store_true", help="legs: skip the plain FP32 comparison (profiling runs)")
     ap.add_argument("--workload", default="cov64", choices=["cov64", "field16", "fq256", "hetero128"],
                     help="cov64: the default line; the others print one line of their own (1 GPU)")
     a = ap.parse_args()
