@@ -649,6 +649,26 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = P * world * a.steps / float(t.item())
 
+    # the memory-effect view of the last step's covariance (offset means, FP32), HBM bound
+    n_off = 15 ** 4
+    R = torch.empty(2 * n_off, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.lib().scmc_cov_offsets_device(Ms.data_ptr(), Mm.data_ptr(), 8, 8, 8, 8, R.data_ptr(), local,
+                                                  stream.cuda_stream))
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    _lib.check(_lib.lib().scmc_cov_offsets_device(Ms.data_ptr(), Mm.data_ptr(), 8, 8, 8, 8, R.data_ptr(), local,
+                                                  stream.cuda_stream))
+    f1.record(stream)
+    torch.cuda.synchronize()
+    off_ms = f0.elapsed_time(f1)
+    Rh = R.cpu().numpy().view(np.complex64).reshape(15, 15, 15, 15, order="F")
+    # along equal view and light tilts (dv = dl along one grid axis) relative to no offset
+    curve = [float(abs(Rh[7 + d, 7, 7 + d, 7]) / abs(Rh[7, 7, 7, 7])) for d in range(8)]
+    memory_effect = {"kernel_ms": off_ms, "hbm_gbs": 2 * 2 * n_out * 8 / (off_ms / 1000.0) / 1e9,
+                     "output": "15x15x15x15 complex f32 (view offset x light offset on the 8x8 grids)",
+                     "abs_R_dv_eq_dl_over_R0": curve}
+
     line = None
     if rank == 0:
         del host_Ms, host_Mm
@@ -737,6 +757,7 @@ def main():
             "other_precision": {"precision": other, "paths": nf, "value": nf / other_small_s},
             "fp32_gpu": {"paths": nf, "value": nf / fp32_s, f"{a.precision}_same_sample": nf / prec_small_s,
                          f"speedup_{a.precision}_over_fp32": fp32_s / prec_small_s},
+            "memory_effect": memory_effect,
             "workloads": legs,
             "serving": served,
             "cpu_baseline": cpu,

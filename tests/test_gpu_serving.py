@@ -143,7 +143,7 @@ def test_poll_and_destroy_with_queue(gpu):
 def test_small_requests_are_packed(gpu, precision):
     """Small CUDA-core field requests submitted together run in packs (one walk,
     accumulation and finalisation per round for many requests), with the same
-    results as alone; a tensor-core-size request and a 2-D one run on their own."""
+    results as each request alone."""
     reqs = WL.served_requests(40, seed=21, paths=(300, 5000), nv_max=48, nl_max=24, side_mfp=(5.0, 12.0))
     with Server(slots=2) as srv:
         tickets = [srv.submit_field(holder(r, precision)) for r in reqs]
