@@ -158,7 +158,7 @@ struct PlaneEpi {
     const float2 *rr;      // [r2][r1]: exp(zexp0 * 2 z_bin), the factor between planes P and P - 2
     const double *gz;      // plane boundaries
     const int *planes;     // plane of each plane slot
-    float *U;              // [r1][r2] complex interleaved FP32, this light
+    double *U;             // [r1][r2] complex interleaved FP64, this light (the sum across planes and batches)
     int nv0;
     int n_uniform;         // planes 0 .. n_uniform-1 have centres bmin_z + (P + 1/2) z_bin
     const unsigned *max_bits;  // the group's operand scale (fq_scale_exponent); the flush undoes it
@@ -352,7 +352,8 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32
 // non-uniform plane, the end of the range) or the segment reached
 // kFqSegMax planes, the epilogue adds exp(zexp0 tz_P) times the
 // accumulator into U (factor with the phase product and reduction in FP64,
-// sincos and exp in FP32) and the chain's next MMA starts it afresh.  While
+// sincos and exp in FP32; the sum across planes and batches is FP64) and the
+// chain's next MMA starts it afresh.  While
 // the epilogue works on one chain the MMAs of the other run.
 // Warp 0 issues the TMA loads of every K block in walk order through the
 // ring, warp 1 the MMAs, warps 4-7 (one TMEM lane quarter each) the
@@ -566,9 +567,11 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
                         out[16 + t] = __float_as_uint(odd ? vi : recv);  // column 16 + t
                     } else {
                         const int n = col0 + c0 + jb + t;
-                        if (row_ok && n < N)
-                            atomicAdd(reinterpret_cast<float2 *>(pe.U + 2 * ((int64_t)r1 * pe.nv0 + n)),
-                                      make_float2(vr, vi));
+                        if (row_ok && n < N) {
+                            double *u = pe.U + 2 * ((int64_t)r1 * pe.nv0 + n);
+                            atomicAdd(u, (double)vr);
+                            atomicAdd(u + 1, (double)vi);
+                        }
                     }
                 }
                 if (cont) tmem_st32(tacc + c0, out);

@@ -1492,15 +1492,15 @@ void validate_fq(const scmc_fq_args *a)
 }
 
 // The per-plane DFT sums of one batch on tcgen05 (fq.cuh, tensor-core form),
-// added into U stored [light][r1][r2] in FP32 (each plane's sum is FP32 in
-// TMEM already).  Tt: the twiddles stored [p][r]; dz: zexp0 stored [r2][r1].
+// added into U stored [light][r1][r2] in FP64 (each plane's sum is FP32 in
+// TMEM; the sum across planes and batches is FP64).  Tt: the twiddles stored [p][r]; dz: zexp0 stored [r2][r1].
 // Nonempty planes are taken in groups of at most group_entries padded entries
 // (operand memory; tuned, 2^20 built in) and kFqTcPlanes planes.
 constexpr int kFqTcPlanes = 16384;
 
 void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
                  const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt, const double2 *dz,
-                 const float2 *rr, int n_uniform, float *U, bool split, int64_t group_entries, cudaStream_t st)
+                 const float2 *rr, int n_uniform, double *U, bool split, int64_t group_entries, cudaStream_t st)
 {
     const int nv0 = F.nv0;
     const int Mr = 2 * nv0;
@@ -1857,7 +1857,7 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
         }
         if (use_tc) {
             fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
-                        reinterpret_cast<float *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
+                        reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
             for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
@@ -1876,9 +1876,9 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     const double norm = total_vert > 0 ? std::sqrt(1.0 / (double)total_vert * V * sigt) : 0.0;  // lines 214, 302-303
     StageScope fin(ST_FINAL, st);
     const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((nout + 255) / 256, 4096));
-    if (use_tc)  // FP32 accumulator in U's memory, stored [light][r1][r2]
-        fq_finalize_kernel<float><<<fgrid, 256, 0, st>>>(reinterpret_cast<const float *>(U), db, (int)Nv, (int)nl_out,
-                                                         norm, d_u, 1);
+    if (use_tc)  // FP64 accumulator stored [light][r1][r2]
+        fq_finalize_kernel<double><<<fgrid, 256, 0, st>>>(reinterpret_cast<const double *>(U), db, (int)Nv, (int)nl_out,
+                                                          norm, d_u, 1);
     else
         fq_finalize_kernel<AccT><<<fgrid, 256, 0, st>>>(U, db, (int)Nv, (int)nl_out, norm, d_u, 0);
     CK(cudaGetLastError());

@@ -108,7 +108,9 @@ struct Server {
     int device = 0;
     int n_slots = 0;
     int64_t budget = 0;
-    size_t chunk_bytes = (size_t)256 << 20;
+    // the library's default operand memory per tensor-core chunk, so that a
+    // request's chunks (and their FP32 sums) are the same on a slot as alone
+    size_t chunk_bytes = (size_t)2 << 30;
     SteadyClock::time_point t0;
 
     std::mutex mu;

@@ -19,7 +19,11 @@ from mcspeckle_b200 import _abi, _lib
 from mcspeckle_b200 import mc as MC
 
 pytestmark = pytest.mark.gpu
-TOL = {"fp64": 1e-10, "mixed": 1e-9, "fp16": 1e-9, "fp32": 1e-5}  # same CUDA-core kernels on both sides
+# Same CUDA-core kernels on both sides.  In the reduced precisions scmc_field
+# walks once and takes its records in any order, so which events one CTA sums
+# in FP32 before its FP64 atomic add differs from the no-alloc entry point's
+# path-ordered records: agreement to FP32 rounding, not bit for bit.
+TOL = {"fp64": 1e-10, "mixed": 1e-6, "fp16": 1e-6, "fp32": 1e-5}
 MIXED_TOL = 1e-3  # against FP64, as the other mixed-precision parity tests
 
 
