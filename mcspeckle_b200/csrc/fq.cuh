@@ -307,12 +307,12 @@ fq_accum_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ 
 // non-negative float).
 __global__ void __launch_bounds__(256)
 fq_scale_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk,
-                int64_t nblk, int light, unsigned *__restrict__ max_bits)
+                int64_t nblk, int bs, int light, unsigned *__restrict__ max_bits)
 {
     float m = 0.f;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nblk * 32; i += (int64_t)gridDim.x * blockDim.x) {
-        const int2 bk = blk[i >> 5];
-        const int t = (int)(i & 31);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nblk * bs; i += (int64_t)gridDim.x * blockDim.x) {
+        const int2 bk = blk[i / bs];
+        const int t = (int)(i % bs);
         if (t < bk.y) {
             const FqEntry en = E[bk.x + t];
             const float2 sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, light, en.xl));
@@ -379,6 +379,69 @@ fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict_
             }
             *reinterpret_cast<__half2 *>(Bm + (int64_t)r * K + col) =
                 __halves2half2(__float2half_rn(bv.x), __float2half_rn(bv.y));
+        }
+    }
+}
+
+// Planar rows for the CTA-pair form (grids of at least 128 angles): per
+// block of 64 entries (a plane's last block zero-padded), K column = entry,
+// A planes Re / Im of s_e(j) T[r1][p1_e] (with the low parts for hi+lo) and B
+// planes Re / Im of T[r2][p2_e], rows r = 0 .. nv0-1, row stride K halves.
+// Thread = (entry e, row group g): a warp's stores of one row are 32
+// consecutive halves of each plane.
+template <bool SPLIT>
+__global__ void __launch_bounds__(256)
+fq_tc_rows_planar_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E,
+                         const int2 *__restrict__ blk, int light, const float2 *__restrict__ Tt, int64_t K,
+                         __half *__restrict__ Are, __half *__restrict__ Aim, __half *__restrict__ Alr,
+                         __half *__restrict__ Ali, __half *__restrict__ Bre, __half *__restrict__ Bim,
+                         const unsigned *__restrict__ max_bits)
+{
+    constexpr int RB = 32;  // twiddle rows staged per pass
+    __shared__ float2 ss[64];
+    __shared__ int sp1[64], sp2[64];
+    __shared__ float2 ta[RB][65], tb[RB][65];  // [r - r0][entry]
+    const float scale = ldexpf(1.f, fq_scale_exponent(max_bits));
+    const int2 bk = blk[blockIdx.x];  // (first entry, entries in this block)
+    if (threadIdx.x < 64) {
+        float2 sv = make_float2(0.f, 0.f);
+        int p1 = 0, p2 = 0;
+        if ((int)threadIdx.x < bk.y) {
+            const FqEntry en = E[bk.x + threadIdx.x];
+            sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, light, en.xl));
+            sv.x *= scale;
+            sv.y *= scale;
+            p1 = en.p1;
+            p2 = en.p2;
+        }
+        ss[threadIdx.x] = sv;
+        sp1[threadIdx.x] = p1;
+        sp2[threadIdx.x] = p2;
+    }
+    const int e = threadIdx.x & 63, g = threadIdx.x >> 6;
+    const int64_t col = (int64_t)blockIdx.x * 64 + e;
+    for (int r0 = 0; r0 < F.nv0; r0 += RB) {
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < 64 * RB; idx += blockDim.x) {
+            const int k = idx / RB, rr = idx % RB, r = r0 + rr;
+            const bool ok = k < bk.y && r < F.nv0;
+            ta[rr][k] = ok ? Tt[(int64_t)sp1[k] * F.nv0 + r] : make_float2(0.f, 0.f);
+            tb[rr][k] = ok ? Tt[(int64_t)sp2[k] * F.nv0 + r] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        const float2 sv = ss[e];
+        for (int rr = g; rr < RB && r0 + rr < F.nv0; rr += 4) {
+            const int64_t o = (int64_t)(r0 + rr) * K + col;
+            const float2 av = cmul(sv, ta[rr][e]), bv = tb[rr][e];
+            const __half hr = __float2half_rn(av.x), hi = __float2half_rn(av.y);
+            Are[o] = hr;
+            Aim[o] = hi;
+            if (SPLIT) {
+                Alr[o] = __float2half_rn(av.x - __half2float(hr));
+                Ali[o] = __float2half_rn(av.y - __half2float(hi));
+            }
+            Bre[o] = __float2half_rn(bv.x);
+            Bim[o] = __float2half_rn(bv.y);
         }
     }
 }

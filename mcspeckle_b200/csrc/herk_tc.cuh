@@ -568,7 +568,7 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
                     } else {
                         const int n = col0 + c0 + jb + t;
                         if (row_ok && n < N) {
-                            double *u = pe.U + 2 * ((int64_t)r1 * pe.nv0 + n);
+                            double *u = pe.U + 2 * ((int64_t)n * pe.nv0 + r1);
                             atomicAdd(u, (double)vr);
                             atomicAdd(u + 1, (double)vi);
                         }
@@ -859,6 +859,294 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
                 const int n_issued = max(mine, peer);
                 for (int kb = (n_issued > Cfg::STAGES ? n_issued - Cfg::STAGES : 0); kb < n_issued; ++kb)
                     (void)mbar_wait(&full[kb % Cfg::STAGES], (kb / Cfg::STAGES) & 1);
+            }
+        }
+    }
+    cluster_sync_all();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC2_TMEM_COLS) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The FourierQuad per-plane sums on a CTA pair from planar operands.
+//
+// For grids of at least 128 angles: A planes (Re, Im of s_e T[r1][p1_e]) and
+// B planes (Re, Im of T[r2][p2_e]), nv0 rows x K entries each, FP16 (plus the
+// low parts of A for hi+lo), one K column per entry, planes padded to blocks
+// of 64 entries.  A pair owns 256 rows r1 x 256 columns r2 (at nv0 = 256 the
+// whole output, so every operand byte is read once per launch) with Re F and
+// Im F in TMEM columns 0-255 and 256-511 of both CTAs (each CTA 128 rows):
+//     Re F += Re A Re B - Im A Im B,   Im F += Im A Re B + Re A Im B
+// (the minus is the MMA's negate-A bit), four M=256 N=256 K=16 MMAs per 16
+// entries, issued by the leader.  The planes of the pair's range are walked
+// from the deepest down in one Horner chain: after plane P's MMAs, when the
+// next plane is P - 1 (uniform planes), the epilogue warps of both CTAs
+// multiply their rows in place by r = exp(zexp0 z_bin) (FP32) and the next
+// plane's MMAs add on top; otherwise (an empty plane, the last non-uniform
+// plane, the range's end, or kFqSegMax steps) they add exp(zexp0 tz_P) times
+// the chain into the FP64 output (factor: phase product and reduction in
+// FP64, sincos and exp in FP32) and the next MMA starts afresh.  Each
+// epilogue thread holds one row r1 with its Re and Im columns, so the complex
+// products need no shuffles.  The epilogues of both CTAs arrive on the
+// leader's acc_empty (count 2) before the next plane's MMAs.  Loads are plain
+// (no multicast), counted on the leader's full barrier; every wait is bounded.
+// ---------------------------------------------------------------------------
+struct PlaneEpi2 {
+    const double2 *zexp0;  // [r2][r1]
+    const float2 *r1step;  // [r2][r1]: exp(zexp0 * z_bin), planes P and P - 1
+    const double *gz;      // plane boundaries
+    const int *planes;     // plane of each plane slot
+    double *U;             // [r2][r1] complex FP64, this light (a warp's rows are consecutive)
+    int nv0;
+    int n_uniform;
+    const unsigned *max_bits;  // the group's operand scale (fq_scale_exponent)
+};
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster_addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ bool fq_chain1_continues(int p_hi, int p_lo, int seg_len, int n_uniform)
+{
+    return p_hi - p_lo == 1 && p_hi < n_uniform && seg_len < kFqSegMax;
+}
+
+template <bool SPLIT, int NSTAGES>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
+fq_pair_planes_kernel(const __grid_constant__ CUtensorMap tm_are, const __grid_constant__ CUtensorMap tm_aim,
+                      const __grid_constant__ CUtensorMap tm_are_lo, const __grid_constant__ CUtensorMap tm_aim_lo,
+                      const __grid_constant__ CUtensorMap tm_bre, const __grid_constant__ CUtensorMap tm_bim,
+                      const int2 *__restrict__ tiles, const int2 *__restrict__ kranges, const int2 *__restrict__ pranges,
+                      const __grid_constant__ PlaneEpi2 pe, int *__restrict__ err, int test_fault)
+{
+    using Cfg = Tc2Cfg<SPLIT, NSTAGES>;
+    constexpr int S = Cfg::STAGES;
+    extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + S * Cfg::STAGE_BYTES);
+    uint64_t *empty = full + S;
+    uint64_t *acc_full = empty + S;
+    uint64_t *acc_empty = acc_full + 1;  // the leader's counts both CTAs' epilogues
+    uint64_t *done = acc_empty + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+    int *issued = abort_flag + 1;
+    int *ep_fail = issued + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int2 tile = tiles[blockIdx.x >> 1];
+    const int arow0 = tile.x * 256 + (int)rank * 128;  // this CTA's A rows (r1)
+    const int col0 = tile.y * 256;                     // the pair's columns (r2)
+    const int brow0 = col0 + (int)rank * 128;          // this CTA's B rows
+    const int2 pr = pranges[blockIdx.y];               // the host makes every range non-empty
+    const int last = pr.x + pr.y - 1;
+    const unsigned long long wait_ns = test_fault ? TC_TEST_WAIT_NS : TC_WAIT_NS;
+    const int N = pe.nv0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, 2);
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        *issued = 0;
+        *ep_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TC2_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    cluster_sync_all();  // both CTAs' barriers exist before any load, commit or remote arrive
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer (both CTAs): K blocks of every plane, deepest first,
+        // completion counted on the leader's full[s]
+        const uint32_t full0 = mapa_shared(smem_u32(&full[0]), 0);
+        int kb = 0;
+        bool stop = test_fault != 0;  // fault test: no copy is ever issued
+        for (int i = 0; i < pr.y && !stop; ++i) {
+            const int2 kr = kranges[last - i];
+            for (int j = 0; j < kr.y; ++j, ++kb) {
+                const int s = kb % S;
+                if (kb >= S && !mbar_wait(&empty[s], ((kb / S) - 1) & 1)) {
+                    atomicExch(abort_flag, 1);
+                    stop = true;
+                    break;
+                }
+                if (*(volatile int *)abort_flag) {
+                    stop = true;
+                    break;
+                }
+                uint8_t *st = base + s * Cfg::STAGE_BYTES;
+                if (rank == 0) mbar_expect_tx(&full[s], 2 * Cfg::STAGE_BYTES);
+                const uint32_t fb = full0 + (uint32_t)(s * sizeof(uint64_t));
+                const int kx = (kr.x + j) * TC_BK;
+                tma_load_2d_pair(st, &tm_are, kx, arow0, fb);
+                tma_load_2d_pair(st + Cfg::TILE, &tm_aim, kx, arow0, fb);
+                if (SPLIT) {
+                    tma_load_2d_pair(st + 2 * Cfg::TILE, &tm_are_lo, kx, arow0, fb);
+                    tma_load_2d_pair(st + 3 * Cfg::TILE, &tm_aim_lo, kx, arow0, fb);
+                }
+                tma_load_2d_pair(st + Cfg::B_OFF, &tm_bre, kx, brow0, fb);
+                tma_load_2d_pair(st + Cfg::B_OFF + Cfg::TILE, &tm_bim, kx, brow0, fb);
+                *(volatile int *)issued = kb + 1;
+            }
+        }
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // MMA issuer (leader only): plane slot i of the walk into the chain
+        constexpr uint32_t idesc = umma_idesc_f16(256, 256);
+        constexpr uint32_t idesc_neg = idesc | (1u << 13);  // negate A
+        const uint32_t t_re = tmem, t_im = tmem + 256;
+        int kb = 0, prev = 0, seg = 0;
+        bool ok = true;
+        for (int i = 0; i < pr.y && ok; ++i) {
+            const int slot = last - i;
+            const int P = pe.planes[slot];
+            const bool start = i == 0 || !fq_chain1_continues(prev, P, seg, pe.n_uniform);
+            seg = start ? 1 : seg + 1;
+            prev = P;
+            if (i >= 1) {  // both CTAs' epilogues have released the chain
+                if (!mbar_wait(acc_empty, (i - 1) & 1, wait_ns)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+            }
+            const int nk = kranges[slot].y;
+            for (int j = 0; j < nk; ++j, ++kb) {
+                const int s = kb % S;
+                if (!mbar_wait(&full[s], (kb / S) & 1, wait_ns)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint8_t *st = base + s * Cfg::STAGE_BYTES;
+                const uint64_t ar = umma_desc_sw128(st), ai = umma_desc_sw128(st + Cfg::TILE);
+                const uint64_t br = umma_desc_sw128(st + Cfg::B_OFF), bi = umma_desc_sw128(st + Cfg::B_OFF + Cfg::TILE);
+#pragma unroll
+                for (int kk = 0; kk < TC_BK / 16; ++kk) {
+                    const uint64_t adv = (uint64_t)(kk * 32) >> 4;
+                    const uint32_t acc = (start && j == 0 && kk == 0) ? 0u : 1u;
+                    umma_f16_pair(t_re, ar + adv, br + adv, idesc, acc);
+                    umma_f16_pair(t_im, ai + adv, br + adv, idesc, acc);
+                    umma_f16_pair(t_re, ai + adv, bi + adv, idesc_neg, 1u);
+                    umma_f16_pair(t_im, ar + adv, bi + adv, idesc, 1u);
+                    if (SPLIT) {
+                        const uint64_t lr = umma_desc_sw128(st + 2 * Cfg::TILE) + adv;
+                        const uint64_t li = umma_desc_sw128(st + 3 * Cfg::TILE) + adv;
+                        umma_f16_pair(t_re, lr, br + adv, idesc, 1u);
+                        umma_f16_pair(t_im, li, br + adv, idesc, 1u);
+                        umma_f16_pair(t_re, li, bi + adv, idesc_neg, 1u);
+                        umma_f16_pair(t_im, lr, bi + adv, idesc, 1u);
+                    }
+                }
+                umma_commit_pair(&empty[s]);
+            }
+            if (ok) umma_commit_pair(acc_full);
+        }
+        if (!ok) atomicExch(abort_flag, 1);
+        umma_commit_pair(done);  // both CTAs' done once every issued MMA has completed
+    } else if (warp >= 4) {
+        // epilogue (both CTAs): TMEM lane = row r1 = arow0 + 32 q + lane,
+        // columns c: Re F (c), Im F (256 + c) of column r2 = col0 + c
+        const int q = warp - 4;
+        const int r1 = arow0 + q * 32 + lane;
+        const bool row_ok = r1 < N;
+        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+        const uint32_t empty0 = mapa_shared(smem_u32(acc_empty), 0);
+        const float unscale = ldexpf(1.f, -fq_scale_exponent(pe.max_bits));
+        int prev = 0, seg = 0;
+        for (int i = 0; i < pr.y; ++i) {
+            const int slot = last - i;
+            const int P = pe.planes[slot];
+            const bool start = i == 0 || !fq_chain1_continues(prev, P, seg, pe.n_uniform);
+            seg = start ? 1 : seg + 1;
+            prev = P;
+            const bool cont = i + 1 < pr.y && fq_chain1_continues(P, pe.planes[slot - 1], seg, pe.n_uniform);
+            if (!__all_sync(0xffffffffu, mbar_wait(acc_full, i & 1, wait_ns)) && lane == 0) atomicExch(ep_fail, 1);
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (*(volatile int *)ep_fail) {
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            tc_fence_after();
+            const double tz = (pe.gz[P] + pe.gz[P + 1]) / 2;
+            for (int c0 = 0; c0 < 256; c0 += 32) {
+                uint32_t re[32], im[32];
+                tmem_ld32(trow + c0, re);
+                tmem_ld32(trow + 256 + c0, im);
+#pragma unroll
+                for (int t = 0; t < 32; ++t) {
+                    const int n = col0 + c0 + t;
+                    const bool ok = row_ok && n < N;
+                    float fx, fy;
+                    if (cont) {
+                        const float2 f = ok ? pe.r1step[(int64_t)n * pe.nv0 + r1] : make_float2(0.f, 0.f);
+                        fx = f.x;
+                        fy = f.y;
+                    } else {
+                        const double2 z = ok ? pe.zexp0[(int64_t)n * pe.nv0 + r1] : make_double2(0.0, 0.0);
+                        float sn, cs;
+                        __sincosf((float)reduce_2pi(z.y * tz), &sn, &cs);
+                        const float mag = ok ? expf((float)(z.x * tz)) * unscale : 0.f;
+                        fx = mag * cs;
+                        fy = mag * sn;
+                    }
+                    const float a = __uint_as_float(re[t]), b = __uint_as_float(im[t]);
+                    const float vr = fx * a - fy * b, vi = fx * b + fy * a;
+                    if (cont) {
+                        re[t] = __float_as_uint(vr);
+                        im[t] = __float_as_uint(vi);
+                    } else if (ok) {
+                        double *u = pe.U + 2 * ((int64_t)r1 * pe.nv0 + n);
+                        atomicAdd(u, (double)vr);
+                        atomicAdd(u + 1, (double)vi);
+                    }
+                }
+                if (cont) {
+                    tmem_st32(trow + c0, re);
+                    tmem_st32(trow + 256 + c0, im);
+                }
+            }
+            if (cont) asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            tc_fence_before();
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (q == 0 && lane == 0) mbar_arrive_cluster(empty0);
+        }
+    }
+    __syncwarp();
+
+    const bool ok = mbar_wait(done, 0);
+    tc_fence_after();
+    __syncthreads();
+    const bool failed = !ok || *(volatile int *)abort_flag;
+    tc_fence_before();
+    cluster_sync_all();
+    if (threadIdx.x == 0) {
+        // after a failure anywhere in the pair the leader waits (bounded) for
+        // the pair's copies still in flight, which are counted on its barriers
+        const int peer_abort = (int)ld_shared_cluster_u32(mapa_shared(smem_u32(abort_flag), rank ^ 1u));
+        if (failed || peer_abort) {
+            atomicExch(err, 1);
+            if (rank == 0) {
+                const int mine = *(volatile int *)issued;
+                const int peer = (int)ld_shared_cluster_u32(mapa_shared(smem_u32(issued), 1));
+                const int n_issued = max(mine, peer);
+                for (int kb = (n_issued > S ? n_issued - S : 0); kb < n_issued; ++kb)
+                    (void)mbar_wait(&full[kb % S], (kb / S) & 1);
             }
         }
     }
@@ -1267,6 +1555,27 @@ inline void tc_gemm_plane_loop_launch(const CUtensorMap &m_ahi, const CUtensorMa
     }
     fq_planes_tc_kernel<SPLIT><<<dim3((unsigned)n_tiles, (unsigned)n_ranges), 256, TcCfg<SPLIT>::SMEM_BYTES, st>>>(
         m_ahi, m_alo, m_b, tiles, kranges, pranges, Mr, N, pe, err, tc_test_fault().load());
+}
+
+// The pair plane loop: grid (2 x tiles, plane ranges), clusters of 2.
+template <bool SPLIT>
+inline void fq_pair_planes_launch(const CUtensorMap *maps, const int2 *tiles, int n_tiles, const int2 *kranges,
+                                  const int2 *pranges, int n_ranges, const PlaneEpi2 &pe, int *err, cudaStream_t st)
+{
+    constexpr int NS = SPLIT ? 2 : 3;
+    using Cfg = Tc2Cfg<SPLIT, NS>;
+    static std::atomic<uint64_t> attr_set{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) throw std::runtime_error("cudaGetDevice failed");
+    if (dev >= 64 || !((attr_set.load() >> dev) & 1)) {
+        if (cudaFuncSetAttribute(fq_pair_planes_kernel<SPLIT, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg::SMEM_BYTES) != cudaSuccess)
+            throw std::runtime_error("cannot reserve shared memory for the FourierQuad pair kernel");
+        if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
+    }
+    fq_pair_planes_kernel<SPLIT, NS><<<dim3(2u * (unsigned)n_tiles, (unsigned)n_ranges), 256, Cfg::SMEM_BYTES, st>>>(
+        maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], tiles, kranges, pranges, pe, err,
+        tc_test_fault().load());
 }
 
 // D[ks][2N][N] += the planar pair product (Re C in even rows, Im C in odd

@@ -1595,7 +1595,7 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
                 CK(cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
                 fq_scale_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((G.nblk * 32 + 255) / 256,
                                                                                    (int64_t)sm_count(c.device) * 8)),
-                                  256, 0, st>>>(F, Es, d_blk + G.blk0, G.nblk, j, d_max);
+                                  256, 0, st>>>(F, Es, d_blk + G.blk0, G.nblk, 32, j, d_max);
                 CK(cudaGetLastError());
                 LAUNCHED();
                 if (split)
@@ -1616,6 +1616,137 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
                 else
                     tc_gemm_plane_loop_launch<false>(m_ahi, m_alo, m_b, d_tiles, (int)tiles.size(), d_kr + G.kr0,
                                                      d_pr + G.pr0, G.n_pr, Mr, nv0, pe, d_err, st);
+                CK(cudaGetLastError());
+                LAUNCHED();
+            }
+            prof_count(0, 0, 8.0 * (double)nv0 * nv0 * (double)G.entries);
+        }
+    }
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));  // the operand memory and metadata are reused by the next batch
+    if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
+}
+
+// The same on CTA pairs from planar operands (grids of at least 128 angles):
+// 64-entry blocks, one K column per entry, a pair per 256 x 256 output tile,
+// one Horner chain per pair (fq_pair_planes_kernel).  r1step: exp(zexp0 z_bin).
+void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
+                      const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt,
+                      const double2 *dz, const float2 *r1step, int n_uniform, double *U, bool split,
+                      int64_t group_entries, cudaStream_t st)
+{
+    const int nv0 = F.nv0;
+    std::vector<int2> tiles;
+    const int nt = (nv0 + 255) / 256;
+    for (int tn = 0; tn < nt; ++tn)
+        for (int tm = 0; tm < nt; ++tm) tiles.push_back(make_int2(tm, tn));
+    struct Group {
+        int64_t nblk, blk0, kr0, pl0, pr0;
+        int n_pl, n_pr;
+        int64_t entries;
+    };
+    std::vector<Group> groups;
+    std::vector<int2> blk, kr, prs;
+    std::vector<int> gpl;
+    int64_t max_nblk = 0;
+    constexpr int64_t kPlaneCost = 1;
+    const int want_max = std::max(1, (sm_count(c.device) / 2) / std::max(1, (int)tiles.size()));
+    for (size_t g0 = 0; g0 < hplanes.size();) {
+        Group G{0, (int64_t)blk.size(), (int64_t)kr.size(), (int64_t)gpl.size(), (int64_t)prs.size(), 0, 0, 0};
+        size_t g1 = g0;
+        while (g1 < hplanes.size() && G.n_pl < kFqTcPlanes) {
+            const int p = hplanes[g1];
+            const int cnt = hcounts[p];
+            const int nb = (cnt + 63) / 64;
+            if (G.n_pl > 0 && (G.nblk + nb) * 64 > group_entries) break;
+            kr.push_back(make_int2((int)G.nblk, nb));
+            for (int b = 0; b < nb; ++b) blk.push_back(make_int2(hoff[p] + 64 * b, std::min(64, cnt - 64 * b)));
+            gpl.push_back(p);
+            G.nblk += nb;
+            G.entries += cnt;
+            ++G.n_pl;
+            ++g1;
+        }
+        const int want = std::min(G.n_pl, want_max);
+        const int64_t per = (G.nblk + kPlaneCost * G.n_pl + want - 1) / want;
+        int first = 0;
+        int64_t acc = 0;
+        for (int i = 0; i < G.n_pl; ++i) {
+            acc += kr[G.kr0 + i].y + kPlaneCost;
+            if (acc >= per || i + 1 == G.n_pl) {
+                prs.push_back(make_int2(first, i - first + 1));
+                first = i + 1;
+                acc = 0;
+            }
+        }
+        G.n_pr = (int)(prs.size() - G.pr0);
+        max_nblk = std::max(max_nblk, G.nblk);
+        groups.push_back(G);
+        g0 = g1;
+    }
+    if (groups.empty()) return;
+    const int64_t Kmax = 64 * max_nblk;
+    const size_t pb = tc_align((size_t)nv0 * Kmax * sizeof(__half));  // one plane of rows
+    const int n_planes = split ? 6 : 4;                                // Re A, Im A, [Re lo, Im lo], Re B, Im B
+    const size_t o_tiles = 0, o_blk = o_tiles + tc_align(tiles.size() * sizeof(int2));
+    const size_t o_kr = o_blk + tc_align(blk.size() * sizeof(int2));
+    const size_t o_pl = o_kr + tc_align(kr.size() * sizeof(int2));
+    const size_t o_pr = o_pl + tc_align(gpl.size() * sizeof(int));
+    const size_t o_err = o_pr + tc_align(prs.size() * sizeof(int2));
+    const size_t o_max = o_err + 256;
+    const size_t meta = o_err + 1024;
+    char *mem = reinterpret_cast<char *>(c.tc_a.ensure(n_planes * pb + meta));
+    __half *are = reinterpret_cast<__half *>(mem), *aim = reinterpret_cast<__half *>(mem + pb);
+    __half *alr = split ? reinterpret_cast<__half *>(mem + 2 * pb) : are;
+    __half *ali = split ? reinterpret_cast<__half *>(mem + 3 * pb) : aim;
+    __half *bre = reinterpret_cast<__half *>(mem + (split ? 4 : 2) * pb);
+    __half *bim = reinterpret_cast<__half *>(mem + (split ? 5 : 3) * pb);
+    char *dmeta = mem + n_planes * pb;
+    std::vector<char> hmeta(o_err, 0);
+    std::memcpy(hmeta.data() + o_tiles, tiles.data(), tiles.size() * sizeof(int2));
+    std::memcpy(hmeta.data() + o_blk, blk.data(), blk.size() * sizeof(int2));
+    std::memcpy(hmeta.data() + o_kr, kr.data(), kr.size() * sizeof(int2));
+    std::memcpy(hmeta.data() + o_pl, gpl.data(), gpl.size() * sizeof(int));
+    std::memcpy(hmeta.data() + o_pr, prs.data(), prs.size() * sizeof(int2));
+    CK(cudaMemcpyAsync(dmeta, hmeta.data(), o_err, cudaMemcpyHostToDevice, st));
+    int2 *d_tiles = reinterpret_cast<int2 *>(dmeta + o_tiles), *d_blk = reinterpret_cast<int2 *>(dmeta + o_blk);
+    int2 *d_kr = reinterpret_cast<int2 *>(dmeta + o_kr), *d_pr = reinterpret_cast<int2 *>(dmeta + o_pr);
+    int *d_pl = reinterpret_cast<int *>(dmeta + o_pl), *d_err = reinterpret_cast<int *>(dmeta + o_err);
+    unsigned *d_max = reinterpret_cast<unsigned *>(dmeta + o_max);
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    for (const Group &G : groups) {
+        const int64_t K = 64 * G.nblk;
+        CUtensorMap maps[6];
+        __half *planes[6] = {are, aim, alr, ali, bre, bim};
+        for (int k = 0; k < 6; ++k) maps[k] = tc_map(planes[k], (uint64_t)K, (uint64_t)nv0, (uint64_t)K * 2, 128);
+        for (int j = 0; j < nl_out; ++j) {
+            {
+                StageScope sc(ST_ROWS, st);
+                CK(cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
+                fq_scale_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((G.nblk * 64 + 255) / 256,
+                                                                                   (int64_t)sm_count(c.device) * 8)),
+                                  256, 0, st>>>(F, Es, d_blk + G.blk0, G.nblk, 64, j, d_max);
+                CK(cudaGetLastError());
+                LAUNCHED();
+                if (split)
+                    fq_tc_rows_planar_kernel<true><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K, are,
+                                                                                       aim, alr, ali, bre, bim, d_max);
+                else
+                    fq_tc_rows_planar_kernel<false><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K,
+                                                                                        are, aim, alr, ali, bre, bim, d_max);
+                CK(cudaGetLastError());
+                LAUNCHED();
+            }
+            {
+                StageScope sc(ST_CONTRACT, st);
+                const PlaneEpi2 pe{dz, r1step, F.gz, d_pl + G.pl0, U + 2 * (int64_t)nv0 * nv0 * j, nv0, n_uniform, d_max};
+                if (split)
+                    fq_pair_planes_launch<true>(maps, d_tiles, (int)tiles.size(), d_kr + G.kr0, d_pr + G.pr0, G.n_pr, pe,
+                                                d_err, st);
+                else
+                    fq_pair_planes_launch<false>(maps, d_tiles, (int)tiles.size(), d_kr + G.kr0, d_pr + G.pr0, G.n_pr,
+                                                 pe, d_err, st);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
@@ -1706,6 +1837,11 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
         const double m = std::exp(zexp0[q].x * 2 * z_bin), ph = zexp0[q].y * 2 * z_bin;
         rrh[q] = make_float2((float)(m * std::cos(ph)), (float)(m * std::sin(ph)));
     }
+    std::vector<float2> r1h(Nv * Nv);  // the pair form's ratio between planes P and P - 1
+    for (int64_t q = 0; q < Nv * Nv; ++q) {
+        const double m = std::exp(zexp0[q].x * z_bin), ph = zexp0[q].y * z_bin;
+        r1h[q] = make_float2((float)(m * std::cos(ph)), (float)(m * std::sin(ph)));
+    }
     const int n_uniform = (int)(ng - 1);
     const double l_end = a->l[3 * (a->nl - 1) + 2];
 
@@ -1760,8 +1896,11 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
                         Nv >= 64;
     // the tensor-core rows read the twiddles transposed, [p][r]
     float2 *Tt = use_tc ? reinterpret_cast<float2 *>(c.fq_twt.ensure(Nv * Nx * sizeof(float2))) : nullptr;
+    // at least 128 angles per axis: the CTA-pair form on planar operands
+    const bool use_pair = use_tc && Nv >= 128;
     float2 *drr = use_tc ? reinterpret_cast<float2 *>(c.fq_rr.ensure(Nv * Nv * sizeof(float2))) : nullptr;
-    if (use_tc) CK(cudaMemcpyAsync(drr, rrh.data(), Nv * Nv * sizeof(float2), cudaMemcpyHostToDevice, st));
+    if (use_tc)
+        CK(cudaMemcpyAsync(drr, use_pair ? r1h.data() : rrh.data(), Nv * Nv * sizeof(float2), cudaMemcpyHostToDevice, st));
     {
         StageScope sc(ST_ROWS, st);
         const int tg = (int)std::max<int64_t>(1, std::min<int64_t>((Nv * Nx + 255) / 256, 4096));
@@ -1856,8 +1995,12 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
             LAUNCHED();
         }
         if (use_tc) {
-            fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
-                        reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
+            if (use_pair)
+                fq_tc_batch_pair(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
+                                 reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
+            else
+                fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
+                            reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
         } else {
             const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
             for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
@@ -1876,9 +2019,9 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     const double norm = total_vert > 0 ? std::sqrt(1.0 / (double)total_vert * V * sigt) : 0.0;  // lines 214, 302-303
     StageScope fin(ST_FINAL, st);
     const int fgrid = (int)std::max<int64_t>(1, std::min<int64_t>((nout + 255) / 256, 4096));
-    if (use_tc)  // FP64 accumulator stored [light][r1][r2]
+    if (use_tc)  // FP64 accumulator stored [light][r1][r2] ([light][r2][r1] by the pair form)
         fq_finalize_kernel<double><<<fgrid, 256, 0, st>>>(reinterpret_cast<const double *>(U), db, (int)Nv, (int)nl_out,
-                                                          norm, d_u, 1);
+                                                          norm, d_u, use_pair ? 0 : 1);
     else
         fq_finalize_kernel<AccT><<<fgrid, 256, 0, st>>>(U, db, (int)Nv, (int)nl_out, norm, d_u, 0);
     CK(cudaGetLastError());
