@@ -383,24 +383,32 @@ fq_tc_rows_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict_
     }
 }
 
-// Planar rows for the CTA-pair form (grids of at least 128 angles): per
-// block of 64 entries (a plane's last block zero-padded), K column = entry,
-// A planes Re / Im of s_e(j) T[r1][p1_e] (with the low parts for hi+lo) and B
-// planes Re / Im of T[r2][p2_e], rows r = 0 .. nv0-1, row stride K halves.
-// Thread = (entry e, row group g): a warp's stores of one row are 32
-// consecutive halves of each plane.
+__device__ __forceinline__ uint32_t h2_bits(__half2 h)
+{
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// Planar rows for the CTA-pair form (grids of at least 128 angles): one block
+// of 64 entries per CTA (a plane's last block zero-padded), written as the
+// contiguous slab [row][64 entries] of each plane at blockIdx.x * nv0 * 64:
+// A planes Re / Im of s_e(j) T[r1][p1_e] (with the low parts for hi+lo), B
+// planes Re / Im of T[r2][p2_e].  Thread = (rows r = r0, r0 + 32, ..., 8
+// consecutive entries): one 16-byte store per plane and row, a warp's stores
+// 512 contiguous bytes.  T[r][p] is linear in r in its phase
+// (fq_twiddle_kernel: T[r + 1][p] = T[r][p] exp(2 pi i P / M)), so each
+// thread reads the twiddles of its first two rows only and steps the rest
+// with the ratio T[r0 + 32][p] conj(T[r0][p]) in FP32 (at most nv0 / 32 - 1
+// steps, far below FP16's rounding).
 template <bool SPLIT>
 __global__ void __launch_bounds__(256)
 fq_tc_rows_planar_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E,
-                         const int2 *__restrict__ blk, int light, const float2 *__restrict__ Tt, int64_t K,
+                         const int2 *__restrict__ blk, int light, const float2 *__restrict__ Tt,
                          __half *__restrict__ Are, __half *__restrict__ Aim, __half *__restrict__ Alr,
                          __half *__restrict__ Ali, __half *__restrict__ Bre, __half *__restrict__ Bim,
                          const unsigned *__restrict__ max_bits)
 {
-    constexpr int RB = 32;  // twiddle rows staged per pass
     __shared__ float2 ss[64];
     __shared__ int sp1[64], sp2[64];
-    __shared__ float2 ta[RB][65], tb[RB][65];  // [r - r0][entry]
     const float scale = ldexpf(1.f, fq_scale_exponent(max_bits));
     const int2 bk = blk[blockIdx.x];  // (first entry, entries in this block)
     if (threadIdx.x < 64) {
@@ -418,31 +426,49 @@ fq_tc_rows_planar_kernel(const __grid_constant__ FqParams F, const FqEntry *__re
         sp1[threadIdx.x] = p1;
         sp2[threadIdx.x] = p2;
     }
-    const int e = threadIdx.x & 63, g = threadIdx.x >> 6;
-    const int64_t col = (int64_t)blockIdx.x * 64 + e;
-    for (int r0 = 0; r0 < F.nv0; r0 += RB) {
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < 64 * RB; idx += blockDim.x) {
-            const int k = idx / RB, rr = idx % RB, r = r0 + rr;
-            const bool ok = k < bk.y && r < F.nv0;
-            ta[rr][k] = ok ? Tt[(int64_t)sp1[k] * F.nv0 + r] : make_float2(0.f, 0.f);
-            tb[rr][k] = ok ? Tt[(int64_t)sp2[k] * F.nv0 + r] : make_float2(0.f, 0.f);
-        }
-        __syncthreads();
-        const float2 sv = ss[e];
-        for (int rr = g; rr < RB && r0 + rr < F.nv0; rr += 4) {
-            const int64_t o = (int64_t)(r0 + rr) * K + col;
-            const float2 av = cmul(sv, ta[rr][e]), bv = tb[rr][e];
-            const __half hr = __float2half_rn(av.x), hi = __float2half_rn(av.y);
-            Are[o] = hr;
-            Aim[o] = hi;
+    __syncthreads();
+    const int e0 = (threadIdx.x & 7) * 8, rsub = threadIdx.x >> 3;
+    float2 av[8], aw[8], bv[8], bw[8];  // current A, B values of the 8 entries and their 32-row ratios
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int64_t o1 = (int64_t)sp1[e0 + j] * F.nv0 + rsub, o2 = (int64_t)sp2[e0 + j] * F.nv0 + rsub;
+        const float2 t1 = Tt[o1], t2 = Tt[o2], u1 = Tt[o1 + 32], u2 = Tt[o2 + 32];  // nv0 >= 128
+        av[j] = cmul(ss[e0 + j], t1);  // zero past the block's entries
+        bv[j] = t2;
+        aw[j] = cmul(u1, make_float2(t1.x, -t1.y));
+        bw[j] = cmul(u2, make_float2(t2.x, -t2.y));
+    }
+    const int64_t slab = (int64_t)blockIdx.x * F.nv0 * 64;
+    for (int r = rsub; r < F.nv0; r += 32) {
+        uint4 are, aim, alr, ali, bre, bim;
+        uint32_t *pre = &are.x, *pim = &aim.x, *plr = &alr.x, *pli = &ali.x, *pbr = &bre.x, *pbi = &bim.x;
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const float2 a0 = av[2 * jj], a1 = av[2 * jj + 1], b0 = bv[2 * jj], b1 = bv[2 * jj + 1];
+            const __half2 hr = __floats2half2_rn(a0.x, a1.x), hi = __floats2half2_rn(a0.y, a1.y);
+            pre[jj] = h2_bits(hr);
+            pim[jj] = h2_bits(hi);
             if (SPLIT) {
-                Alr[o] = __float2half_rn(av.x - __half2float(hr));
-                Ali[o] = __float2half_rn(av.y - __half2float(hi));
+                plr[jj] = h2_bits(__floats2half2_rn(a0.x - __low2float(hr), a1.x - __high2float(hr)));
+                pli[jj] = h2_bits(__floats2half2_rn(a0.y - __low2float(hi), a1.y - __high2float(hi)));
             }
-            Bre[o] = __float2half_rn(bv.x);
-            Bim[o] = __float2half_rn(bv.y);
+            pbr[jj] = h2_bits(__floats2half2_rn(b0.x, b1.x));
+            pbi[jj] = h2_bits(__floats2half2_rn(b0.y, b1.y));
         }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            av[j] = cmul(av[j], aw[j]);
+            bv[j] = cmul(bv[j], bw[j]);
+        }
+        const int64_t o = slab + (int64_t)r * 64 + e0;
+        *reinterpret_cast<uint4 *>(Are + o) = are;
+        *reinterpret_cast<uint4 *>(Aim + o) = aim;
+        if (SPLIT) {
+            *reinterpret_cast<uint4 *>(Alr + o) = alr;
+            *reinterpret_cast<uint4 *>(Ali + o) = ali;
+        }
+        *reinterpret_cast<uint4 *>(Bre + o) = bre;
+        *reinterpret_cast<uint4 *>(Bim + o) = bim;
     }
 }
 

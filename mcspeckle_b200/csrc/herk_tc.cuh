@@ -334,6 +334,29 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32
         : "memory");
 }
 
+// 16 columns of this warp's 32 TMEM lanes, without waiting (tmem_wait_ld).
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // The FourierQuad per-plane sums with the plane loop inside the CTA.
 //
@@ -568,7 +591,7 @@ fq_planes_tc_kernel(const __grid_constant__ CUtensorMap tm_ahi, const __grid_con
                     } else {
                         const int n = col0 + c0 + jb + t;
                         if (row_ok && n < N) {
-                            double *u = pe.U + 2 * ((int64_t)n * pe.nv0 + r1);
+                            double *u = pe.U + 2 * ((int64_t)r1 * pe.nv0 + n);
                             atomicAdd(u, (double)vr);
                             atomicAdd(u + 1, (double)vi);
                         }
@@ -672,6 +695,17 @@ __device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *m
         "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
         "%3}], [%4];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar_cluster)
+        : "memory");
+}
+
+// The same for a 3-D map (K-block-major operands: x = entry in the block, y = row, z = block).
+__device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                                 uint32_t bar_cluster)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+        "%3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar_cluster)
         : "memory");
 }
 
@@ -873,9 +907,10 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
 // The FourierQuad per-plane sums on a CTA pair from planar operands.
 //
 // For grids of at least 128 angles: A planes (Re, Im of s_e T[r1][p1_e]) and
-// B planes (Re, Im of T[r2][p2_e]), nv0 rows x K entries each, FP16 (plus the
-// low parts of A for hi+lo), one K column per entry, planes padded to blocks
-// of 64 entries.  A pair owns 256 rows r1 x 256 columns r2 (at nv0 = 256 the
+// B planes (Re, Im of T[r2][p2_e]), FP16 (plus the low parts of A for hi+lo),
+// K-block-major: per block of 64 entries (a plane's last block zero-padded) a
+// contiguous nv0 x 64 slab, so a tile load is one contiguous 16 KB read.  A
+// pair owns 256 rows r1 x 256 columns r2 (at nv0 = 256 the
 // whole output, so every operand byte is read once per launch) with Re F and
 // Im F in TMEM columns 0-255 and 256-511 of both CTAs (each CTA 128 rows):
 //     Re F += Re A Re B - Im A Im B,   Im F += Im A Re B + Re A Im B
@@ -889,8 +924,11 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
 // the chain into the FP64 output (factor: phase product and reduction in
 // FP64, sincos and exp in FP32) and the next MMA starts afresh.  Each
 // epilogue thread holds one row r1 with its Re and Im columns, so the complex
-// products need no shuffles.  The epilogues of both CTAs arrive on the
-// leader's acc_empty (count 2) before the next plane's MMAs.  Loads are plain
+// products need no shuffles; 8 warps per CTA (two per TMEM lane quarter, half
+// the columns each) keep the per-plane step short, since the MMAs wait for
+// it.  The epilogues of both CTAs arrive on the leader's acc_empty (count 2)
+// before the next plane's MMAs.  Warp 0 lane 0 issues the loads, warp 1 lane
+// 0 the MMAs (leader), warps 2-3 only wait.  Loads are plain
 // (no multicast), counted on the leader's full barrier; every wait is bounded.
 // ---------------------------------------------------------------------------
 struct PlaneEpi2 {
@@ -915,7 +953,7 @@ __device__ __forceinline__ bool fq_chain1_continues(int p_hi, int p_lo, int seg_
 }
 
 template <bool SPLIT, int NSTAGES>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(256, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(384, 1)
 fq_pair_planes_kernel(const __grid_constant__ CUtensorMap tm_are, const __grid_constant__ CUtensorMap tm_aim,
                       const __grid_constant__ CUtensorMap tm_are_lo, const __grid_constant__ CUtensorMap tm_aim_lo,
                       const __grid_constant__ CUtensorMap tm_bre, const __grid_constant__ CUtensorMap tm_bim,
@@ -993,15 +1031,15 @@ fq_pair_planes_kernel(const __grid_constant__ CUtensorMap tm_are, const __grid_c
                 uint8_t *st = base + s * Cfg::STAGE_BYTES;
                 if (rank == 0) mbar_expect_tx(&full[s], 2 * Cfg::STAGE_BYTES);
                 const uint32_t fb = full0 + (uint32_t)(s * sizeof(uint64_t));
-                const int kx = (kr.x + j) * TC_BK;
-                tma_load_2d_pair(st, &tm_are, kx, arow0, fb);
-                tma_load_2d_pair(st + Cfg::TILE, &tm_aim, kx, arow0, fb);
+                const int kz = kr.x + j;  // the K block (64 entries, one contiguous nv0 x 64 slab per plane)
+                tma_load_3d_pair(st, &tm_are, 0, arow0, kz, fb);
+                tma_load_3d_pair(st + Cfg::TILE, &tm_aim, 0, arow0, kz, fb);
                 if (SPLIT) {
-                    tma_load_2d_pair(st + 2 * Cfg::TILE, &tm_are_lo, kx, arow0, fb);
-                    tma_load_2d_pair(st + 3 * Cfg::TILE, &tm_aim_lo, kx, arow0, fb);
+                    tma_load_3d_pair(st + 2 * Cfg::TILE, &tm_are_lo, 0, arow0, kz, fb);
+                    tma_load_3d_pair(st + 3 * Cfg::TILE, &tm_aim_lo, 0, arow0, kz, fb);
                 }
-                tma_load_2d_pair(st + Cfg::B_OFF, &tm_bre, kx, brow0, fb);
-                tma_load_2d_pair(st + Cfg::B_OFF + Cfg::TILE, &tm_bim, kx, brow0, fb);
+                tma_load_3d_pair(st + Cfg::B_OFF, &tm_bre, 0, brow0, kz, fb);
+                tma_load_3d_pair(st + Cfg::B_OFF + Cfg::TILE, &tm_bim, 0, brow0, kz, fb);
                 *(volatile int *)issued = kb + 1;
             }
         }
@@ -1060,14 +1098,21 @@ fq_pair_planes_kernel(const __grid_constant__ CUtensorMap tm_are, const __grid_c
         if (!ok) atomicExch(abort_flag, 1);
         umma_commit_pair(done);  // both CTAs' done once every issued MMA has completed
     } else if (warp >= 4) {
-        // epilogue (both CTAs): TMEM lane = row r1 = arow0 + 32 q + lane,
-        // columns c: Re F (c), Im F (256 + c) of column r2 = col0 + c
-        const int q = warp - 4;
+        // epilogue (both CTAs, 8 warps): TMEM lane = row r1 = arow0 + 32 q +
+        // lane (q = warp mod 4, the warp's lane quarter); warps 4-7 take
+        // columns 0-127, warps 8-11 columns 128-255 (Re F in TMEM column c,
+        // Im F in 256 + c).  The ratio table is read in chunks of 16 columns,
+        // the next chunk's loads issued before this chunk's arithmetic, every
+        // address valid (clamped to the grid) so the loads need no branches.
+        const int q = warp & 3;
+        const int cb = ((warp - 4) >> 2) * 128;
         const int r1 = arow0 + q * 32 + lane;
         const bool row_ok = r1 < N;
+        const int64_t r1c = row_ok ? r1 : N - 1;
         const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
         const uint32_t empty0 = mapa_shared(smem_u32(acc_empty), 0);
         const float unscale = ldexpf(1.f, -fq_scale_exponent(pe.max_bits));
+        auto col_idx = [&](int c) -> int64_t { return (int64_t)min(col0 + cb + c, N - 1) * pe.nv0 + r1c; };
         int prev = 0, seg = 0;
         for (int i = 0; i < pr.y; ++i) {
             const int slot = last - i;
@@ -1077,54 +1122,74 @@ fq_pair_planes_kernel(const __grid_constant__ CUtensorMap tm_are, const __grid_c
             prev = P;
             const bool cont = i + 1 < pr.y && fq_chain1_continues(P, pe.planes[slot - 1], seg, pe.n_uniform);
             if (!__all_sync(0xffffffffu, mbar_wait(acc_full, i & 1, wait_ns)) && lane == 0) atomicExch(ep_fail, 1);
-            asm volatile("bar.sync 1, 128;" ::: "memory");
+            asm volatile("bar.sync 1, 256;" ::: "memory");
             if (*(volatile int *)ep_fail) {
                 atomicExch(abort_flag, 1);
                 break;
             }
             tc_fence_after();
-            const double tz = (pe.gz[P] + pe.gz[P + 1]) / 2;
-            for (int c0 = 0; c0 < 256; c0 += 32) {
-                uint32_t re[32], im[32];
-                tmem_ld32(trow + c0, re);
-                tmem_ld32(trow + 256 + c0, im);
+            if (cont) {
+                // the chain continues: F <- r F in place (FP32)
+                float2 f[16];
 #pragma unroll
-                for (int t = 0; t < 32; ++t) {
-                    const int n = col0 + c0 + t;
-                    const bool ok = row_ok && n < N;
-                    float fx, fy;
-                    if (cont) {
-                        const float2 f = ok ? pe.r1step[(int64_t)n * pe.nv0 + r1] : make_float2(0.f, 0.f);
-                        fx = f.x;
-                        fy = f.y;
-                    } else {
-                        const double2 z = ok ? pe.zexp0[(int64_t)n * pe.nv0 + r1] : make_double2(0.0, 0.0);
-                        float sn, cs;
-                        __sincosf((float)reduce_2pi(z.y * tz), &sn, &cs);
-                        const float mag = ok ? expf((float)(z.x * tz)) * unscale : 0.f;
-                        fx = mag * cs;
-                        fy = mag * sn;
+                for (int t = 0; t < 16; ++t) f[t] = __ldg(&pe.r1step[col_idx(t)]);
+#pragma unroll
+                for (int c0 = 0; c0 < 128; c0 += 16) {
+                    float2 g[16];
+                    if (c0 + 16 < 128) {
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) g[t] = __ldg(&pe.r1step[col_idx(c0 + 16 + t)]);
                     }
-                    const float a = __uint_as_float(re[t]), b = __uint_as_float(im[t]);
-                    const float vr = fx * a - fy * b, vi = fx * b + fy * a;
-                    if (cont) {
-                        re[t] = __float_as_uint(vr);
-                        im[t] = __float_as_uint(vi);
-                    } else if (ok) {
-                        double *u = pe.U + 2 * ((int64_t)r1 * pe.nv0 + n);
-                        atomicAdd(u, (double)vr);
-                        atomicAdd(u + 1, (double)vi);
+                    uint32_t re[16], im[16];
+                    tmem_ld16_async(trow + cb + c0, re);
+                    tmem_ld16_async(trow + 256 + cb + c0, im);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) {
+                        const float a = __uint_as_float(re[t]), b = __uint_as_float(im[t]);
+                        re[t] = __float_as_uint(f[t].x * a - f[t].y * b);
+                        im[t] = __float_as_uint(f[t].x * b + f[t].y * a);
+                    }
+                    tmem_st16(trow + cb + c0, re);
+                    tmem_st16(trow + 256 + cb + c0, im);
+                    if (c0 + 16 < 128) {
+#pragma unroll
+                        for (int t = 0; t < 16; ++t) f[t] = g[t];
                     }
                 }
-                if (cont) {
-                    tmem_st32(trow + c0, re);
-                    tmem_st32(trow + 256 + c0, im);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            } else {
+                // the chain ends here: U += exp(zexp0 tz_P) F (factor in FP32
+                // from FP64 phase and reduction; sum in FP64)
+                const double tz = (pe.gz[P] + pe.gz[P + 1]) / 2;
+#pragma unroll 1
+                for (int c0 = 0; c0 < 128; c0 += 16) {
+                    double2 z[16];
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) z[t] = __ldg(&pe.zexp0[col_idx(c0 + t)]);
+                    uint32_t re[16], im[16];
+                    tmem_ld16_async(trow + cb + c0, re);
+                    tmem_ld16_async(trow + 256 + cb + c0, im);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) {
+                        const int n = col0 + cb + c0 + t;
+                        float sn, cs;
+                        __sincosf((float)reduce_2pi(z[t].y * tz), &sn, &cs);
+                        const float mag = expf((float)(z[t].x * tz)) * unscale;
+                        const float a = __uint_as_float(re[t]), b = __uint_as_float(im[t]);
+                        const float fx = mag * cs, fy = mag * sn;
+                        if (row_ok && n < N) {
+                            double *u = pe.U + 2 * ((int64_t)n * pe.nv0 + r1);
+                            atomicAdd(u, (double)(fx * a - fy * b));
+                            atomicAdd(u + 1, (double)(fx * b + fy * a));
+                        }
+                    }
                 }
             }
-            if (cont) asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
             tc_fence_before();
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            if (q == 0 && lane == 0) mbar_arrive_cluster(empty0);
+            asm volatile("bar.sync 1, 256;" ::: "memory");
+            if (q == 0 && cb == 0 && lane == 0) mbar_arrive_cluster(empty0);
         }
     }
     __syncwarp();
@@ -1459,6 +1524,21 @@ inline CUtensorMap tc_map(const void *base, uint64_t cols, uint64_t rows, uint64
     return m;
 }
 
+// A K-block-major operand plane: [nblk][rows][64] FP16, boxes of 64 x 128 x 1.
+inline CUtensorMap tc_map_kblocks(const void *base, uint64_t rows, uint64_t nblk)
+{
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)TC_BK, rows, nblk};
+    cuuint64_t strides[2] = {(cuuint64_t)TC_BK * 2, rows * TC_BK * 2};
+    cuuint32_t box[3] = {(cuuint32_t)TC_BK, 128, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = tc_encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<void *>(base), dims, strides, box,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed");
+    return m;
+}
+
 inline TcOperands tc_make_operands(const TcPlan &p, void *mem, cudaStream_t st)
 {
     TcOperands o{};
@@ -1573,7 +1653,7 @@ inline void fq_pair_planes_launch(const CUtensorMap *maps, const int2 *tiles, in
             throw std::runtime_error("cannot reserve shared memory for the FourierQuad pair kernel");
         if (dev < 64) attr_set.fetch_or((uint64_t)1 << dev);
     }
-    fq_pair_planes_kernel<SPLIT, NS><<<dim3(2u * (unsigned)n_tiles, (unsigned)n_ranges), 256, Cfg::SMEM_BYTES, st>>>(
+    fq_pair_planes_kernel<SPLIT, NS><<<dim3(2u * (unsigned)n_tiles, (unsigned)n_ranges), 384, Cfg::SMEM_BYTES, st>>>(
         maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], tiles, kranges, pranges, pe, err,
         tc_test_fault().load());
 }

@@ -141,12 +141,18 @@ __device__ __forceinline__ double hg_sigma_tri(const HGrid &g, const double *x)
 // The optical depth of trilinear sigma from x along -dir over min(nd, the
 // distance to the box): the ray is cut where it crosses a voxel-centre plane
 // of any axis; on each piece sigma(t) is a polynomial of degree <= 3 and
-// Simpson's rule (t1 - t0)/6 (s0 + 4 s_mid + s1) is exact.
+// Simpson's rule (t1 - t0)/6 (s0 + 4 s_mid + s1) is exact.  The 2^DIM corner
+// values of the piece's dual cell stay in registers: the next piece, one
+// plane further along one axis, shares half of them, so it loads only the
+// other half (all of them when more than one axis changes at once).
 template <int DIM>
 __device__ __forceinline__ double hg_optical_depth_tri(const HGrid &g, const double *x, const double *dir, double nd)
 {
-    double m[3] = {0, 0, 0}, tn[3], dt[3];
+    constexpr int NC = 1 << DIM;
+    double m[3] = {0, 0, 0}, tn[3], dt[3], u0[3], du[3];
+    int64_t off[3];
     double tend = INFINITY;
+    int64_t stride = 1;
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
         m[k] = -dir[k];
@@ -155,6 +161,8 @@ __device__ __forceinline__ double hg_optical_depth_tri(const HGrid &g, const dou
         else if (m[k] < 0) tend = fmin(tend, (x[k] - g.bmin[k]) / -m[k]);
         // the next voxel-centre plane crossing and the spacing of crossings
         const double u = (x[k] - g.bmin[k]) * g.ibbin[k] - 0.5;
+        u0[k] = u;
+        du[k] = m[k] * g.ibbin[k];
         if (m[k] > 0) {
             tn[k] = (floor(u) + 1.0 - u) * g.bbin[k] / m[k];
             dt[k] = g.bbin[k] / m[k];
@@ -165,9 +173,32 @@ __device__ __forceinline__ double hg_optical_depth_tri(const HGrid &g, const dou
             tn[k] = INFINITY;
             dt[k] = INFINITY;
         }
+        off[k] = g.nb[k] > 1 ? stride : 0;  // a corner's step along axis k (none on a one-voxel axis)
+        stride *= g.nb[k];
     }
     tend = fmax(fmin(tend, nd), 0.0);
-    double t0 = 0.0, s0 = hg_sigma_tri<DIM>(g, x), tau = 0.0, p[3];
+    int cell[3] = {-2, -2, -2};  // no corners loaded yet
+    double cs[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) cs[c] = 0.0;
+    // sigma on the loaded cell at ray parameter t (clamped fractions: constant in the outer half voxels)
+    auto sig = [&](double t) {
+        double f[3];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k)
+            f[k] = g.nb[k] > 1 ? fmin(fmax(fma(t, du[k], u0[k]) - (double)cell[k], 0.0), 1.0) : 0.0;
+        double v[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) v[c] = cs[c];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            const int h = 1 << (DIM - 1 - k);
+#pragma unroll
+            for (int c = 0; c < h; ++c) v[c] = fma(f[k], v[2 * c + 1] - v[2 * c], v[2 * c]);
+        }
+        return v[0];
+    };
+    double t0 = 0.0, s0 = 0.0, tau = 0.0;
     for (int guard = 0; guard < (1 << 22) && t0 < tend; ++guard) {
         double t1 = tend;
 #pragma unroll
@@ -176,12 +207,58 @@ __device__ __forceinline__ double hg_optical_depth_tri(const HGrid &g, const dou
         for (int k = 0; k < DIM; ++k)
             if (tn[k] <= t1) tn[k] += dt[k];
         const double tm = 0.5 * (t0 + t1);
+        // the piece's dual cell, from its midpoint
+        int nc[3] = {0, 0, 0}, n_changed = 0, axis = 0, step = 0;
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) p[k] = x[k] + tm * m[k];
-        const double sm = hg_sigma_tri<DIM>(g, p);
+        for (int k = 0; k < DIM; ++k) {
+            const double u = fmin(fmax(fma(tm, du[k], u0[k]), 0.0), (double)(g.nb[k] - 1));
+            int i = (int)floor(u);
+            i = i > g.nb[k] - 2 ? g.nb[k] - 2 : i;
+            nc[k] = i < 0 ? 0 : i;
+            if (nc[k] != cell[k]) {
+                ++n_changed;
+                axis = k;
+                step = nc[k] - cell[k];
+            }
+        }
+        if (n_changed) {
+            int64_t base = 0;
+            int64_t st = 1;
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) p[k] = x[k] + t1 * m[k];
-        const double s1 = hg_sigma_tri<DIM>(g, p);
+            for (int k = 0; k < DIM; ++k) {
+                base += (int64_t)nc[k] * st;
+                st *= g.nb[k];
+            }
+            const bool shift = n_changed == 1 && (step == 1 || step == -1);
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) {
+                if (shift && a == axis) {
+                    // the shared face moves to the other side; the far face is loaded
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        const int b = (c >> a) & 1;
+                        if (step > 0 && b == 0) cs[c] = cs[c | (1 << a)];
+                        if (step < 0 && b == 1) cs[c] = cs[c & ~(1 << a)];
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                bool load = !shift;
+                int64_t idx = base;
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) {
+                    const int b = (c >> k) & 1;
+                    idx += b ? off[k] : 0;
+                    if (shift && k == axis) load = (b == 1) == (step > 0);
+                }
+                if (load) cs[c] = g.sigt[idx];
+            }
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) cell[k] = nc[k];
+        }
+        if (guard == 0) s0 = sig(t0);
+        const double sm = sig(tm), s1 = sig(t1);
         tau += (t1 - t0) * (1.0 / 6.0) * (s0 + 4.0 * sm + s1);
         t0 = t1;
         s0 = s1;

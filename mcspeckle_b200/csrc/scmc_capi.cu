@@ -1686,8 +1686,7 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
         g0 = g1;
     }
     if (groups.empty()) return;
-    const int64_t Kmax = 64 * max_nblk;
-    const size_t pb = tc_align((size_t)nv0 * Kmax * sizeof(__half));  // one plane of rows
+    const size_t pb = tc_align((size_t)nv0 * 64 * max_nblk * sizeof(__half));  // one plane: [block][row][64]
     const int n_planes = split ? 6 : 4;                                // Re A, Im A, [Re lo, Im lo], Re B, Im B
     const size_t o_tiles = 0, o_blk = o_tiles + tc_align(tiles.size() * sizeof(int2));
     const size_t o_kr = o_blk + tc_align(blk.size() * sizeof(int2));
@@ -1716,10 +1715,9 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
     unsigned *d_max = reinterpret_cast<unsigned *>(dmeta + o_max);
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     for (const Group &G : groups) {
-        const int64_t K = 64 * G.nblk;
         CUtensorMap maps[6];
         __half *planes[6] = {are, aim, alr, ali, bre, bim};
-        for (int k = 0; k < 6; ++k) maps[k] = tc_map(planes[k], (uint64_t)K, (uint64_t)nv0, (uint64_t)K * 2, 128);
+        for (int k = 0; k < 6; ++k) maps[k] = tc_map_kblocks(planes[k], (uint64_t)nv0, (uint64_t)G.nblk);
         for (int j = 0; j < nl_out; ++j) {
             {
                 StageScope sc(ST_ROWS, st);
@@ -1730,11 +1728,11 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
                 CK(cudaGetLastError());
                 LAUNCHED();
                 if (split)
-                    fq_tc_rows_planar_kernel<true><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K, are,
+                    fq_tc_rows_planar_kernel<true><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, are,
                                                                                        aim, alr, ali, bre, bim, d_max);
                 else
-                    fq_tc_rows_planar_kernel<false><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, K,
-                                                                                        are, aim, alr, ali, bre, bim, d_max);
+                    fq_tc_rows_planar_kernel<false><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, are,
+                                                                                        aim, alr, ali, bre, bim, d_max);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }

@@ -28,6 +28,12 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-10
 MIXED_TOL = 1e-3
+# FourierQuad in FP16 rounds both operands, A = s_e T (the event's amplitude
+# times its twiddle) and B = T, to 2^-11 relative; on the near field of a
+# point source the terms cancel into a sum several times smaller than their
+# RMS, so the FP16 form lands near 1.3e-3 there (hi+lo "mixed" rounds only B
+# and stays under 1e-3).
+FQ_FP16_TOL = 2e-3
 THREADS = os.cpu_count() or 1
 
 
@@ -59,9 +65,9 @@ def test_fq256_geometry_against_oracle(gpu, oracle_lib, extended):
     mask = WL.fq256_propagating()
     u = FQ.field_fourier_quad_from_args(h)
     assert rel(u, uo, mask) < FP64_TOL
-    for prec in ("fp16", "mixed"):
+    for prec, tol in (("fp16", FQ_FP16_TOL), ("mixed", MIXED_TOL)):
         hp = WL.fq256_args(40, extended=extended, seed=78, precision=prec)
-        assert rel(FQ.field_fourier_quad_from_args(hp), uo, mask) < MIXED_TOL, prec
+        assert rel(FQ.field_fourier_quad_from_args(hp), uo, mask) < tol, prec
 
 
 def _device_cov_hetero(h):

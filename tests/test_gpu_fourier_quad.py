@@ -75,6 +75,12 @@ TC_CASES = {
                          v_stp=0.01, lam=1.0, cbs=1, smp=2, lmean0=None, vsign=-1, n=200),
     "tc_wide_angles": dict(sigt=0.12, albedo=1.0, box_min=[-8, -8, 0], box_max=[8, 8, 10], v_max=0.9, v_stp=0.025,
                            lam=0.8, cbs=1, smp=2, lmean0=None, vsign=-1, n=200),
+    # 128 angles and more: the CTA-pair form.  161: one 256 x 256 tile, rows
+    # and columns past the grid zero-filled; 301: 2 x 2 tiles per plane range
+    "tc_pair_161": dict(sigt=0.1, albedo=0.9, box_min=[-30, -30, 0], box_max=[30, 30, 12], v_max=0.8, v_stp=0.01,
+                        lam=1.0, cbs=1, smp=2, lmean0=None, vsign=-1, n=200),
+    "tc_pair_301": dict(sigt=0.12, albedo=0.95, box_min=[-20, -20, 0], box_max=[20, 20, 10], v_max=0.9,
+                        v_stp=0.006, lam=1.0, cbs=0, smp=2, lmean0=[0.0, 0.05, 1.0], vsign=-1, n=120),
 }
 
 
@@ -98,11 +104,13 @@ def test_fourier_quad_tensor_cores_close_to_fp64(gpu, name, precision):
     assert rel(u, u64) < 1e-3
 
 
-def test_fourier_quad_tensor_cores_several_plane_groups(gpu):
+@pytest.mark.parametrize("name", ["tc_wide_cbs", "tc_pair_161"])
+def test_fourier_quad_tensor_cores_several_plane_groups(gpu, name):
     """More entries than one group of the tensor-core form holds (2^20), so a
-    batch's plane groups run back to back from one metadata upload."""
+    batch's plane groups run back to back from one metadata upload (both the
+    single-CTA and the CTA-pair forms)."""
     from mcspeckle_b200 import _lib
-    c = dict(TC_CASES["tc_wide_cbs"], n=400000)
+    c = dict(TC_CASES[name], n=400000)
     u64 = FQ.field_fourier_quad_from_args(args_for(c, "fp64"))
     h = args_for(c, "fp16")
     _lib.profile_read(reset=True)
@@ -132,7 +140,7 @@ def weights(n, seed=9):
 
 
 OW_CASES = {k: FQ_CASES[k] for k in ("wide_cbs_exp", "narrow_nocbs_unif", "even_grid")}
-OW_CASES.update({k: TC_CASES[k] for k in ("tc_wide_cbs", "tc_even_grid")})
+OW_CASES.update({k: TC_CASES[k] for k in ("tc_wide_cbs", "tc_even_grid", "tc_pair_161")})
 
 
 @pytest.mark.parametrize("name", list(OW_CASES))
@@ -164,6 +172,7 @@ EXT_CASES = {
     "hg_plane_wave": (dict(FQ_CASES["wide_angles"], n=300), dict(hg_g=0.6)),
     "tc_point_source_hg": (dict(TC_CASES["tc_wide_cbs"], n=250), dict(light_point=True, hg_g=0.9)),
     "tc_hg_plane_wave": (dict(TC_CASES["tc_narrow_nocbs"], n=250), dict(hg_g=-0.4)),
+    "tc_pair_point_source_hg": (dict(TC_CASES["tc_pair_161"], n=200), dict(light_point=True, hg_g=0.9)),
 }
 
 
