@@ -323,8 +323,8 @@ class Leg:
             self.host = FQ.field_fourier_quad_from_args
             self.oracle = lambda h, O: O.field_fourier_quad(h.args, O.Rng.philox(), h.nv0)
             self.mask = WL.fq256_propagating()
-            self.kernel, self.bound, self.stage = "fq_planes_tc_kernel", "tensor", "contract"
-            self.traffic_file, self.unit_name = "fq_planes_tc_kernel_fq256_traffic.json", "entry"
+            self.kernel, self.bound, self.stage = "fq_pair_planes_kernel", "tensor", "contract"
+            self.traffic_file, self.unit_name = "fq_pair_planes_kernel_fq256_traffic.json", "entry"
             self.h2d = 3 * 8 + 256 * 256 * 16 * 2
             self.cpu_threads = 1
         elif name == "hetero128":

@@ -134,8 +134,10 @@ field_tc_rows_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t s
     const int total = nv + nl;
     for (int m0 = 0; m0 < total; m0 += kFtRows) {
         const int mc = min(kFtRows, total - m0);
+        // lanes take consecutive directions of one event (converged marches
+        // in a heterogeneous medium: one event's rays have similar lengths)
         for (int idx = threadIdx.x; idx < 32 * mc; idx += blockDim.x) {
-            const int k = idx % 32, r = idx / 32, m = m0 + r;
+            const int k = idx / mc, r = idx - k * mc, m = m0 + r;
             float2 p = make_float2(0.f, 0.f), q = make_float2(0.f, 0.f);
             if (k < ne) {
                 const EventView &ev = sev[k];

@@ -388,87 +388,92 @@ __device__ __forceinline__ uint32_t h2_bits(__half2 h)
     return *reinterpret_cast<const uint32_t *>(&h);
 }
 
-// Planar rows for the CTA-pair form (grids of at least 128 angles): one block
-// of 64 entries per CTA (a plane's last block zero-padded), written as the
-// contiguous slab [row][64 entries] of each plane at blockIdx.x * nv0 * 64:
-// A planes Re / Im of s_e(j) T[r1][p1_e] (with the low parts for hi+lo), B
-// planes Re / Im of T[r2][p2_e].  Thread = (rows r = r0, r0 + 32, ..., 8
-// consecutive entries): one 16-byte store per plane and row, a warp's stores
-// 512 contiguous bytes.  T[r][p] is linear in r in its phase
-// (fq_twiddle_kernel: T[r + 1][p] = T[r][p] exp(2 pi i P / M)), so each
-// thread reads the twiddles of its first two rows only and steps the rest
-// with the ratio T[r0 + 32][p] conj(T[r0][p]) in FP32 (at most nv0 / 32 - 1
-// steps, far below FP16's rounding).
-template <bool SPLIT>
+// The CTA-pair form's per-entry inputs in K-column order (block * 64 + t,
+// a plane's last block zero-padded): sv = c0 * light factor (FP32, unscaled)
+// and the pixel pair (p1, p2); also max |sv| for the group's operand scale.
 __global__ void __launch_bounds__(256)
-fq_tc_rows_planar_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E,
-                         const int2 *__restrict__ blk, int light, const float2 *__restrict__ Tt,
-                         __half *__restrict__ Are, __half *__restrict__ Aim, __half *__restrict__ Alr,
-                         __half *__restrict__ Ali, __half *__restrict__ Bre, __half *__restrict__ Bim,
-                         const unsigned *__restrict__ max_bits)
+fq_pair_prep_kernel(const __grid_constant__ FqParams F, const FqEntry *__restrict__ E, const int2 *__restrict__ blk,
+                    int64_t nblk, int light, float2 *__restrict__ svk, int2 *__restrict__ ppk,
+                    unsigned *__restrict__ max_bits)
 {
-    __shared__ float2 ss[64];
-    __shared__ int sp1[64], sp2[64];
-    const float scale = ldexpf(1.f, fq_scale_exponent(max_bits));
-    const int2 bk = blk[blockIdx.x];  // (first entry, entries in this block)
-    if (threadIdx.x < 64) {
+    float m = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nblk * 64; i += (int64_t)gridDim.x * blockDim.x) {
+        const int2 bk = blk[i >> 6];
+        const int t = (int)(i & 63);
         float2 sv = make_float2(0.f, 0.f);
-        int p1 = 0, p2 = 0;
-        if ((int)threadIdx.x < bk.y) {
-            const FqEntry en = E[bk.x + threadIdx.x];
+        int2 pp = make_int2(0, 0);
+        if (t < bk.y) {
+            const FqEntry en = E[bk.x + t];
             sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, light, en.xl));
-            sv.x *= scale;
-            sv.y *= scale;
-            p1 = en.p1;
-            p2 = en.p2;
+            pp = make_int2(en.p1, en.p2);
+            m = fmaxf(m, fmaxf(fabsf(sv.x), fabsf(sv.y)));
         }
-        ss[threadIdx.x] = sv;
-        sp1[threadIdx.x] = p1;
-        sp2[threadIdx.x] = p2;
+        svk[i] = sv;
+        ppk[i] = pp;
     }
-    __syncthreads();
-    const int e0 = (threadIdx.x & 7) * 8, rsub = threadIdx.x >> 3;
-    float2 av[8], aw[8], bv[8], bw[8];  // current A, B values of the 8 entries and their 32-row ratios
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && isfinite(m)) atomicMax(max_bits, __float_as_uint(m));
+}
+
+// Planar rows for the CTA-pair form (grids of at least 128 angles): one block
+// of 64 K columns per CTA, written as the contiguous slab [row][64 entries] of
+// each plane at blockIdx.x * nv0 * 64: A planes Re / Im of s_e(j) T[r1][p1_e]
+// (with the low parts for hi+lo), B planes Re / Im of T[r2][p2_e].  Thread =
+// (rows r = r0, r0 + 16, ..., 4 consecutive entries): one 8-byte store per
+// plane and row, a warp's stores two consecutive rows (256 contiguous bytes).
+// T[r][p] is linear in r in its phase (fq_twiddle_kernel: T[r + 1][p] =
+// T[r][p] exp(2 pi i P / M)), so each thread reads the twiddles of its first
+// two rows only and steps the rest with the ratio T[r0 + 16][p] conj(T[r0][p])
+// in FP32 (at most nv0 / 16 - 1 steps, far below FP16's rounding).  No shared
+// memory and no barrier: several CTAs per SM keep the stores streaming.
+template <bool SPLIT>
+__global__ void __launch_bounds__(256, 4)
+fq_tc_rows_planar_kernel(int nv0, const float2 *__restrict__ svk, const int2 *__restrict__ ppk,
+                         const float2 *__restrict__ Tt, __half *__restrict__ Are, __half *__restrict__ Aim,
+                         __half *__restrict__ Alr, __half *__restrict__ Ali, __half *__restrict__ Bre,
+                         __half *__restrict__ Bim, const unsigned *__restrict__ max_bits)
+{
+    const float scale = ldexpf(1.f, fq_scale_exponent(max_bits));
+    const int e0 = (threadIdx.x & 15) * 4, rsub = threadIdx.x >> 4;
+    const int64_t c0 = (int64_t)blockIdx.x * 64 + e0;
+    float2 av[4], aw[4], bv[4], bw[4];  // current A, B values of the 4 entries and their 16-row ratios
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        const int64_t o1 = (int64_t)sp1[e0 + j] * F.nv0 + rsub, o2 = (int64_t)sp2[e0 + j] * F.nv0 + rsub;
-        const float2 t1 = Tt[o1], t2 = Tt[o2], u1 = Tt[o1 + 32], u2 = Tt[o2 + 32];  // nv0 >= 128
-        av[j] = cmul(ss[e0 + j], t1);  // zero past the block's entries
+    for (int j = 0; j < 4; ++j) {
+        float2 sv = svk[c0 + j];  // zero in a block's padding
+        sv.x *= scale;
+        sv.y *= scale;
+        const int2 pp = ppk[c0 + j];
+        const int64_t o1 = (int64_t)pp.x * nv0 + rsub, o2 = (int64_t)pp.y * nv0 + rsub;
+        const float2 t1 = Tt[o1], t2 = Tt[o2], u1 = Tt[o1 + 16], u2 = Tt[o2 + 16];  // nv0 >= 128
+        av[j] = cmul(sv, t1);
         bv[j] = t2;
         aw[j] = cmul(u1, make_float2(t1.x, -t1.y));
         bw[j] = cmul(u2, make_float2(t2.x, -t2.y));
     }
-    const int64_t slab = (int64_t)blockIdx.x * F.nv0 * 64;
-    for (int r = rsub; r < F.nv0; r += 32) {
-        uint4 are, aim, alr, ali, bre, bim;
-        uint32_t *pre = &are.x, *pim = &aim.x, *plr = &alr.x, *pli = &ali.x, *pbr = &bre.x, *pbi = &bim.x;
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) {
-            const float2 a0 = av[2 * jj], a1 = av[2 * jj + 1], b0 = bv[2 * jj], b1 = bv[2 * jj + 1];
-            const __half2 hr = __floats2half2_rn(a0.x, a1.x), hi = __floats2half2_rn(a0.y, a1.y);
-            pre[jj] = h2_bits(hr);
-            pim[jj] = h2_bits(hi);
-            if (SPLIT) {
-                plr[jj] = h2_bits(__floats2half2_rn(a0.x - __low2float(hr), a1.x - __high2float(hr)));
-                pli[jj] = h2_bits(__floats2half2_rn(a0.y - __low2float(hi), a1.y - __high2float(hi)));
-            }
-            pbr[jj] = h2_bits(__floats2half2_rn(b0.x, b1.x));
-            pbi[jj] = h2_bits(__floats2half2_rn(b0.y, b1.y));
+    const int64_t slab = (int64_t)blockIdx.x * nv0 * 64;
+    for (int r = rsub; r < nv0; r += 16) {
+        const __half2 r01 = __floats2half2_rn(av[0].x, av[1].x), r23 = __floats2half2_rn(av[2].x, av[3].x);
+        const __half2 i01 = __floats2half2_rn(av[0].y, av[1].y), i23 = __floats2half2_rn(av[2].y, av[3].y);
+        const int64_t o = slab + (int64_t)r * 64 + e0;
+        *reinterpret_cast<uint2 *>(Are + o) = make_uint2(h2_bits(r01), h2_bits(r23));
+        *reinterpret_cast<uint2 *>(Aim + o) = make_uint2(h2_bits(i01), h2_bits(i23));
+        if (SPLIT) {
+            *reinterpret_cast<uint2 *>(Alr + o) = make_uint2(
+                h2_bits(__floats2half2_rn(av[0].x - __low2float(r01), av[1].x - __high2float(r01))),
+                h2_bits(__floats2half2_rn(av[2].x - __low2float(r23), av[3].x - __high2float(r23))));
+            *reinterpret_cast<uint2 *>(Ali + o) = make_uint2(
+                h2_bits(__floats2half2_rn(av[0].y - __low2float(i01), av[1].y - __high2float(i01))),
+                h2_bits(__floats2half2_rn(av[2].y - __low2float(i23), av[3].y - __high2float(i23))));
         }
+        *reinterpret_cast<uint2 *>(Bre + o) = make_uint2(h2_bits(__floats2half2_rn(bv[0].x, bv[1].x)),
+                                                         h2_bits(__floats2half2_rn(bv[2].x, bv[3].x)));
+        *reinterpret_cast<uint2 *>(Bim + o) = make_uint2(h2_bits(__floats2half2_rn(bv[0].y, bv[1].y)),
+                                                         h2_bits(__floats2half2_rn(bv[2].y, bv[3].y)));
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
+        for (int j = 0; j < 4; ++j) {
             av[j] = cmul(av[j], aw[j]);
             bv[j] = cmul(bv[j], bw[j]);
         }
-        const int64_t o = slab + (int64_t)r * 64 + e0;
-        *reinterpret_cast<uint4 *>(Are + o) = are;
-        *reinterpret_cast<uint4 *>(Aim + o) = aim;
-        if (SPLIT) {
-            *reinterpret_cast<uint4 *>(Alr + o) = alr;
-            *reinterpret_cast<uint4 *>(Ali + o) = ali;
-        }
-        *reinterpret_cast<uint4 *>(Bre + o) = bre;
-        *reinterpret_cast<uint4 *>(Bim + o) = bim;
     }
 }
 

@@ -1248,9 +1248,12 @@ __device__ __forceinline__ void tc_rows_terms(const NeeParams &Q, const SingleRe
         sev[threadIdx.x] = ev;
     }
     __syncthreads();
+    // lanes take consecutive directions of one event: the rays of one event to
+    // nearby views (or lights) have about the same length, so a warp's
+    // attenuation marches (heterogeneous medium) stay converged
     const int per = nv + nl;
     for (int idx = threadIdx.x; idx < 32 * per; idx += blockDim.x) {
-        const int k = idx % 32, m = idx / 32;
+        const int k = idx / per, m = idx - k * per;
         float2 p = make_float2(0.f, 0.f), q = make_float2(0.f, 0.f);
         if (k < ne) {
             const EventView &ev = sev[k];

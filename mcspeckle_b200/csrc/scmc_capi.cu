@@ -1694,7 +1694,9 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
     const size_t o_pr = o_pl + tc_align(gpl.size() * sizeof(int));
     const size_t o_err = o_pr + tc_align(prs.size() * sizeof(int2));
     const size_t o_max = o_err + 256;
-    const size_t meta = o_err + 1024;
+    const size_t o_sv = o_err + 1024;                                   // sv per K column
+    const size_t o_pp = o_sv + tc_align((size_t)64 * max_nblk * sizeof(float2));  // (p1, p2) per K column
+    const size_t meta = o_pp + tc_align((size_t)64 * max_nblk * sizeof(int2));
     char *mem = reinterpret_cast<char *>(c.tc_a.ensure(n_planes * pb + meta));
     __half *are = reinterpret_cast<__half *>(mem), *aim = reinterpret_cast<__half *>(mem + pb);
     __half *alr = split ? reinterpret_cast<__half *>(mem + 2 * pb) : are;
@@ -1713,6 +1715,8 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
     int2 *d_kr = reinterpret_cast<int2 *>(dmeta + o_kr), *d_pr = reinterpret_cast<int2 *>(dmeta + o_pr);
     int *d_pl = reinterpret_cast<int *>(dmeta + o_pl), *d_err = reinterpret_cast<int *>(dmeta + o_err);
     unsigned *d_max = reinterpret_cast<unsigned *>(dmeta + o_max);
+    float2 *d_sv = reinterpret_cast<float2 *>(dmeta + o_sv);
+    int2 *d_pp = reinterpret_cast<int2 *>(dmeta + o_pp);
     CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     for (const Group &G : groups) {
         CUtensorMap maps[6];
@@ -1722,17 +1726,17 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
             {
                 StageScope sc(ST_ROWS, st);
                 CK(cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
-                fq_scale_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((G.nblk * 64 + 255) / 256,
-                                                                                   (int64_t)sm_count(c.device) * 8)),
-                                  256, 0, st>>>(F, Es, d_blk + G.blk0, G.nblk, 64, j, d_max);
+                fq_pair_prep_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((G.nblk * 64 + 255) / 256,
+                                                                                       (int64_t)sm_count(c.device) * 8)),
+                                      256, 0, st>>>(F, Es, d_blk + G.blk0, G.nblk, j, d_sv, d_pp, d_max);
                 CK(cudaGetLastError());
                 LAUNCHED();
                 if (split)
-                    fq_tc_rows_planar_kernel<true><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, are,
-                                                                                       aim, alr, ali, bre, bim, d_max);
+                    fq_tc_rows_planar_kernel<true><<<(unsigned)G.nblk, 256, 0, st>>>(nv0, d_sv, d_pp, Tt, are, aim, alr,
+                                                                                       ali, bre, bim, d_max);
                 else
-                    fq_tc_rows_planar_kernel<false><<<(unsigned)G.nblk, 256, 0, st>>>(F, Es, d_blk + G.blk0, j, Tt, are,
-                                                                                        aim, alr, ali, bre, bim, d_max);
+                    fq_tc_rows_planar_kernel<false><<<(unsigned)G.nblk, 256, 0, st>>>(nv0, d_sv, d_pp, Tt, are, aim, alr,
+                                                                                        ali, bre, bim, d_max);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
