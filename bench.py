@@ -530,10 +530,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp16", choices=["mixed", "fp16"],
                     help="mixed: FP16 hi+lo split (2 tensor products); fp16: one FP16 product")
-    ap.add_argument("--served-requests", type=int, default=60)
+    ap.add_argument("--served-requests", type=int, default=24)
     ap.add_argument("--served-paths-min", type=float, default=1e5)
     ap.add_argument("--served-paths-max", type=float, default=1e8)
-    ap.add_argument("--served-fp32-seconds", type=float, default=20.0)
+    ap.add_argument("--served-fp32-seconds", type=float, default=10.0)
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--legs", default="field16,fq256,hetero128",
