@@ -141,125 +141,120 @@ __device__ __forceinline__ double hg_sigma_tri(const HGrid &g, const double *x)
 // The optical depth of trilinear sigma from x along -dir over min(nd, the
 // distance to the box): the ray is cut where it crosses a voxel-centre plane
 // of any axis; on each piece sigma(t) is a polynomial of degree <= 3 and
-// Simpson's rule (t1 - t0)/6 (s0 + 4 s_mid + s1) is exact.  The 2^DIM corner
-// values of the piece's dual cell stay in registers: the next piece, one
-// plane further along one axis, shares half of them, so it loads only the
-// other half (all of them when more than one axis changes at once).
+// Simpson's rule (t1 - t0)/6 (s0 + 4 s_mid + s1) is exact.  Per axis the
+// march keeps the integer floor of the centre coordinate on the current piece
+// (stepped by one at each crossing, so no rounding per piece), from which the
+// piece's dual cell and its fraction follow: f = u - cell inside the grid of
+// centres, 0 or 1 in the outer half voxels (sigma is clamped to the outer
+// centres there).  The cell's 2^DIM corner values stay in registers until the
+// cell changes; indices are 32-bit.
 template <int DIM>
 __device__ __forceinline__ double hg_optical_depth_tri(const HGrid &g, const double *x, const double *dir, double nd)
 {
     constexpr int NC = 1 << DIM;
-    double m[3] = {0, 0, 0}, tn[3], dt[3], u0[3], du[3];
-    int64_t off[3];
+    double tn[3], dt[3], u0[3], du[3];
+    int fl[3], st[3], off[3], nbm2[3], strd[3];
     double tend = INFINITY;
-    int64_t stride = 1;
+    int stride = 1;
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {
-        m[k] = -dir[k];
+        const double m = -dir[k];
         // distance to the box face along m (cubeDist.m without the 1e-7 floor for |m| = 0)
-        if (m[k] > 0) tend = fmin(tend, (g.bmax[k] - x[k]) / m[k]);
-        else if (m[k] < 0) tend = fmin(tend, (x[k] - g.bmin[k]) / -m[k]);
-        // the next voxel-centre plane crossing and the spacing of crossings
+        if (m > 0) tend = fmin(tend, (g.bmax[k] - x[k]) / m);
+        else if (m < 0) tend = fmin(tend, (x[k] - g.bmin[k]) / -m);
+        // the centre coordinate u(t) = u0 + t du, the next plane crossing, the spacing of crossings
         const double u = (x[k] - g.bmin[k]) * g.ibbin[k] - 0.5;
         u0[k] = u;
-        du[k] = m[k] * g.ibbin[k];
-        if (m[k] > 0) {
-            tn[k] = (floor(u) + 1.0 - u) * g.bbin[k] / m[k];
-            dt[k] = g.bbin[k] / m[k];
-        } else if (m[k] < 0) {
-            tn[k] = (u - (ceil(u) - 1.0)) * g.bbin[k] / -m[k];
-            dt[k] = g.bbin[k] / -m[k];
+        du[k] = m * g.ibbin[k];
+        if (m > 0) {
+            tn[k] = (floor(u) + 1.0 - u) * g.bbin[k] / m;
+            dt[k] = g.bbin[k] / m;
+            fl[k] = (int)floor(u);
+            st[k] = 1;
+        } else if (m < 0) {
+            tn[k] = (u - (ceil(u) - 1.0)) * g.bbin[k] / -m;
+            dt[k] = g.bbin[k] / -m;
+            fl[k] = (int)ceil(u) - 1;
+            st[k] = -1;
         } else {
             tn[k] = INFINITY;
             dt[k] = INFINITY;
+            fl[k] = (int)floor(u);
+            st[k] = 0;
         }
+        nbm2[k] = g.nb[k] - 2;
         off[k] = g.nb[k] > 1 ? stride : 0;  // a corner's step along axis k (none on a one-voxel axis)
+        strd[k] = stride;
         stride *= g.nb[k];
     }
     tend = fmax(fmin(tend, nd), 0.0);
-    int cell[3] = {-2, -2, -2};  // no corners loaded yet
     double cs[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) cs[c] = 0.0;
-    // sigma on the loaded cell at ray parameter t (clamped fractions: constant in the outer half voxels)
-    auto sig = [&](double t) {
-        double f[3];
-#pragma unroll
-        for (int k = 0; k < DIM; ++k)
-            f[k] = g.nb[k] > 1 ? fmin(fmax(fma(t, du[k], u0[k]) - (double)cell[k], 0.0), 1.0) : 0.0;
-        double v[NC];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) v[c] = cs[c];
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) {
-            const int h = 1 << (DIM - 1 - k);
-#pragma unroll
-            for (int c = 0; c < h; ++c) v[c] = fma(f[k], v[2 * c + 1] - v[2 * c], v[2 * c]);
-        }
-        return v[0];
-    };
+    int loaded = -1;  // base index of the corners in cs
     double t0 = 0.0, s0 = 0.0, tau = 0.0;
     for (int guard = 0; guard < (1 << 22) && t0 < tend; ++guard) {
         double t1 = tend;
 #pragma unroll
         for (int k = 0; k < DIM; ++k) t1 = fmin(t1, tn[k]);
-#pragma unroll
-        for (int k = 0; k < DIM; ++k)
-            if (tn[k] <= t1) tn[k] += dt[k];
-        const double tm = 0.5 * (t0 + t1);
-        // the piece's dual cell, from its midpoint
-        int nc[3] = {0, 0, 0}, n_changed = 0, axis = 0, step = 0;
+        // this piece's cell and fractions f_k(t) = c0_k + c1_k t
+        double c0[3], c1[3];
+        int base = 0;
 #pragma unroll
         for (int k = 0; k < DIM; ++k) {
-            const double u = fmin(fmax(fma(tm, du[k], u0[k]), 0.0), (double)(g.nb[k] - 1));
-            int i = (int)floor(u);
-            i = i > g.nb[k] - 2 ? g.nb[k] - 2 : i;
-            nc[k] = i < 0 ? 0 : i;
-            if (nc[k] != cell[k]) {
-                ++n_changed;
-                axis = k;
-                step = nc[k] - cell[k];
+            int cell;
+            if (nbm2[k] < 0) {  // one voxel along k
+                cell = 0;
+                c0[k] = 0.0;
+                c1[k] = 0.0;
+            } else if (fl[k] < 0) {
+                cell = 0;
+                c0[k] = 0.0;
+                c1[k] = 0.0;
+            } else if (fl[k] > nbm2[k]) {
+                cell = nbm2[k];
+                c0[k] = 1.0;
+                c1[k] = 0.0;
+            } else {
+                cell = fl[k];
+                c0[k] = u0[k] - (double)cell;
+                c1[k] = du[k];
             }
+            base += cell * strd[k];
         }
-        if (n_changed) {
-            int64_t base = 0;
-            int64_t st = 1;
-#pragma unroll
-            for (int k = 0; k < DIM; ++k) {
-                base += (int64_t)nc[k] * st;
-                st *= g.nb[k];
-            }
-            const bool shift = n_changed == 1 && (step == 1 || step == -1);
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) {
-                if (shift && a == axis) {
-                    // the shared face moves to the other side; the far face is loaded
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        const int b = (c >> a) & 1;
-                        if (step > 0 && b == 0) cs[c] = cs[c | (1 << a)];
-                        if (step < 0 && b == 1) cs[c] = cs[c & ~(1 << a)];
-                    }
-                }
-            }
+        if (base != loaded) {
 #pragma unroll
             for (int c = 0; c < NC; ++c) {
-                bool load = !shift;
-                int64_t idx = base;
+                int idx = base;
 #pragma unroll
-                for (int k = 0; k < DIM; ++k) {
-                    const int b = (c >> k) & 1;
-                    idx += b ? off[k] : 0;
-                    if (shift && k == axis) load = (b == 1) == (step > 0);
-                }
-                if (load) cs[c] = g.sigt[idx];
+                for (int k = 0; k < DIM; ++k) idx += ((c >> k) & 1) ? off[k] : 0;
+                cs[c] = g.sigt[idx];
             }
-#pragma unroll
-            for (int k = 0; k < DIM; ++k) cell[k] = nc[k];
+            loaded = base;
         }
+        auto sig = [&](double t) {
+            double v[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) v[c] = cs[c];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                const double f = fma(t, c1[k], c0[k]);
+                const int h = 1 << (DIM - 1 - k);
+#pragma unroll
+                for (int c = 0; c < h; ++c) v[c] = fma(f, v[2 * c + 1] - v[2 * c], v[2 * c]);
+            }
+            return v[0];
+        };
         if (guard == 0) s0 = sig(t0);
-        const double sm = sig(tm), s1 = sig(t1);
+        const double sm = sig(0.5 * (t0 + t1)), s1 = sig(t1);
         tau += (t1 - t0) * (1.0 / 6.0) * (s0 + 4.0 * sm + s1);
+        // the crossings that end this piece
+#pragma unroll
+        for (int k = 0; k < DIM; ++k)
+            if (tn[k] <= t1) {
+                tn[k] += dt[k];
+                fl[k] += st[k];
+            }
         t0 = t1;
         s0 = s1;
     }
