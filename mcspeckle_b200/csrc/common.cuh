@@ -48,6 +48,7 @@ struct HGrid {
     double lrad;
     double basis[6];         // null(meanl'), dim x (dim-1) column-major
     int trilinear;           // extension: sigt trilinear between voxel centres
+    const float *sigt_f;     // FP32 copy of sigt for the reduced-precision NEE march (trilinear), or nullptr
 };
 
 // Everything the walk needs, passed by value.

@@ -261,4 +261,121 @@ __device__ __forceinline__ double hg_optical_depth_tri(const HGrid &g, const dou
     return tau;
 }
 
+// The same march in FP32 for the reduced precisions (NEE only; the FP64
+// mode keeps hg_optical_depth_tri).  The per-ray set-up (centre coordinate,
+// first crossing, distance to the box) is formed in FP64 and rounded once;
+// each crossing time is the first one plus an integer count of spacings (one
+// FMA, no accumulated rounding), so the pieces stay within FP32 rounding of
+// the planes (about 3e-5 of a wavelength at 500 wavelengths), where a shift
+// changes the integral only to second order because sigma is continuous.
+template <int DIM>
+__device__ __forceinline__ float hg_optical_depth_tri_f32(const HGrid &g, const double *x, const double *dir, double nd)
+{
+    constexpr int NC = 1 << DIM;
+    float tb[3], dt[3], u0[3], du[3];
+    int fl[3], st[3], cnt[3], off[3], nbm2[3], strd[3];
+    double tend_d = INFINITY;
+    int stride = 1;
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        const double m = -dir[k];
+        if (m > 0) tend_d = fmin(tend_d, (g.bmax[k] - x[k]) / m);
+        else if (m < 0) tend_d = fmin(tend_d, (x[k] - g.bmin[k]) / -m);
+        const double u = (x[k] - g.bmin[k]) * g.ibbin[k] - 0.5;
+        u0[k] = (float)u;
+        du[k] = (float)(m * g.ibbin[k]);
+        if (m > 0) {
+            tb[k] = (float)((floor(u) + 1.0 - u) * g.bbin[k] / m);
+            dt[k] = (float)(g.bbin[k] / m);
+            fl[k] = (int)floor(u);
+            st[k] = 1;
+        } else if (m < 0) {
+            tb[k] = (float)((u - (ceil(u) - 1.0)) * g.bbin[k] / -m);
+            dt[k] = (float)(g.bbin[k] / -m);
+            fl[k] = (int)ceil(u) - 1;
+            st[k] = -1;
+        } else {
+            tb[k] = INFINITY;
+            dt[k] = 0.f;
+            fl[k] = (int)floor(u);
+            st[k] = 0;
+        }
+        cnt[k] = 0;
+        nbm2[k] = g.nb[k] - 2;
+        off[k] = g.nb[k] > 1 ? stride : 0;
+        strd[k] = stride;
+        stride *= g.nb[k];
+    }
+    const float tend = (float)fmax(fmin(tend_d, nd), 0.0);
+    float cs[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) cs[c] = 0.f;
+    int loaded = -1;
+    float t0 = 0.f, s0 = 0.f, tau = 0.f;
+    for (int guard = 0; guard < (1 << 22) && t0 < tend; ++guard) {
+        float tn[3];
+        float t1 = tend;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            tn[k] = st[k] ? fmaf((float)cnt[k], dt[k], tb[k]) : INFINITY;
+            t1 = fminf(t1, tn[k]);
+        }
+        float c0[3], c1[3];
+        int base = 0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) {
+            int cell;
+            if (nbm2[k] < 0 || fl[k] < 0) {
+                cell = 0;
+                c0[k] = 0.f;
+                c1[k] = 0.f;
+            } else if (fl[k] > nbm2[k]) {
+                cell = nbm2[k];
+                c0[k] = 1.f;
+                c1[k] = 0.f;
+            } else {
+                cell = fl[k];
+                c0[k] = u0[k] - (float)cell;
+                c1[k] = du[k];
+            }
+            base += cell * strd[k];
+        }
+        if (base != loaded) {
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                int idx = base;
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) idx += ((c >> k) & 1) ? off[k] : 0;
+                cs[c] = g.sigt_f[idx];
+            }
+            loaded = base;
+        }
+        auto sig = [&](float t) {
+            float v[NC];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) v[c] = cs[c];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                const float f = fmaf(t, c1[k], c0[k]);
+                const int h = 1 << (DIM - 1 - k);
+#pragma unroll
+                for (int c = 0; c < h; ++c) v[c] = fmaf(f, v[2 * c + 1] - v[2 * c], v[2 * c]);
+            }
+            return v[0];
+        };
+        if (guard == 0) s0 = sig(t0);
+        const float sm = sig(0.5f * (t0 + t1)), s1 = sig(t1);
+        tau = fmaf((t1 - t0) * (1.f / 6.f), s0 + 4.f * sm + s1, tau);
+#pragma unroll
+        for (int k = 0; k < DIM; ++k)
+            if (tn[k] <= t1) {
+                ++cnt[k];
+                fl[k] += st[k];
+            }
+        t0 = t1;
+        s0 = s1;
+    }
+    return tau;
+}
+
 }  // namespace scmc

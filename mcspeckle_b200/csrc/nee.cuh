@@ -100,7 +100,13 @@ phaseatt_hetero(const double *x, const double *d, int is_ff, const NeeParams &Q)
         pv = nd;
         rv = (DIM == 3) ? 1.0 / (nd + 0.01 * Q.lambda) : 1.0 / sqrt(nd + 0.01 * Q.lambda);
     }
-    const double wbdv = hg_optical_depth<DIM>(Q.hg, x, dir, nd);
+    double wbdv;
+    if constexpr (POL != P64) {  // reduced precisions: the trilinear march in FP32 when the grid has a copy
+        wbdv = (Q.hg.trilinear && Q.hg.sigt_f) ? (double)hg_optical_depth_tri_f32<DIM>(Q.hg, x, dir, nd)
+                                               : hg_optical_depth<DIM>(Q.hg, x, dir, nd);
+    } else {
+        wbdv = hg_optical_depth<DIM>(Q.hg, x, dir, nd);
+    }
     const double ph = Q.kw * pv;
     if constexpr (POL == P64) {
         double s, c;

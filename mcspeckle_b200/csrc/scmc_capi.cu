@@ -1326,7 +1326,7 @@ __global__ void philox_stream_kernel(uint64_t seed, uint64_t path, int tag, int6
 // heterogeneous medium (MCCovHetro / MCsampleHetro)
 // ---------------------------------------------------------------------------
 struct HeteroBufs {
-    DevBuf sigt, alb, cdf, mean1, zeros;
+    DevBuf sigt, sigt_f, alb, cdf, mean1, zeros;
 };
 HeteroBufs g_hbufs[64];
 
@@ -1392,6 +1392,14 @@ Prepared prepare_hetero(Ctx &c, const scmc_hetero_args *h, int want_phase, bool 
     CK(cudaMemcpyAsync(dcdf, cdf.data(), nv * sizeof(double), cudaMemcpyHostToDevice, st));
     g.sigt = dsig;
     g.cdf = dcdf;
+    g.sigt_f = nullptr;
+    std::vector<float> sig_f;
+    if (g.trilinear && mc.precision != SCMC_PREC_FP64) {  // the FP32 NEE march reads an FP32 copy
+        sig_f.assign(h->sigt_grid, h->sigt_grid + nv);
+        float *dsf = reinterpret_cast<float *>(hb.sigt_f.ensure(nv * sizeof(float)));
+        CK(cudaMemcpyAsync(dsf, sig_f.data(), nv * sizeof(float), cudaMemcpyHostToDevice, st));
+        g.sigt_f = dsf;
+    }
     g.alb_scalar = mc.albedo;
     g.alb = nullptr;
     if (h->albedo_grid) {
