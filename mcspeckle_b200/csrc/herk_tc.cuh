@@ -1335,29 +1335,77 @@ tc_rows_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, M
     }
 }
 
+// NEE terms of the block's events toward directions m_lo .. m_lo + cnt - 1
+// (views below nv, then lights) into p[(m - m_lo) * ld + k] and q[...]; lanes
+// take consecutive directions of one event (converged heterogeneous marches).
+template <int DIM, bool SINGLE>
+__device__ __forceinline__ void tc_rows_dirs(const NeeParams &Q, const EventView *sev, int ne, int m_lo, int cnt,
+                                             int ld, float2 *p_out, float2 *q_out)
+{
+    const int nv = Q.nv;
+    for (int idx = threadIdx.x; idx < 32 * cnt; idx += blockDim.x) {
+        const int k = idx / cnt, mm = idx - k * cnt, m = m_lo + mm;
+        float2 p = make_float2(0.f, 0.f), q = make_float2(0.f, 0.f);
+        if (k < ne) {
+            const EventView &ev = sev[k];
+            if (m < nv) {
+                if (SINGLE) p = phaseatt<DIM, PMIX>(ev.x1, Q.vs + 3 * m, Q.is_ff_v, Q);
+                else nee_view<DIM, PMIX, float2>(Q, m, ev.x, ev.ow, ev.x1, ev.w1, ev.w0p, p, q);
+            } else {
+                const int j = m - nv;
+                if (SINGLE) p = phaseatt<DIM, PMIX>(ev.x1, Q.l + 3 * j, Q.is_ff_l, Q);
+                else nee_light<DIM, PMIX, float2>(Q, j, ev.x, ev.ow, ev.x1, ev.w1, ev.w0p, p, q);
+            }
+        }
+        p_out[mm * ld + k] = p;
+        q_out[mm * ld + k] = q;
+    }
+}
+
+// Shared memory of the planar rows kernel: view terms for vc views, light
+// terms for all lights, 32 events each, plus the events.
+inline size_t tc_rows_planar_smem(int vc, int nl)
+{
+    return sizeof(float2) * 32 * 2 * (size_t)(vc + nl) + 32 * sizeof(float) + 32 * sizeof(EventView) + 64;
+}
+
 // Planar rows (CTA-pair kernel): Re t_i and Im t_i in separate planes, rows of
 // K events; Rhi / Rlo the Re planes, Ihi / Ilo the Im planes.  Lane = a pair
 // of adjacent events and half-warp = a view, so each thread reads both
 // events' factors with one 16-byte shared load, rounds them with one packed
-// conversion and writes one half2 per plane.
+// conversion and writes one half2 per plane.  The light terms are computed
+// once; the view terms in chunks of vc views (all of them when they fit), so
+// that with many views two CTAs still share an SM.
 template <int DIM, bool SINGLE, bool SPLIT>
 __global__ void __launch_bounds__(256)
 tc_rows_planar_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t e0, int64_t n_ev,
                       int64_t K, __half *__restrict__ Rhi, __half *__restrict__ Rlo, __half *__restrict__ Ihi,
-                      __half *__restrict__ Ilo, const float2 *__restrict__ af_tab)
+                      __half *__restrict__ Ilo, const float2 *__restrict__ af_tab, int vc)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nv = Q.nv, nl = Q.nl;
-    float2 *sa = reinterpret_cast<float2 *>(smem_raw);  // [nv][32]
-    float2 *sa0 = sa + nv * 32;
-    float2 *sb = sa0 + nv * 32;  // [nl][32]
+    float2 *sa = reinterpret_cast<float2 *>(smem_raw);  // [vc][32]
+    float2 *sa0 = sa + vc * 32;
+    float2 *sb = sa0 + vc * 32;  // [nl][32]
     float2 *sb2 = sb + nl * 32;
     float *ssc = reinterpret_cast<float *>(sb2 + nl * 32);  // [32]
     EventView *sev = reinterpret_cast<EventView *>(ssc + 32);
 
     const int64_t g0 = (int64_t)blockIdx.x * 32;
     const int ne = (int)max((int64_t)0, min((int64_t)32, n_ev - g0));
-    tc_rows_terms<DIM, SINGLE>(Q, S, scap, M, mcap, e0, g0, ne, 32, sa, sa0, sb, sb2, ssc, sev);
+    if (threadIdx.x < 32) {
+        EventView ev;
+        if ((int)threadIdx.x < ne) {
+            load_event<DIM, SINGLE>(Q, S, scap, M, mcap, e0 + g0 + threadIdx.x, ev);
+            ssc[threadIdx.x] = (float)sqrt(ev.wpx);
+        } else {
+            ssc[threadIdx.x] = 0.f;
+            ev = EventView{};
+        }
+        sev[threadIdx.x] = ev;
+    }
+    __syncthreads();
+    tc_rows_dirs<DIM, SINGLE>(Q, sev, ne, nv, nl, 32, sb, sb2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int h = lane >> 4, kp = lane & 15;  // view parity, event pair (events 2 kp, 2 kp + 1)
     const float s0 = ssc[2 * kp], s1 = ssc[2 * kp + 1];
@@ -1366,43 +1414,49 @@ tc_rows_planar_kernel(const __grid_constant__ NeeParams Q, SingleRec S, int64_t 
     const int64_t col = g0 + 2 * kp;
     const int64_t step = 16 * K;  // 16 views
     const bool cbs = !SINGLE && Q.cbs;
-    for (int lj = 0; lj < nl; ++lj) {
-        float4 b = sb4[lj * 16 + kp], b2 = sb24[lj * 16 + kp];
-        b = make_float4(b.x * s0, b.y * s0, b.z * s1, b.w * s1);
-        b2 = make_float4(b2.x * s0, b2.y * s0, b2.z * s1, b2.w * s1);
-        const int v0 = 2 * warp + h;
-        const int64_t o0 = ((int64_t)nv * lj + v0) * K + col;
-        __half *pr = Rhi + o0, *pi = Ihi + o0, *qr = Rlo + o0, *qi = Ilo + o0;
-        for (int vi = v0; vi < nv; vi += 16, pr += step, pi += step, qr += step, qi += step) {
-            const float4 a = sa4[vi * 16 + kp];
-            float2 t0 = cmul(make_float2(a.x, a.y), make_float2(b.x, b.y));
-            float2 t1 = cmul(make_float2(a.z, a.w), make_float2(b.z, b.w));
-            if (SINGLE) {
-                float2 f0, f1;
-                if (af_tab) {
-                    f0 = f1 = af_tab[vi + nv * lj];
-                } else {
-                    f0 = to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[2 * kp].x1));
-                    f1 = to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[2 * kp + 1].x1));
+    for (int vc0 = 0; vc0 < nv; vc0 += vc) {
+        const int cnt = min(vc, nv - vc0);
+        if (vc0 > 0) __syncthreads();  // the previous chunk's products have read sa / sa0
+        tc_rows_dirs<DIM, SINGLE>(Q, sev, ne, vc0, cnt, 32, sa, sa0);
+        __syncthreads();
+        for (int lj = 0; lj < nl; ++lj) {
+            float4 b = sb4[lj * 16 + kp], b2 = sb24[lj * 16 + kp];
+            b = make_float4(b.x * s0, b.y * s0, b.z * s1, b.w * s1);
+            b2 = make_float4(b2.x * s0, b2.y * s0, b2.z * s1, b2.w * s1);
+            const int v0 = vc0 + 2 * warp + h;
+            const int64_t o0 = ((int64_t)nv * lj + v0) * K + col;
+            __half *pr = Rhi + o0, *pi = Ihi + o0, *qr = Rlo + o0, *qi = Ilo + o0;
+            for (int vi = v0; vi < vc0 + cnt; vi += 16, pr += step, pi += step, qr += step, qi += step) {
+                const float4 a = sa4[(vi - vc0) * 16 + kp];
+                float2 t0 = cmul(make_float2(a.x, a.y), make_float2(b.x, b.y));
+                float2 t1 = cmul(make_float2(a.z, a.w), make_float2(b.z, b.w));
+                if (SINGLE) {
+                    float2 f0, f1;
+                    if (af_tab) {
+                        f0 = f1 = af_tab[vi + nv * lj];
+                    } else {
+                        f0 = to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[2 * kp].x1));
+                        f1 = to_c<float2>(single_amp<DIM>(Q, vi, lj, sev[2 * kp + 1].x1));
+                    }
+                    t0 = cmul(t0, f0);
+                    t1 = cmul(t1, f1);
+                } else if (cbs) {
+                    const float4 a0 = sa04[(vi - vc0) * 16 + kp];
+                    const float2 u0 = cmul(make_float2(a0.x, a0.y), make_float2(b2.x, b2.y));
+                    const float2 u1 = cmul(make_float2(a0.z, a0.w), make_float2(b2.z, b2.w));
+                    t0.x += u0.x;
+                    t0.y += u0.y;
+                    t1.x += u1.x;
+                    t1.y += u1.y;
                 }
-                t0 = cmul(t0, f0);
-                t1 = cmul(t1, f1);
-            } else if (cbs) {
-                const float4 a0 = sa04[vi * 16 + kp];
-                const float2 u0 = cmul(make_float2(a0.x, a0.y), make_float2(b2.x, b2.y));
-                const float2 u1 = cmul(make_float2(a0.z, a0.w), make_float2(b2.z, b2.w));
-                t0.x += u0.x;
-                t0.y += u0.y;
-                t1.x += u1.x;
-                t1.y += u1.y;
-            }
-            const __half2 re = __floats2half2_rn(t0.x, t1.x), im = __floats2half2_rn(t0.y, t1.y);
-            *reinterpret_cast<__half2 *>(pr) = re;
-            *reinterpret_cast<__half2 *>(pi) = im;
-            if (SPLIT) {
-                const float2 fr = __half22float2(re), fi = __half22float2(im);
-                *reinterpret_cast<__half2 *>(qr) = __floats2half2_rn(t0.x - fr.x, t1.x - fr.y);
-                *reinterpret_cast<__half2 *>(qi) = __floats2half2_rn(t0.y - fi.x, t1.y - fi.y);
+                const __half2 re = __floats2half2_rn(t0.x, t1.x), im = __floats2half2_rn(t0.y, t1.y);
+                *reinterpret_cast<__half2 *>(pr) = re;
+                *reinterpret_cast<__half2 *>(pi) = im;
+                if (SPLIT) {
+                    const float2 fr = __half22float2(re), fi = __half22float2(im);
+                    *reinterpret_cast<__half2 *>(qr) = __floats2half2_rn(t0.x - fr.x, t1.x - fr.y);
+                    *reinterpret_cast<__half2 *>(qi) = __floats2half2_rn(t0.y - fi.x, t1.y - fi.y);
+                }
             }
         }
     }
@@ -1583,11 +1637,17 @@ inline void tc_rows(const TcPlan &p, const TcOperands &o, const NeeParams &Q, co
     const float2 *af = use_af_table ? o.af : nullptr;
     if (p.pair) {
         auto kern = tc_rows_planar_kernel<DIM, SINGLE, SPLIT>;
-        if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        // all views at once when two CTAs fit on an SM; else chunks of a multiple of 16 views
+        constexpr size_t kTwoPerSm = 110 * 1024;
+        int vc = Q.nv;
+        while (vc > 16 && tc_rows_planar_smem(vc, Q.nl) > kTwoPerSm) vc = ((vc + 1) / 2 + 15) / 16 * 16;
+        const size_t psmem = tc_rows_planar_smem(vc, Q.nl);
+        if (psmem > 48 * 1024 &&
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) != cudaSuccess)
             throw std::runtime_error("too many lights/views for the tensor-core row kernel");
         // every column of the 64-event blocks the product reads is written (zeros past n)
         const int grid = (int)((n + 63) / 64 * 2);
-        kern<<<grid, 256, smem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, o.ihi, o.ilo, af);
+        kern<<<grid, 256, psmem, st>>>(Q, S, scap, M, mcap, e0, n, p.K, o.ahi, o.alo, o.ihi, o.ilo, af, vc);
     } else {
         auto kern = tc_rows_kernel<DIM, SINGLE, SPLIT>;
         if (smem > 48 * 1024 && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
