@@ -328,10 +328,11 @@ struct Ctx {
     double multi_per_path = 8.0;  // multiple-scattering events per path seen so far (one-pass capacity)
     size_t tc_chunk_bytes = (size_t)2 << 30;  // operand memory per tensor-core chunk
     // Extra streams and events of the covariance pipeline: the walk and row
-    // generation run on `aux`, contractions alternate between the caller's
-    // stream and `aux2`.
-    cudaStream_t aux = nullptr, aux2 = nullptr;
-    cudaEvent_t ev[9] = {};
+    // generation run on `aux` (lowest priority), contractions alternate
+    // between `aux3` and `aux2` (highest priority, so that when an SM frees
+    // the block scheduler places the contraction before more rows).
+    cudaStream_t aux = nullptr, aux2 = nullptr, aux3 = nullptr;
+    cudaEvent_t ev[10] = {};
 
     void destroy_aux()
     {
@@ -342,13 +343,17 @@ struct Ctx {
         }
         cudaStreamDestroy(aux);
         cudaStreamDestroy(aux2);
-        aux = aux2 = nullptr;
+        cudaStreamDestroy(aux3);
+        aux = aux2 = aux3 = nullptr;
     }
     void make_aux()
     {
         if (aux) return;
-        CK(cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking));
-        CK(cudaStreamCreateWithFlags(&aux2, cudaStreamNonBlocking));
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CK(cudaStreamCreateWithPriority(&aux, cudaStreamNonBlocking, least));
+        CK(cudaStreamCreateWithPriority(&aux2, cudaStreamNonBlocking, greatest));
+        CK(cudaStreamCreateWithPriority(&aux3, cudaStreamNonBlocking, greatest));
         for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
 
@@ -1136,11 +1141,12 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
         LAUNCHED();
     }
     c.make_aux();
-    cudaStream_t rs = c.aux, cs1 = c.aux2;
+    cudaStream_t rs = c.aux, cs0 = c.aux3, cs1 = c.aux2;
     cudaEvent_t *ev_rows = &c.ev[0], *ev_free = &c.ev[3];
-    cudaEvent_t ev_setup = c.ev[6], ev_end_rs = c.ev[7], ev_end_c1 = c.ev[8];
+    cudaEvent_t ev_setup = c.ev[6], ev_end_rs = c.ev[7], ev_end_c1 = c.ev[8], ev_end_c0 = c.ev[9];
     CK(cudaEventRecord(ev_setup, st));
     CK(cudaStreamWaitEvent(rs, ev_setup, 0));   // accumulators, operands, af table, mean1
+    CK(cudaStreamWaitEvent(cs0, ev_setup, 0));
     CK(cudaStreamWaitEvent(cs1, ev_setup, 0));
     int64_t chunk_id = 0;
     WalkParams W = P.W;
@@ -1156,7 +1162,7 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
             for (int64_t e0 = 0; e0 < n_ev; e0 += chunk, ++chunk_id) {
                 const int64_t n = std::min(chunk, n_ev - e0);
                 const int b = (int)(chunk_id % NB), d = (int)(chunk_id & 1);
-                cudaStream_t cs = d ? cs1 : st;
+                cudaStream_t cs = d ? cs1 : cs0;
                 if (chunk_id >= NB) CK(cudaStreamWaitEvent(rs, ev_free[b], 0));  // chunk_id - NB has read buffer b
                 {
                     StageScope sc(ST_ROWS, rs);
@@ -1185,8 +1191,10 @@ void cov_run_tc(Ctx &c, const scmc_mc_args *a, const Prepared &P, double2 *d_Ms,
         done += nb;
     }
     CK(cudaEventRecord(ev_end_rs, rs));
+    CK(cudaEventRecord(ev_end_c0, cs0));
     CK(cudaEventRecord(ev_end_c1, cs1));
     CK(cudaStreamWaitEvent(st, ev_end_rs, 0));
+    CK(cudaStreamWaitEvent(st, ev_end_c0, 0));
     CK(cudaStreamWaitEvent(st, ev_end_c1, 0));
     int herr[NB] = {0, 0, 0};
     for (int k = 0; k < NB; ++k) CK(cudaMemcpyAsync(&herr[k], ops[k].err, sizeof(int), cudaMemcpyDeviceToHost, st));
