@@ -10,10 +10,13 @@
 //   B  = [N  x K]  row j    = ( Re t_j,  Im t_j)  (= the even rows of A)
 //   D  = A B^T     D[2i][j] = Re C[i][j],  D[2i+1][j] = Im C[i][j]
 //
-// Precision: A is split into FP16 hi + lo parts (A = hi + lo to ~2^-22),
-// B is the FP16 hi part; both products accumulate in FP32 in TMEM, so
-// D = (A_hi + A_lo) B_hi^T.  After the chunk the tile is added into an FP64
-// accumulator, which carries the sum across chunks.
+// Precision: A is split into FP16 hi + lo parts (A = hi + lo to ~2^-22).
+// This single-CTA kernel (and the field and FourierQuad forms) computes
+// D = (A_hi + A_lo) B_hi^T, compensating A's rounding only; the CTA-pair
+// covariance kernel (herk_tc2_kernel) adds a second sweep A_hi B_lo^T, so
+// only A_lo B_lo^T is left out.  Products accumulate in FP32 in TMEM; after
+// the chunk the tile is added into an FP64 accumulator, which carries the sum
+// across chunks.
 //
 // Kernel shape: one CTA per 128 x 256 output tile of the upper triangle
 // (complex rows 64*tm .. 64*tm+63 against complex columns 256*tn ..).
@@ -756,6 +759,10 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
     const int kb0 = (int)blockIdx.y * kb_per_split;
     const int nkb = min(num_kb, kb0 + kb_per_split) - kb0;
     if (nkb <= 0) return;
+    // hi+lo: a first sweep of (A hi + A lo) B hi over the K blocks and a
+    // second of A hi B lo, so both operands' FP16 rounding is compensated
+    // (only A lo B lo, about 2^-22 relative, is left out)
+    const int nk_all = SPLIT ? 2 * nkb : nkb;
     const int Mr = 2 * N;
     D += (int64_t)blockIdx.y * Mr * N;
     const int2 tile = tiles[blockIdx.x >> 1];
@@ -788,7 +795,7 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
     if (warp == 0 && lane == 0) {
         // TMA producer (both CTAs; none in a fault test); completion counted on the leader's full[s]
         const uint32_t full0 = mapa_shared(smem_u32(&full[0]), 0);
-        for (int kb = 0; kb < (test_fault ? 0 : nkb); ++kb) {
+        for (int kb = 0; kb < (test_fault ? 0 : nk_all); ++kb) {
             const int s = kb % Cfg::STAGES;
             if (kb >= Cfg::STAGES && !mbar_wait(&empty[s], ((kb / Cfg::STAGES) - 1) & 1)) {
                 atomicExch(abort_flag, 1);
@@ -796,17 +803,23 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
             }
             if (*(volatile int *)abort_flag) break;
             uint8_t *st = base + s * Cfg::STAGE_BYTES;
-            if (rank == 0) mbar_expect_tx(&full[s], 2 * Cfg::STAGE_BYTES);
+            const bool sweep2 = SPLIT && kb >= nkb;  // A hi x B lo
+            if (rank == 0) mbar_expect_tx(&full[s], sweep2 ? 2 * 4 * Cfg::TILE : 2 * Cfg::STAGE_BYTES);
             const uint32_t fb = full0 + (uint32_t)(s * sizeof(uint64_t));
-            const int kx = (kb0 + kb) * TC_BK;
+            const int kx = (kb0 + (sweep2 ? kb - nkb : kb)) * TC_BK;
             tma_load_2d_pair(st, &tm_re, kx, crow0, fb);
             tma_load_2d_pair(st + Cfg::TILE, &tm_im, kx, crow0, fb);
-            if (SPLIT) {
-                tma_load_2d_pair(st + 2 * Cfg::TILE, &tm_re_lo, kx, crow0, fb);
-                tma_load_2d_pair(st + 3 * Cfg::TILE, &tm_im_lo, kx, crow0, fb);
+            if (sweep2) {
+                tma_load_2d_pair(st + Cfg::B_OFF, &tm_re_lo, kx, brow0, fb);
+                tma_load_2d_pair(st + Cfg::B_OFF + Cfg::TILE, &tm_im_lo, kx, brow0, fb);
+            } else {
+                if (SPLIT) {
+                    tma_load_2d_pair(st + 2 * Cfg::TILE, &tm_re_lo, kx, crow0, fb);
+                    tma_load_2d_pair(st + 3 * Cfg::TILE, &tm_im_lo, kx, crow0, fb);
+                }
+                tma_load_2d_pair(st + Cfg::B_OFF, &tm_re, kx, brow0, fb);
+                tma_load_2d_pair(st + Cfg::B_OFF + Cfg::TILE, &tm_im, kx, brow0, fb);
             }
-            tma_load_2d_pair(st + Cfg::B_OFF, &tm_re, kx, brow0, fb);
-            tma_load_2d_pair(st + Cfg::B_OFF + Cfg::TILE, &tm_im, kx, brow0, fb);
             *(volatile int *)issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0 && rank == 0) {
@@ -814,13 +827,14 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
         constexpr uint32_t idesc = umma_idesc_f16(256, 256);
         constexpr uint32_t idesc_neg = idesc | (1u << 13);  // negate A
         const uint32_t t_re = tmem, t_im = tmem + 256;
-        for (int kb = 0; kb < nkb; ++kb) {
+        for (int kb = 0; kb < nk_all; ++kb) {
             const int s = kb % Cfg::STAGES;
             if (!mbar_wait(&full[s], (kb / Cfg::STAGES) & 1, wait_ns)) {
                 atomicExch(abort_flag, 1);
                 break;
             }
             tc_fence_after();
+            const bool sweep2 = SPLIT && kb >= nkb;  // the stage holds A hi and B lo
             uint8_t *st = base + s * Cfg::STAGE_BYTES;
             const uint64_t ar = umma_desc_sw128(st), ai = umma_desc_sw128(st + Cfg::TILE);
             const uint64_t br = umma_desc_sw128(st + Cfg::B_OFF), bi = umma_desc_sw128(st + Cfg::B_OFF + Cfg::TILE);
@@ -832,7 +846,7 @@ herk_tc2_kernel(const __grid_constant__ CUtensorMap tm_re, const __grid_constant
                 umma_f16_pair(t_im, ai + adv, br + adv, idesc, first);
                 umma_f16_pair(t_re, ai + adv, bi + adv, idesc, 1u);
                 umma_f16_pair(t_im, ar + adv, bi + adv, idesc_neg, 1u);
-                if (SPLIT) {
+                if (SPLIT && !sweep2) {
                     const uint64_t lr = umma_desc_sw128(st + 2 * Cfg::TILE) + adv;
                     const uint64_t li = umma_desc_sw128(st + 3 * Cfg::TILE) + adv;
                     umma_f16_pair(t_re, lr, br + adv, idesc, 1u);
@@ -1513,11 +1527,15 @@ inline TcPlan tc_plan(int N, bool split, size_t chunk_bytes = (size_t)1 << 30, i
     // 32 events real-expanded, 64 planar.
     const int64_t per_event = (p.pair ? 4 : 8) * (split ? 2 : 1) * (int64_t)N;
     const int64_t eb = p.pair ? 64 : 32;
-    // The FP32 sums in TMEM over a chunk dominate the error (FP16: 4.4e-4 at
-    // 65536 events, 2.9e-4 at 32768 on the 64 x 64 covariance); the hi+lo
-    // split keeps chunks of at most 32768 events to stay the accurate mode.
+    // The error of the FP32 sums in TMEM grows in proportion to the chunk's
+    // events (hi+lo on the 64 x 64 covariance, 1e5 paths: 2.0e-5 at 2048,
+    // 4.0e-5 at 4096, 7.6e-5 at 8192, 2.6e-4 at 32768, at 0.88, 0.99, 1.05 and
+    // 1.08e6 paths/s); once both operands are compensated it is the hi+lo
+    // mode's only error of note, so that mode takes 4096-event chunks by
+    // default (tunable up to 32768).  FP16 keeps 65536 (4.2e-4 in all, its
+    // operands' rounding included).
     const int64_t e_max = split ? 32768 : 65536;
-    int64_t e = chunk_events > 0 ? chunk_events : (int64_t)chunk_bytes / per_event;
+    int64_t e = chunk_events > 0 ? chunk_events : split ? 4096 : (int64_t)chunk_bytes / per_event;
     e = std::max<int64_t>(eb, std::min<int64_t>(e, e_max));
     e = (e / eb) * eb;
     p.events_per_chunk = e;
