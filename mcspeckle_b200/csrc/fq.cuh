@@ -97,6 +97,15 @@ struct FqEntry {
     int plane;
 };
 
+// With one output light (one light, or the weighted sum of MCfieldFourierQuadOnWave)
+// and the CTA-pair form, an entry needs only its factor and pixels: 16 bytes
+// instead of 56 through the plane sort.
+struct FqEntryC {
+    float2 sv;                 // c0 * light factor (FP32, as the operands use it)
+    unsigned short p1, p2;     // pixel indices (< 65536, checked on the host)
+    int plane;
+};
+
 __device__ __forceinline__ double fq_mround(double x) { return x < 0 ? -floor(-x + 0.5) : floor(x + 0.5); }
 
 // Plane of a view-side depth: plane j holds gz[j] <= z < gz[j+1]; depths at
@@ -117,8 +126,9 @@ __device__ __forceinline__ int fq_plane(const FqParams &F, double z)
 
 // Build the entries of a batch: singles are paths 0..n_paths-1, multis
 // follow.  counts[plane] is incremented for the counting sort.
+template <bool COMPACT>
 __global__ void fq_entries_kernel(const __grid_constant__ FqParams F, SingleRec S, int64_t scap, MultiRec M, int64_t mcap, int64_t n_paths,
-                                  int64_t n_multi, FqEntry *__restrict__ out, int *__restrict__ counts)
+                                  int64_t n_multi, void *__restrict__ out_v, int *__restrict__ counts)
 {
     const int64_t nvert = n_paths + n_multi;
     const int passes = F.cbs ? 2 : 1;
@@ -164,16 +174,26 @@ __global__ void fq_entries_kernel(const __grid_constant__ FqParams F, SingleRec 
         // exp(-2 pi i/lambda (-z + tz)) (MCfieldFourierQuad.m:272; OnWave: vsign for -1)
         sincos(F.vsign_vertex * F.kw * (-xv[2] + tz), &sd, &cd);
         en.c0 = make_double2(s * (cp * cd - sp * sd), s * (cp * sd + sp * cd));
-        out[k] = en;
+        if constexpr (COMPACT) {
+            FqEntryC ec;
+            ec.sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, 0, en.xl));
+            ec.p1 = (unsigned short)en.p1;
+            ec.p2 = (unsigned short)en.p2;
+            ec.plane = en.plane;
+            reinterpret_cast<FqEntryC *>(out_v)[k] = ec;
+        } else {
+            reinterpret_cast<FqEntry *>(out_v)[k] = en;
+        }
         if (en.plane >= 0) atomicAdd(&counts[en.plane], 1);
     }
 }
 
-__global__ void fq_scatter_kernel(const FqEntry *__restrict__ in, int64_t n, const int *__restrict__ offsets,
-                                  int *__restrict__ cursor, FqEntry *__restrict__ out)
+template <typename E>
+__global__ void fq_scatter_kernel(const E *__restrict__ in, int64_t n, const int *__restrict__ offsets,
+                                  int *__restrict__ cursor, E *__restrict__ out)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        const FqEntry e = in[k];
+        const E e = in[k];
         if (e.plane < 0) continue;
         const int pos = offsets[e.plane] + atomicAdd(&cursor[e.plane], 1);
         out[pos] = e;
@@ -405,6 +425,30 @@ fq_pair_prep_kernel(const __grid_constant__ FqParams F, const FqEntry *__restric
         if (t < bk.y) {
             const FqEntry en = E[bk.x + t];
             sv = cmul(to_c<float2>(en.c0), fq_light_factor<PMIX>(F, light, en.xl));
+            pp = make_int2(en.p1, en.p2);
+            m = fmaxf(m, fmaxf(fabsf(sv.x), fabsf(sv.y)));
+        }
+        svk[i] = sv;
+        ppk[i] = pp;
+    }
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && isfinite(m)) atomicMax(max_bits, __float_as_uint(m));
+}
+
+// The same from compact entries (factor already applied).
+__global__ void __launch_bounds__(256)
+fq_pair_prep_compact_kernel(const FqEntryC *__restrict__ E, const int2 *__restrict__ blk, int64_t nblk,
+                            float2 *__restrict__ svk, int2 *__restrict__ ppk, unsigned *__restrict__ max_bits)
+{
+    float m = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nblk * 64; i += (int64_t)gridDim.x * blockDim.x) {
+        const int2 bk = blk[i >> 6];
+        const int t = (int)(i & 63);
+        float2 sv = make_float2(0.f, 0.f);
+        int2 pp = make_int2(0, 0);
+        if (t < bk.y) {
+            const FqEntryC en = E[bk.x + t];
+            sv = en.sv;
             pp = make_int2(en.p1, en.p2);
             m = fmaxf(m, fmaxf(fabsf(sv.x), fabsf(sv.y)));
         }

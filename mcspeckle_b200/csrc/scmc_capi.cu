@@ -315,14 +315,37 @@ struct DevBuf {
     template <typename T> T *as() { return reinterpret_cast<T *>(p); }
 };
 
+// Pinned host staging that grows on demand (copies from it are truly
+// asynchronous; a pageable source would make the copy wait for its stream).
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    void *ensure(size_t bytes)
+    {
+        if (bytes <= n) return p;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        const size_t want = bytes + bytes / 4;
+        CK(cudaMallocHost(&p, want));
+        n = want;
+        return p;
+    }
+    ~PinnedBuf()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+
 struct Ctx {
     int device = -1;
     std::mutex mu;
+    PinnedBuf fq_hmeta[2];  // FourierQuad pair-form metadata, per batch parity
     DevBuf counts, mcnt, moff, scan_tmp, ctr, err;
     DevBuf s_x1, s_w1, s_wpx, s_xi, s_nev;
     DevBuf m_x, m_ow, m_wpx, m_xi, m_path, m_plen;
     DevBuf dirs_l, dirs_v, dirs_vs, tab0_amp, tab0_icdf, tab1_amp, tab1_icdf;
-    DevBuf acc_s, acc_m, acc_f, rows, tiles, tc_a, out0, out1, out2, wl, offs, mcap_bounds;
+    DevBuf acc_s, acc_m, acc_f, rows, rows2, tiles, tc_a, out0, out1, out2, wl, offs, mcap_bounds, fq_err;
     DevBuf fq_gz, fq_zexp, fq_box, fq_tw, fq_twt, fq_rr, fq_counts, fq_offsets, fq_cursor, fq_planes;
     int64_t scap = 0, mcap = 0;
     double multi_per_path = 8.0;  // multiple-scattering events per path seen so far (one-pass capacity)
@@ -362,7 +385,7 @@ struct Ctx {
         DevBuf *all[] = {&counts, &mcnt, &moff, &scan_tmp, &ctr, &err, &s_x1, &s_w1, &s_wpx, &s_xi, &s_nev,
                          &m_x, &m_ow, &m_wpx, &m_xi, &m_path, &m_plen, &dirs_l, &dirs_v, &dirs_vs, &tab0_amp,
                          &tab0_icdf, &tab1_amp, &tab1_icdf, &acc_s, &acc_m, &acc_f, &rows, &tiles, &tc_a, &out0, &wl, &offs,
-                         &mcap_bounds,
+                         &mcap_bounds, &rows2, &fq_err,
                          &out1, &out2, &fq_gz, &fq_zexp, &fq_box, &fq_tw, &fq_twt, &fq_rr, &fq_counts, &fq_offsets,
                          &fq_cursor, &fq_planes};
         for (DevBuf *b : all) f(*b);
@@ -1647,10 +1670,10 @@ void fq_tc_batch(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const
 // The same on CTA pairs from planar operands (grids of at least 128 angles):
 // 64-entry blocks, one K column per entry, a pair per 256 x 256 output tile,
 // one Horner chain per pair (fq_pair_planes_kernel).  r1step: exp(zexp0 z_bin).
-void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, const std::vector<int> &hcounts,
+void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const void *Es, bool compact, const std::vector<int> &hcounts,
                       const std::vector<int> &hoff, const std::vector<int> &hplanes, const float2 *Tt,
                       const double2 *dz, const float2 *r1step, int n_uniform, double *U, bool split,
-                      int64_t group_entries, cudaStream_t st)
+                      int64_t group_entries, int *d_err, PinnedBuf &hpin, cudaStream_t st)
 {
     const int nv0 = F.nv0;
     std::vector<int2> tiles;
@@ -1720,20 +1743,21 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
     __half *bre = reinterpret_cast<__half *>(mem + (split ? 4 : 2) * pb);
     __half *bim = reinterpret_cast<__half *>(mem + (split ? 5 : 3) * pb);
     char *dmeta = mem + n_planes * pb;
-    std::vector<char> hmeta(o_err, 0);
-    std::memcpy(hmeta.data() + o_tiles, tiles.data(), tiles.size() * sizeof(int2));
-    std::memcpy(hmeta.data() + o_blk, blk.data(), blk.size() * sizeof(int2));
-    std::memcpy(hmeta.data() + o_kr, kr.data(), kr.size() * sizeof(int2));
-    std::memcpy(hmeta.data() + o_pl, gpl.data(), gpl.size() * sizeof(int));
-    std::memcpy(hmeta.data() + o_pr, prs.data(), prs.size() * sizeof(int2));
-    CK(cudaMemcpyAsync(dmeta, hmeta.data(), o_err, cudaMemcpyHostToDevice, st));
+    // the caller guarantees that the previous copy out of hpin has completed
+    char *hmeta = reinterpret_cast<char *>(hpin.ensure(o_err));
+    std::memset(hmeta, 0, o_err);
+    std::memcpy(hmeta + o_tiles, tiles.data(), tiles.size() * sizeof(int2));
+    std::memcpy(hmeta + o_blk, blk.data(), blk.size() * sizeof(int2));
+    std::memcpy(hmeta + o_kr, kr.data(), kr.size() * sizeof(int2));
+    std::memcpy(hmeta + o_pl, gpl.data(), gpl.size() * sizeof(int));
+    std::memcpy(hmeta + o_pr, prs.data(), prs.size() * sizeof(int2));
+    CK(cudaMemcpyAsync(dmeta, hmeta, o_err, cudaMemcpyHostToDevice, st));
     int2 *d_tiles = reinterpret_cast<int2 *>(dmeta + o_tiles), *d_blk = reinterpret_cast<int2 *>(dmeta + o_blk);
     int2 *d_kr = reinterpret_cast<int2 *>(dmeta + o_kr), *d_pr = reinterpret_cast<int2 *>(dmeta + o_pr);
-    int *d_pl = reinterpret_cast<int *>(dmeta + o_pl), *d_err = reinterpret_cast<int *>(dmeta + o_err);
+    int *d_pl = reinterpret_cast<int *>(dmeta + o_pl);
     unsigned *d_max = reinterpret_cast<unsigned *>(dmeta + o_max);
     float2 *d_sv = reinterpret_cast<float2 *>(dmeta + o_sv);
     int2 *d_pp = reinterpret_cast<int2 *>(dmeta + o_pp);
-    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     for (const Group &G : groups) {
         CUtensorMap maps[6];
         __half *planes[6] = {are, aim, alr, ali, bre, bim};
@@ -1742,9 +1766,14 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
             {
                 StageScope sc(ST_ROWS, st);
                 CK(cudaMemsetAsync(d_max, 0, sizeof(unsigned), st));
-                fq_pair_prep_kernel<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((G.nblk * 64 + 255) / 256,
-                                                                                       (int64_t)sm_count(c.device) * 8)),
-                                      256, 0, st>>>(F, Es, d_blk + G.blk0, G.nblk, j, d_sv, d_pp, d_max);
+                const unsigned pg = (unsigned)std::max<int64_t>(
+                    1, std::min<int64_t>((G.nblk * 64 + 255) / 256, (int64_t)sm_count(c.device) * 8));
+                if (compact)
+                    fq_pair_prep_compact_kernel<<<pg, 256, 0, st>>>(reinterpret_cast<const FqEntryC *>(Es), d_blk + G.blk0,
+                                                                    G.nblk, d_sv, d_pp, d_max);
+                else
+                    fq_pair_prep_kernel<<<pg, 256, 0, st>>>(F, reinterpret_cast<const FqEntry *>(Es), d_blk + G.blk0,
+                                                            G.nblk, j, d_sv, d_pp, d_max);
                 CK(cudaGetLastError());
                 LAUNCHED();
                 if (split)
@@ -1771,10 +1800,9 @@ void fq_tc_batch_pair(Ctx &c, const FqParams &F, int nl_out, const FqEntry *Es, 
             prof_count(0, 0, 8.0 * (double)nv0 * nv0 * (double)G.entries);
         }
     }
-    int herr = 0;
-    CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));  // the operand memory and metadata are reused by the next batch
-    if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
+    // no synchronisation: the next batch's metadata and operands are written on
+    // the same stream after these kernels; d_err (set only on a failed wait)
+    // is read once at the end of the solve
 }
 
 // Wl == null: MCfieldFourierQuad.m.  Wl (nl complex, host): MCfieldFourierQuadOnWave.m,
@@ -1971,27 +1999,55 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     const scmc_tuning tune = tuning_for(SCMC_TUNE_FQ, a->precision, Nv * Nv);
     int64_t total_vert = 0;
     const int passes = a->do_cbs ? 2 : 1;
-    for (int64_t done = 0; done < a->max_itr;) {
+    // The pair form pipelines batches: the walk, the entries and the plane
+    // sort of a batch run on `ps` (with entry buffers of their own parity)
+    // while the previous batch's operands and products run on `st`; the host
+    // plans a batch's plane groups meanwhile.  Other forms stay on `st`.
+    const bool pipe = use_pair;
+    cudaStream_t ps = st;
+    int *d_err = reinterpret_cast<int *>(c.fq_err.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    if (pipe) {
+        c.make_aux();
+        ps = c.aux;
+        CK(cudaEventRecord(c.ev[4], st));  // accumulator, twiddles, tables
+        CK(cudaStreamWaitEvent(ps, c.ev[4], 0));
+    }
+    cudaEvent_t *ev_prod = &c.ev[0], *ev_cons = &c.ev[2];  // per parity
+    int64_t bi = 0;
+    for (int64_t done = 0; done < a->max_itr; ++bi) {
+        const int par = (int)(bi & 1);
         const int64_t nb = path_batch_size(a->max_itr - done, tune.path_batch);
         W.path_base = a->path_offset + (uint64_t)done;
         Batch B;
-        walk_batch(c, W, nb, st, B);
+        if (pipe && bi >= 2) CK(cudaStreamWaitEvent(ps, ev_cons[par], 0));  // batch bi - 2 has read this parity's entries
+        walk_batch(c, W, nb, ps, B);
         const int64_t nvert = B.n_paths + B.n_multi;
         total_vert += nvert;
         const int64_t nent = nvert * passes;
         if (nent > INT32_MAX) fail(SCMC_ERR_INVALID, "batch too large");
-        FqEntry *Ein = reinterpret_cast<FqEntry *>(c.rows.ensure(2 * nent * sizeof(FqEntry)));
-        FqEntry *Es = Ein + nent;
-        CK(cudaMemsetAsync(counts, 0, (Nz + 1) * sizeof(int), st));
+        // one output light on the pair form: 16-byte entries with the light factor applied
+        const bool compact = use_pair && nl_out == 1 && Nx <= 65535;
+        const size_t rec = compact ? sizeof(FqEntryC) : sizeof(FqEntry);
+        DevBuf &ebuf = (pipe && par) ? c.rows2 : c.rows;
+        char *Ein_b = reinterpret_cast<char *>(ebuf.ensure(2 * nent * rec));
+        char *Es_b = Ein_b + nent * rec;
+        FqEntry *Es = reinterpret_cast<FqEntry *>(Es_b);  // the full-entry forms
+        CK(cudaMemsetAsync(counts, 0, (Nz + 1) * sizeof(int), ps));
         {
-            StageScope sc(ST_ROWS, st);
-            fq_entries_kernel<<<(int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16), 256, 0, st>>>(
-                F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein, counts);
+            StageScope sc(ST_ROWS, ps);
+            const int eg = (int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16);
+            if (compact)
+                fq_entries_kernel<true><<<eg, 256, 0, ps>>>(F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein_b,
+                                                             counts);
+            else
+                fq_entries_kernel<false><<<eg, 256, 0, ps>>>(F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein_b,
+                                                              counts);
             CK(cudaGetLastError());
             LAUNCHED();
         }
-        CK(cudaMemcpyAsync(hcounts.data(), counts, Nz * sizeof(int), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        CK(cudaMemcpyAsync(hcounts.data(), counts, Nz * sizeof(int), cudaMemcpyDeviceToHost, ps));
+        CK(cudaStreamSynchronize(ps));
         std::vector<int> hoff(Nz + 1, 0);
         hplanes.clear();
         for (int64_t k = 0; k < Nz; ++k) {
@@ -2002,20 +2058,31 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
             done += nb;
             continue;
         }
-        CK(cudaMemcpyAsync(offsets, hoff.data(), (Nz + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(planes, hplanes.data(), hplanes.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemsetAsync(cursor, 0, (Nz + 1) * sizeof(int), st));
+        CK(cudaMemcpyAsync(offsets, hoff.data(), (Nz + 1) * sizeof(int), cudaMemcpyHostToDevice, ps));
+        CK(cudaMemcpyAsync(planes, hplanes.data(), hplanes.size() * sizeof(int), cudaMemcpyHostToDevice, ps));
+        CK(cudaMemsetAsync(cursor, 0, (Nz + 1) * sizeof(int), ps));
         {
-            StageScope sc(ST_ROWS, st);
-            fq_scatter_kernel<<<(int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16), 256, 0, st>>>(
-                Ein, nent, offsets, cursor, Es);
+            StageScope sc(ST_ROWS, ps);
+            const int sg = (int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16);
+            if (compact)
+                fq_scatter_kernel<FqEntryC><<<sg, 256, 0, ps>>>(reinterpret_cast<const FqEntryC *>(Ein_b), nent, offsets,
+                                                                cursor, reinterpret_cast<FqEntryC *>(Es_b));
+            else
+                fq_scatter_kernel<FqEntry><<<sg, 256, 0, ps>>>(reinterpret_cast<const FqEntry *>(Ein_b), nent, offsets,
+                                                               cursor, Es);
             CK(cudaGetLastError());
             LAUNCHED();
         }
+        if (pipe) {
+            CK(cudaEventRecord(ev_prod[par], ps));
+            CK(cudaStreamWaitEvent(st, ev_prod[par], 0));
+            CK(cudaEventSynchronize(ev_cons[par]));  // batch bi - 2's metadata copy out of fq_hmeta[par] is done
+        }
         if (use_tc) {
             if (use_pair)
-                fq_tc_batch_pair(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
-                                 reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
+                fq_tc_batch_pair(c, F, (int)nl_out, Es_b, compact, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
+                                 reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries,
+                                 d_err, c.fq_hmeta[par], st);
             else
                 fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
                             reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
@@ -2030,8 +2097,15 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
                 LAUNCHED();
             }
         }
-        CK(cudaStreamSynchronize(st));  // host vectors above are reused next batch
+        if (pipe) CK(cudaEventRecord(ev_cons[par], st));
+        else CK(cudaStreamSynchronize(st));  // host vectors above are reused next batch
         done += nb;
+    }
+    {
+        int herr = 0;  // a bounded wait of the pair form gave up somewhere in the solve
+        CK(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr) fail(SCMC_ERR_TIMEOUT, "tensor-core contraction: a bounded wait gave up");
     }
     const double V = bw[0] * bw[1] * bw[2];
     const double norm = total_vert > 0 ? std::sqrt(1.0 / (double)total_vert * V * sigt) : 0.0;  // lines 214, 302-303
