@@ -42,11 +42,14 @@ enum { SCMC_SCT_ISOTROPIC = 1, SCMC_SCT_TABULATED = 2, SCMC_SCT_HG = 3 };
  *  FP64  - reference arithmetic (every step in double); parity mode.
  *  MIXED - phase argument k*(w.x) reduced mod 2pi in FP64, sincos/exp in FP32,
  *          contraction on tcgen05 tensor cores with FP16 hi+lo split operands
- *          and FP32 accumulation, cross-batch sums in FP64.
+ *          and FP32 accumulation, cross-batch sums in FP64.  The covariance
+ *          compensates both operands (three products per term) in 4096-event
+ *          chunks: about a tenth of FP16's error at a third of its speed; the
+ *          field and FourierQuad forms compensate one operand.
  *  FP32  - plain FP32: FP32 phases without FP64 reduction, FP32 CUDA-core
  *          contraction, FP32 accumulation (the comparison baseline).
- *  FP16  - as MIXED but one FP16 product (no lo part): half the tensor work,
- *          about sqrt(2) times MIXED's error.
+ *  FP16  - as MIXED but one FP16 product (no lo part), chunks of up to 65536
+ *          events: the fastest mode, within 1e-3 of FP64.
  * The random walk itself is FP64 in every mode, so all modes see the same
  * paths for the same seed. */
 enum { SCMC_PREC_FP64 = 0, SCMC_PREC_MIXED = 1, SCMC_PREC_FP32 = 2, SCMC_PREC_FP16 = 3 };
@@ -450,7 +453,8 @@ int scmc_cov_offsets_device(const double *d_C1, const double *d_C2, int32_t nvx,
  *   kind precision n_lo n_hi path_batch chunk_events stages ksplit group_entries
  * with kind field | cov | fq and precision fp64 | mixed | fp32 | fp16; '#'
  * starts a comment.  The covariance's chunk is capped where its FP32 tensor
- * sums would exceed the mixed tolerance (65536 events FP16, 32768 hi+lo).
+ * sums would exceed the tolerance (65536 events FP16, 32768 hi+lo; hi+lo
+ * takes 4096 by default, its error growing with the chunk).
  * ------------------------------------------------------------------------- */
 enum { SCMC_TUNE_FIELD = 0, SCMC_TUNE_COV = 1, SCMC_TUNE_FQ = 2 };
 
