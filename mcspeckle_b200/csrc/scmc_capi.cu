@@ -2015,91 +2015,98 @@ void fq_run(Ctx &c, const scmc_fq_args *a, const double *Wl, double2 *d_u, cudaS
     }
     cudaEvent_t *ev_prod = &c.ev[0], *ev_cons = &c.ev[2];  // per parity
     int64_t bi = 0;
-    for (int64_t done = 0; done < a->max_itr; ++bi) {
-        const int par = (int)(bi & 1);
-        const int64_t nb = path_batch_size(a->max_itr - done, tune.path_batch);
-        W.path_base = a->path_offset + (uint64_t)done;
-        Batch B;
-        if (pipe && bi >= 2) CK(cudaStreamWaitEvent(ps, ev_cons[par], 0));  // batch bi - 2 has read this parity's entries
-        walk_batch(c, W, nb, ps, B);
-        const int64_t nvert = B.n_paths + B.n_multi;
-        total_vert += nvert;
-        const int64_t nent = nvert * passes;
-        if (nent > INT32_MAX) fail(SCMC_ERR_INVALID, "batch too large");
-        // one output light on the pair form: 16-byte entries with the light factor applied
-        const bool compact = use_pair && nl_out == 1 && Nx <= 65535;
-        const size_t rec = compact ? sizeof(FqEntryC) : sizeof(FqEntry);
-        DevBuf &ebuf = (pipe && par) ? c.rows2 : c.rows;
-        char *Ein_b = reinterpret_cast<char *>(ebuf.ensure(2 * nent * rec));
-        char *Es_b = Ein_b + nent * rec;
-        FqEntry *Es = reinterpret_cast<FqEntry *>(Es_b);  // the full-entry forms
-        CK(cudaMemsetAsync(counts, 0, (Nz + 1) * sizeof(int), ps));
-        {
-            StageScope sc(ST_ROWS, ps);
-            const int eg = (int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16);
-            if (compact)
-                fq_entries_kernel<true><<<eg, 256, 0, ps>>>(F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein_b,
-                                                             counts);
-            else
-                fq_entries_kernel<false><<<eg, 256, 0, ps>>>(F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein_b,
-                                                              counts);
-            CK(cudaGetLastError());
-            LAUNCHED();
-        }
-        CK(cudaMemcpyAsync(hcounts.data(), counts, Nz * sizeof(int), cudaMemcpyDeviceToHost, ps));
-        CK(cudaStreamSynchronize(ps));
-        std::vector<int> hoff(Nz + 1, 0);
-        hplanes.clear();
-        for (int64_t k = 0; k < Nz; ++k) {
-            hoff[k + 1] = hoff[k] + hcounts[k];
-            if (hcounts[k] > 0 && k < Nz - 1) hplanes.push_back((int)k);
-        }
-        if (hplanes.empty()) {
-            done += nb;
-            continue;
-        }
-        CK(cudaMemcpyAsync(offsets, hoff.data(), (Nz + 1) * sizeof(int), cudaMemcpyHostToDevice, ps));
-        CK(cudaMemcpyAsync(planes, hplanes.data(), hplanes.size() * sizeof(int), cudaMemcpyHostToDevice, ps));
-        CK(cudaMemsetAsync(cursor, 0, (Nz + 1) * sizeof(int), ps));
-        {
-            StageScope sc(ST_ROWS, ps);
-            const int sg = (int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16);
-            if (compact)
-                fq_scatter_kernel<FqEntryC><<<sg, 256, 0, ps>>>(reinterpret_cast<const FqEntryC *>(Ein_b), nent, offsets,
-                                                                cursor, reinterpret_cast<FqEntryC *>(Es_b));
-            else
-                fq_scatter_kernel<FqEntry><<<sg, 256, 0, ps>>>(reinterpret_cast<const FqEntry *>(Ein_b), nent, offsets,
-                                                               cursor, Es);
-            CK(cudaGetLastError());
-            LAUNCHED();
-        }
-        if (pipe) {
-            CK(cudaEventRecord(ev_prod[par], ps));
-            CK(cudaStreamWaitEvent(st, ev_prod[par], 0));
-            CK(cudaEventSynchronize(ev_cons[par]));  // batch bi - 2's metadata copy out of fq_hmeta[par] is done
-        }
-        if (use_tc) {
-            if (use_pair)
-                fq_tc_batch_pair(c, F, (int)nl_out, Es_b, compact, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
-                                 reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries,
-                                 d_err, c.fq_hmeta[par], st);
-            else
-                fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
-                            reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
-        } else {
-            const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
-            for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
-                const unsigned gy = (unsigned)std::min<size_t>(65535, hplanes.size() - p0);
-                dim3 grid((unsigned)(nvt * nvt * nl_out), gy);
-                StageScope sc(ST_CONTRACT, st);
-                fq_accum_kernel<POL, AccT><<<grid, 256, 0, st>>>(F, Es, offsets, planes + p0, T, dz, U);
+    try {
+        for (int64_t done = 0; done < a->max_itr; ++bi) {
+            const int par = (int)(bi & 1);
+            const int64_t nb = path_batch_size(a->max_itr - done, tune.path_batch);
+            W.path_base = a->path_offset + (uint64_t)done;
+            Batch B;
+            if (pipe && bi >= 2) CK(cudaStreamWaitEvent(ps, ev_cons[par], 0));  // batch bi - 2 has read this parity's entries
+            walk_batch(c, W, nb, ps, B);
+            const int64_t nvert = B.n_paths + B.n_multi;
+            total_vert += nvert;
+            const int64_t nent = nvert * passes;
+            if (nent > INT32_MAX) fail(SCMC_ERR_INVALID, "batch too large");
+            // one output light on the pair form: 16-byte entries with the light factor applied
+            const bool compact = use_pair && nl_out == 1 && Nx <= 65535;
+            const size_t rec = compact ? sizeof(FqEntryC) : sizeof(FqEntry);
+            DevBuf &ebuf = (pipe && par) ? c.rows2 : c.rows;
+            char *Ein_b = reinterpret_cast<char *>(ebuf.ensure(2 * nent * rec));
+            char *Es_b = Ein_b + nent * rec;
+            FqEntry *Es = reinterpret_cast<FqEntry *>(Es_b);  // the full-entry forms
+            CK(cudaMemsetAsync(counts, 0, (Nz + 1) * sizeof(int), ps));
+            {
+                StageScope sc(ST_ROWS, ps);
+                const int eg = (int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16);
+                if (compact)
+                    fq_entries_kernel<true><<<eg, 256, 0, ps>>>(F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein_b,
+                                                                 counts);
+                else
+                    fq_entries_kernel<false><<<eg, 256, 0, ps>>>(F, B.S, c.scap, B.M, c.mcap, B.n_paths, B.n_multi, Ein_b,
+                                                                  counts);
                 CK(cudaGetLastError());
                 LAUNCHED();
             }
+            CK(cudaMemcpyAsync(hcounts.data(), counts, Nz * sizeof(int), cudaMemcpyDeviceToHost, ps));
+            CK(cudaStreamSynchronize(ps));
+            std::vector<int> hoff(Nz + 1, 0);
+            hplanes.clear();
+            for (int64_t k = 0; k < Nz; ++k) {
+                hoff[k + 1] = hoff[k] + hcounts[k];
+                if (hcounts[k] > 0 && k < Nz - 1) hplanes.push_back((int)k);
+            }
+            if (hplanes.empty()) {
+                done += nb;
+                continue;
+            }
+            CK(cudaMemcpyAsync(offsets, hoff.data(), (Nz + 1) * sizeof(int), cudaMemcpyHostToDevice, ps));
+            CK(cudaMemcpyAsync(planes, hplanes.data(), hplanes.size() * sizeof(int), cudaMemcpyHostToDevice, ps));
+            CK(cudaMemsetAsync(cursor, 0, (Nz + 1) * sizeof(int), ps));
+            {
+                StageScope sc(ST_ROWS, ps);
+                const int sg = (int)std::min<int64_t>((nent + 255) / 256, (int64_t)sms * 16);
+                if (compact)
+                    fq_scatter_kernel<FqEntryC><<<sg, 256, 0, ps>>>(reinterpret_cast<const FqEntryC *>(Ein_b), nent, offsets,
+                                                                    cursor, reinterpret_cast<FqEntryC *>(Es_b));
+                else
+                    fq_scatter_kernel<FqEntry><<<sg, 256, 0, ps>>>(reinterpret_cast<const FqEntry *>(Ein_b), nent, offsets,
+                                                                   cursor, Es);
+                CK(cudaGetLastError());
+                LAUNCHED();
+            }
+            if (pipe) {
+                CK(cudaEventRecord(ev_prod[par], ps));
+                CK(cudaStreamWaitEvent(st, ev_prod[par], 0));
+                CK(cudaEventSynchronize(ev_cons[par]));  // batch bi - 2's metadata copy out of fq_hmeta[par] is done
+            }
+            if (use_tc) {
+                if (use_pair)
+                    fq_tc_batch_pair(c, F, (int)nl_out, Es_b, compact, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
+                                     reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries,
+                                     d_err, c.fq_hmeta[par], st);
+                else
+                    fq_tc_batch(c, F, (int)nl_out, Es, hcounts, hoff, hplanes, Tt, dz, drr, n_uniform,
+                                reinterpret_cast<double *>(U), a->precision == SCMC_PREC_MIXED, tune.group_entries, st);
+            } else {
+                const int nvt = (int)((Nv + kFqTile - 1) / kFqTile);
+                for (size_t p0 = 0; p0 < hplanes.size(); p0 += 65535) {
+                    const unsigned gy = (unsigned)std::min<size_t>(65535, hplanes.size() - p0);
+                    dim3 grid((unsigned)(nvt * nvt * nl_out), gy);
+                    StageScope sc(ST_CONTRACT, st);
+                    fq_accum_kernel<POL, AccT><<<grid, 256, 0, st>>>(F, Es, offsets, planes + p0, T, dz, U);
+                    CK(cudaGetLastError());
+                    LAUNCHED();
+                }
+            }
+            if (pipe) CK(cudaEventRecord(ev_cons[par], st));
+            else CK(cudaStreamSynchronize(st));  // host vectors above are reused next batch
+            done += nb;
         }
-        if (pipe) CK(cudaEventRecord(ev_cons[par], st));
-        else CK(cudaStreamSynchronize(st));  // host vectors above are reused next batch
-        done += nb;
+    } catch (...) {
+        // nothing of the failed solve stays in flight on either stream
+        if (pipe) cudaStreamSynchronize(ps);
+        cudaStreamSynchronize(st);
+        throw;
     }
     {
         int herr = 0;  // a bounded wait of the pair form gave up somewhere in the solve
